@@ -1,0 +1,182 @@
+/*
+ * pftcc_b200.h -- C ABI of the B200 polar Fourier correlation search.
+ *
+ * Each entry point replaces one type-bound procedure of SIMPLE 3.0's
+ * polarft_corrcalc (src/main/simple_polarft_corrcalc.f90, cited below by line)
+ * so that a Fortran shim type with the same procedure names can forward to it
+ * through ISO_C_BINDING.  Conventions:
+ *   - every function returns an int status (PFTCC_OK = 0); the shim maps a
+ *     non-zero status to THROW_HARD, which is what the reference does on error;
+ *   - indices are 1-based as in the reference: iref in 1..nrefs, iptcl a GLOBAL
+ *     particle index in pfromto(1)..pfromto(2) mapped through pinds, irot in
+ *     1..nrots with irot = 1 the zero rotation;
+ *   - a polar FT is nrots/2 x (kto-kfrom+1) complex single precision, Fortran
+ *     column-major pft(pftsz, kfrom:kto), passed as interleaved (re, im) floats;
+ *   - all buffers are host memory unless the name ends in _dev; the library
+ *     copies what it is given and never keeps a caller pointer;
+ *   - calls on one handle are serialised by the caller (the reference's setters
+ *     are likewise called outside the OpenMP search loops); the per-pair
+ *     correlation calls are thread safe (an internal lock orders them).
+ */
+#ifndef PFTCC_B200_H
+#define PFTCC_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PFTCC_OK = 0,
+    PFTCC_ERR_ARG = 1,          /* bad dimensions, sizes or flags            */
+    PFTCC_ERR_INDEX = 2,        /* iref / iptcl / irot out of range          */
+    PFTCC_ERR_STATE = 3,        /* call out of order (e.g. no CTF matrices)  */
+    PFTCC_ERR_CUDA = 4,         /* CUDA runtime or launch error              */
+    PFTCC_ERR_OOM = 5,          /* device allocation failed                  */
+    PFTCC_ERR_TIMEOUT = 6,      /* a bounded device wait ran out             */
+    PFTCC_ERR_NODEV = 7,        /* no usable sm_100 device                   */
+    PFTCC_ERR_UNSUPPORTED = 8   /* a reference mode this build does not serve */
+};
+
+enum { PFTCC_FRAME_REF = 0,     /* |CTF| applied to the reference at the reference's own
+                                   polar index, exactly as prep_ref4corr :982 / :1527     */
+       PFTCC_FRAME_PTCL = 1 };  /* |CTF| at the particle's polar index n+rot with the
+                                   rotation-dependent normaliser sum |ref|^2 CTF^2(n+rot);
+                                   equal to FRAME_REF for an isotropic CTF               */
+
+enum { PFTCC_PREC_EXACT = 0,    /* FP32 direct sums per (ref, ptcl, shift), FRAME_REF/PTCL  */
+       PFTCC_PREC_FP32 = 1,     /* m-domain contraction on CUDA cores (FP32), FRAME_PTCL    */
+       PFTCC_PREC_BF16X3 = 2 }; /* m-domain contraction on tcgen05, BF16 hi+lo split with
+                                   three products and FP32 accumulation, FRAME_PTCL         */
+
+typedef struct pftcc_handle pftcc_handle;
+
+/* new() arguments plus the params_glob fields polarft_corrcalc reads implicitly
+ * (boxmatch :235, ring2 -> nrots :251-252, kfromto/kstop :256-258, ctf :355-356,
+ * l_match_filt :254). */
+typedef struct {
+    int nrefs;            /* new(nrefs, ...)                                    */
+    int pfromto[2];       /* new(..., pfromto, ...), global particle index range */
+    int box;              /* params_glob%boxmatch, even                         */
+    int nrots;            /* 2*magic_pftsz(ring2), even                         */
+    int kfromto[2];       /* params_glob%kfromto                                */
+    int kstop;            /* params_glob%kstop, kfromto(1) <= kstop <= kfromto(2) */
+    int with_ctf;         /* params_glob%ctf /= 'no'                            */
+    int match_filt;       /* params_glob%l_match_filt: branch of gencorr_*_for_rot_8 */
+    int ctf_frame;        /* PFTCC_FRAME_REF (reference semantics) or PFTCC_FRAME_PTCL */
+    int device;           /* CUDA device ordinal                                */
+} pftcc_config;
+
+/* spproj%get_ctfparams (simple_polarft_corrcalc.f90:948) for one particle */
+typedef struct {
+    float smpd, kv, cs, fraca;  /* A/pixel, kV, mm, amplitude contrast         */
+    float dfx, dfy, angast;     /* microns, microns, degrees                   */
+    float phshift;              /* radians (phase plate)                       */
+    int l_phaseplate;
+} pftcc_ctfparams;
+
+/* one search result per particle: 16 bytes */
+typedef struct { int iref; int irot; int ishift; float corr; } pftcc_best;
+
+/* one request of the adjoint: f and d f / d(shift_x, shift_y, defocus) */
+typedef struct { int iref, iptcl, irot, pad; double sx, sy, ddf; } pftcc_grad_req;
+
+/* ---- construction / destruction ------------------------------------------------ */
+/* new :209-422.  ptcl_mask (length pfromto(2)-pfromto(1)+1, nullable) selects the
+ * particles held (:245-249, :276-288); eoarr (same length, nullable) the even/odd
+ * assignment (:289-306; -1 everywhere = all even). */
+int pftcc_new(const pftcc_config *cfg, const int *ptcl_mask, const int *eoarr, pftcc_handle **out);
+/* kill :2234-2279 */
+int pftcc_kill(pftcc_handle *h);
+/* reallocate_ptcls :509-555 (pinds = global indices of the nptcls particles) */
+int pftcc_reallocate_ptcls(pftcc_handle *h, int nptcls, const int *pinds);
+
+/* ---- setters -------------------------------------------------------------------- */
+int pftcc_set_ref_pft(pftcc_handle *h, int iref, const float *pft, int iseven);           /* :426-436 */
+int pftcc_set_ptcl_pft(pftcc_handle *h, int iptcl, const float *pft);                     /* :438-445 */
+int pftcc_set_ref_fcomp(pftcc_handle *h, int iref, int irot, int k, const float *comp, int iseven); /* :447-457 */
+int pftcc_cp_even2odd_ref(pftcc_handle *h, int iref);                                     /* :485-489 */
+int pftcc_cp_even_ref2ptcl(pftcc_handle *h, int iref, int iptcl);                         /* :497-502 */
+int pftcc_swap_ptclsevenodd(pftcc_handle *h);                                             /* :504-507 */
+int pftcc_set_eo(pftcc_handle *h, int iptcl, int is_even);                                /* :557-562 */
+int pftcc_set_eos(pftcc_handle *h, const int *eoarr);                                     /* :564-579 */
+int pftcc_zero_refs_beyond_kstop(pftcc_handle *h);                                        /* :747-754 */
+/* bulk setters (no reference counterpart; what a batched shim uses): refs [n][K][P] */
+int pftcc_set_refs(pftcc_handle *h, int first_iref, int n, const float *pfts, int iseven);
+int pftcc_set_ptcls(pftcc_handle *h, int first_slot, int n, const float *pfts);
+
+/* ---- CTF ------------------------------------------------------------------------ */
+/* create_polar_absctfmats :906-959 given the per-particle parameters (params[i]
+ * belongs to the particle in slot i, i.e. global index pinds^-1(i)) */
+int pftcc_create_polar_absctfmats(pftcc_handle *h, const pftcc_ctfparams *params);
+
+/* ---- polarizer ------------------------------------------------------------------ */
+/* init_polarizer + polarize (simple_polarizer.f90:41-151) for n particles in slots
+ * first_slot.. from half-plane FTs cmat(box/2+1, box) (Fortran order, complex
+ * interleaved); griddev as params_glob%griddev == 'yes' */
+int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cmats, int griddev);
+int pftcc_polarize_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *cmats_dev, int griddev);
+int pftcc_polarize_refs(pftcc_handle *h, int first_iref, int n, const float *cmats, int iseven, int griddev);
+
+/* ---- memoisers ------------------------------------------------------------------ */
+/* memoize_ffts :848-861: prepares the particle-side angular spectra of the
+ * m-domain search (no-op for the exact path, which needs none) */
+int pftcc_memoize_ffts(pftcc_handle *h);
+
+/* ---- correlators ---------------------------------------------------------------- */
+/* gencorrs_1 / gencorrs_2 (:1594-1617 -> :1486-1534); shvec nullable -> gencorrs_cc_1 */
+int pftcc_gencorrs(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *cc);
+/* gencorr_for_rot :1619-1630 and gencorr_for_rot_8 :1632-1643 */
+int pftcc_gencorr_for_rot(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot, float *cc);
+int pftcc_gencorr_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot, double *cc);
+/* gencorr_grad_for_rot_8 :1849-1861 and gencorr_grad_only_for_rot_8 :1927-1939 */
+int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                 double *f, double *grad);
+int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                      double *grad);
+
+/* ---- batched entry points (no single reference counterpart) ---------------------- */
+/* all correlations: cc[slot][iref-1][ishift][irot-1] for every held particle,
+ * reference and shift (the loop strategy2D_greedy :42 runs over gencorrs) */
+int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc);
+/* best (ref, rot, shift) per particle over all references and a shift grid, the
+ * greedy strategies' maxloc (simple_strategy2D_greedy.f90:42-43) fused with the
+ * coarse shift grid of minimize_exhaustive (simple_pftcc_shsrch_grad.f90:182-199).
+ * ntop > 0 re-scores the ntop best (ref, shift) candidates per particle with the
+ * exact FP32 path in cfg.ctf_frame. */
+int pftcc_search_best(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop,
+                      pftcc_best *out);
+int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop,
+                          void *out_dev);
+/* adjoint: f and grad3 = d f / d(shift_x, shift_y, defocus[micron]) per request, with
+ * the particle's CTF evaluated at defocus + ddf; the shift part is
+ * gencorr_grad_for_rot_8 (:1863-1925) in the branch cfg.match_filt selects */
+int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);
+
+/* ---- getters (:597-710) ----------------------------------------------------------- */
+int pftcc_get_nrots(const pftcc_handle *h, int *nrots);
+int pftcc_get_pftsz(const pftcc_handle *h, int *pftsz);
+int pftcc_get_pdim(const pftcc_handle *h, int pdim[3]);
+int pftcc_get_box(const pftcc_handle *h, int *box);
+int pftcc_get_nrefs(const pftcc_handle *h, int *nrefs);
+int pftcc_get_nptcls(const pftcc_handle *h, int *nptcls);
+int pftcc_get_rot(const pftcc_handle *h, int roind, float *rot);
+int pftcc_get_roind(const pftcc_handle *h, float rot, int *roind);
+int pftcc_get_coord(const pftcc_handle *h, int rot, int k, float xy[2]);
+int pftcc_ptcl_iseven(const pftcc_handle *h, int iptcl, int *iseven);
+int pftcc_get_ref_pft(pftcc_handle *h, int iref, int iseven, float *pft);
+int pftcc_get_ptcl_pft(pftcc_handle *h, int iptcl, float *pft);
+int pftcc_get_sqsum_ptcl(pftcc_handle *h, int iptcl, float *sqsum);
+int pftcc_exists(const pftcc_handle *h, int *exists);
+
+/* ---- runtime ------------------------------------------------------------------------ */
+const char *pftcc_strerror(int status);
+/* last error message recorded on the handle (never NULL) */
+const char *pftcc_last_error(const pftcc_handle *h);
+/* number of kernels this handle has launched so far (for launch accounting) */
+long long pftcc_kernel_launches(const pftcc_handle *h);
+/* block until all device work of the handle is done */
+int pftcc_synchronize(pftcc_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,246 @@
+"""numpy front-end of the CPU oracle (oracle/pftcc_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` as
+the parity checker and by ``bench.py`` for its cpu_baseline / reference arm.
+The product library never imports this module.  Array conventions follow the
+reference's Fortran storage (see pftcc_oracle.h): a polar FT is a complex64
+array of shape (K, P), i.e. ``pft[k - kfrom, n]``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, OpenMP) and return the .so path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class Geom(C.Structure):
+    _fields_ = [("nrots", C.c_int), ("pftsz", C.c_int), ("kfrom", C.c_int),
+                ("kto", C.c_int), ("kstop", C.c_int), ("box", C.c_int)]
+
+    @property
+    def K(self) -> int:
+        return self.kto - self.kfrom + 1
+
+    @property
+    def Ks(self) -> int:
+        return self.kstop - self.kfrom + 1
+
+
+class Ctf(C.Structure):
+    _fields_ = [("smpd", C.c_float), ("kv", C.c_float), ("cs", C.c_float), ("fraca", C.c_float),
+                ("dfx", C.c_float), ("dfy", C.c_float), ("angast", C.c_float),
+                ("phshift", C.c_float), ("l_phaseplate", C.c_int)]
+
+
+def geom(nrots: int, kfrom: int, kto: int, box: int, kstop: int | None = None) -> Geom:
+    return Geom(nrots, nrots // 2, kfrom, kto, kto if kstop is None else kstop, box)
+
+
+def _P(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        fp, dp, ip = C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
+        G = C.POINTER(Geom)
+        L.orc_tables.argtypes = [G, fp, dp, dp]
+        L.orc_ctfmat.argtypes = [G, fp, C.POINTER(Ctf), dp]
+        L.orc_dctfmat_ddf.argtypes = [G, fp, C.POINTER(Ctf), dp]
+        L.orc_shmat.argtypes = [G, dp, dp, C.c_double, C.c_double, dp]
+        L.orc_gencorrs.argtypes = [G, fp, fp, dp, dp, dp, dp, dp]
+        L.orc_gencorrs_ptclframe.argtypes = [G, fp, fp, dp, dp, dp, dp, dp]
+        L.orc_gencorr_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, C.c_int, dp, dp]
+        L.orc_gencorr_for_rot.restype = C.c_double
+        L.orc_gencorr_grad3.argtypes = [G, fp, fp, dp, dp, dp, C.c_int, C.c_int, dp, dp, dp, dp]
+        L.orc_polarize.argtypes = [G, fp, fp, C.c_int, dp]
+        L.orc_kb_apod.argtypes = [C.c_double]
+        L.orc_kb_apod.restype = C.c_double
+        L.orc_fftpath_new.argtypes = [G]
+        L.orc_fftpath_new.restype = C.c_void_p
+        L.orc_fftpath_free.argtypes = [C.c_void_p]
+        L.orc_fftpath_memo_size.argtypes = [G]
+        L.orc_fftpath_memo_size.restype = C.c_long
+        L.orc_fftpath_memoize.argtypes = [C.c_void_p, fp, fp]
+        L.orc_fftpath_gencorrs.argtypes = [C.c_void_p, fp, fp, C.c_float, fp, fp, dp, dp, fp]
+        L.orc_cpu_search.argtypes = [G, C.c_int, fp, C.c_int, fp, fp, C.c_int, fp, ip, ip, ip, fp, C.c_int]
+        L.orc_cpu_search.restype = C.c_int
+        L.orc_cfft.argtypes = [C.c_int, dp, dp, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _c64(x) -> np.ndarray:
+    """complex64 (K, P) -> contiguous float32 view of interleaved (re, im)"""
+    return np.ascontiguousarray(x, dtype=np.complex64).view(np.float32)
+
+
+def _c128_out(shape) -> np.ndarray:
+    return np.zeros(shape, dtype=np.complex128)
+
+
+@dataclass
+class Tables:
+    polar: np.ndarray        # float32 (K, 2N)
+    argtransf: np.ndarray    # float64 (K, N)
+    argtransf1: np.ndarray   # float64 (N,)
+
+
+def tables(g: Geom) -> Tables:
+    polar = np.zeros((g.K, 2 * g.nrots), np.float32)
+    at = np.zeros((g.K, g.nrots), np.float64)
+    at1 = np.zeros(g.nrots, np.float64)
+    lib().orc_tables(C.byref(g), _P(polar, C.c_float), _P(at, C.c_double), _P(at1, C.c_double))
+    return Tables(polar, at, at1)
+
+
+def make_ctf(smpd=1.3, kv=300.0, cs=2.7, fraca=0.1, dfx=2.0, dfy=2.0, angast=0.0, phshift=0.0, phaseplate=False) -> Ctf:
+    return Ctf(smpd, kv, cs, fraca, dfx, dfy, angast, phshift, int(phaseplate))
+
+
+def ctfmat(g: Geom, t: Tables, c: Ctf) -> np.ndarray:
+    out = np.zeros((g.K, g.pftsz), np.float64)
+    lib().orc_ctfmat(C.byref(g), _P(t.polar, C.c_float), C.byref(c), _P(out, C.c_double))
+    return out
+
+
+def dctfmat_ddf(g: Geom, t: Tables, c: Ctf) -> np.ndarray:
+    out = np.zeros((g.K, g.pftsz), np.float64)
+    lib().orc_dctfmat_ddf(C.byref(g), _P(t.polar, C.c_float), C.byref(c), _P(out, C.c_double))
+    return out
+
+
+def shmat(g: Geom, t: Tables, sx: float, sy: float) -> np.ndarray:
+    out = _c128_out((g.K, g.pftsz))
+    lib().orc_shmat(C.byref(g), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double), sx, sy,
+                    out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def _shv(shvec):
+    return None if shvec is None else np.asarray(shvec, np.float64)
+
+
+def _ctf_arg(ctf):
+    return None if ctf is None else np.ascontiguousarray(ctf, np.float64)
+
+
+def gencorrs(g: Geom, t: Tables, ref, ptcl, ctf=None, shvec=None) -> np.ndarray:
+    """gencorrs_cc_1 (shvec None) / gencorrs_cc_2, FP64, reference frame"""
+    cc = np.zeros(g.nrots, np.float64)
+    lib().orc_gencorrs(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float), _P(_ctf_arg(ctf), C.c_double),
+                       _P(_shv(shvec), C.c_double), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
+                       _P(cc, C.c_double))
+    return cc
+
+
+def gencorrs_ptclframe(g: Geom, t: Tables, ref, ptcl, ctf=None, shvec=None) -> np.ndarray:
+    cc = np.zeros(g.nrots, np.float64)
+    lib().orc_gencorrs_ptclframe(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                                 _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double),
+                                 _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double), _P(cc, C.c_double))
+    return cc
+
+
+def gencorr_for_rot(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=None, match_filt=False) -> float:
+    return lib().orc_gencorr_for_rot(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                                     _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double), int(irot),
+                                     int(bool(match_filt)), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double))
+
+
+def gencorr_grad3(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, dctf=None, shvec=None, match_filt=False):
+    """(f, grad3) with grad3 = d f / d(shift_x, shift_y, defocus[micron]), reference frame"""
+    f = np.zeros(1, np.float64)
+    g3 = np.zeros(3, np.float64)
+    lib().orc_gencorr_grad3(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                            _P(_ctf_arg(ctf), C.c_double), _P(_ctf_arg(dctf), C.c_double), _P(_shv(shvec), C.c_double),
+                            int(irot), int(bool(match_filt)), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
+                            _P(f, C.c_double), _P(g3, C.c_double))
+    return float(f[0]), g3
+
+
+def polarize(g: Geom, t: Tables, cmat, griddev=False) -> np.ndarray:
+    """cmat: complex64 (box, box//2+1) half-plane FT (image%cmat transposed to C order)"""
+    out = _c128_out((g.K, g.pftsz))
+    lib().orc_polarize(C.byref(g), _P(t.polar, C.c_float), _P(_c64(cmat), C.c_float), int(bool(griddev)),
+                       out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def kb_apod(x: float) -> float:
+    return lib().orc_kb_apod(float(x))
+
+
+def cfft(x, sign=-1) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.complex128)
+    out = np.zeros_like(x)
+    lib().orc_cfft(len(x), x.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                   out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)), int(sign))
+    return out
+
+
+class FFTPath:
+    """FP32 FFT path in the reference's loop structure (the timed CPU baseline)."""
+
+    def __init__(self, g: Geom):
+        self.g = g
+        self.t = tables(g)
+        self.h = lib().orc_fftpath_new(C.byref(g))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_fftpath_free(self.h)
+            self.h = None
+
+    def memoize(self, ptcl) -> np.ndarray:
+        memo = np.zeros(lib().orc_fftpath_memo_size(C.byref(self.g)), np.float32)
+        lib().orc_fftpath_memoize(self.h, _P(_c64(ptcl), C.c_float), _P(memo, C.c_float))
+        return memo
+
+    def gencorrs(self, ref, ptcl, ctf=None, shvec=None) -> np.ndarray:
+        memo = self.memoize(ptcl)
+        Ks = self.g.Ks
+        sqp = np.float32(np.sum(np.abs(np.asarray(ptcl, np.complex64)[:Ks]) ** 2, dtype=np.float32))
+        cc = np.zeros(self.g.nrots, np.float32)
+        ctf32 = None if ctf is None else np.ascontiguousarray(ctf, np.float32)
+        sh = np.asarray(shvec if shvec is not None else (0.0, 0.0), np.float32)
+        lib().orc_fftpath_gencorrs(self.h, _P(_c64(ref), C.c_float), _P(memo, C.c_float), float(sqp),
+                                   _P(ctf32, C.c_float), _P(sh, C.c_float), _P(self.t.argtransf, C.c_double),
+                                   _P(self.t.argtransf1, C.c_double), _P(cc, C.c_float))
+        return cc
+
+
+def cpu_search(g: Geom, refs, ptcls, ctfmats, shifts, nthreads: int = 0):
+    """Exhaustive FP32 FFT-path search over refs x shifts for each particle.
+    Returns (best_ref 0-based, best_irot 1-based, best_shift_idx, best_cc, threads_used)."""
+    refs = np.ascontiguousarray(refs, np.complex64)
+    ptcls = np.ascontiguousarray(ptcls, np.complex64)
+    nr, npt = refs.shape[0], ptcls.shape[0]
+    ctf32 = None if ctfmats is None else np.ascontiguousarray(ctfmats, np.float32)
+    sh = np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+    br = np.zeros(npt, np.int32)
+    bro = np.zeros(npt, np.int32)
+    bs = np.zeros(npt, np.int32)
+    bcc = np.zeros(npt, np.float32)
+    used = lib().orc_cpu_search(C.byref(g), nr, _P(refs.view(np.float32), C.c_float), npt,
+                                _P(ptcls.view(np.float32), C.c_float), _P(ctf32, C.c_float), sh.shape[0],
+                                _P(sh, C.c_float), _P(br, C.c_int), _P(bro, C.c_int), _P(bs, C.c_int),
+                                _P(bcc, C.c_float), int(nthreads))
+    return br, bro, bs, bcc, used

@@ -1,0 +1,644 @@
+/*
+ * pftcc_oracle.c -- CPU restatement of SIMPLE 3.0's polar Fourier correlation
+ * search, TEST INFRASTRUCTURE ONLY (the checker for tests/, smoke() and the
+ * cpu_baseline / reference arm of bench.py).  See pftcc_oracle.h for the array
+ * conventions and the parity status.  Every function cites the reference
+ * routine it restates (paths relative to the SIMPLE 3.0 source tree).
+ */
+#include "pftcc_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define K_OF(g) ((g)->kto - (g)->kfrom + 1)
+
+/* ------------------------------------------------------------------------- */
+/* tables: simple_polarft_corrcalc.f90:261-274 (polar, in single precision
+ * exactly as the reference: ang = TWOPI/real(nrots), angtab = real(irot-1)*ang,
+ * x = sin(angtab)*real(k), y = -cos(angtab)*real(k)) and :311-317 (argtransf in
+ * double: real(polar,dp) * DPI/real(box/2,dp)). */
+void orc_tables(const orc_geom *g, float *polar, double *argtransf, double *argtransf_shellone)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g);
+    const float twopi = 2.0f * acosf(-1.0f);
+    const float ang = twopi / (float)N;
+    const double A = acos(-1.0) / (double)(g->box / 2);
+    for (int ik = 0; ik < K; ++ik) {
+        const int k = g->kfrom + ik;
+        for (int irot = 0; irot < N; ++irot) {
+            const float a = (float)irot * ang;
+            polar[ik * 2 * N + irot]     =  sinf(a) * (float)k;
+            polar[ik * 2 * N + N + irot] = -cosf(a) * (float)k;
+        }
+        for (int irot = 0; irot < P; ++irot) {
+            argtransf[ik * N + irot]     = (double)polar[ik * 2 * N + irot] * A;       /* x-part */
+            argtransf[ik * N + P + irot] = (double)polar[ik * 2 * N + N + irot] * A;   /* y-part */
+        }
+    }
+    for (int irot = 0; irot < P; ++irot) {
+        const float a = (float)irot * ang;
+        argtransf_shellone[irot]     = (double)sinf(a) * A;
+        argtransf_shellone[P + irot] = (double)(-cosf(a)) * A;
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* CTF: simple_ctf.f90 constructor :54-70 (wl = kV2wl/smpd, Cs*1e7/smpd,
+ * amp_contr_const = atan(fraca/sqrt(1-fraca^2))), init :73-81 (defocus in
+ * pixels, angast in radians), evalPhSh :88-98, eval_df :185-189, kV2wl :522-525;
+ * polar sampling from create_polar_absctfmats :926-935, |CTF| at :952-954. */
+typedef struct { double wl, cs, ampc, dfx, dfy, angast, phshift, dfscale; } ctf_consts;
+
+static ctf_consts ctf_setup(const orc_ctf *c)
+{
+    ctf_consts k;
+    const double kv = c->kv * 1000.0;
+    const double wl_A = 12.26 / sqrt(kv + 0.9784 * kv * kv / 1.0e6);
+    k.wl = wl_A / c->smpd;
+    k.cs = (c->cs * 1.0e7) / c->smpd;
+    k.ampc = atan(c->fraca / sqrt(1.0 - (double)c->fraca * c->fraca));
+    k.dfscale = 1.0e4 / c->smpd;
+    k.dfx = c->dfx * k.dfscale;
+    k.dfy = c->dfy * k.dfscale;
+    k.angast = c->angast / 180.0 * acos(-1.0);
+    k.phshift = c->l_phaseplate ? c->phshift : 0.0;
+    return k;
+}
+
+static void polar_freq(const orc_geom *g, const float *polar, int ik, int irot, double *spafreqsq, double *ang)
+{
+    const int N = g->nrots;
+    const double x = polar[ik * 2 * N + irot], y = polar[ik * 2 * N + N + irot];
+    const double hinv = x / g->box, kinv = y / g->box;
+    *spafreqsq = hinv * hinv + kinv * kinv;
+    *ang = atan2(y, x);
+}
+
+static double ctf_chi(const ctf_consts *k, double s2, double ang)
+{
+    const double df = 0.5 * (k->dfx + k->dfy + cos(2.0 * (ang - k->angast)) * (k->dfx - k->dfy));
+    return acos(-1.0) * k->wl * s2 * (df - 0.5 * k->wl * k->wl * s2 * k->cs) + k->phshift + k->ampc;
+}
+
+void orc_ctfmat(const orc_geom *g, const float *polar, const orc_ctf *c, double *ctfmat)
+{
+    const int P = g->pftsz, K = K_OF(g);
+    const ctf_consts k = ctf_setup(c);
+    for (int ik = 0; ik < K; ++ik)
+        for (int irot = 0; irot < P; ++irot) {
+            double s2, ang;
+            polar_freq(g, polar, ik, irot, &s2, &ang);
+            ctfmat[ik * P + irot] = fabs(sin(ctf_chi(&k, s2, ang)));
+        }
+}
+
+void orc_dctfmat_ddf(const orc_geom *g, const float *polar, const orc_ctf *c, double *dctfmat)
+{
+    const int P = g->pftsz, K = K_OF(g);
+    const ctf_consts k = ctf_setup(c);
+    for (int ik = 0; ik < K; ++ik)
+        for (int irot = 0; irot < P; ++irot) {
+            double s2, ang;
+            polar_freq(g, polar, ik, irot, &s2, &ang);
+            const double chi = ctf_chi(&k, s2, ang);
+            const double dchi = acos(-1.0) * k.wl * s2 * k.dfscale;  /* d chi / d df[micron] */
+            const double s = sin(chi);
+            dctfmat[ik * P + irot] = (s >= 0.0 ? 1.0 : -1.0) * cos(chi) * dchi;
+        }
+}
+
+/* ------------------------------------------------------------------------- */
+/* gen_shmat_8, simple_polarft_corrcalc.f90:1098-1120: first shell analytic,
+ * later shells by the de Moivre recurrence with the shell-one phase vector. */
+void orc_shmat(const orc_geom *g, const double *argtransf, const double *argtransf_shellone,
+               double sx, double sy, double *shmat)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g);
+    for (int n = 0; n < P; ++n) {
+        const double a = argtransf[n] * sx + argtransf[P + n] * sy;
+        shmat[2 * n] = cos(a);
+        shmat[2 * n + 1] = sin(a);
+    }
+    for (int n = 0; n < P; ++n) {
+        const double a1 = argtransf_shellone[n] * sx + argtransf_shellone[P + n] * sy;
+        const double vr = cos(a1), vi = sin(a1);
+        for (int ik = 1; ik < K; ++ik) {
+            const double pr = shmat[2 * ((ik - 1) * P + n)], pi = shmat[2 * ((ik - 1) * P + n) + 1];
+            shmat[2 * (ik * P + n)]     = pr * vr - pi * vi;
+            shmat[2 * (ik * P + n) + 1] = pr * vi + pi * vr;
+        }
+    }
+    (void)N;
+}
+
+/* prepared reference: pft_ref = ref * ctf * shmat in double (prep_ref4corr :961-985
+ * and gencorrs_cc_2 :1516-1530) */
+static void prep_ref(const orc_geom *g, const float *ref, const double *ctfmat, const double *shvec,
+                     const double *argtransf, const double *argtransf_shellone, double *out)
+{
+    const int P = g->pftsz, K = K_OF(g);
+    double *sh = NULL;
+    if (shvec) {
+        sh = (double *)malloc(sizeof(double) * 2 * K * P);
+        orc_shmat(g, argtransf, argtransf_shellone, shvec[0], shvec[1], sh);
+    }
+    for (int i = 0; i < K * P; ++i) {
+        double re = ref[2 * i], im = ref[2 * i + 1];
+        if (ctfmat) { re *= ctfmat[i]; im *= ctfmat[i]; }
+        if (sh) {
+            const double sr = sh[2 * i], si = sh[2 * i + 1];
+            const double tr = re * sr - im * si, ti = re * si + im * sr;
+            re = tr; im = ti;
+        }
+        out[2 * i] = re; out[2 * i + 1] = im;
+    }
+    free(sh);
+}
+
+/* calc_corrk_for_rot_8 (:1364-1390): Re sum_n ref(n) * conj(ptcl~(n + irot - 1)),
+ * where ptcl~ is the particle extended over the full circle by ptcl~(j + P) =
+ * conj(ptcl(j)).  The reference's four-way case split on irot is exactly this
+ * cyclic index with the conjugation rule. */
+static double corrk_for_rot(int P, const double *ref_k, const float *ptcl_k, int irot)
+{
+    const int N = 2 * P, s = irot - 1;
+    double acc = 0.0;
+    for (int n = 0; n < P; ++n) {
+        int j = (n + s) % N;
+        double qr, qi;
+        if (j < P) { qr = ptcl_k[2 * j]; qi = ptcl_k[2 * j + 1]; }
+        else { qr = ptcl_k[2 * (j - P)]; qi = -ptcl_k[2 * (j - P) + 1]; }
+        /* Re(a * conj(q)) = ar*qr + ai*qi */
+        acc += ref_k[2 * n] * qr + ref_k[2 * n + 1] * qi;
+    }
+    return acc;
+}
+
+static double sqsum_k(int P, const double *x)
+{
+    double s = 0.0;
+    for (int n = 0; n < P; ++n) s += x[2 * n] * x[2 * n] + x[2 * n + 1] * x[2 * n + 1];
+    return s;
+}
+
+static double sqsum_kf(int P, const float *x)
+{
+    double s = 0.0;
+    for (int n = 0; n < P; ++n) s += (double)x[2 * n] * x[2 * n] + (double)x[2 * n + 1] * x[2 * n + 1];
+    return s;
+}
+
+/* gencorrs_cc_1 (:1486-1500) / gencorrs_cc_2 (:1502-1534).  Note the reference's
+ * asymmetry: cc_1 takes sqsum_ref over kfrom..kstop (prep_ref4corr :984) while
+ * cc_2 takes it over all shells kfrom..kto (:1531).  The correlation always runs
+ * over kfrom..kstop (:1498, :1532), as does sqsums_ptcls (memoize_sqsum_ptcl :844). */
+void orc_gencorrs(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                  const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                  double *cc)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    double sqr = 0.0, sqp = 0.0;
+    const int ksq = shvec ? K : Ks;
+    for (int ik = 0; ik < ksq; ++ik) sqr += sqsum_k(P, pr + 2 * ik * P);
+    for (int ik = 0; ik < Ks; ++ik) sqp += sqsum_kf(P, ptcl + 2 * ik * P);
+    const double den = sqrt(sqr * sqp);
+    for (int irot = 1; irot <= N; ++irot) {
+        double c = 0.0;
+        for (int ik = 0; ik < Ks; ++ik) c += corrk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot);
+        cc[irot - 1] = c / den;
+    }
+    free(pr);
+}
+
+/* gencorr_cc_for_rot_8 (:1690-1733).  match_filt: unweighted sums normalised by
+ * sqsum over kfrom..kstop (:1729-1731).  Otherwise the shell-weighted ("jacobian")
+ * form sum_k k*corr_k / sqrt(sum_k k|ref_k|^2 * sum_k k|ptcl_k|^2) (:1717-1727). */
+double orc_gencorr_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                           const double *shvec, int irot, int match_filt,
+                           const double *argtransf, const double *argtransf_shellone)
+{
+    const int P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    const double zero[2] = {0.0, 0.0};
+    prep_ref(g, ref, ctfmat, shvec ? shvec : zero, argtransf, argtransf_shellone, pr);
+    double corr = 0.0, sqr = 0.0, sqp = 0.0;
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double w = match_filt ? 1.0 : (double)(g->kfrom + ik);
+        sqr += w * sqsum_k(P, pr + 2 * ik * P);
+        sqp += w * sqsum_kf(P, ptcl + 2 * ik * P);
+        corr += w * corrk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot);
+    }
+    free(pr);
+    return corr / sqrt(sqr * sqp);
+}
+
+/* gencorr_cc_grad_for_rot_8 (:1863-1925) extended with a defocus derivative.
+ * d/dsx multiplies the shifted reference by i*argtransf_x (:1896, :1914), d/dsy by
+ * i*argtransf_y (:1899, :1918); the denominator is shift invariant.  For the
+ * defocus, d pft_ref = ref * dctf * shmat and the quotient rule adds
+ * -f/2 * d(sqsum_ref)/sqsum_ref. */
+void orc_gencorr_grad3(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                       const double *dctfmat, const double *shvec, int irot, int match_filt,
+                       const double *argtransf, const double *argtransf_shellone,
+                       double *f, double *grad3)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    double *tmp = (double *)malloc(sizeof(double) * 2 * K * P);
+    double *dr = (double *)malloc(sizeof(double) * 2 * K * P);
+    const double zero[2] = {0.0, 0.0};
+    const double *sv = shvec ? shvec : zero;
+    prep_ref(g, ref, ctfmat, sv, argtransf, argtransf_shellone, pr);
+    double corr = 0.0, sqr = 0.0, sqp = 0.0, gx = 0.0, gy = 0.0, gdn = 0.0, dsq = 0.0;
+    if (dctfmat) prep_ref(g, ref, dctfmat, sv, argtransf, argtransf_shellone, dr);
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double w = match_filt ? 1.0 : (double)(g->kfrom + ik);
+        const double *prk = pr + 2 * ik * P;
+        sqr += w * sqsum_k(P, prk);
+        sqp += w * sqsum_kf(P, ptcl + 2 * ik * P);
+        corr += w * corrk_for_rot(P, prk, ptcl + 2 * ik * P, irot);
+        for (int d = 0; d < 2; ++d) {
+            double *tk = tmp + 2 * ik * P;
+            for (int n = 0; n < P; ++n) {
+                const double a = argtransf[ik * N + d * P + n];
+                /* (re + i im) * i * a = -im*a + i re*a */
+                tk[2 * n] = -prk[2 * n + 1] * a;
+                tk[2 * n + 1] = prk[2 * n] * a;
+            }
+            const double c = w * corrk_for_rot(P, tk, ptcl + 2 * ik * P, irot);
+            if (d == 0) gx += c; else gy += c;
+        }
+        if (dctfmat) {
+            const double *drk = dr + 2 * ik * P;
+            gdn += w * corrk_for_rot(P, drk, ptcl + 2 * ik * P, irot);
+            for (int n = 0; n < P; ++n) dsq += w * 2.0 * (prk[2 * n] * drk[2 * n] + prk[2 * n + 1] * drk[2 * n + 1]);
+        }
+    }
+    const double den = sqrt(sqr * sqp);
+    *f = corr / den;
+    grad3[0] = gx / den;
+    grad3[1] = gy / den;
+    grad3[2] = dctfmat ? (gdn / den - 0.5 * (*f) * dsq / sqr) : 0.0;
+    free(pr); free(tmp); free(dr);
+}
+
+void orc_gencorr_grad_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                              const double *shvec, int irot, int match_filt,
+                              const double *argtransf, const double *argtransf_shellone,
+                              double *f, double *grad)
+{
+    double g3[3];
+    orc_gencorr_grad3(g, ref, ptcl, ctfmat, NULL, shvec, irot, match_filt, argtransf, argtransf_shellone, f, g3);
+    grad[0] = g3[0];
+    grad[1] = g3[1];
+}
+
+/* particle-frame objective (see header): numerator Re sum_n (ref*shmat)(n) *
+ * conj(ctf~(n+s) * ptcl~(n+s)) with ctf~(j) = ctf(j mod P), normaliser
+ * sum_n |ref(n)|^2 ctf~(n+s)^2 (shift invariant since |shmat| = 1). */
+void orc_gencorrs_ptclframe(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                            const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                            double *cc)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, NULL, shvec, argtransf, argtransf_shellone, pr);
+    double sqp = 0.0;
+    for (int ik = 0; ik < Ks; ++ik) sqp += sqsum_kf(P, ptcl + 2 * ik * P);
+    for (int s = 0; s < N; ++s) {
+        double num = 0.0, den = 0.0;
+        for (int ik = 0; ik < Ks; ++ik) {
+            const double *a = pr + 2 * ik * P;
+            const float *q = ptcl + 2 * ik * P;
+            for (int n = 0; n < P; ++n) {
+                const int j = (n + s) % N;
+                const int jp = j % P;
+                double qr = q[2 * jp], qi = q[2 * jp + 1];
+                if (j >= P) qi = -qi;
+                const double c = ctfmat ? ctfmat[ik * P + jp] : 1.0;
+                num += c * (a[2 * n] * qr + a[2 * n + 1] * qi);
+                const double r2 = (double)ref[2 * (ik * P + n)] * ref[2 * (ik * P + n)]
+                                + (double)ref[2 * (ik * P + n) + 1] * ref[2 * (ik * P + n) + 1];
+                den += r2 * c * c;
+            }
+        }
+        cc[s] = num / sqrt(den * sqp);
+    }
+    free(pr);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Kaiser-Bessel window, simple_kbinterpol.f90: new :92-109 with Whalf = KBWINSZ
+ * = 1.5 (simple_defs.f90:131) -> W = 3, beta = 7.4 (the Whalf <= 1.5 branch),
+ * apod :130-141, bessi0 :229-252 (Abramowitz & Stegun 9.8.1 / 9.8.2 polynomial
+ * approximations of I0). */
+static double bessi0(double x)
+{
+    const double ax = x;
+    if (ax < 3.75) {
+        double y = x / 3.75;
+        y = y * y;
+        return 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 + y * (0.2659732 + y * (0.0360768 + y * 0.0045813)))));
+    }
+    const double y = 3.75 / ax;
+    return (0.39894228 + y * (0.01328592 + y * (0.00225319 + y * (-0.00157565 + y * (0.00916281 +
+            y * (-0.02057706 + y * (0.02635537 + y * (-0.01647633 + y * 0.00392377)))))))) * exp(ax) / sqrt(ax);
+}
+
+double orc_kb_apod(double x)
+{
+    const double whalf = 1.5, W = 3.0, beta = 7.4;
+    if (fabs(x) > whalf) return 0.0;
+    double arg = (2.0 / W) * x;
+    arg = 1.0 - arg * arg;
+    if (arg < 0.0) arg = 0.0;
+    return (1.0 / W) * bessi0(beta * sqrt(arg));
+}
+
+/* Fortran nint: round half away from zero */
+static int f_nint(double x) { return (int)(x >= 0.0 ? floor(x + 0.5) : -floor(-x + 0.5)); }
+
+/* cyci_1d, simple_math.f90:746-757 */
+static int cyci_1d(int lo, int hi, int i)
+{
+    if (i > hi) return lo + (i - hi) - 1;
+    if (i < lo) return hi - (lo - i) + 1;
+    return i;
+}
+
+/* get_fcomp2D, simple_image.f90:1894-1907: Hermitian half-plane gather */
+static void get_fcomp2d(const float *cmat, int box, int h, int k, double *re, double *im)
+{
+    const int ld = box / 2 + 1;
+    int p1, p2;
+    double sgn = 1.0;
+    if (h >= 0) { p1 = h; p2 = k + (k < 0 ? box : 0); }
+    else { p1 = -h; p2 = -k + (-k < 0 ? box : 0); sgn = -1.0; }
+    *re = cmat[2 * (p2 * ld + p1)];
+    *im = sgn * cmat[2 * (p2 * ld + p1) + 1];
+}
+
+/* init_polarizer :41-92 (3x3 window sqwin_2d around nint(loc), weights the outer
+ * product of apod(win - loc), normalised by their sum unless griddev, cyclic
+ * addresses over the logical limits [-box/2, box/2] x [-box/2, box/2-1]) and
+ * polarize :120-151 (pft(i,k) = sum w * F(h,k)); rotations 1..P only. */
+void orc_polarize(const orc_geom *g, const float *polar, const float *cmat, int griddev, double *pft)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), box = g->box;
+    for (int ik = 0; ik < K; ++ik)
+        for (int i = 0; i < P; ++i) {
+            const double lx = polar[ik * 2 * N + i], ly = polar[ik * 2 * N + N + i];
+            const int wx = f_nint(lx) - 1, wy = f_nint(ly) - 1;
+            double w[3][3], wsum = 0.0;
+            for (int l = 0; l < 3; ++l)
+                for (int m = 0; m < 3; ++m) {
+                    w[l][m] = orc_kb_apod((double)(wx + l) - lx) * orc_kb_apod((double)(wy + m) - ly);
+                    wsum += w[l][m];
+                }
+            double accr = 0.0, acci = 0.0;
+            for (int l = 0; l < 3; ++l) {
+                const int h = cyci_1d(-box / 2, box / 2, wx + l);
+                for (int m = 0; m < 3; ++m) {
+                    const int kk = cyci_1d(-box / 2, box / 2 - 1, wy + m);
+                    double re, im;
+                    get_fcomp2d(cmat, box, h, kk, &re, &im);
+                    const double ww = griddev ? w[l][m] : w[l][m] / wsum;
+                    accr += ww * re;
+                    acci += ww * im;
+                }
+            }
+            pft[2 * (ik * P + i)] = accr;
+            pft[2 * (ik * P + i) + 1] = acci;
+        }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Project-written mixed-radix FFT (recursive decimation in time, radices 4, 2,
+ * 3, 5 and a plain DFT for any other prime factor).  Stands in for FFTW. */
+typedef struct { int n; int nf; int f[32]; double *tw; float *twf; } fftplan;
+
+static void fftplan_init(fftplan *p, int n)
+{
+    p->n = n; p->nf = 0;
+    int m = n;
+    const int rad[4] = {4, 2, 3, 5};
+    for (int r = 0; r < 4; ++r) while (m % rad[r] == 0) { p->f[p->nf++] = rad[r]; m /= rad[r]; }
+    for (int q = 7; m > 1; q += 2) while (m % q == 0) { p->f[p->nf++] = q; m /= q; }
+    p->tw = (double *)malloc(sizeof(double) * 2 * n);
+    p->twf = (float *)malloc(sizeof(float) * 2 * n);
+    for (int j = 0; j < n; ++j) {
+        const double a = -2.0 * acos(-1.0) * j / n;
+        p->tw[2 * j] = cos(a); p->tw[2 * j + 1] = sin(a);
+        p->twf[2 * j] = (float)cos(a); p->twf[2 * j + 1] = (float)sin(a);
+    }
+}
+
+static void fftplan_free(fftplan *p) { free(p->tw); free(p->twf); }
+
+#define DEFINE_FFT(NAME, T, TW)                                                                   \
+static void NAME(const fftplan *p, int lvl, int n, const T *in, int stride, T *out, int sign)     \
+{                                                                                                  \
+    if (n == 1) { out[0] = in[0]; out[1] = in[1]; return; }                                        \
+    const int r = p->f[lvl], m = n / r, step = p->n / n;                                          \
+    for (int q = 0; q < r; ++q) NAME(p, lvl + 1, m, in + 2 * q * stride, stride * r, out + 2 * q * m, sign); \
+    T tr[64], ti[64];                                                                              \
+    for (int k = 0; k < m; ++k) {                                                                  \
+        for (int q = 0; q < r; ++q) {                                                              \
+            const int ti_ = (q * k * step) % p->n;                                                 \
+            const T wr = p->TW[2 * ti_], wi = -sign * p->TW[2 * ti_ + 1];                          \
+            const T xr = out[2 * (q * m + k)], xi = out[2 * (q * m + k) + 1];                      \
+            tr[q] = xr * wr - xi * wi; ti[q] = xr * wi + xi * wr;                                 \
+        }                                                                                          \
+        for (int s = 0; s < r; ++s) {                                                              \
+            T ar = 0, ai = 0;                                                                      \
+            for (int q = 0; q < r; ++q) {                                                          \
+                const int e = ((q * s) % r) * (p->n / r);                                          \
+                const T wr = p->TW[2 * e], wi = -sign * p->TW[2 * e + 1];                          \
+                ar += tr[q] * wr - ti[q] * wi; ai += tr[q] * wi + ti[q] * wr;                     \
+            }                                                                                      \
+            out[2 * (s * m + k)] = ar; out[2 * (s * m + k) + 1] = ai;                              \
+        }                                                                                          \
+    }                                                                                              \
+}
+/* the combine above writes in place over the sub-transforms it has already read
+ * for the same k only (all r inputs of column k are consumed before any output of
+ * column k is written, and columns do not overlap), so no scratch is needed. */
+DEFINE_FFT(fft_rec_d, double, tw)
+DEFINE_FFT(fft_rec_f, float, twf)
+
+void orc_cfft(int n, const double *in, double *out, int sign)
+{
+    fftplan p;
+    fftplan_init(&p, n);
+    fft_rec_d(&p, 0, n, in, 1, out, sign);
+    fftplan_free(&p);
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP32 FFT path: memoize_fft (:864-877) and calc_corrs_over_k (:1132-1162).
+ * r2c(P) of Re(x) keeps P/2+1 outputs; c2c(P) of Im(x)*fft_factors with
+ * fft_factors(n) = exp(-i*pi*n/P) (:410-413); the product spectrum interleaves
+ * 4*conj(ref_re)*ptcl_re at the odd 1-based slots and 4*conj(ref_im)*ptcl_im at
+ * the even ones, then a c2r(N) per shell, accumulated and divided by 2N. */
+struct orc_fftpath {
+    orc_geom g;
+    fftplan pP, pN;
+    float *ff;               /* fft_factors, P complex                  */
+};
+
+orc_fftpath *orc_fftpath_new(const orc_geom *g)
+{
+    orc_fftpath *p = (orc_fftpath *)calloc(1, sizeof(orc_fftpath));
+    p->g = *g;
+    fftplan_init(&p->pP, g->pftsz);
+    fftplan_init(&p->pN, g->nrots);
+    p->ff = (float *)malloc(sizeof(float) * 2 * g->pftsz);
+    const float pif = acosf(-1.0f);
+    for (int n = 0; n < g->pftsz; ++n) {
+        const float a = -pif * (float)n / (float)g->pftsz;
+        p->ff[2 * n] = cosf(a); p->ff[2 * n + 1] = sinf(a);
+    }
+    return p;
+}
+
+void orc_fftpath_free(orc_fftpath *p)
+{
+    if (!p) return;
+    fftplan_free(&p->pP); fftplan_free(&p->pN); free(p->ff); free(p);
+}
+
+long orc_fftpath_memo_size(const orc_geom *g)
+{
+    return (long)K_OF(g) * 2 * 2 * g->pftsz;   /* per shell: re-transform (P cplx slots) + im-transform (P cplx) */
+}
+
+/* transforms of one shell: xr_out = fft_P(Re x) (first P/2+1 valid), xi_out = fft_P(Im x * ff) */
+static void shell_transforms(const orc_fftpath *p, const float *x, float *work, float *xr_out, float *xi_out)
+{
+    const int P = p->g.pftsz;
+    float *a = work, *b = work + 2 * P;
+    for (int n = 0; n < P; ++n) { a[2 * n] = x[2 * n]; a[2 * n + 1] = 0.0f; }
+    fft_rec_f(&p->pP, 0, P, a, 1, xr_out, -1);
+    for (int n = 0; n < P; ++n) {
+        const float im = x[2 * n + 1];
+        b[2 * n] = im * p->ff[2 * n]; b[2 * n + 1] = im * p->ff[2 * n + 1];
+    }
+    fft_rec_f(&p->pP, 0, P, b, 1, xi_out, -1);
+}
+
+void orc_fftpath_memoize(orc_fftpath *p, const float *ptcl, float *memo)
+{
+    const int P = p->g.pftsz, K = K_OF(&p->g);
+    float *work = (float *)malloc(sizeof(float) * 4 * P);
+    for (int ik = 0; ik < K; ++ik)
+        shell_transforms(p, ptcl + 2 * ik * P, work, memo + ik * 4 * P, memo + ik * 4 * P + 2 * P);
+    free(work);
+}
+
+void orc_fftpath_gencorrs(orc_fftpath *p, const float *ref, const float *ptcl_memo, float sqsum_ptcl,
+                          const float *ctfmat, const float *shvec, const double *argtransf,
+                          const double *argtransf_shellone, float *cc)
+{
+    const orc_geom *g = &p->g;
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    float *pr = (float *)malloc(sizeof(float) * 2 * K * P);
+    float *work = (float *)malloc(sizeof(float) * (4 * P + 4 * P + 2 * N + 2 * N + 2 * N));
+    float *rre = work + 4 * P, *rim = rre + 2 * P, *prod = work + 8 * P, *full = prod + 2 * N, *bt = full + 2 * N;
+    float *acc = (float *)calloc(N, sizeof(float));
+    /* reference preparation in single precision: pft_ref = (ref*ctf)*cmplx(shmat_8) */
+    double *sh8 = NULL;
+    if (shvec) {
+        sh8 = (double *)malloc(sizeof(double) * 2 * K * P);
+        orc_shmat(g, argtransf, argtransf_shellone, (double)shvec[0], (double)shvec[1], sh8);
+    }
+    float sqr = 0.0f;
+    for (int i = 0; i < K * P; ++i) {
+        float re = ref[2 * i], im = ref[2 * i + 1];
+        if (ctfmat) { re *= ctfmat[i]; im *= ctfmat[i]; }
+        if (sh8) {
+            const float sr = (float)sh8[2 * i], si = (float)sh8[2 * i + 1];
+            const float tr = re * sr - im * si, ti = re * si + im * sr;
+            re = tr; im = ti;
+        }
+        pr[2 * i] = re; pr[2 * i + 1] = im;
+        sqr += re * re + im * im;      /* gencorrs_cc_2: sum over all shells */
+    }
+    for (int ik = 0; ik < Ks; ++ik) {
+        shell_transforms(p, pr + 2 * ik * P, work, rre, rim);
+        const float *mre = ptcl_memo + ik * 4 * P, *mim = mre + 2 * P;
+        /* product spectrum X(m), m = 0..N/2: even m = 2j from the re-transforms,
+         * odd m = 2j+1 from the im-transforms */
+        for (int m = 0; m <= N / 2; ++m) {
+            const int j = m / 2;
+            const float *a = (m & 1) ? rim : rre, *b = (m & 1) ? mim : mre;
+            const float ar = a[2 * j], ai = -a[2 * j + 1], br = b[2 * j], bi = b[2 * j + 1];
+            prod[2 * m] = 4.0f * (ar * br - ai * bi);
+            prod[2 * m + 1] = 4.0f * (ar * bi + ai * br);
+        }
+        /* c2r(N): Hermitian extension, backward transform, real part */
+        for (int m = 0; m <= N / 2; ++m) { full[2 * m] = prod[2 * m]; full[2 * m + 1] = prod[2 * m + 1]; }
+        full[1] = 0.0f; full[2 * (N / 2) + 1] = 0.0f;
+        for (int m = N / 2 + 1; m < N; ++m) { full[2 * m] = prod[2 * (N - m)]; full[2 * m + 1] = -prod[2 * (N - m) + 1]; }
+        fft_rec_f(&p->pN, 0, N, full, 1, bt, +1);
+        for (int r = 0; r < N; ++r) acc[r] += bt[2 * r];
+    }
+    const float den = sqrtf(sqr * sqsum_ptcl);
+    for (int r = 0; r < N; ++r) cc[r] = (acc[r] / (float)(2 * N)) / den;
+    free(pr); free(work); free(acc); free(sh8);
+}
+
+/* exhaustive search: the greedy strategy's loop over all references
+ * (simple_strategy2D_greedy.f90:33-58) with the shift grid of the exhaustive
+ * in-plane search (simple_pftcc_shsrch_grad.f90:182-199), each call a
+ * gencorrs_cc_2 through the FFT path and a maxloc over rotations; OpenMP over
+ * particles as in the 3D matcher (simple_strategy3D_matcher.f90:204). */
+int orc_cpu_search(const orc_geom *g, int nrefs, const float *refs, int nptcls, const float *ptcls,
+                   const float *ctfmats, int nshifts, const float *shifts,
+                   int *best_ref, int *best_rot, int *best_shift, float *best_cc, int nthreads)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    float *polar = (float *)malloc(sizeof(float) * 2 * N * K);
+    double *at = (double *)malloc(sizeof(double) * N * K);
+    double *at1 = (double *)malloc(sizeof(double) * N);
+    orc_tables(g, polar, at, at1);
+    int used = 1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    #pragma omp parallel
+    {
+#ifdef _OPENMP
+        #pragma omp single
+        used = omp_get_num_threads();
+#endif
+        orc_fftpath *fp = orc_fftpath_new(g);
+        float *memo = (float *)malloc(sizeof(float) * orc_fftpath_memo_size(g));
+        float *cc = (float *)malloc(sizeof(float) * N);
+        #pragma omp for schedule(static)
+        for (int i = 0; i < nptcls; ++i) {
+            const float *pt = ptcls + (size_t)i * 2 * K * P;
+            orc_fftpath_memoize(fp, pt, memo);
+            float sqp = 0.0f;
+            for (int j = 0; j < 2 * Ks * P; ++j) sqp += pt[j] * pt[j];
+            float bcc = -INFINITY; int br = -1, bro = -1, bs = -1;
+            for (int r = 0; r < nrefs; ++r)
+                for (int s = 0; s < nshifts; ++s) {
+                    orc_fftpath_gencorrs(fp, refs + (size_t)r * 2 * K * P, memo, sqp,
+                                         ctfmats ? ctfmats + (size_t)i * K * P : NULL,
+                                         shifts + 2 * s, at, at1, cc);
+                    for (int rot = 0; rot < N; ++rot)
+                        if (cc[rot] > bcc) { bcc = cc[rot]; br = r; bro = rot + 1; bs = s; }
+                }
+            best_ref[i] = br; best_rot[i] = bro; best_shift[i] = bs; best_cc[i] = bcc;
+        }
+        free(memo); free(cc);
+        orc_fftpath_free(fp);
+    }
+    free(polar); free(at); free(at1);
+    return used;
+}

@@ -1,0 +1,125 @@
+/*
+ * pftcc_oracle.h -- CPU restatement of SIMPLE 3.0's polar Fourier correlation
+ * search (polarft_corrcalc), used ONLY as test infrastructure: the checker in
+ * tests/, the smoke() parity check and bench.py's cpu_baseline / reference arm.
+ * Nothing in the product library links, loads or calls this code.
+ *
+ * Parity status: the reference (Fortran 2008 + FFTW3) cannot be compiled in
+ * this environment (no Fortran compiler, no FFTW), and the reference ships no
+ * golden vectors for this path.  The restatement is therefore pinned by
+ * known-answer tests derived from the reference formulas (self-correlation,
+ * rotation and shift recovery, FFT path == direct path, finite-difference
+ * gradients, KB weights summing to one) -- "parity unpinned" against
+ * reference-produced outputs.
+ *
+ * Array conventions (all follow the reference's Fortran column-major storage,
+ * written here 0-based):
+ *   pft  [K][P] complex   -> pfts_refs_even(P, kfrom:kto, :)      (simple_polarft_corrcalc.f90:319)
+ *   polar[K][2N] float    -> polar(2*nrots, kfrom:kto)            (:258-267)
+ *   argtransf[K][N] double-> argtransf(nrots, kfrom:kto)          (:308-317)
+ *   ctfmat[K][P]          -> ctfmats(P, kfrom:kto, :)             (:924)
+ *   cmat [box][box/2+1]   -> image%cmat(box/2+1, box, 1)          (simple_image.f90:1894-1907)
+ * complex values are interleaved (re, im) pairs.
+ */
+#ifndef PFTCC_ORACLE_H
+#define PFTCC_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int nrots;   /* N, number of in-plane rotations = 2*pftsz        */
+    int pftsz;   /* P                                                 */
+    int kfrom;   /* params_glob%kfromto(1)                            */
+    int kto;     /* params_glob%kfromto(2)                            */
+    int kstop;   /* params_glob%kstop (<= kto)                        */
+    int box;     /* params_glob%boxmatch (even)                       */
+} orc_geom;
+
+typedef struct {
+    float smpd, kv, cs, fraca;   /* A, kV, mm, amplitude contrast fraction       */
+    float dfx, dfy, angast;      /* microns, microns, degrees                    */
+    float phshift;               /* radians, used when l_phaseplate != 0         */
+    int   l_phaseplate;
+} orc_ctf;
+
+/* polar / argtransf tables (simple_polarft_corrcalc.f90:261-317) */
+void orc_tables(const orc_geom *g, float *polar, double *argtransf, double *argtransf_shellone);
+
+/* |CTF| on the polar grid for one particle (create_polar_absctfmats :906-959) */
+void orc_ctfmat(const orc_geom *g, const float *polar, const orc_ctf *c, double *ctfmat);
+
+/* shift phase matrix, FP64 de Moivre recurrence (gen_shmat_8 :1098-1120); out [K][P] complex */
+void orc_shmat(const orc_geom *g, const double *argtransf, const double *argtransf_shellone,
+               double sx, double sy, double *shmat);
+
+/* gencorrs, FP64 direct sums (gencorrs_cc_1 :1486-1500 when shvec == NULL,
+ * gencorrs_cc_2 :1502-1534 otherwise).  ref/ptcl are FP32 pfts, ctfmat may be NULL. */
+void orc_gencorrs(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                  const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                  double *cc);
+
+/* gencorr_cc_for_rot_8 (:1690-1733), both branches selected by match_filt; irot is 1-based */
+double orc_gencorr_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                           const double *shvec, int irot, int match_filt,
+                           const double *argtransf, const double *argtransf_shellone);
+
+/* gencorr_cc_grad_for_rot_8 (:1863-1925), both branches; grad[2] = d/d(sx, sy) */
+void orc_gencorr_grad_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                              const double *shvec, int irot, int match_filt,
+                              const double *argtransf, const double *argtransf_shellone,
+                              double *f, double *grad);
+
+/* particle-frame objective: the particle's |CTF| is applied at the particle's own polar
+ * index (n + rot), with the rotation-dependent normaliser sum |ref|^2 CTF^2(n + rot).
+ * Identical to gencorrs_cc_2 when the CTF is isotropic.  Sums run over kfrom..kstop. */
+void orc_gencorrs_ptclframe(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                            const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                            double *cc);
+
+/* f and d f / d(shift_x, shift_y, defocus) at one rotation, reference frame, both
+ * branches of gencorr_cc_grad_for_rot_8 (:1863-1925).  The shift part equals the
+ * reference's grad(1:2); the defocus part (no counterpart in the reference) uses
+ * dctfmat = d|CTF|/d(defocus) on the grid in 1/micron (NULL -> grad3[2] = 0). */
+void orc_gencorr_grad3(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                       const double *dctfmat, const double *shvec, int irot, int match_filt,
+                       const double *argtransf, const double *argtransf_shellone,
+                       double *f, double *grad3);
+
+/* d|CTF|/d(mean defocus) in 1/micron, with dfx and dfy both moved by the same amount */
+void orc_dctfmat_ddf(const orc_geom *g, const float *polar, const orc_ctf *c, double *dctfmat);
+
+/* Kaiser-Bessel gridding (init_polarizer / polarize, simple_polarizer.f90:41-151) */
+void orc_polarize(const orc_geom *g, const float *polar, const float *cmat, int griddev, double *pft);
+double orc_kb_apod(double x);   /* simple_kbinterpol.f90:130-141 with Whalf=1.5, alpha=sqrt(2) */
+
+/* ---------------------------------------------------------------------------
+ * FP32 FFT path, the reference's loop structure (memoize_fft :864-877 and
+ * calc_corrs_over_k :1132-1162) on a project-written mixed-radix FFT that stands
+ * in for FFTW.  Used as the timed CPU baseline. */
+typedef struct orc_fftpath orc_fftpath;
+orc_fftpath *orc_fftpath_new(const orc_geom *g);
+void orc_fftpath_free(orc_fftpath *p);
+/* memoised particle transforms: out buffer of K*(P/2+1)*2 + K*P*2 floats (see orc_fftpath_memo_size) */
+long orc_fftpath_memo_size(const orc_geom *g);
+void orc_fftpath_memoize(orc_fftpath *p, const float *ptcl, float *memo);
+/* gencorrs_cc_2 through the FFT path: ref prepared with ctf (float, nullable) and shift */
+void orc_fftpath_gencorrs(orc_fftpath *p, const float *ref, const float *ptcl_memo, float sqsum_ptcl,
+                          const float *ctfmat, const float *shvec, const double *argtransf,
+                          const double *argtransf_shellone, float *cc);
+
+/* exhaustive CPU search (greedy strategy over all refs x shift grid, OpenMP over particles).
+ * refs [nrefs][K][P], ptcls [nptcls][K][P], ctfmats [nptcls][K][P] (float, nullable),
+ * shifts [nshifts][2].  Output per particle: best ref (0-based), best irot (1-based),
+ * best shift index, best cc.  Returns the number of OpenMP threads used. */
+int orc_cpu_search(const orc_geom *g, int nrefs, const float *refs, int nptcls, const float *ptcls,
+                   const float *ctfmats, int nshifts, const float *shifts,
+                   int *best_ref, int *best_rot, int *best_shift, float *best_cc, int nthreads);
+
+/* complex FFT helpers exposed for tests: forward (sign=-1) or backward (+1), unnormalised */
+void orc_cfft(int n, const double *in, double *out, int sign);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,938 @@
+// pftcc_capi.cu -- the C ABI of libpftcc_b200.so (declared in include/pftcc_b200.h):
+// handle life cycle, host-side tables (polar grid, shift constants, gridding taps),
+// setters/getters and the per-pair and batched correlation entry points.
+#include "pftcc_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+using namespace pftcc;
+
+namespace pftcc {
+
+int set_err(pftcc_handle *h, int code, const std::string &msg)
+{
+    if (h) h->last_err = msg;
+    return code;
+}
+
+int cuda_err(pftcc_handle *h, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return PFTCC_OK;
+    const int code = (e == cudaErrorMemoryAllocation) ? PFTCC_ERR_OOM : PFTCC_ERR_CUDA;
+    return set_err(h, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what)
+{
+    *p = nullptr;
+    if (bytes == 0) return PFTCC_OK;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return set_err(h, PFTCC_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" +
+                                              std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
+    }
+    return PFTCC_OK;
+}
+
+int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *what)
+{
+    if (*cap >= bytes && *p) return PFTCC_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    int st = dev_alloc(h, p, bytes, what);
+    if (st == PFTCC_OK) *cap = bytes;
+    return st;
+}
+
+}  // namespace pftcc
+
+#define CK(expr, what)                                             \
+    do {                                                           \
+        cudaError_t e_ = (expr);                                   \
+        if (e_ != cudaSuccess) return cuda_err(h, e_, what);       \
+    } while (0)
+#define ST(expr)                     \
+    do {                             \
+        int s_ = (expr);             \
+        if (s_ != PFTCC_OK) return s_; \
+    } while (0)
+
+static int slot_of(const pftcc_handle *h, int iptcl)
+{
+    if (iptcl < h->pfrom || iptcl > h->pto) return -1;
+    return h->pinds[iptcl - h->pfrom] - 1;
+}
+
+#define SLOT_OR_FAIL(slot, iptcl)                                                                  \
+    const int slot = slot_of(h, iptcl);                                                            \
+    if (slot < 0)                                                                                  \
+        return set_err(h, PFTCC_ERR_INDEX, "particle index " + std::to_string(iptcl) +             \
+                                               " is not held (pfromto/pinds)");
+
+#define REF_OR_FAIL(iref)                                                                            \
+    if ((iref) < 1 || (iref) > h->nrefs)                                                             \
+        return set_err(h, PFTCC_ERR_INDEX, "reference index " + std::to_string(iref) + " out of range");
+
+// ---------------------------------------------------------------------------------------
+// host tables: polar grid and shift constants (new :261-317), single precision where the
+// reference is single precision
+static void build_tables(pftcc_handle *h)
+{
+    const Geom &g = h->g;
+    const int N = g.N, P = g.P, K = g.K;
+    h->h_polar.assign((size_t)K * 2 * N, 0.f);
+    h->h_argtransf.assign((size_t)K * N, 0.0);
+    h->h_argtransf1.assign(N, 0.0);
+    h->angtab.assign(N, 0.f);
+    const float twopi = 2.0f * acosf(-1.0f);
+    const float ang = twopi / (float)N;
+    const float pif = acosf(-1.0f);
+    const double A = acos(-1.0) / (double)(g.box / 2);
+    for (int irot = 0; irot < N; ++irot) {
+        const float a = (float)irot * ang;
+        for (int ik = 0; ik < K; ++ik) {
+            const int k = g.kfrom + ik;
+            h->h_polar[(size_t)ik * 2 * N + irot] = sinf(a) * (float)k;
+            h->h_polar[(size_t)ik * 2 * N + N + irot] = -cosf(a) * (float)k;
+        }
+        h->angtab[irot] = (a / pif) * 180.0f;   // rad2deg
+    }
+    for (int ik = 0; ik < K; ++ik)
+        for (int irot = 0; irot < P; ++irot) {
+            h->h_argtransf[(size_t)ik * N + irot] = (double)h->h_polar[(size_t)ik * 2 * N + irot] * A;
+            h->h_argtransf[(size_t)ik * N + P + irot] = (double)h->h_polar[(size_t)ik * 2 * N + N + irot] * A;
+        }
+    for (int irot = 0; irot < P; ++irot) {
+        const float a = (float)irot * ang;
+        h->h_argtransf1[irot] = (double)sinf(a) * A;
+        h->h_argtransf1[P + irot] = (double)(-cosf(a)) * A;
+    }
+}
+
+// Kaiser-Bessel window with Whalf = KBWINSZ = 1.5 and alpha = KBALPHA = sqrt(2)
+// (simple_defs.f90:131-132): W = 3, beta = 7.4 (simple_kbinterpol.f90:92-109), apod
+// in single precision around the double precision I0 of :229-252 (Abramowitz &
+// Stegun 9.8.1 / 9.8.2).
+static double kb_bessi0(double x)
+{
+    if (x < 3.75) {
+        double y = x / 3.75;
+        y = y * y;
+        return 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 + y * (0.2659732 + y * (0.0360768 + y * 0.0045813)))));
+    }
+    const double y = 3.75 / x;
+    return (0.39894228 + y * (0.01328592 + y * (0.00225319 + y * (-0.00157565 + y * (0.00916281 +
+            y * (-0.02057706 + y * (0.02635537 + y * (-0.01647633 + y * 0.00392377)))))))) * exp(x) / sqrt(x);
+}
+
+static float kb_apod(float x)
+{
+    const float whalf = 1.5f, W = 3.0f, beta = 7.4f;
+    const float twooW = 2.0f / W, oneoW = 1.0f / W;
+    if (fabsf(x) > whalf) return 0.f;
+    float arg = twooW * x;
+    arg = 1.0f - arg * arg;
+    return (float)((double)oneoW * kb_bessi0((double)(beta * sqrtf(arg))));
+}
+
+static int f_nint(float x) { return (int)(x >= 0.f ? floorf(x + 0.5f) : -floorf(-x + 0.5f)); }
+
+static int cyci(int lo, int hi, int i)
+{
+    if (i > hi) return lo + (i - hi) - 1;
+    if (i < lo) return hi - (lo - i) + 1;
+    return i;
+}
+
+// init_polarizer (simple_polarizer.f90:41-92): taps [K][P][9] in the order of
+// reshape(w, wlen) (window index in x fastest), offsets into cmat(box/2+1, box) with
+// the conjugation of get_fcomp2D (simple_image.f90:1894-1907) as a bitwise complement.
+static int build_polarizer(pftcc_handle *h, int griddev)
+{
+    if (h->pol_griddev == griddev && h->pol_off) return PFTCC_OK;
+    const Geom &g = h->g;
+    const int N = g.N, P = g.P, K = g.K, box = g.box, ld = box / 2 + 1;
+    std::vector<int> off((size_t)K * P * 9);
+    std::vector<float> wt((size_t)K * P * 9);
+    for (int ik = 0; ik < K; ++ik)
+        for (int i = 0; i < P; ++i) {
+            const float lx = h->h_polar[(size_t)ik * 2 * N + i], ly = h->h_polar[(size_t)ik * 2 * N + N + i];
+            const int w1 = f_nint(lx) - 1, w2 = f_nint(ly) - 1;
+            float ax[3], ay[3], w[3][3], wsum = 0.f;
+            for (int l = 0; l < 3; ++l) {
+                ax[l] = kb_apod((float)(w1 + l) - lx);
+                ay[l] = kb_apod((float)(w2 + l) - ly);
+            }
+            for (int m = 0; m < 3; ++m)
+                for (int l = 0; l < 3; ++l) {
+                    w[l][m] = ax[l] * ay[m];
+                    wsum += w[l][m];   // column-major sum(w)
+                }
+            for (int m = 0; m < 3; ++m)
+                for (int l = 0; l < 3; ++l) {
+                    const int t = m * 3 + l;
+                    const int hh = cyci(-box / 2, box / 2, w1 + l);
+                    const int kk = cyci(-box / 2, box / 2 - 1, w2 + m);
+                    int p1, p2, conj = 0;
+                    if (hh >= 0) { p1 = hh; p2 = kk + (kk < 0 ? box : 0); }
+                    else { p1 = -hh; p2 = -kk + (-kk < 0 ? box : 0); conj = 1; }
+                    const int o = p2 * ld + p1;
+                    off[((size_t)ik * P + i) * 9 + t] = conj ? ~o : o;
+                    wt[((size_t)ik * P + i) * 9 + t] = griddev ? w[l][m] : w[l][m] / wsum;
+                }
+        }
+    if (!h->pol_off) {
+        ST(dev_alloc(h, (void **)&h->pol_off, off.size() * sizeof(int), "gridding offsets"));
+        ST(dev_alloc(h, (void **)&h->pol_w, wt.size() * sizeof(float), "gridding weights"));
+    }
+    CK(cudaMemcpyAsync(h->pol_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream), "taps");
+    CK(cudaMemcpyAsync(h->pol_w, wt.data(), wt.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream), "taps");
+    CK(cudaStreamSynchronize(h->stream), "taps");
+    h->pol_griddev = griddev;
+    return PFTCC_OK;
+}
+
+static void free_all(pftcc_handle *h)
+{
+    void *ptrs[] = {h->refs_even, h->refs_odd, h->ptcls, h->sqsums, h->ctfmats, h->d_iseven, h->d_ctfp, h->polar,
+                    h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
+                    h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
+                    h->ws.D, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
+                    h->ws.cand_ref};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+static int alloc_ptcl_arrays(pftcc_handle *h)
+{
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    const size_t n = std::max(1, h->nptcls);
+    ST(dev_alloc(h, (void **)&h->ptcls, n * KP * sizeof(float2), "particle pfts"));
+    ST(dev_alloc(h, (void **)&h->sqsums, n * sizeof(float), "particle square sums"));
+    ST(dev_alloc(h, (void **)&h->d_iseven, n, "particle eo flags"));
+    ST(dev_alloc(h, (void **)&h->d_ctfp, n * sizeof(pftcc_ctfparams), "ctf parameters"));
+    CK(cudaMemsetAsync(h->ptcls, 0, n * KP * sizeof(float2), h->stream), "zero ptcls");
+    CK(cudaMemsetAsync(h->sqsums, 0, n * sizeof(float), h->stream), "zero sqsums");
+    h->iseven.assign(n, 1);
+    CK(cudaMemcpyAsync(h->d_iseven, h->iseven.data(), n, cudaMemcpyHostToDevice, h->stream), "eo");
+    h->h_ctfp.assign(n, pftcc_ctfparams{});
+    return PFTCC_OK;
+}
+
+static int push_iseven(pftcc_handle *h)
+{
+    CK(cudaMemcpyAsync(h->d_iseven, h->iseven.data(), h->iseven.size(), cudaMemcpyHostToDevice, h->stream), "eo");
+    CK(cudaStreamSynchronize(h->stream), "eo");
+    return PFTCC_OK;
+}
+
+extern "C" {
+
+const char *pftcc_strerror(int s)
+{
+    switch (s) {
+    case PFTCC_OK: return "ok";
+    case PFTCC_ERR_ARG: return "invalid argument";
+    case PFTCC_ERR_INDEX: return "index out of range";
+    case PFTCC_ERR_STATE: return "call out of order";
+    case PFTCC_ERR_CUDA: return "CUDA error";
+    case PFTCC_ERR_OOM: return "device out of memory";
+    case PFTCC_ERR_TIMEOUT: return "device wait timed out";
+    case PFTCC_ERR_NODEV: return "no usable sm_100 device";
+    case PFTCC_ERR_UNSUPPORTED: return "unsupported mode";
+    default: return "unknown status";
+    }
+}
+
+const char *pftcc_last_error(const pftcc_handle *h) { return h ? h->last_err.c_str() : "null handle"; }
+long long pftcc_kernel_launches(const pftcc_handle *h) { return h ? h->launches : 0; }
+
+int pftcc_new(const pftcc_config *cfg, const int *ptcl_mask, const int *eoarr, pftcc_handle **out)
+{
+    if (!cfg || !out) return PFTCC_ERR_ARG;
+    *out = nullptr;
+    pftcc_handle *h = new (std::nothrow) pftcc_handle();
+    if (!h) return PFTCC_ERR_OOM;
+    auto fail = [&](int code, const std::string &msg) {
+        fprintf(stderr, "pftcc_new: %s\n", msg.c_str());
+        free_all(h);
+        delete h;
+        return code;
+    };
+    const pftcc_config c = *cfg;
+    // error checks of new :227-243
+    if (c.pfromto[1] - c.pfromto[0] + 1 < 1) return fail(PFTCC_ERR_ARG, "nptcls (# of particles) must be > 0");
+    if (c.nrefs < 1) return fail(PFTCC_ERR_ARG, "nrefs (# of reference sections) must be > 0");
+    if (c.box < 2 || (c.box & 1)) return fail(PFTCC_ERR_ARG, "only even logical dims supported");
+    if (c.nrots < 4 || (c.nrots & 1) || c.nrots > 768) return fail(PFTCC_ERR_ARG, "nrots must be even, in [4, 768]");
+    if (c.kfromto[0] < 1 || c.kfromto[1] < c.kfromto[0] || c.kstop < c.kfromto[0] || c.kstop > c.kfromto[1])
+        return fail(PFTCC_ERR_ARG, "need 1 <= kfromto(1) <= kstop <= kfromto(2)");
+    if (c.kfromto[1] + 2 > c.box / 2) return fail(PFTCC_ERR_ARG, "kfromto(2) beyond the gridding window of the box");
+    if (c.ctf_frame != PFTCC_FRAME_REF && c.ctf_frame != PFTCC_FRAME_PTCL) return fail(PFTCC_ERR_ARG, "bad ctf_frame");
+    h->cfg = c;
+    h->g.N = c.nrots;
+    h->g.P = c.nrots / 2;
+    h->g.kfrom = c.kfromto[0];
+    h->g.kto = c.kfromto[1];
+    h->g.kstop = c.kstop;
+    h->g.K = c.kfromto[1] - c.kfromto[0] + 1;
+    h->g.Ks = c.kstop - c.kfromto[0] + 1;
+    h->g.box = c.box;
+    h->nrefs = c.nrefs;
+    h->pfrom = c.pfromto[0];
+    h->pto = c.pfromto[1];
+    const int span = h->pto - h->pfrom + 1;
+    h->pinds.assign(span, 0);
+    int cnt = 0;
+    for (int i = 0; i < span; ++i)
+        if (!ptcl_mask || ptcl_mask[i]) h->pinds[i] = ++cnt;   // :278-288
+    if (cnt < 1) return fail(PFTCC_ERR_ARG, "the particle mask selects no particle");
+    h->nptcls = cnt;
+    // device: sm_100 only, no fallback
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(PFTCC_ERR_NODEV, "no CUDA device visible");
+    }
+    if (c.device < 0 || c.device >= ndev) return fail(PFTCC_ERR_NODEV, "device ordinal out of range");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess || prop.major != 10)
+        return fail(PFTCC_ERR_NODEV, "device is not sm_100 (B200)");
+    h->dev = c.device;
+    if (cudaSetDevice(h->dev) != cudaSuccess) return fail(PFTCC_ERR_NODEV, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(PFTCC_ERR_CUDA, "stream creation failed");
+    build_tables(h);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    int st = PFTCC_OK;
+    if ((st = dev_alloc(h, (void **)&h->refs_even, (size_t)h->nrefs * KP * sizeof(float2), "refs even")) ||
+        (st = dev_alloc(h, (void **)&h->refs_odd, (size_t)h->nrefs * KP * sizeof(float2), "refs odd")) ||
+        (st = dev_alloc(h, (void **)&h->polar, h->h_polar.size() * sizeof(float), "polar")) ||
+        (st = dev_alloc(h, (void **)&h->argtransf, h->h_argtransf.size() * sizeof(double), "argtransf")) ||
+        (st = dev_alloc(h, (void **)&h->argtransf1, h->h_argtransf1.size() * sizeof(double), "argtransf1")) ||
+        (st = alloc_ptcl_arrays(h)))
+        return fail(st, h->last_err);
+    if (cudaMemsetAsync(h->refs_even, 0, (size_t)h->nrefs * KP * sizeof(float2), h->stream) ||
+        cudaMemsetAsync(h->refs_odd, 0, (size_t)h->nrefs * KP * sizeof(float2), h->stream) ||
+        cudaMemcpyAsync(h->polar, h->h_polar.data(), h->h_polar.size() * sizeof(float), cudaMemcpyHostToDevice,
+                        h->stream) ||
+        cudaMemcpyAsync(h->argtransf, h->h_argtransf.data(), h->h_argtransf.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, h->stream) ||
+        cudaMemcpyAsync(h->argtransf1, h->h_argtransf1.data(), h->h_argtransf1.size() * sizeof(double),
+                        cudaMemcpyHostToDevice, h->stream))
+        return fail(PFTCC_ERR_CUDA, "initial uploads failed");
+    // eo assignment :289-306
+    if (eoarr) {
+        bool all_m1 = true;
+        for (int i = 0; i < span; ++i)
+            if (eoarr[i] != -1) all_m1 = false;
+        if (!all_m1)
+            for (int i = 0; i < span; ++i)
+                if (h->pinds[i] > 0) h->iseven[h->pinds[i] - 1] = eoarr[i] == 0;
+    }
+    if (push_iseven(h) != PFTCC_OK) return fail(PFTCC_ERR_CUDA, h->last_err);
+    *out = h;
+    return PFTCC_OK;
+}
+
+int pftcc_kill(pftcc_handle *h)
+{
+    if (!h) return PFTCC_OK;
+    cudaSetDevice(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return PFTCC_OK;
+}
+
+int pftcc_reallocate_ptcls(pftcc_handle *h, int nptcls, const int *pinds)
+{
+    if (!h || nptcls < 1 || !pinds) return set_err(h, PFTCC_ERR_ARG, "reallocate_ptcls: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    int lo = pinds[0], hi = pinds[0];
+    for (int i = 0; i < nptcls; ++i) { lo = std::min(lo, pinds[i]); hi = std::max(hi, pinds[i]); }
+    h->pfrom = lo;
+    h->pto = hi;
+    h->pinds.assign(hi - lo + 1, 0);
+    for (int i = 0; i < nptcls; ++i) h->pinds[pinds[i] - lo] = i + 1;   // :551-554
+    if (nptcls != h->nptcls) {
+        CK(cudaStreamSynchronize(h->stream), "sync");
+        void *old[] = {h->ptcls, h->sqsums, h->d_iseven, h->d_ctfp, h->ctfmats};
+        for (void *p : old)
+            if (p) cudaFree(p);
+        h->ptcls = nullptr; h->sqsums = nullptr; h->d_iseven = nullptr; h->d_ctfp = nullptr; h->ctfmats = nullptr;
+        h->nptcls = nptcls;
+        ST(alloc_ptcl_arrays(h));
+    } else {
+        const size_t KP = (size_t)h->g.K * h->g.P;
+        CK(cudaMemsetAsync(h->ptcls, 0, (size_t)nptcls * KP * sizeof(float2), h->stream), "zero ptcls");
+        CK(cudaMemsetAsync(h->sqsums, 0, (size_t)nptcls * sizeof(float), h->stream), "zero sqsums");
+        h->iseven.assign(nptcls, 1);
+    }
+    h->ctf_ready = 0;
+    h->ws.ptcl_spectra_valid = 0;
+    return push_iseven(h);
+}
+
+// ---- setters ---------------------------------------------------------------------------
+int pftcc_set_refs(pftcc_handle *h, int first_iref, int n, const float *pfts, int iseven)
+{
+    if (!h || !pfts || n < 0) return set_err(h, PFTCC_ERR_ARG, "set_refs: bad arguments");
+    if (first_iref < 1 || first_iref + n - 1 > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "set_refs: range");
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    float2 *dst = (iseven ? h->refs_even : h->refs_odd) + (size_t)(first_iref - 1) * KP;
+    CK(cudaMemcpyAsync(dst, pfts, (size_t)n * KP * sizeof(float2), cudaMemcpyHostToDevice, h->stream), "set_refs");
+    CK(cudaStreamSynchronize(h->stream), "set_refs");
+    return PFTCC_OK;
+}
+
+int pftcc_set_ref_pft(pftcc_handle *h, int iref, const float *pft, int iseven)
+{
+    return pftcc_set_refs(h, iref, 1, pft, iseven);
+}
+
+int pftcc_set_ptcls(pftcc_handle *h, int first_slot, int n, const float *pfts)
+{
+    if (!h || !pfts || n < 0) return set_err(h, PFTCC_ERR_ARG, "set_ptcls: bad arguments");
+    if (first_slot < 0 || first_slot + n > h->nptcls) return set_err(h, PFTCC_ERR_INDEX, "set_ptcls: range");
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    CK(cudaMemcpyAsync(h->ptcls + (size_t)first_slot * KP, pfts, (size_t)n * KP * sizeof(float2),
+                       cudaMemcpyHostToDevice, h->stream), "set_ptcls");
+    CK(launch_sqsums(h, first_slot, n), "sqsums");
+    CK(cudaStreamSynchronize(h->stream), "set_ptcls");
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_set_ptcl_pft(pftcc_handle *h, int iptcl, const float *pft)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    SLOT_OR_FAIL(slot, iptcl);
+    return pftcc_set_ptcls(h, slot, 1, pft);
+}
+
+int pftcc_set_ref_fcomp(pftcc_handle *h, int iref, int irot, int k, const float *comp, int iseven)
+{
+    if (!h || !comp) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    if (irot < 1 || irot > h->g.P || k < h->g.kfrom || k > h->g.kto)
+        return set_err(h, PFTCC_ERR_INDEX, "set_ref_fcomp: (irot, k) out of range");
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    float2 *dst = (iseven ? h->refs_even : h->refs_odd) + (size_t)(iref - 1) * KP +
+                  (size_t)(k - h->g.kfrom) * h->g.P + (irot - 1);
+    CK(cudaMemcpyAsync(dst, comp, sizeof(float2), cudaMemcpyHostToDevice, h->stream), "set_ref_fcomp");
+    CK(cudaStreamSynchronize(h->stream), "set_ref_fcomp");
+    return PFTCC_OK;
+}
+
+int pftcc_cp_even2odd_ref(pftcc_handle *h, int iref)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    CK(cudaMemcpyAsync(h->refs_odd + (iref - 1) * KP, h->refs_even + (iref - 1) * KP, KP * sizeof(float2),
+                       cudaMemcpyDeviceToDevice, h->stream), "cp_even2odd_ref");
+    CK(cudaStreamSynchronize(h->stream), "cp_even2odd_ref");
+    return PFTCC_OK;
+}
+
+int pftcc_cp_even_ref2ptcl(pftcc_handle *h, int iref, int iptcl)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    SLOT_OR_FAIL(slot, iptcl);
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    CK(cudaMemcpyAsync(h->ptcls + slot * KP, h->refs_even + (iref - 1) * KP, KP * sizeof(float2),
+                       cudaMemcpyDeviceToDevice, h->stream), "cp_even_ref2ptcl");
+    CK(launch_sqsums(h, slot, 1), "sqsums");
+    CK(cudaStreamSynchronize(h->stream), "cp_even_ref2ptcl");
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_swap_ptclsevenodd(pftcc_handle *h)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    for (auto &e : h->iseven) e = !e;
+    return push_iseven(h);
+}
+
+int pftcc_set_eo(pftcc_handle *h, int iptcl, int is_even)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    SLOT_OR_FAIL(slot, iptcl);
+    h->iseven[slot] = is_even ? 1 : 0;
+    return push_iseven(h);
+}
+
+int pftcc_set_eos(pftcc_handle *h, const int *eoarr)
+{
+    if (!h || !eoarr) return PFTCC_ERR_ARG;
+    bool all_m1 = true;
+    for (int i = 0; i < h->nptcls; ++i)
+        if (eoarr[i] != -1) all_m1 = false;
+    for (int i = 0; i < h->nptcls; ++i) h->iseven[i] = all_m1 ? 1 : (eoarr[i] == 0);
+    return push_iseven(h);
+}
+
+int pftcc_zero_refs_beyond_kstop(pftcc_handle *h)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    cudaSetDevice(h->dev);
+    CK(launch_zero_beyond_kstop(h), "zero_refs_beyond_kstop");
+    CK(cudaStreamSynchronize(h->stream), "zero_refs_beyond_kstop");
+    return PFTCC_OK;
+}
+
+// ---- CTF ---------------------------------------------------------------------------------
+int pftcc_create_polar_absctfmats(pftcc_handle *h, const pftcc_ctfparams *params)
+{
+    if (!h || !params) return set_err(h, PFTCC_ERR_ARG, "create_polar_absctfmats: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    for (int i = 0; i < h->nptcls; ++i) {
+        const pftcc_ctfparams &p = params[i];
+        if (!(p.smpd > 0.f) || !(p.kv > 0.f) || !(p.fraca >= 0.f && p.fraca < 1.f))
+            return set_err(h, PFTCC_ERR_ARG, "create_polar_absctfmats: bad ctf parameters for slot " +
+                                                 std::to_string(i));
+    }
+    h->h_ctfp.assign(params, params + h->nptcls);
+    if (!h->ctfmats)
+        ST(dev_alloc(h, (void **)&h->ctfmats, (size_t)h->nptcls * h->g.K * h->g.P * sizeof(float), "ctfmats"));
+    CK(cudaMemcpyAsync(h->d_ctfp, params, (size_t)h->nptcls * sizeof(pftcc_ctfparams), cudaMemcpyHostToDevice,
+                       h->stream), "ctf params");
+    for (int c0 = 0; c0 < h->nptcls; c0 += 65535) {
+        const int n = std::min(65535, h->nptcls - c0);
+        CK(launch_ctfmat(h, h->d_ctfp + c0, n, h->ctfmats + (size_t)c0 * h->g.K * h->g.P, 0.f, 0), "ctfmat");
+    }
+    CK(cudaStreamSynchronize(h->stream), "ctfmat");
+    h->ctf_ready = 1;
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+// ---- polarizer -----------------------------------------------------------------------------
+static int polarize_dev(pftcc_handle *h, int first_slot, int n, const float2 *src_dev, int griddev)
+{
+    ST(build_polarizer(h, griddev));
+    for (int c0 = 0; c0 < n; c0 += 65535) {
+        const int m = std::min(65535, n - c0);
+        const size_t img = (size_t)h->g.box * (h->g.box / 2 + 1);
+        CK(launch_polarize(h, src_dev + (size_t)c0 * img, m, first_slot + c0), "polarize");
+    }
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_polarize_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *cmats_dev, int griddev)
+{
+    if (!h || !cmats_dev || n < 0) return set_err(h, PFTCC_ERR_ARG, "polarize_ptcls_dev: bad arguments");
+    if (first_slot < 0 || first_slot + n > h->nptcls) return set_err(h, PFTCC_ERR_INDEX, "polarize: slot range");
+    if (((uintptr_t)cmats_dev & 15) != 0) return set_err(h, PFTCC_ERR_ARG, "polarize: images must be 16-byte aligned");
+    cudaSetDevice(h->dev);
+    ST(polarize_dev(h, first_slot, n, (const float2 *)cmats_dev, griddev));
+    CK(cudaStreamSynchronize(h->stream), "polarize");
+    return PFTCC_OK;
+}
+
+int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cmats, int griddev)
+{
+    if (!h || !cmats || n < 0) return set_err(h, PFTCC_ERR_ARG, "polarize_ptcls: bad arguments");
+    if (first_slot < 0 || first_slot + n > h->nptcls) return set_err(h, PFTCC_ERR_INDEX, "polarize: slot range");
+    cudaSetDevice(h->dev);
+    const size_t img = (size_t)h->g.box * (h->g.box / 2 + 1) * sizeof(float2);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, (256u << 20) / img));
+    ST(ensure(h, &h->pol_stage, &h->pol_stage_bytes, (size_t)chunk * img, "polarize staging"));
+    for (int c0 = 0; c0 < n; c0 += chunk) {
+        const int m = std::min(chunk, n - c0);
+        CK(cudaMemcpyAsync(h->pol_stage, (const char *)cmats + (size_t)c0 * img, (size_t)m * img,
+                           cudaMemcpyHostToDevice, h->stream), "polarize upload");
+        ST(polarize_dev(h, first_slot + c0, m, (const float2 *)h->pol_stage, griddev));
+    }
+    CK(cudaStreamSynchronize(h->stream), "polarize");
+    return PFTCC_OK;
+}
+
+int pftcc_polarize_refs(pftcc_handle *h, int first_iref, int n, const float *cmats, int iseven, int griddev)
+{
+    // polarize into the particle slots' layout through a temporary handle-less path:
+    // the gridding is identical, only the destination differs (polarize :144-148)
+    if (!h || !cmats || n < 0) return set_err(h, PFTCC_ERR_ARG, "polarize_refs: bad arguments");
+    if (first_iref < 1 || first_iref + n - 1 > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "polarize_refs: range");
+    cudaSetDevice(h->dev);
+    ST(build_polarizer(h, griddev));
+    const size_t img = (size_t)h->g.box * (h->g.box / 2 + 1) * sizeof(float2);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    ST(ensure(h, &h->pol_stage, &h->pol_stage_bytes, std::max<size_t>((size_t)n * img, 1), "polarize staging"));
+    CK(cudaMemcpyAsync(h->pol_stage, cmats, (size_t)n * img, cudaMemcpyHostToDevice, h->stream), "upload");
+    // reuse the particle kernel with a redirected destination
+    float2 *save_p = h->ptcls;
+    float *save_s = h->sqsums;
+    h->ptcls = (iseven ? h->refs_even : h->refs_odd) + (size_t)(first_iref - 1) * KP;
+    float *dummy = nullptr;
+    ST(dev_alloc(h, (void **)&dummy, (size_t)n * sizeof(float), "ref sqsums"));
+    h->sqsums = dummy;
+    cudaError_t e = launch_polarize(h, (const float2 *)h->pol_stage, n, 0);
+    h->ptcls = save_p;
+    h->sqsums = save_s;
+    cudaError_t e2 = cudaStreamSynchronize(h->stream);
+    cudaFree(dummy);
+    CK(e, "polarize refs");
+    CK(e2, "polarize refs");
+    return PFTCC_OK;
+}
+
+int pftcc_memoize_ffts(pftcc_handle *h)
+{
+    // the exact path reads the particle pfts directly; the m-domain search prepares its
+    // particle spectra lazily (they depend on the CTF matrices), so only invalidate here
+    if (!h) return PFTCC_ERR_ARG;
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+// ---- correlators -----------------------------------------------------------------------------
+static int ensure_small(pftcc_handle *h, size_t nwork, size_t ngroups, size_t nout, size_t nshifts)
+{
+    ST(ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>(nwork * sizeof(Work), 4096), "work"));
+    ST(ensure(h, (void **)&h->d_groups, &h->group_cap, std::max<size_t>(ngroups * sizeof(Group), 256), "groups"));
+    ST(ensure(h, (void **)&h->d_out, &h->out_cap, std::max<size_t>(nout * sizeof(float), 256), "out"));
+    ST(ensure(h, (void **)&h->d_shifts, &h->shifts_cap, std::max<size_t>(nshifts * 2 * sizeof(float), 64), "shifts"));
+    ST(ensure(h, (void **)&h->d_dout, &h->dout_cap, 4096, "dout"));
+    return PFTCC_OK;
+}
+
+static int check_ctf_state(pftcc_handle *h)
+{
+    if (h->cfg.with_ctf && !h->ctf_ready)
+        return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    return PFTCC_OK;
+}
+
+int pftcc_gencorrs(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *cc)
+{
+    if (!h || !cc) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    SLOT_OR_FAIL(slot, iptcl);
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    ST(ensure_small(h, 1, 1, h->g.N, 1));
+    Work w{iref - 1, shvec ? 0 : -1, 0};
+    Group gr{slot, 0, 1, 0};
+    CK(cudaMemcpyAsync(h->d_work, &w, sizeof(w), cudaMemcpyHostToDevice, h->stream), "gencorrs");
+    CK(cudaMemcpyAsync(h->d_groups, &gr, sizeof(gr), cudaMemcpyHostToDevice, h->stream), "gencorrs");
+    if (shvec) CK(cudaMemcpyAsync(h->d_shifts, shvec, 2 * sizeof(float), cudaMemcpyHostToDevice, h->stream), "gencorrs");
+    CK(launch_exact(h, h->d_groups, 1, h->d_work, h->d_shifts, MODE_FULL, h->cfg.ctf_frame, 1, h->d_out, nullptr),
+       "gencorrs kernel");
+    CK(cudaMemcpyAsync(cc, h->d_out, h->g.N * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "gencorrs");
+    CK(cudaStreamSynchronize(h->stream), "gencorrs");
+    return PFTCC_OK;
+}
+
+static int for_rot_common(pftcc_handle *h, int iref, int iptcl, double sx, double sy, int irot, double *out5)
+{
+    REF_OR_FAIL(iref);
+    SLOT_OR_FAIL(slot, iptcl);
+    if (irot < 1 || irot > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "irot out of range");
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "single-rotation correlations are served in the reference frame");
+    ST(check_ctf_state(h));
+    ST(ensure_small(h, 1, 1, h->g.N, 1));
+    CK(launch_for_rot(h, iref - 1, slot, sx, sy, irot, h->cfg.match_filt, 1, 0.0, h->d_dout), "for_rot kernel");
+    CK(cudaMemcpyAsync(out5, h->d_dout, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "for_rot");
+    CK(cudaStreamSynchronize(h->stream), "for_rot");
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot, double *cc)
+{
+    if (!h || !cc || !shvec) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    double o[5];
+    ST(for_rot_common(h, iref, iptcl, shvec[0], shvec[1], irot, o));
+    *cc = o[0];
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_for_rot(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot, float *cc)
+{
+    if (!h || !cc || !shvec) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    double o[5];
+    ST(for_rot_common(h, iref, iptcl, (double)shvec[0], (double)shvec[1], irot, o));
+    *cc = (float)o[0];
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot, double *f,
+                                 double *grad)
+{
+    if (!h || !f || !grad || !shvec) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    double o[5];
+    ST(for_rot_common(h, iref, iptcl, shvec[0], shvec[1], irot, o));
+    *f = o[0];
+    grad[0] = o[1];
+    grad[1] = o[2];
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                      double *grad)
+{
+    double f;
+    return pftcc_gencorr_grad_for_rot_8(h, iref, iptcl, shvec, irot, &f, grad);
+}
+
+int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
+{
+    if (!h || !cc || nshifts < 0 || (nshifts > 0 && !shifts)) return set_err(h, PFTCC_ERR_ARG, "corr_all: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    const int ns = std::max(1, nshifts);
+    const size_t per_ptcl = (size_t)h->nrefs * ns;
+    // bounded output chunks of particles
+    const size_t out_per_ptcl = per_ptcl * h->g.N;
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(h->nptcls, (size_t)(512u << 20) / (out_per_ptcl * 4)));
+    ST(ensure_small(h, (size_t)chunk * per_ptcl, chunk, (size_t)chunk * out_per_ptcl, ns));
+    if (nshifts > 0)
+        CK(cudaMemcpyAsync(h->d_shifts, shifts, 2 * sizeof(float) * nshifts, cudaMemcpyHostToDevice, h->stream), "shifts");
+    std::vector<Work> work((size_t)chunk * per_ptcl);
+    std::vector<Group> groups(chunk);
+    for (int c0 = 0; c0 < h->nptcls; c0 += chunk) {
+        const int m = std::min(chunk, h->nptcls - c0);
+        size_t wi = 0;
+        for (int i = 0; i < m; ++i) {
+            groups[i] = Group{c0 + i, (int)wi, (int)per_ptcl, i};
+            for (int r = 0; r < h->nrefs; ++r)
+                for (int s = 0; s < ns; ++s) {
+                    work[wi] = Work{r, nshifts > 0 ? s : -1, (long long)(((size_t)i * h->nrefs + r) * ns + s) * h->g.N};
+                    ++wi;
+                }
+        }
+        CK(cudaMemcpyAsync(h->d_work, work.data(), wi * sizeof(Work), cudaMemcpyHostToDevice, h->stream), "work");
+        CK(cudaMemcpyAsync(h->d_groups, groups.data(), m * sizeof(Group), cudaMemcpyHostToDevice, h->stream), "groups");
+        CK(launch_exact(h, h->d_groups, m, h->d_work, h->d_shifts, MODE_FULL, h->cfg.ctf_frame, 1, h->d_out, nullptr),
+           "corr_all kernel");
+        CK(cudaMemcpyAsync(cc + (size_t)c0 * out_per_ptcl, h->d_out, (size_t)m * out_per_ptcl * sizeof(float),
+                           cudaMemcpyDeviceToHost, h->stream), "corr_all download");
+        CK(cudaStreamSynchronize(h->stream), "corr_all");
+    }
+    return PFTCC_OK;
+}
+
+static int search_exact(pftcc_handle *h, int nshifts, const float *shifts, pftcc_best *out_dev)
+{
+    const int ns = std::max(1, nshifts);
+    const size_t per_ptcl = (size_t)h->nrefs * ns;
+    ST(ensure_small(h, (size_t)h->nptcls * per_ptcl, h->nptcls, 1, ns));
+    if (nshifts > 0)
+        CK(cudaMemcpyAsync(h->d_shifts, shifts, 2 * sizeof(float) * nshifts, cudaMemcpyHostToDevice, h->stream), "shifts");
+    std::vector<Work> work((size_t)h->nptcls * per_ptcl);
+    std::vector<Group> groups(h->nptcls);
+    size_t wi = 0;
+    for (int i = 0; i < h->nptcls; ++i) {
+        groups[i] = Group{i, (int)wi, (int)per_ptcl, i};
+        for (int r = 0; r < h->nrefs; ++r)
+            for (int s = 0; s < ns; ++s) work[wi++] = Work{r, nshifts > 0 ? s : -1, 0};
+    }
+    CK(cudaMemcpyAsync(h->d_work, work.data(), wi * sizeof(Work), cudaMemcpyHostToDevice, h->stream), "work");
+    CK(cudaMemcpyAsync(h->d_groups, groups.data(), groups.size() * sizeof(Group), cudaMemcpyHostToDevice, h->stream),
+       "groups");
+    CK(launch_exact(h, h->d_groups, h->nptcls, h->d_work, h->d_shifts, MODE_BEST, h->cfg.ctf_frame, 1, nullptr, out_dev),
+       "search exact");
+    return PFTCC_OK;
+}
+
+int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, void *out_dev)
+{
+    if (!h || !out_dev || nshifts < 0 || (nshifts > 0 && !shifts) || ntop < 0 || ntop > 8)
+        return set_err(h, PFTCC_ERR_ARG, "search_best: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    if (precision == PFTCC_PREC_EXACT) {
+        ST(search_exact(h, nshifts, shifts, (pftcc_best *)out_dev));
+    } else if (precision == PFTCC_PREC_FP32 || precision == PFTCC_PREC_BF16X3) {
+        ST(search_mdomain(h, nshifts, shifts, precision, ntop, (pftcc_best *)out_dev));
+    } else {
+        return set_err(h, PFTCC_ERR_ARG, "search_best: unknown precision");
+    }
+    CK(cudaStreamSynchronize(h->stream), "search_best");
+    return PFTCC_OK;
+}
+
+int pftcc_search_best(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out)
+{
+    if (!h || !out) return set_err(h, PFTCC_ERR_ARG, "search_best: bad arguments");
+    {
+        std::lock_guard<std::mutex> lk(h->mtx);
+        cudaSetDevice(h->dev);
+        ST(ensure(h, (void **)&h->d_best, &h->best_cap, (size_t)h->nptcls * sizeof(pftcc_best), "best"));
+    }
+    ST(pftcc_search_best_dev(h, nshifts, shifts, precision, ntop, h->d_best));
+    CK(cudaMemcpy(out, h->d_best, (size_t)h->nptcls * sizeof(pftcc_best), cudaMemcpyDeviceToHost), "search download");
+    return PFTCC_OK;
+}
+
+int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3)
+{
+    if (!h || nreq < 0 || (nreq > 0 && (!req || !f || !grad3))) return set_err(h, PFTCC_ERR_ARG, "grad_batch: bad arguments");
+    if (nreq == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the adjoint is served in the reference frame");
+    ST(check_ctf_state(h));
+    std::vector<int> slots(nreq);
+    for (int i = 0; i < nreq; ++i) {
+        if (req[i].iref < 1 || req[i].iref > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "grad_batch: iref");
+        if (req[i].irot < 1 || req[i].irot > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "grad_batch: irot");
+        const int s = slot_of(h, req[i].iptcl);
+        if (s < 0) return set_err(h, PFTCC_ERR_INDEX, "grad_batch: iptcl");
+        slots[i] = s;
+    }
+    // device layout: [req][slots][RotReq work area][out]
+    const size_t rq_bytes = (size_t)nreq * sizeof(pftcc_grad_req);
+    ST(ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)nreq * 48, 4096), "grad work"));
+    ST(ensure(h, (void **)&h->d_dout, &h->dout_cap, (size_t)nreq * 5 * sizeof(double) + rq_bytes + (size_t)nreq * 4 + 64,
+              "grad out"));
+    char *base = (char *)h->d_dout;
+    double *dout = (double *)base;
+    pftcc_grad_req *dreq = (pftcc_grad_req *)(base + (size_t)nreq * 5 * sizeof(double));
+    int *dslots = (int *)((char *)dreq + rq_bytes);
+    CK(cudaMemcpyAsync(dreq, req, rq_bytes, cudaMemcpyHostToDevice, h->stream), "grad upload");
+    CK(cudaMemcpyAsync(dslots, slots.data(), (size_t)nreq * sizeof(int), cudaMemcpyHostToDevice, h->stream), "grad upload");
+    CK(launch_grad_batch(h, dreq, dslots, nreq, dout), "grad kernel");
+    std::vector<double> o((size_t)nreq * 5);
+    CK(cudaMemcpyAsync(o.data(), dout, o.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "grad download");
+    CK(cudaStreamSynchronize(h->stream), "grad");
+    for (int i = 0; i < nreq; ++i) {
+        f[i] = o[5 * i];
+        grad3[3 * i] = o[5 * i + 1];
+        grad3[3 * i + 1] = o[5 * i + 2];
+        grad3[3 * i + 2] = o[5 * i + 3];
+    }
+    return PFTCC_OK;
+}
+
+// ---- getters -------------------------------------------------------------------------------
+int pftcc_get_nrots(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->g.N; return PFTCC_OK; }
+int pftcc_get_pftsz(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->g.P; return PFTCC_OK; }
+int pftcc_get_box(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->g.box; return PFTCC_OK; }
+int pftcc_get_nrefs(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->nrefs; return PFTCC_OK; }
+int pftcc_get_nptcls(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->nptcls; return PFTCC_OK; }
+int pftcc_exists(const pftcc_handle *h, int *v) { if (!v) return PFTCC_ERR_ARG; *v = h != nullptr; return PFTCC_OK; }
+
+int pftcc_get_pdim(const pftcc_handle *h, int pdim[3])
+{
+    if (!h || !pdim) return PFTCC_ERR_ARG;
+    pdim[0] = h->g.P; pdim[1] = h->g.kfrom; pdim[2] = h->g.kto;
+    return PFTCC_OK;
+}
+
+// get_rot :624-634
+int pftcc_get_rot(const pftcc_handle *h, int roind, float *rot)
+{
+    if (!h || !rot) return PFTCC_ERR_ARG;
+    if (roind < 1 || roind > h->g.N) return PFTCC_ERR_INDEX;
+    *rot = h->angtab[roind - 1];
+    return PFTCC_OK;
+}
+
+// get_roind :638-647: argmin of the cyclic angular distance, first minimum
+int pftcc_get_roind(const pftcc_handle *h, float rot, int *roind)
+{
+    if (!h || !roind) return PFTCC_ERR_ARG;
+    float best = INFINITY;
+    int loc = 1;
+    for (int i = 0; i < h->g.N; ++i) {
+        float d = fabsf(h->angtab[i] - rot);
+        if (d > 180.f) d = 360.f - d;
+        if (d < best) { best = d; loc = i + 1; }
+    }
+    *roind = loc;
+    return PFTCC_OK;
+}
+
+// get_coord :651-657
+int pftcc_get_coord(const pftcc_handle *h, int rot, int k, float xy[2])
+{
+    if (!h || !xy) return PFTCC_ERR_ARG;
+    if (rot < 1 || rot > h->g.N || k < h->g.kfrom || k > h->g.kto) return PFTCC_ERR_INDEX;
+    const int ik = k - h->g.kfrom;
+    xy[0] = h->h_polar[(size_t)ik * 2 * h->g.N + rot - 1];
+    xy[1] = h->h_polar[(size_t)ik * 2 * h->g.N + h->g.N + rot - 1];
+    return PFTCC_OK;
+}
+
+int pftcc_ptcl_iseven(const pftcc_handle *h, int iptcl, int *iseven)
+{
+    if (!h || !iseven) return PFTCC_ERR_ARG;
+    const int s = slot_of(h, iptcl);
+    if (s < 0) return PFTCC_ERR_INDEX;
+    *iseven = h->iseven[s];
+    return PFTCC_OK;
+}
+
+int pftcc_get_ref_pft(pftcc_handle *h, int iref, int iseven, float *pft)
+{
+    if (!h || !pft) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    CK(cudaMemcpyAsync(pft, (iseven ? h->refs_even : h->refs_odd) + (iref - 1) * KP, KP * sizeof(float2),
+                       cudaMemcpyDeviceToHost, h->stream), "get_ref_pft");
+    CK(cudaStreamSynchronize(h->stream), "get_ref_pft");
+    return PFTCC_OK;
+}
+
+int pftcc_get_ptcl_pft(pftcc_handle *h, int iptcl, float *pft)
+{
+    if (!h || !pft) return PFTCC_ERR_ARG;
+    SLOT_OR_FAIL(slot, iptcl);
+    cudaSetDevice(h->dev);
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    CK(cudaMemcpyAsync(pft, h->ptcls + slot * KP, KP * sizeof(float2), cudaMemcpyDeviceToHost, h->stream), "get_ptcl_pft");
+    CK(cudaStreamSynchronize(h->stream), "get_ptcl_pft");
+    return PFTCC_OK;
+}
+
+int pftcc_get_sqsum_ptcl(pftcc_handle *h, int iptcl, float *sq)
+{
+    if (!h || !sq) return PFTCC_ERR_ARG;
+    SLOT_OR_FAIL(slot, iptcl);
+    cudaSetDevice(h->dev);
+    CK(cudaMemcpyAsync(sq, h->sqsums + slot, sizeof(float), cudaMemcpyDeviceToHost, h->stream), "sqsum");
+    CK(cudaStreamSynchronize(h->stream), "sqsum");
+    return PFTCC_OK;
+}
+
+int pftcc_synchronize(pftcc_handle *h)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    cudaSetDevice(h->dev);
+    CK(cudaStreamSynchronize(h->stream), "synchronize");
+    return PFTCC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// pftcc_internal.cuh -- handle layout, launch helpers and kernel entry points
+// shared by the translation units of libpftcc_b200.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pftcc_b200.h"
+
+namespace pftcc {
+
+// Layout of the data held in HBM (all "K" counts run over kfrom..kto, "Ks" over
+// kfrom..kstop):
+//   refs_even/odd [nrefs][K][P] float2     (pfts_refs_even/odd(P, kfrom:kto, nrefs))
+//   ptcls         [nptcls][K][P] float2    (pfts_ptcls(P, kfrom:kto, nptcls))
+//   ctfmats       [nptcls][K][P] float     (ctfmats(P, kfrom:kto, nptcls))
+//   polar         [K][2N] float            (polar(2N, kfrom:kto))
+//   argtransf     [K][N] double, argtransf1 [N] double
+struct Geom {
+    int N, P, K, Ks, kfrom, kto, kstop, box;
+};
+
+// per-shift phase tables used by the exact kernels: shmat for a list of shifts is
+// generated on the device from argtransf in double precision (gen_shmat_8)
+struct Work {           // one (reference, shift) correlation for the particle of a group
+    int iref;           // 0-based
+    int ishift;         // index into the shift list (-1 = no shift, gencorrs_cc_1)
+    long long out;      // output offset (MODE_FULL) or candidate id (MODE_BEST)
+};
+
+struct Group {          // all work items of one particle slot
+    int slot;
+    int first, count;   // range in the Work array
+    int out_best;       // index of the pftcc_best written in MODE_BEST
+};
+
+enum { MODE_FULL = 0, MODE_BEST = 1 };
+
+// m-domain search workspace (sized on first use, reused across calls)
+struct SearchWS {
+    int nshifts = 0, nrs = 0, nrs_pad = 0, np_pad = 0, M = 0, Mpad = 0;
+    float2 *UA = nullptr;        // [M][nrs_pad][Ks] ref-side spectra (FP32 path)
+    float2 *UB = nullptr;        // [M][np_pad][Ks] particle-side spectra (FP32 path)
+    double2 *RU = nullptr;       // [nrefs][J][Ks] spectra of |ref|^2, J = P/2+1
+    double2 *CV = nullptr;       // [np_pad][J][Ks] spectra of CTF^2
+    float *D = nullptr;          // [wave refs][np_pad][P] rotation-dependent normaliser
+    float2 *X = nullptr;         // [M][wave rows][wave cols] stage-1 output of one wave
+    size_t X_elems = 0;
+    float2 *cand = nullptr;      // [np_pad][8] packed (cc, rs*N+rot) candidates
+    float *sqp = nullptr;        // [np_pad]
+    __nv_bfloat16 *A16 = nullptr;  // tcgen05 operands, see k_umma.cu
+    __nv_bfloat16 *B16 = nullptr;
+    size_t A16_elems = 0, B16_elems = 0;
+    float *shifts = nullptr;     // [nshifts][2]
+    pftcc_best *best = nullptr;  // [np_pad]
+    int *cand_ref = nullptr;
+    int ptcl_spectra_valid = 0;  // particle spectra current for this handle state
+};
+
+}  // namespace pftcc
+
+struct pftcc_handle {
+    pftcc_config cfg{};
+    pftcc::Geom g{};
+    int nrefs = 0, nptcls = 0;
+    int pfrom = 0, pto = 0;
+    std::vector<int> pinds;              // global - pfrom -> slot + 1 (0 = not held)
+    std::vector<uint8_t> iseven;         // per slot
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    // device data
+    float2 *refs_even = nullptr, *refs_odd = nullptr, *ptcls = nullptr;
+    float *sqsums = nullptr, *ctfmats = nullptr;
+    uint8_t *d_iseven = nullptr;
+    pftcc_ctfparams *d_ctfp = nullptr;
+    std::vector<pftcc_ctfparams> h_ctfp;
+    int ctf_ready = 0;
+    float *polar = nullptr;
+    double *argtransf = nullptr, *argtransf1 = nullptr;
+    std::vector<float> h_polar;
+    std::vector<double> h_argtransf, h_argtransf1;
+    std::vector<float> angtab;           // degrees
+    // polarizer tables
+    int *pol_off = nullptr;
+    float *pol_w = nullptr;
+    int pol_griddev = -1;
+    void *pol_stage = nullptr;           // device staging of host images
+    size_t pol_stage_bytes = 0;
+    // small per-call device buffers
+    pftcc::Work *d_work = nullptr;
+    pftcc::Group *d_groups = nullptr;
+    size_t work_cap = 0, group_cap = 0;
+    float *d_out = nullptr;
+    size_t out_cap = 0;
+    float *d_shifts = nullptr;
+    size_t shifts_cap = 0;
+    double *d_dout = nullptr;
+    size_t dout_cap = 0;
+    pftcc_best *d_best = nullptr;
+    size_t best_cap = 0;
+    pftcc::SearchWS ws;
+    std::mutex mtx;
+    std::string last_err;
+    long long launches = 0;
+};
+
+namespace pftcc {
+
+int set_err(pftcc_handle *h, int code, const std::string &msg);
+int cuda_err(pftcc_handle *h, cudaError_t e, const char *what);
+int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what);
+int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *what);
+
+// ---- kernels (launch wrappers return cudaError_t of the launch) ---------------------
+cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int first_slot);
+cudaError_t launch_ctfmat(pftcc_handle *h, const pftcc_ctfparams *params, int n, float *out, float ddf,
+                          int derivative);
+cudaError_t launch_sqsums(pftcc_handle *h, int first_slot, int n);
+cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, const Work *work,
+                         const float *shifts, int mode, int frame, int cc1_kstop, float *out,
+                         pftcc_best *best);
+cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, double sy, int irot,
+                           int match_filt, int want_grad, double ddf, double *out5);
+cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, const int *slots_dev, int nreq,
+                              double *out4);
+cudaError_t launch_zero_beyond_kstop(pftcc_handle *h);
+
+// m-domain search (k_search.cu)
+int search_mdomain(pftcc_handle *h, int nshifts, const float *shifts_host, int precision, int ntop,
+                   pftcc_best *out_dev);
+
+}  // namespace pftcc
+
+#define PFTCC_LAUNCH(h) (++(h)->launches)

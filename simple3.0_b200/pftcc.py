@@ -1,0 +1,340 @@
+"""Host-side mirror of SIMPLE 3.0's ``polarft_corrcalc`` over libpftcc_b200.so.
+
+The class keeps the reference's procedure names, argument meaning, 1-based
+indices and error behaviour (the reference's THROW_HARD stops the program; here
+a :class:`PftccError` is raised), so code written against the reference's
+operator surface reads the same:
+
+    pftcc = polarft_corrcalc()
+    pftcc.new(nrefs, [fromp, top], box=128, nrots=360, kfromto=(2, 40))
+    pftcc.set_ref_pft(iref, pft, iseven=True)
+    pftcc.set_ptcl_pft(iptcl, pft)
+    pftcc.create_polar_absctfmats(ctfparams)
+    cc = pftcc.gencorrs(iref, iptcl, shvec)
+
+A polar FT is a complex64 numpy array of shape (K, P) = (kto-kfrom+1, nrots/2),
+i.e. the memory layout of the reference's Fortran pft(P, kfrom:kto).  Every
+computation runs in the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+FRAME_REF, FRAME_PTCL = _lib.FRAME_REF, _lib.FRAME_PTCL
+PREC_EXACT, PREC_FP32, PREC_BF16X3 = _lib.PREC_EXACT, _lib.PREC_FP32, _lib.PREC_BF16X3
+_FRAMES = {"ref": FRAME_REF, "ptcl": FRAME_PTCL, FRAME_REF: FRAME_REF, FRAME_PTCL: FRAME_PTCL}
+_PRECS = {"exact": PREC_EXACT, "fp32": PREC_FP32, "bf16x3": PREC_BF16X3,
+          PREC_EXACT: PREC_EXACT, PREC_FP32: PREC_FP32, PREC_BF16X3: PREC_BF16X3}
+
+
+class PftccError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"pftcc error {status}: {msg}")
+        self.status = status
+
+
+def _f32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _cplx(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.complex64)
+    if shape is not None and a.shape != tuple(shape):
+        raise PftccError(_lib.ERR_ARG, f"expected a polar FT of shape {tuple(shape)}, got {a.shape}")
+    return a
+
+
+def ctfparams_array(n, smpd=1.3, kv=300.0, cs=2.7, fraca=0.1, dfx=None, dfy=None, angast=None,
+                    phshift=0.0, l_phaseplate=False):
+    """per-particle CTF parameters (spproj%get_ctfparams) as a ctypes array"""
+    arr = (_lib.CtfParams * n)()
+    dfx = np.broadcast_to(np.asarray(2.0 if dfx is None else dfx, np.float32), (n,))
+    dfy = np.broadcast_to(np.asarray(dfx if dfy is None else dfy, np.float32), (n,))
+    ang = np.broadcast_to(np.asarray(0.0 if angast is None else angast, np.float32), (n,))
+    for i in range(n):
+        arr[i] = _lib.CtfParams(smpd, kv, cs, fraca, float(dfx[i]), float(dfy[i]), float(ang[i]), phshift,
+                                int(l_phaseplate))
+    return arr
+
+
+class polarft_corrcalc:
+    """B200 implementation of the polarft_corrcalc operator (simple_polarft_corrcalc.f90:68-198)."""
+
+    def __init__(self):
+        self._h = None
+        self._L = _lib.load()
+
+    # ---- helpers ------------------------------------------------------------------------
+    def _check(self, st: int):
+        if st != _lib.OK:
+            msg = self._L.pftcc_last_error(self._h).decode() if self._h else self._L.pftcc_strerror(st).decode()
+            raise PftccError(st, msg or self._L.pftcc_strerror(st).decode())
+
+    def _geti(self, fn) -> int:
+        v = C.c_int()
+        self._check(fn(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- CONSTRUCTOR -----------------------------------------------------------------------
+    def new(self, nrefs: int, pfromto, *, box: int, nrots: int, kfromto, kstop: int | None = None,
+            ctf: bool = True, match_filt: bool = False, ctf_frame="ref", ptcl_mask=None, eoarr=None,
+            device: int = 0):
+        """new(nrefs, pfromto, ptcl_mask, eoarr) with the params_glob fields passed explicitly."""
+        self.kill()
+        cfg = _lib.Config()
+        cfg.nrefs = int(nrefs)
+        cfg.pfromto[0], cfg.pfromto[1] = int(pfromto[0]), int(pfromto[1])
+        cfg.box, cfg.nrots = int(box), int(nrots)
+        cfg.kfromto[0], cfg.kfromto[1] = int(kfromto[0]), int(kfromto[1])
+        cfg.kstop = int(kfromto[1] if kstop is None else kstop)
+        cfg.with_ctf, cfg.match_filt = int(bool(ctf)), int(bool(match_filt))
+        cfg.ctf_frame = _FRAMES[ctf_frame]
+        cfg.device = int(device)
+        span = cfg.pfromto[1] - cfg.pfromto[0] + 1
+        mask = None if ptcl_mask is None else np.ascontiguousarray(np.asarray(ptcl_mask, bool).astype(np.int32))
+        eo = None if eoarr is None else np.ascontiguousarray(eoarr, np.int32)
+        for a in (mask, eo):
+            if a is not None and a.size != span:
+                raise PftccError(_lib.ERR_ARG, "ptcl_mask/eoarr must cover pfromto")
+        h = C.c_void_p()
+        st = self._L.pftcc_new(C.byref(cfg), None if mask is None else mask.ctypes.data_as(C.POINTER(C.c_int)),
+                               None if eo is None else eo.ctypes.data_as(C.POINTER(C.c_int)), C.byref(h))
+        if st != _lib.OK:
+            raise PftccError(st, self._L.pftcc_strerror(st).decode())
+        self._h = h
+        self.cfg = cfg
+        self.K = cfg.kfromto[1] - cfg.kfromto[0] + 1
+        self.P = cfg.nrots // 2
+        return self
+
+    def kill(self):
+        if self._h:
+            self._L.pftcc_kill(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.kill()
+        except Exception:
+            pass
+
+    def exists(self) -> bool:
+        return self._h is not None
+
+    # ---- SETTERS ----------------------------------------------------------------------------
+    def reallocate_ptcls(self, nptcls: int, pinds):
+        p = np.ascontiguousarray(pinds, np.int32)
+        self._check(self._L.pftcc_reallocate_ptcls(self._h, int(nptcls), p.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def set_ref_pft(self, iref: int, pft, iseven: bool):
+        a = _cplx(pft, (self.K, self.P))
+        self._check(self._L.pftcc_set_ref_pft(self._h, int(iref), _f32p(a.view(np.float32)), int(bool(iseven))))
+
+    def set_refs(self, first_iref: int, pfts, iseven: bool):
+        a = _cplx(pfts)
+        self._check(self._L.pftcc_set_refs(self._h, int(first_iref), a.shape[0], _f32p(a.view(np.float32)),
+                                           int(bool(iseven))))
+
+    def set_ptcl_pft(self, iptcl: int, pft):
+        a = _cplx(pft, (self.K, self.P))
+        self._check(self._L.pftcc_set_ptcl_pft(self._h, int(iptcl), _f32p(a.view(np.float32))))
+
+    def set_ptcls(self, first_slot: int, pfts):
+        a = _cplx(pfts)
+        self._check(self._L.pftcc_set_ptcls(self._h, int(first_slot), a.shape[0], _f32p(a.view(np.float32))))
+
+    def set_ref_fcomp(self, iref: int, irot: int, k: int, comp: complex, iseven: bool):
+        a = np.asarray([comp], np.complex64)
+        self._check(self._L.pftcc_set_ref_fcomp(self._h, int(iref), int(irot), int(k), _f32p(a.view(np.float32)),
+                                                int(bool(iseven))))
+
+    def cp_even2odd_ref(self, iref: int):
+        self._check(self._L.pftcc_cp_even2odd_ref(self._h, int(iref)))
+
+    def cp_even_ref2ptcl(self, iref: int, iptcl: int):
+        self._check(self._L.pftcc_cp_even_ref2ptcl(self._h, int(iref), int(iptcl)))
+
+    def swap_ptclsevenodd(self):
+        self._check(self._L.pftcc_swap_ptclsevenodd(self._h))
+
+    def set_eo(self, iptcl: int, is_even: bool):
+        self._check(self._L.pftcc_set_eo(self._h, int(iptcl), int(bool(is_even))))
+
+    def set_eos(self, eoarr):
+        e = np.ascontiguousarray(eoarr, np.int32)
+        self._check(self._L.pftcc_set_eos(self._h, e.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def zero_refs_beyond_kstop(self):
+        self._check(self._L.pftcc_zero_refs_beyond_kstop(self._h))
+
+    # ---- CTF / memoisers -------------------------------------------------------------------
+    def create_polar_absctfmats(self, ctfparams):
+        """ctfparams: ctypes array of CtfParams, one per held particle slot (see ctfparams_array)"""
+        self._check(self._L.pftcc_create_polar_absctfmats(self._h, ctfparams))
+
+    def memoize_ffts(self):
+        self._check(self._L.pftcc_memoize_ffts(self._h))
+
+    # ---- polarizer (simple_polarizer.f90) ----------------------------------------------------
+    def polarize_ptcls(self, first_slot: int, cmats, griddev: bool = False):
+        """cmats: complex64 (n, box, box//2+1) = image%cmat(box/2+1, box) per image"""
+        a = np.ascontiguousarray(cmats, np.complex64)
+        self._check(self._L.pftcc_polarize_ptcls(self._h, int(first_slot), a.shape[0], _f32p(a.view(np.float32)),
+                                                 int(bool(griddev))))
+
+    def polarize_ptcls_dev(self, first_slot: int, n: int, dev_ptr: int, griddev: bool = False):
+        self._check(self._L.pftcc_polarize_ptcls_dev(self._h, int(first_slot), int(n), C.c_void_p(dev_ptr),
+                                                     int(bool(griddev))))
+
+    def polarize_refs(self, first_iref: int, cmats, iseven: bool, griddev: bool = False):
+        a = np.ascontiguousarray(cmats, np.complex64)
+        self._check(self._L.pftcc_polarize_refs(self._h, int(first_iref), a.shape[0], _f32p(a.view(np.float32)),
+                                                int(bool(iseven)), int(bool(griddev))))
+
+    # ---- CALCULATORS -----------------------------------------------------------------------
+    def gencorrs(self, iref: int, iptcl: int, shvec=None) -> np.ndarray:
+        cc = np.zeros(self.cfg.nrots, np.float32)
+        sh = None if shvec is None else np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_gencorrs(self._h, int(iref), int(iptcl), None if sh is None else _f32p(sh), _f32p(cc)))
+        return cc
+
+    def gencorr_for_rot(self, iref: int, iptcl: int, shvec, irot: int) -> float:
+        out = C.c_float()
+        sh = np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_gencorr_for_rot(self._h, int(iref), int(iptcl), _f32p(sh), int(irot), C.byref(out)))
+        return out.value
+
+    def gencorr_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int) -> float:
+        out = C.c_double()
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_for_rot_8(self._h, int(iref), int(iptcl),
+                                                    sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot), C.byref(out)))
+        return out.value
+
+    def gencorr_grad_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        f = C.c_double()
+        g = np.zeros(2, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_grad_for_rot_8(self._h, int(iref), int(iptcl),
+                                                         sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot),
+                                                         C.byref(f), g.ctypes.data_as(C.POINTER(C.c_double))))
+        return f.value, g
+
+    def gencorr_grad_only_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        g = np.zeros(2, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_grad_only_for_rot_8(self._h, int(iref), int(iptcl),
+                                                              sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot),
+                                                              g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
+
+    # ---- batched entry points ----------------------------------------------------------------
+    def corr_all(self, shifts=None) -> np.ndarray:
+        """cc[slot, iref-1, ishift, irot-1] for every held particle, reference and shift"""
+        n = self.get_nptcls()
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        out = np.zeros((n, self.cfg.nrefs, max(1, ns), self.cfg.nrots), np.float32)
+        self._check(self._L.pftcc_corr_all(self._h, ns, None if sh is None else _f32p(sh), _f32p(out)))
+        return out
+
+    def search_best(self, shifts=None, precision="exact", ntop: int = 0) -> np.ndarray:
+        """structured array (iref, irot, ishift, corr) per held particle slot"""
+        n = self.get_nptcls()
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        out = (_lib.Best * n)()
+        self._check(self._L.pftcc_search_best(self._h, ns, None if sh is None else _f32p(sh), _PRECS[precision],
+                                              int(ntop), out))
+        dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("ishift", np.int32), ("corr", np.float32)])
+        return np.frombuffer(out, dtype=dt).copy()
+
+    def search_best_dev(self, shifts, precision, ntop: int, out_dev_ptr: int):
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        self._check(self._L.pftcc_search_best_dev(self._h, ns, None if sh is None else _f32p(sh), _PRECS[precision],
+                                                  int(ntop), C.c_void_p(out_dev_ptr)))
+
+    def grad_batch(self, iref, iptcl, irot, sx, sy, ddf):
+        """f and grad3 = d f / d(shift_x, shift_y, defocus) for arrays of requests"""
+        iref, iptcl, irot, sx, sy, ddf = np.broadcast_arrays(*(np.asarray(v) for v in (iref, iptcl, irot, sx, sy, ddf)))
+        n = iref.size
+        req = (_lib.GradReq * n)()
+        for i in range(n):
+            req[i] = _lib.GradReq(int(iref.flat[i]), int(iptcl.flat[i]), int(irot.flat[i]), 0, float(sx.flat[i]),
+                                  float(sy.flat[i]), float(ddf.flat[i]))
+        f = np.zeros(n, np.float64)
+        g = np.zeros((n, 3), np.float64)
+        self._check(self._L.pftcc_grad_batch(self._h, n, req, f.ctypes.data_as(C.POINTER(C.c_double)),
+                                             g.ctypes.data_as(C.POINTER(C.c_double))))
+        return f, g
+
+    # ---- GETTERS ----------------------------------------------------------------------------
+    def get_nrots(self) -> int:
+        return self._geti(self._L.pftcc_get_nrots)
+
+    def get_pftsz(self) -> int:
+        return self._geti(self._L.pftcc_get_pftsz)
+
+    def get_box(self) -> int:
+        return self._geti(self._L.pftcc_get_box)
+
+    def get_nrefs(self) -> int:
+        return self._geti(self._L.pftcc_get_nrefs)
+
+    def get_nptcls(self) -> int:
+        return self._geti(self._L.pftcc_get_nptcls)
+
+    def get_pdim(self):
+        p = np.zeros(3, np.int32)
+        self._check(self._L.pftcc_get_pdim(self._h, p.ctypes.data_as(C.POINTER(C.c_int))))
+        return [int(v) for v in p]
+
+    def get_rot(self, roind: int) -> float:
+        v = C.c_float()
+        self._check(self._L.pftcc_get_rot(self._h, int(roind), C.byref(v)))
+        return v.value
+
+    def get_roind(self, rot: float) -> int:
+        v = C.c_int()
+        self._check(self._L.pftcc_get_roind(self._h, float(rot), C.byref(v)))
+        return v.value
+
+    def get_coord(self, rot: int, k: int):
+        xy = np.zeros(2, np.float32)
+        self._check(self._L.pftcc_get_coord(self._h, int(rot), int(k), _f32p(xy)))
+        return xy
+
+    def ptcl_iseven(self, iptcl: int) -> bool:
+        v = C.c_int()
+        self._check(self._L.pftcc_ptcl_iseven(self._h, int(iptcl), C.byref(v)))
+        return bool(v.value)
+
+    def get_ref_pft(self, iref: int, iseven: bool) -> np.ndarray:
+        out = np.zeros((self.K, self.P), np.complex64)
+        self._check(self._L.pftcc_get_ref_pft(self._h, int(iref), int(bool(iseven)), _f32p(out.view(np.float32))))
+        return out
+
+    def get_ptcl_pft(self, iptcl: int) -> np.ndarray:
+        out = np.zeros((self.K, self.P), np.complex64)
+        self._check(self._L.pftcc_get_ptcl_pft(self._h, int(iptcl), _f32p(out.view(np.float32))))
+        return out
+
+    def get_sqsum_ptcl(self, iptcl: int) -> float:
+        v = C.c_float()
+        self._check(self._L.pftcc_get_sqsum_ptcl(self._h, int(iptcl), C.byref(v)))
+        return v.value
+
+    def kernel_launches(self) -> int:
+        return int(self._L.pftcc_kernel_launches(self._h))
+
+    def synchronize(self):
+        self._check(self._L.pftcc_synchronize(self._h))
