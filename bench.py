@@ -1,0 +1,354 @@
+"""Benchmark of the polar Fourier correlation search on B200.
+
+One step = one pass of the hot path over the workload's particle batch: Kaiser-
+Bessel gridding of the particles' half-plane FTs to polar, their |CTF| matrices,
+and the exhaustive search over all references x the shift grid x all in-plane
+rotations (best (ref, rot, shift) per particle, the top-8 re-scored in FP32).
+
+Workload (default): 128^3 Gaussian-blob volume, 500 references, 20,000 particles,
+81 shifts (9x9 grid, 0.5 px), 360 rotations, shells 2..40, i.e.
+500 x 20,000 x 81 x 360 = 2.916e11 correlation evaluations per step.  Inputs are
+seeded synthetic data with those shapes and distributions (no dataset exists for
+this path); the particle inputs (1.33 GB) exceed L2, so no flush is needed.
+
+Arms:
+  default           libpftcc_b200 through its C ABI (value: inputs resident in HBM;
+                    e2e: host buffers, host<->device copies inside the timed region)
+  --impl reference  the reference algorithm on the host cores (the FP32 FFT path of
+                    polarft_corrcalc restated in C with OpenMP), bounded sample
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as entry  # noqa: E402
+
+METRIC = "ref x ptcl x rot corr evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32", "exact"])
+    ap.add_argument("--workload", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--nptcls", type=int, default=0, help="override the particle count (testing)")
+    ap.add_argument("--nrefs", type=int, default=0, help="override the reference count (testing)")
+    ap.add_argument("--ntop", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    return ap.parse_args()
+
+
+def workload(pkg, args):
+    w = getattr(pkg.synth, args.workload)()
+    if args.nptcls:
+        w.nptcls = args.nptcls
+    if args.nrefs:
+        w.nrefs = args.nrefs
+    return w
+
+
+def shifts_of(w):
+    g = w.shift_grid if w.shift_grid else ((0.0, 0.0),)
+    return np.asarray(g, np.float32)
+
+
+def evals_per_step(w, nshifts):
+    return float(w.nrefs) * w.nptcls * nshifts * w.nrots
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region"""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_sample(pkg, O, w, shifts, seconds: float):
+    """time the oracle's OpenMP FFT-path search (reference loop structure) on a bounded
+    sample: all host threads, nthreads particles x R references x all shifts"""
+    nthreads = os.cpu_count() or 1
+    g = O.geom(w.nrots, w.kfrom, w.kto, w.box)
+    t = O.tables(g)
+    refs, R = pkg.synth.make_refs(w)
+    refs = refs.numpy()
+    npart = nthreads
+    parts = pkg.synth.make_particles(w, R, count=npart)
+    ptcls = np.stack([O.polarize(g, t, parts.cmat[i].numpy()) for i in range(npart)]).astype(np.complex64)
+    ctfs = np.stack([O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]),
+                                               float(parts.dfy[i]), float(parts.angast[i])))
+                     for i in range(npart)]).astype(np.float32)
+    # calibrate: one particle, one reference, all shifts, single thread
+    t0 = time.perf_counter()
+    O.cpu_search(g, refs[:1], ptcls[:1], ctfs[:1], shifts, nthreads=1)
+    per_call = (time.perf_counter() - t0) / len(shifts)
+    nr = int(max(1, min(w.nrefs, seconds / (per_call * len(shifts)))))
+    t0 = time.perf_counter()
+    _, _, _, _, used = O.cpu_search(g, refs[:nr], ptcls, ctfs, shifts, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    evals = float(nr) * npart * len(shifts) * w.nrots
+    return {"value": evals / dt, "unit": "evals/s", "cores": int(used), "kind": "port",
+            "sample": f"{npart} particles x {nr} refs x {len(shifts)} shifts x {w.nrots} rots "
+                      f"({evals:.3g} evals, FP32 FFT path in the reference's loop structure, "
+                      f"project-written mixed-radix FFT in place of FFTW, {dt:.1f} s)"}
+
+
+def run_reference(args):
+    pkg = entry.load_package()
+    O = entry.load_oracle()
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(pkg, args)
+    shifts = shifts_of(w)
+    vals = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_sample(pkg, O, w, shifts, args.cpu_seconds / 2 if i < args.warmup else args.cpu_seconds)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            base = r
+    v = float(statistics.median(vals))
+    base["value"] = v
+    line = {"metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": evals_per_step(w, len(shifts)) / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded Gaussian-blob volume, analytic sections, CTF, SNR 0.1)",
+            "config": {"workload": w.name, "nrefs": w.nrefs, "nptcls": w.nptcls, "nshifts": len(shifts),
+                       "nrots": w.nrots, "kfromto": [w.kfrom, w.kto], "box": w.box},
+            "impl": "reference", "cpu_baseline": base,
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def algorithmic_costs(w, nshifts, kernel):
+    """algorithmic work per step for each kernel class: (flops, bytes)"""
+    P, N = w.pftsz, w.nrots
+    Ks = w.K
+    trip = float(w.nrefs) * nshifts * w.nptcls
+    F = 8.0 * Ks * (P + 1)                      # complex MACs of the m-domain contraction per triple
+    if kernel == "stage1":
+        return 3.0 * F * trip, 0.0               # BF16 hi+lo: three issued products
+    if kernel == "stage2":
+        return 0.0, trip * (P + 1) * 8.0         # the contraction output read back once
+    if kernel == "polarize":
+        return 0.0, w.nptcls * (w.box * (w.box // 2 + 1) * 8.0 + Ks * P * 8.0)
+    return 0.0, 0.0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    pkg = entry.load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = workload(pkg, args)
+    # weak scaling: every rank searches its own particle batch (distinct seeds)
+    w.seed_base += 100000 * rank
+    shifts = shifts_of(w)
+    ns = len(shifts)
+    refs, R = pkg.synth.make_refs(w, device=dev)
+    parts = pkg.synth.make_particles(w, R, device=dev)
+    cmats = parts.cmat.contiguous()                               # resident in HBM
+    pc = pkg.polarft_corrcalc()
+    pc.new(w.nrefs, (1, w.nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True,
+           ctf_frame="ptcl", device=local)
+    stream = torch.cuda.current_stream(dev)
+    pc.set_stream(stream.cuda_stream)
+    r_host = refs.cpu().numpy()
+    pc.set_refs(1, r_host, True)
+    pc.set_refs(1, r_host, False)
+    ctfp = pkg.ctfparams_array(w.nptcls, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca, dfx=parts.dfx,
+                               dfy=parts.dfy, angast=parts.angast)
+    best = torch.empty((w.nptcls, 4), dtype=torch.int32, device=dev)     # 16-byte pftcc_best records
+    gathered = torch.empty((world, w.nptcls, 4), dtype=torch.int32, device=dev) if world > 1 else None
+
+    def step():
+        pc.polarize_ptcls_dev(0, w.nptcls, cmats.data_ptr())
+        pc.create_polar_absctfmats(ctfp)
+        pc.search_best_dev(shifts, args.precision, args.ntop if args.precision != "exact" else 0, best.data_ptr())
+        if world > 1:
+            dist.all_gather_into_tensor(gathered, best)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    pc.prof_reset()
+    pc.prof_enable(True)
+    launches0 = pc.kernel_launches()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    launches = pc.kernel_launches() - launches0
+    prof = pc.prof_read()
+    pc.prof_enable(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    evals = evals_per_step(w, ns)
+    value = evals * world / (ms / 1e3)
+
+    # dominant kernel and its roofline
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    tc_peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    peak_src = "measured" if peaks else "fallback"
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    shares = {k: round(v[0] / max(1e-9, sum(x[0] for x in prof.values())), 4) for k, v in prof.items() if v[1]}
+    flops, byts = algorithmic_costs(w, ns, dom)
+    per_launch_s = dom_ms / 1e3 / max(1, dom_n)
+    n_launch_per_step = dom_n / args.steps
+    if dom == "stage1" and args.precision == "bf16x3":
+        ach = flops / n_launch_per_step / per_launch_s / 1e12
+        roof = {"bound": "tensor", "achieved": ach, "peak": tc_peak, "unit": "TFLOP/s", "frac": ach / tc_peak,
+                "traffic": None, "kernel": "k_umma_stage1", "peak_source": f"{peak_src} bf16 sustained"}
+    else:
+        flops_b, byts_b = algorithmic_costs(w, ns, dom)
+        ach = byts_b / n_launch_per_step / per_launch_s / 1e9 if byts_b else 0.0
+        roof = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                "traffic": None, "kernel": f"k_{dom}", "peak_source": f"{peak_src} hbm copy"}
+    roof["kernel_ms_per_step"] = {k: round(v[0] / args.steps, 3) for k, v in prof.items() if v[1]}
+    roof["kernel_share"] = shares
+
+    # e2e: host inputs through the public API, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        host_cm = torch.empty(cmats.shape, dtype=cmats.dtype, pin_memory=True)
+        host_cm.copy_(cmats)
+        host_np = host_cm.numpy()
+        pc.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = None
+        for _ in range(args.steps):
+            pc.polarize_ptcls(0, host_np)
+            pc.create_polar_absctfmats(ctfp)
+            out = pc.search_best(shifts, args.precision, args.ntop if args.precision != "exact" else 0)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": evals * world / (ems / 1e3), "unit": "evals/s",
+               "h2d_bytes_per_step": int(host_cm.numel() * host_cm.element_size() + w.nptcls * 36),
+               "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": ems}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_sample(pkg, entry.load_oracle(), w, shifts, args.cpu_seconds)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": {"bf16x3": "bf16x3 (bf16 hi+lo products, fp32 accumulate)",
+                                               "fp32": "fp32", "exact": "fp32"}[args.precision],
+                "data": "synthetic (seeded Gaussian-blob volume, analytic sections, CTF, SNR 0.1)",
+                "config": {"workload": w.name, "nrefs": w.nrefs, "nptcls": w.nptcls, "nshifts": ns,
+                           "nrots": w.nrots, "kfromto": [w.kfrom, w.kto], "box": w.box,
+                           "precision": args.precision, "ntop_rescore": args.ntop, "ctf_frame": "ptcl",
+                           "l2": "inputs larger than L2 (1.33 GB particle FTs)", "parallelism": f"dp{world}"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    pc.kill()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

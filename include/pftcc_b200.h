@@ -137,6 +137,10 @@ int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, cons
 /* all correlations: cc[slot][iref-1][ishift][irot-1] for every held particle,
  * reference and shift (the loop strategy2D_greedy :42 runs over gencorrs) */
 int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc);
+/* all correlations through the m-domain path in the given precision (PFTCC_PREC_FP32 or
+ * PFTCC_PREC_BF16X3; PFTCC_PREC_EXACT = pftcc_corr_all), particle frame, same layout
+ * as pftcc_corr_all: the full array the precision report measures */
+int pftcc_corr_all_prec(pftcc_handle *h, int nshifts, const float *shifts, int precision, float *cc);
 /* best (ref, rot, shift) per particle over all references and a shift grid, the
  * greedy strategies' maxloc (simple_strategy2D_greedy.f90:42-43) fused with the
  * coarse shift grid of minimize_exhaustive (simple_pftcc_shsrch_grad.f90:182-199).
@@ -175,6 +179,19 @@ const char *pftcc_last_error(const pftcc_handle *h);
 long long pftcc_kernel_launches(const pftcc_handle *h);
 /* block until all device work of the handle is done */
 int pftcc_synchronize(pftcc_handle *h);
+/* run the handle's work on a caller's CUDA stream (a cudaStream_t; NULL restores the
+ * handle's own stream) -- lets a caller order the library with its own kernels and
+ * time it with events on that stream */
+int pftcc_set_stream(pftcc_handle *h, void *stream);
+/* per-kernel device timing with CUDA events recorded on the handle's stream around
+ * each launch of a kernel class (PFTCC_K_*): enable, then read total milliseconds and
+ * launch counts (reading synchronises the stream), reset clears the totals */
+enum { PFTCC_K_POLARIZE = 0, PFTCC_K_CTFMAT = 1, PFTCC_K_SPEC_PTCL = 2, PFTCC_K_SPEC_REF = 3, PFTCC_K_PACK = 4,
+       PFTCC_K_STAGE1 = 5, PFTCC_K_NORM = 6, PFTCC_K_STAGE2 = 7, PFTCC_K_EXACT = 8, PFTCC_K_OTHER = 9,
+       PFTCC_K_COUNT = 10 };
+int pftcc_prof_enable(pftcc_handle *h, int on);
+int pftcc_prof_read(pftcc_handle *h, int kernel_class, double *total_ms, long long *launches);
+int pftcc_prof_reset(pftcc_handle *h);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,7 @@ SIGNATURES = {
     "pftcc_gencorr_grad_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
     "pftcc_gencorr_grad_only_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp],
     "pftcc_corr_all": [_h, C.c_int, _fp, _fp],
+    "pftcc_corr_all_prec": [_h, C.c_int, _fp, C.c_int, _fp],
     "pftcc_search_best": [_h, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],
     "pftcc_search_best_dev": [_h, C.c_int, _fp, C.c_int, C.c_int, _vp],
     "pftcc_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
@@ -86,7 +87,15 @@ SIGNATURES = {
     "pftcc_last_error": ([_h], C.c_char_p),
     "pftcc_kernel_launches": ([_h], C.c_longlong),
     "pftcc_synchronize": [_h],
+    "pftcc_set_stream": [_h, _vp],
+    "pftcc_prof_enable": [_h, C.c_int],
+    "pftcc_prof_read": [_h, C.c_int, _dp, C.POINTER(C.c_longlong)],
+    "pftcc_prof_reset": [_h],
 }
+
+# kernel classes of the per-kernel timing (PFTCC_K_*)
+KERNEL_CLASSES = ["polarize", "ctfmat", "spec_ptcl", "spec_ref", "pack", "stage1", "norm", "stage2", "exact",
+                  "other"]
 
 _LIB = None
 

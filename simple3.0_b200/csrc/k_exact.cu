@@ -69,6 +69,7 @@ cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int fir
     cudaError_t e = cudaFuncSetAttribute(k_polarize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_POLARIZE);
     k_polarize<<<n, 256, smem, h->stream>>>(g, cmats, img_elems, h->pol_off, h->pol_w,
                                            h->ptcls + (size_t)first_slot * g.K * g.P, h->sqsums + first_slot);
     return cudaGetLastError();
@@ -150,6 +151,7 @@ cudaError_t launch_ctfmat(pftcc_handle *h, const pftcc_ctfparams *params, int n,
     const int per = h->g.K * h->g.P;
     dim3 grid((per + 255) / 256, n);
     PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_CTFMAT);
     k_ctfmat<<<grid, 256, 0, h->stream>>>(h->g, h->polar, params, out, ddf, derivative);
     return cudaGetLastError();
 }
@@ -190,6 +192,7 @@ cudaError_t launch_zero_beyond_kstop(pftcc_handle *h)
 // FRAME_PTCL: A = ref * shmat(n), Qt = ctf~(j) ptcl~(j),
 //             cc = corr / sqrt(sum_n |ref(n)|^2 ctf~(n+s)^2 * sqsum_ptcl)
 constexpr int EX_THREADS = 256;
+__host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) & ~size_t(15); }
 constexpr int EX_RPT = 3;      // rotations per thread: N <= 768
 
 template <int FRAME>
@@ -202,13 +205,17 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P;
-    float2 *Qt = reinterpret_cast<float2 *>(smem4);          // [KC][N]
-    float2 *A = Qt + KC * N;                                 // [KC][P]
-    double2 *sh = reinterpret_cast<double2 *>(A + KC * P);   // [P] running shmat
-    double2 *sv = sh + P;                                    // [P] shell-one phase vector
-    float *C2t = reinterpret_cast<float *>(sv + P);          // [KC][N] (PTCL)
-    float *R2 = C2t + (FRAME == PFTCC_FRAME_PTCL ? KC * N : 0);  // [KC][P] (PTCL)
-    __shared__ float red[EX_THREADS / 32];
+    // shared layout (16-byte aligned sections, see exact_smem): sh [P] double2 running
+    // shmat, sv [P] double2 shell-one phase vector, Qt [KC][N] float2, A [KC][P] float2,
+    // then for the particle frame C2t [KC][N] float and R2 [KC][P] float
+    char *base = reinterpret_cast<char *>(smem4);
+    double2 *sh = reinterpret_cast<double2 *>(base);
+    double2 *sv = sh + P;
+    float2 *Qt = reinterpret_cast<float2 *>(base + al16(2 * P * sizeof(double2)));
+    float2 *A = reinterpret_cast<float2 *>(reinterpret_cast<char *>(Qt) + al16(KC * N * sizeof(float2)));
+    float *C2t = reinterpret_cast<float *>(reinterpret_cast<char *>(A) + al16(KC * P * sizeof(float2)));
+    float *R2 = reinterpret_cast<float *>(reinterpret_cast<char *>(C2t) + al16(KC * N * sizeof(float)));
+    __shared__ double red[EX_THREADS / 32];
     __shared__ float bcc[EX_THREADS / 32];
     __shared__ int brot[EX_THREADS / 32];
 
@@ -237,10 +244,10 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                 sv[n] = make_double2(c, s);
             }
         }
-        float acc[EX_RPT], dacc[EX_RPT];
+        double acc[EX_RPT], dacc[EX_RPT];
 #pragma unroll
-        for (int u = 0; u < EX_RPT; ++u) { acc[u] = 0.f; dacc[u] = 0.f; }
-        float sqr = 0.f;
+        for (int u = 0; u < EX_RPT; ++u) { acc[u] = 0.0; dacc[u] = 0.0; }
+        double sqr = 0.0;
         const int ksq = (has_shift || !cc1_kstop) ? g.K : g.Ks;   // cc_2 sums all shells, cc_1 to kstop
         for (int k0 = 0; k0 < g.K; k0 += KC) {
             const int kc = min(KC, g.K - k0);
@@ -267,7 +274,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                         st = make_double2(nr, ni);
                     }
                     A[kk * P + n] = make_float2(ar, ai);
-                    if (ik < ksq) sqr += ar * ar + ai * ai;
+                    if (ik < ksq) sqr += (double)ar * ar + (double)ai * ai;
                 }
                 if (has_shift) sh[n] = st;
             }
@@ -291,22 +298,22 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
             for (int u = 0; u < EX_RPT; ++u) {
                 const int s = threadIdx.x + u * EX_THREADS;
                 if (s >= N) break;
-                float a_tot = 0.f, d_tot = 0.f;
+                // products of the FP32 operands accumulated in FP64: the accumulation then
+                // adds no rounding beyond the operands' own (FP32 sums over P*Ks terms
+                // would add ~1e-5 relative on correlations near 1e-3)
+                double a_tot = 0.0, d_tot = 0.0;
                 for (int kk = 0; kk < kend; ++kk) {
                     const float2 *Ak = A + kk * P;
                     const float2 *Qk = Qt + kk * N;
-                    float a_k = 0.f, d_k = 0.f;
                     int j = s;
                     for (int n = 0; n < P; ++n) {
                         const float2 av = Ak[n];
                         const float2 qv = Qk[j];
-                        a_k = fmaf(av.x, qv.x, a_k);
-                        a_k = fmaf(av.y, qv.y, a_k);
-                        if (FRAME == PFTCC_FRAME_PTCL) d_k = fmaf(R2[kk * P + n], C2t[kk * N + j], d_k);
+                        a_tot = fma((double)av.x, (double)qv.x, a_tot);
+                        a_tot = fma((double)av.y, (double)qv.y, a_tot);
+                        if (FRAME == PFTCC_FRAME_PTCL) d_tot = fma((double)R2[kk * P + n], (double)C2t[kk * N + j], d_tot);
                         if (++j == N) j = 0;
                     }
-                    a_tot += a_k;
-                    d_tot += d_k;
                 }
                 acc[u] += a_tot;
                 dacc[u] += d_tot;
@@ -316,7 +323,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
         for (int o = 16; o > 0; o >>= 1) sqr += __shfl_xor_sync(0xffffffffu, sqr, o);
         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sqr;
         __syncthreads();
-        float sqr_tot = 0.f;
+        double sqr_tot = 0.0;
 #pragma unroll
         for (int wi = 0; wi < EX_THREADS / 32; ++wi) sqr_tot += red[wi];
         float my_best = -INFINITY;
@@ -325,8 +332,8 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
         for (int u = 0; u < EX_RPT; ++u) {
             const int s = threadIdx.x + u * EX_THREADS;
             if (s >= N) break;
-            const float den = FRAME == PFTCC_FRAME_REF ? sqrtf(sqr_tot * sqp) : sqrtf(dacc[u] * sqp);
-            const float cc = acc[u] / den;
+            const double den = FRAME == PFTCC_FRAME_REF ? sqrt(sqr_tot * sqp) : sqrt(dacc[u] * sqp);
+            const float cc = (float)(acc[u] / den);
             if (mode == MODE_FULL) out[w.out + s] = cc;
             if (cc > my_best) { my_best = cc; my_rot = s; }
         }
@@ -362,13 +369,19 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     }
 }
 
+static size_t exact_smem(const Geom &g, int frame, int kc)
+{
+    size_t b = al16(2 * g.P * sizeof(double2)) + al16((size_t)kc * g.N * sizeof(float2)) +
+               al16((size_t)kc * g.P * sizeof(float2));
+    if (frame == PFTCC_FRAME_PTCL) b += al16((size_t)kc * g.N * sizeof(float)) + al16((size_t)kc * g.P * sizeof(float));
+    return b;
+}
+
 static int exact_kc(const Geom &g, int frame, size_t *smem)
 {
-    const size_t per = (size_t)g.N * sizeof(float2) + (size_t)g.P * sizeof(float2) +
-                       (frame == PFTCC_FRAME_PTCL ? (size_t)g.N * 4 + (size_t)g.P * 4 : 0);
     int kc = 8;
-    while (kc > 1 && per * kc + 2 * g.P * sizeof(double2) > 100 * 1024) --kc;
-    *smem = per * kc + 2 * g.P * sizeof(double2);
+    while (kc > 1 && exact_smem(g, frame, kc) > 100 * 1024) --kc;
+    *smem = exact_smem(g, frame, kc);
     return kc;
 }
 
@@ -383,6 +396,7 @@ cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, cons
         e = cudaFuncSetAttribute(k_exact<PFTCC_FRAME_PTCL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         PFTCC_LAUNCH(h);
+        KTimer kt(h, PFTCC_K_EXACT);
         k_exact<PFTCC_FRAME_PTCL><<<ngroups, EX_THREADS, smem, h->stream>>>(
             h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
             h->argtransf1, groups, work, shifts, mode, cc1_kstop, out, best);
@@ -390,6 +404,7 @@ cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, cons
         e = cudaFuncSetAttribute(k_exact<PFTCC_FRAME_REF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         PFTCC_LAUNCH(h);
+        KTimer kt(h, PFTCC_K_EXACT);
         k_exact<PFTCC_FRAME_REF><<<ngroups, EX_THREADS, smem, h->stream>>>(
             h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
             h->argtransf1, groups, work, shifts, mode, cc1_kstop, out, best);

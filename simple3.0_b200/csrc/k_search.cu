@@ -1,8 +1,722 @@
-// k_search.cu -- m-domain search (placeholder until the contraction kernels land)
+// k_search.cu -- the m-domain correlation search (particle-frame CTF).
+//
+// The reference correlates one (reference, particle) pair at a time with K FFT
+// triples (calc_corrs_over_k, simple_polarft_corrcalc.f90:1132-1162).  Writing
+// that computation out: with x~ the half-circle polar FT extended to the full
+// circle by conjugate symmetry and U(m,k) = sum_{n<P} v_m(n,k) w_N^{-mn}
+// (v_m = Re x for even m, Im x for odd m -- the r2c(P) and fft_factors-weighted
+// c2c(P) transforms of memoize_fft :869-876 interleaved), the correlation is
+//     corr(rot) = (2/N) * sum_{m<N} X(m) w_N^{-m rot},
+//     X(m)      = sum_k U_A(m,k) conj(U_B(m,k))     (Hermitian in m),
+// so for every angular frequency m = 0..P the work over all (ref, shift) x
+// particle pairs is one complex contraction over the shells k, followed by one
+// real inverse transform of length N per pair.  A is the reference times the
+// shift phases of gen_shmat_8 (:1098-1120, reference side), B the particle times
+// its |CTF| at the particle's own polar index (the particle frame; identical to
+// the reference's prep_ref4corr :982 for an isotropic CTF), and the normaliser
+// D(rot) = sum_k sum_n |ref(n,k)|^2 CTF^2(n+rot,k), P-periodic in rot, is the
+// same kind of contraction over the P-point spectra of |ref|^2 and CTF^2, in FP64.
+//
+// Pipeline per call (all on the handle's stream):
+//   k_spec_ptcl   particle spectra UB[m][col][k] (FP32) and CTF^2 spectra CV (FP64)
+//   k_spec_r2     |ref|^2 spectra RU (FP64)
+//   for each parity group (even/odd references, prep_ref4corr :970-974):
+//     k_spec_ref  (ref, shift) spectra UA[m][rs][k] (FP32)
+//     for each wave of rows (rs) x columns (particles):
+//       stage 1   X[m][col][rs] = 4 sum_k UA conj(UB)   (FP32 CUDA cores, or tcgen05)
+//       k_norm    D[r][col][rho] for the wave's references (FP64)
+//       k_stage2  per (col, rs): length-P complex FFT of the packed Hermitian X,
+//                 cc = (2/N) y / sqrt(D sqsum_ptcl), argmax over rotations, merge
+//                 into the particle's running top-8 (cc, rs*N + rot)
+//   k_finish      top-1, or the exact FP32 re-score of the top-ntop (ref, shift)
 #include "pftcc_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 namespace pftcc {
-int search_mdomain(pftcc_handle *h, int, const float *, int, int, pftcc_best *)
+
+int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int nrs_w, int rows_pad,
+                const float2 *UB, int c0, int ncols_w, int cols_pad, float2 *X, int prepare, int parity_group);
+
+static constexpr int MAXF = 12;
+struct FFTPlan {
+    int nf;
+    int f[MAXF];     // radices, top level first
+};
+
+static FFTPlan make_plan(int P)
 {
-    return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search not built yet");
+    FFTPlan p{};
+    int m = P;
+    const int rad[4] = {4, 2, 3, 5};
+    for (int r = 0; r < 4; ++r)
+        while (m % rad[r] == 0 && p.nf < MAXF) { p.f[p.nf++] = rad[r]; m /= rad[r]; }
+    for (int q = 7; m > 1 && p.nf < MAXF; q += 2)
+        while (m % q == 0) { p.f[p.nf++] = q; m /= q; }
+    return p;
 }
+
+// position of input element i after the mixed-radix digit reversal that makes the
+// in-place decimation-in-time passes produce natural-order output
+static int digit_rev(const FFTPlan &p, int P, int i)
+{
+    int pos = 0, n = P;
+    for (int l = 0; l < p.nf; ++l) {
+        const int r = p.f[l];
+        n /= r;
+        pos += (i % r) * n;
+        i /= r;
+    }
+    return pos;
+}
+
+// ---------------------------------------------------------------------------
+// spectra of the (reference, shift) rows: U(m,k) = sum_n v_m(n,k) w_N^{-mn}
+constexpr int SPEC_THREADS = 256;
+
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
+    Geom g, int nshifts, const float2 *__restrict__ refs, const float *__restrict__ shifts,
+    const double *__restrict__ argtransf, const double *__restrict__ argtransf1, int rs0, int nrs, int rows_pad,
+    float2 *__restrict__ UA)
+{
+    extern __shared__ float4 smem4[];
+    const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1;
+    float2 *tw = reinterpret_cast<float2 *>(smem4);     // [N] w_N^{-e}
+    float2 *a = tw + N;                                  // [Ks][P]
+    const int row = blockIdx.x;                          // local row
+    const int rs = rs0 + row;
+    float2 *dst = UA;
+    if (rs >= nrs) {   // zero padding rows
+        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+            const int m = e / Ks, k = e - m * Ks;
+            dst[((size_t)m * rows_pad + row) * Ks + k] = make_float2(0.f, 0.f);
+        }
+        return;
+    }
+    const int r = rs / nshifts, s = rs - r * nshifts;
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / N, &sn, &cs);
+        tw[e] = make_float2((float)cs, (float)sn);
+    }
+    const float2 *R = refs + (size_t)r * g.K * P;
+    const double sx = shifts ? (double)shifts[2 * s] : 0.0, sy = shifts ? (double)shifts[2 * s + 1] : 0.0;
+    for (int n = threadIdx.x; n < P; n += blockDim.x) {
+        // gen_shmat_8: analytic first shell, de Moivre recurrence, cast to single precision
+        double sr, si, vr, vi;
+        sincos(argtransf[n] * sx + argtransf[P + n] * sy, &si, &sr);
+        sincos(argtransf1[n] * sx + argtransf1[P + n] * sy, &vi, &vr);
+        for (int k = 0; k < Ks; ++k) {
+            const float2 x = R[(size_t)k * P + n];
+            const float fr = (float)sr, fi = (float)si;
+            a[k * P + n] = make_float2(x.x * fr - x.y * fi, x.x * fi + x.y * fr);
+            const double nr = sr * vr - si * vi, ni = sr * vi + si * vr;
+            sr = nr; si = ni;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+        const int m = e / Ks, k = e - m * Ks;
+        const float2 *ak = a + k * P;
+        float ur = 0.f, ui = 0.f;
+        int idx = 0;
+        if (m & 1) {
+            for (int n = 0; n < P; ++n) {
+                const float v = ak[n].y;
+                ur = fmaf(v, tw[idx].x, ur);
+                ui = fmaf(v, tw[idx].y, ui);
+                idx += m; if (idx >= N) idx -= N;
+            }
+        } else {
+            for (int n = 0; n < P; ++n) {
+                const float v = ak[n].x;
+                ur = fmaf(v, tw[idx].x, ur);
+                ui = fmaf(v, tw[idx].y, ui);
+                idx += m; if (idx >= N) idx -= N;
+            }
+        }
+        dst[((size_t)m * rows_pad + row) * Ks + k] = make_float2(ur, ui);
+    }
+}
+
+// particle-side spectra: B = |CTF| * ptcl (particle frame), UB[m][col][k]; and the
+// FP64 spectra of CTF^2 over P points, CV[col][j][k], j = 0..P/2
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
+    Geom g, const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const int *__restrict__ perm,
+    int ncols, int cols_pad, float2 *__restrict__ UB, double2 *__restrict__ CV, float *__restrict__ sqp_out,
+    const float *__restrict__ sqsums)
+{
+    extern __shared__ float4 smem4[];
+    const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
+    float2 *tw = reinterpret_cast<float2 *>(smem4);   // [N]
+    float2 *b = tw + N;                                // [Ks][P]
+    float *c2 = reinterpret_cast<float *>(b + Ks * P); // [Ks][P]
+    const int col = blockIdx.x;
+    if (col >= ncols) {
+        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+            const int m = e / Ks, k = e - m * Ks;
+            UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2(0.f, 0.f);
+        }
+        for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) CV[(size_t)col * J * Ks + e] = make_double2(0.0, 0.0);
+        if (threadIdx.x == 0) sqp_out[col] = 1.f;
+        return;
+    }
+    const int slot = perm[col];
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / N, &sn, &cs);
+        tw[e] = make_float2((float)cs, (float)sn);
+    }
+    const float2 *Q = ptcls + (size_t)slot * g.K * P;
+    const float *C = ctfmats ? ctfmats + (size_t)slot * g.K * P : nullptr;
+    for (int e = threadIdx.x; e < Ks * P; e += blockDim.x) {
+        const float c = C ? C[e] : 1.f;
+        const float2 q = Q[e];
+        b[e] = make_float2(c * q.x, c * q.y);
+        c2[e] = c * c;
+    }
+    if (threadIdx.x == 0) sqp_out[col] = sqsums[slot];
+    __syncthreads();
+    for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+        const int m = e / Ks, k = e - m * Ks;
+        const float2 *bk = b + k * P;
+        float ur = 0.f, ui = 0.f;
+        int idx = 0;
+        for (int n = 0; n < P; ++n) {
+            const float v = (m & 1) ? bk[n].y : bk[n].x;
+            ur = fmaf(v, tw[idx].x, ur);
+            ui = fmaf(v, tw[idx].y, ui);
+            idx += m; if (idx >= N) idx -= N;
+        }
+        UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2(ur, ui);
+    }
+    // CTF^2 spectra over P points in FP64: w_P^{-jn} = w_N^{-2jn}
+    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
+        const int j = e / Ks, k = e - j * Ks;
+        double ur = 0.0, ui = 0.0;
+        for (int n = 0; n < P; ++n) {
+            double sn, cs;
+            sincospi(-2.0 * (double)((j * n) % P) / P, &sn, &cs);
+            ur += (double)c2[k * P + n] * cs;
+            ui += (double)c2[k * P + n] * sn;
+        }
+        CV[(size_t)col * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
+    }
+}
+
+// |ref|^2 spectra over P points (FP64): RU[r][j][k]
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *__restrict__ refs,
+                                                          double2 *__restrict__ RU)
+{
+    const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
+    const int r = blockIdx.x;
+    const float2 *R = refs + (size_t)r * g.K * P;
+    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
+        const int j = e / Ks, k = e - j * Ks;
+        double ur = 0.0, ui = 0.0;
+        for (int n = 0; n < P; ++n) {
+            const float2 x = R[(size_t)k * P + n];
+            const double u = (double)x.x * x.x + (double)x.y * x.y;
+            double sn, cs;
+            sincospi(-2.0 * (double)((j * n) % P) / P, &sn, &cs);
+            ur += u * cs;
+            ui += u * sn;
+        }
+        RU[(size_t)r * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage 1 on CUDA cores: X[m][col][row] = 4 * sum_k UA[m][row][k] * conj(UB[m][col][k])
+// block tile 64 cols x 64 rows, 256 threads with 4 x 4 complex micro-tiles, the whole
+// shell range staged in shared memory (Ks <= 64).
+constexpr int S1_TILE = 64;
+constexpr int COL_TILE = 128;
+
+__global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, const float2 *__restrict__ UA, int rows_pad, int row0,
+                                                     const float2 *__restrict__ UB, int cols_pad, int col0,
+                                                     float2 *__restrict__ X, int xrows, int xcols)
+{
+    extern __shared__ float4 smem4[];
+    float2 *sa = reinterpret_cast<float2 *>(smem4);   // [Ks][64] rows
+    float2 *sb = sa + Ks * S1_TILE;                    // [Ks][64] cols
+    const int m = blockIdx.z;
+    const int rt = blockIdx.x * S1_TILE, ct = blockIdx.y * S1_TILE;
+    const float2 *A = UA + ((size_t)m * rows_pad + row0 + rt) * Ks;
+    const float2 *B = UB + ((size_t)m * cols_pad + col0 + ct) * Ks;
+    for (int e = threadIdx.x; e < S1_TILE * Ks; e += blockDim.x) {
+        const int i = e / Ks, k = e - i * Ks;
+        sa[k * S1_TILE + i] = A[e];
+        sb[k * S1_TILE + i] = B[e];
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows 4*tx.., cols 4*ty..
+    float accr[4][4], acci[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { accr[i][j] = 0.f; acci[i][j] = 0.f; }
+    for (int k = 0; k < Ks; ++k) {
+        const float4 a01 = *reinterpret_cast<const float4 *>(sa + k * S1_TILE + 4 * tx);
+        const float4 a23 = *reinterpret_cast<const float4 *>(sa + k * S1_TILE + 4 * tx + 2);
+        const float4 b01 = *reinterpret_cast<const float4 *>(sb + k * S1_TILE + 4 * ty);
+        const float4 b23 = *reinterpret_cast<const float4 *>(sb + k * S1_TILE + 4 * ty + 2);
+        const float ar[4] = {a01.x, a01.z, a23.x, a23.z}, ai[4] = {a01.y, a01.w, a23.y, a23.w};
+        const float br[4] = {b01.x, b01.z, b23.x, b23.z}, bi[4] = {b01.y, b01.w, b23.y, b23.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                // a * conj(b)
+                accr[i][j] = fmaf(ar[i], br[j], fmaf(ai[i], bi[j], accr[i][j]));
+                acci[i][j] = fmaf(ai[i], br[j], fmaf(-ar[i], bi[j], acci[i][j]));
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int col = ct + 4 * ty + j;
+        if (col >= xcols) continue;
+        float2 *dst = X + ((size_t)m * xcols + col) * xrows + rt + 4 * tx;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (rt + 4 * tx + i < xrows) dst[i] = make_float2(4.f * accr[i][j], 4.f * acci[i][j]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// rotation-dependent normaliser D[rl][col][rho] = (1/P) sum_j Y(j) w_P^{j rho} with
+// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k], all in FP64; a block handles one
+// reference and NORM_COLS particle columns.
+constexpr int NORM_COLS = 8;
+
+__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
+                                              int r0, int nr, int c0, int ncols, int cols_pad, float *__restrict__ D)
+{
+    extern __shared__ double2 sd[];
+    const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
+    double2 *Y = sd;                       // [NORM_COLS][J]
+    double2 *tw = Y + NORM_COLS * J;       // [P] w_P^{+e}
+    const int rl = blockIdx.x, r = r0 + rl;
+    const int cb = blockIdx.y * NORM_COLS;
+    for (int e = threadIdx.x; e < P; e += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * e / P, &sn, &cs);
+        tw[e] = make_double2(cs, sn);
+    }
+    for (int e = threadIdx.x; e < NORM_COLS * J; e += blockDim.x) {
+        const int cl = e / J, j = e - cl * J;
+        const int col = c0 + cb + cl;
+        double yr = 0.0, yi = 0.0;
+        if (cb + cl < ncols) {
+            const double2 *ru = RU + ((size_t)r * J + j) * Ks;
+            const double2 *cv = CV + ((size_t)col * J + j) * Ks;
+            for (int k = 0; k < Ks; ++k) {
+                const double2 u = ru[k], v = cv[k];
+                yr += u.x * v.x + u.y * v.y;     // conj(u) * v
+                yi += u.x * v.y - u.y * v.x;
+            }
+        }
+        Y[e] = make_double2(yr, yi);
+    }
+    __syncthreads();
+    const bool peven = (P & 1) == 0;
+    for (int e = threadIdx.x; e < NORM_COLS * P; e += blockDim.x) {
+        const int cl = e / P, rho = e - cl * P;
+        if (cb + cl >= ncols) continue;
+        const double2 *y = Y + cl * J;
+        double acc = y[0].x;
+        const int jmax = peven ? P / 2 - 1 : (P - 1) / 2;
+        int idx = 0;
+        for (int j = 1; j <= jmax; ++j) {
+            idx += rho; if (idx >= P) idx -= P;
+            acc += 2.0 * (y[j].x * tw[idx].x - y[j].y * tw[idx].y);
+        }
+        if (peven) acc += y[P / 2].x * ((rho & 1) ? -1.0 : 1.0);
+        D[((size_t)rl * cols_pad + (cb + cl)) * P + rho] = (float)(acc / P);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage 2: per (col, row) the length-P FFT of Z(j) = [X(j) + conj X(P-j)] +
+// i [X(j) - conj X(P-j)] w_N^{-j} gives z(l) = y(2l) + i y(2l+1), y(rot) =
+// sum_{m<N} X(m) w_N^{-m rot}; cc(rot) = (2/N) y / sqrt(D(rot mod P) * sqsum_ptcl).
+// One block per particle column; each thread transforms whole rows in its own
+// shared-memory slab (element-major, thread-minor: conflict-free), digit-reversed
+// on load so the in-place decimation-in-time passes leave natural order.
+struct S2Params {
+    int N, P, nf, T;
+    int f[MAXF];
+    int rows;          // rows of the wave (local)
+    int xrows, xcols;  // X dims
+    int row0;          // global row of local row 0
+    int nshifts;
+    int r0;            // first reference of the wave's D
+    int dcols;         // D column stride
+    int col0;          // global column of the wave's first column
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+__global__ void k_stage2(S2Params sp, const float2 *__restrict__ X, const float *__restrict__ D,
+                         const float *__restrict__ sqp, const int *__restrict__ rev, float2 *__restrict__ cand,
+                         float *__restrict__ ccall, const int *__restrict__ perm, int nrs_total)
+{
+    extern __shared__ float4 smem4[];
+    const int P = sp.P, N = sp.N, T = sp.T;
+    float2 *twP = reinterpret_cast<float2 *>(smem4);   // [P] w_P^{-e}
+    float2 *twN = twP + P;                             // [P] w_N^{-j}
+    float2 *buf = twN + P;                             // [P][T]
+    float *ccs = reinterpret_cast<float *>(buf + (size_t)P * T);   // [rows + 8]
+    int *ids = reinterpret_cast<int *>(ccs + sp.rows + 8);         // [rows + 8]
+    const int cl = blockIdx.x;           // local column
+    const int t = threadIdx.x;
+    for (int e = t; e < P; e += T) {
+        double sn, cs;
+        sincospi(-2.0 * e / P, &sn, &cs);
+        twP[e] = make_float2((float)cs, (float)sn);
+        sincospi(-2.0 * e / N, &sn, &cs);
+        twN[e] = make_float2((float)cs, (float)sn);
+    }
+    __syncthreads();
+    const size_t plane = (size_t)sp.xcols * sp.xrows;
+    const float2 *Xc = X + (size_t)cl * sp.xrows;
+    const float sq = sqp[sp.col0 + cl];
+    const float scale = 2.0f / (float)N;
+    for (int row = t; row < sp.rows; row += T) {
+        // packed Hermitian input, digit-reversed into the slab
+        for (int j = 0; j <= P / 2; ++j) {
+            const float2 a = Xc[(size_t)j * plane + row];
+            const float2 b = Xc[(size_t)(P - j) * plane + row];
+            if (j == 0) {
+                // X(0), X(P) are real
+                buf[(size_t)rev[0] * T + t] = make_float2(a.x + b.x, a.x - b.x);
+                continue;
+            }
+            // Z(j) from a = X(j), conj b
+            {
+                const float2 E = make_float2(a.x + b.x, a.y - b.y);
+                const float2 O = cmul(make_float2(a.x - b.x, a.y + b.y), twN[j]);
+                buf[(size_t)rev[j] * T + t] = make_float2(E.x - O.y, E.y + O.x);
+            }
+            if (P - j != j) {
+                // Z(P-j) from b = X(P-j), conj a
+                const float2 E = make_float2(b.x + a.x, b.y - a.y);
+                const float2 O = cmul(make_float2(b.x - a.x, b.y + a.y), twN[P - j]);
+                buf[(size_t)rev[P - j] * T + t] = make_float2(E.x - O.y, E.y + O.x);
+            }
+        }
+        // in-place mixed-radix DIT passes, innermost radix first
+        int span = 1;   // m_l of the current level
+        for (int l = sp.nf - 1; l >= 0; --l) {
+            const int r = sp.f[l];
+            const int nl = span * r;
+            const int tstep = P / nl, rstep = P / r;
+            for (int b0 = 0; b0 < P; b0 += nl) {
+                for (int k = 0; k < span; ++k) {
+                    float2 y[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (q < r) {
+                            const float2 v = buf[(size_t)(b0 + q * span + k) * T + t];
+                            y[q] = (q == 0 || k == 0) ? v : cmul(v, twP[(q * k * tstep) % P]);
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < 8; ++s) {
+                        if (s < r) {
+                            float2 acc = y[0];
+#pragma unroll
+                            for (int q = 1; q < 8; ++q)
+                                if (q < r) {
+                                    const float2 w = twP[((q * s) % r) * rstep];
+                                    acc.x += y[q].x * w.x - y[q].y * w.y;
+                                    acc.y += y[q].x * w.y + y[q].y * w.x;
+                                }
+                            buf[(size_t)(b0 + s * span + k) * T + t] = acc;
+                        }
+                    }
+                }
+            }
+            span = nl;
+        }
+        // correlations and the argmax over rotations (lowest rotation on ties)
+        const int grow = sp.row0 + row;
+        const int rl = grow / sp.nshifts - sp.r0;
+        const float *Dr = D + ((size_t)rl * sp.dcols + cl) * P;
+        float best = -INFINITY;
+        int brot = 0;
+        float *cc_out = ccall ? ccall + ((size_t)perm[sp.col0 + cl] * nrs_total + grow) * N : nullptr;
+        for (int l = 0; l < P; ++l) {
+            const float2 z = buf[(size_t)l * T + t];
+            const int r0 = 2 * l, r1 = 2 * l + 1;
+            const float c0 = scale * z.x * rsqrtf(Dr[r0 % P] * sq);
+            const float c1 = scale * z.y * rsqrtf(Dr[r1 % P] * sq);
+            if (cc_out) { cc_out[r0] = c0; cc_out[r1] = c1; }
+            if (c0 > best) { best = c0; brot = r0; }
+            if (c1 > best) { best = c1; brot = r1; }
+        }
+        ccs[row] = best;
+        ids[row] = grow * N + brot;
+    }
+    // merge with the running top-8 of this particle
+    float2 *cp = cand + (size_t)(sp.col0 + cl) * 8;
+    if (t < 8) {
+        const float2 c = cp[t];
+        ccs[sp.rows + t] = c.x;
+        ids[sp.rows + t] = __float_as_int(c.y);
+    }
+    __syncthreads();
+    if (t < 32) {
+        const int n = sp.rows + 8;
+        float sel_cc[8];
+        int sel_id[8];
+        for (int it = 0; it < 8; ++it) {
+            float bc = -INFINITY;
+            int bi = 0x7fffffff, bpos = -1;
+            for (int e = t; e < n; e += 32) {
+                const float c = ccs[e];
+                const int id = ids[e];
+                if (c > bc || (c == bc && id < bi && c != -INFINITY)) { bc = c; bi = id; bpos = e; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+                if (oc > bc || (oc == bc && oi < bi)) { bc = oc; bi = oi; bpos = op; }
+            }
+            sel_cc[it] = bc;
+            sel_id[it] = bi;
+            if (bpos >= 0 && t == (bpos & 31)) ccs[bpos] = -INFINITY;
+            __syncwarp();
+        }
+        if (t < 8) {
+            float c = sel_cc[0];
+            int id = sel_id[0];
+#pragma unroll
+            for (int it = 1; it < 8; ++it)
+                if (t == it) { c = sel_cc[it]; id = sel_id[it]; }
+            cp[t] = make_float2(c, __int_as_float(c == -INFINITY ? -1 : id));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void k_cand_init(float2 *cand, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n * 8) cand[i] = make_float2(-INFINITY, __int_as_float(-1));
+}
+
+// top-1 out of the candidates, or the work list of the exact re-score
+__global__ void k_finish(const float2 *__restrict__ cand, const int *__restrict__ perm, int ncols, int N, int nshifts,
+                         int has_shifts, int ntop, pftcc_best *__restrict__ out, Work *__restrict__ work,
+                         Group *__restrict__ groups)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    const float2 *cp = cand + (size_t)c * 8;
+    const int slot = perm[c];
+    if (ntop == 0) {
+        const int id = __float_as_int(cp[0].y);
+        pftcc_best b;
+        if (id < 0) { b.iref = 0; b.irot = 0; b.ishift = -1; b.corr = -INFINITY; }
+        else {
+            const int rs = id / N, rot = id - rs * N;
+            b.iref = rs / nshifts + 1;
+            b.ishift = has_shifts ? rs % nshifts : -1;
+            b.irot = rot + 1;
+            b.corr = cp[0].x;
+        }
+        out[slot] = b;
+        return;
+    }
+    int cnt = 0;
+    for (int i = 0; i < ntop; ++i) {
+        const int id = __float_as_int(cp[i].y);
+        if (id < 0) continue;
+        const int rs = id / N;
+        work[(size_t)c * ntop + cnt] = Work{rs / nshifts, has_shifts ? rs % nshifts : -1, 0};
+        ++cnt;
+    }
+    groups[c] = Group{slot, c * ntop, cnt, slot};
+}
+
+// ---------------------------------------------------------------------------
+static int ensure_ws(pftcc_handle *h, void **p, size_t bytes, const char *what)
+{
+    // workspace buffers grow monotonically; size kept implicitly by the caller's max
+    return dev_alloc(h, p, bytes, what);
+}
+
+struct WsSizes { size_t UA, UB, RU, CV, D, X, cand, sqp, perm; };
+
+int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, int precision, int ntop, pftcc_best *out_dev,
+                   float *ccall_dev)
+{
+    const Geom &g = h->g;
+    const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
+    if (Ks > 64) return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search supports at most 64 shells");
+    const FFTPlan plan = make_plan(P);
+    for (int i = 0; i < plan.nf; ++i)
+        if (plan.f[i] > 8) return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search needs nrots/2 with prime factors <= 7");
+    const int ns = std::max(1, nshifts_in);
+    const long long nrs_ll = (long long)h->nrefs * ns;
+    if (nrs_ll * N >= (1LL << 31)) return set_err(h, PFTCC_ERR_ARG, "nrefs * nshifts * nrots too large for candidate ids");
+    const int nrs = (int)nrs_ll;
+    const int np = h->nptcls;
+    SearchWS &ws = h->ws;
+    // parity groups: columns ordered even slots first, then odd slots
+    std::vector<int> perm;
+    perm.reserve(np);
+    for (int i = 0; i < np; ++i) if (h->iseven[i]) perm.push_back(i);
+    const int n_even = (int)perm.size();
+    for (int i = 0; i < np; ++i) if (!h->iseven[i]) perm.push_back(i);
+    // columns in tiles of COL_TILE (the tcgen05 M tile): a parity group may start
+    // mid-tile, so one spare tile of zero columns
+    const int cols_pad = (np + COL_TILE - 1) / COL_TILE * COL_TILE + COL_TILE;
+    const int rows_pad = (nrs + S1_TILE - 1) / S1_TILE * S1_TILE;
+    // wave sizes: rows x cols per stage-1/stage-2 round, X scratch ~ 3 GiB max
+    int W_rows = std::min(rows_pad, 1024);
+    int W_cols = std::min(cols_pad - COL_TILE, 4096);
+    while ((size_t)M * W_rows * W_cols * sizeof(float2) > (3ull << 30) && W_cols > COL_TILE) W_cols /= 2;
+    const int nr_wave_max = (W_rows + ns - 1) / ns + 2;
+    // (re)allocate the workspace when the geometry or counts change
+    const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M;
+    if (realloc) {
+        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref};
+        for (void *b : bufs) if (b) cudaFree(b);
+        ws = SearchWS{};
+        int st;
+        if ((st = ensure_ws(h, (void **)&ws.UA, (size_t)M * rows_pad * Ks * sizeof(float2), "UA")) ||
+            (st = ensure_ws(h, (void **)&ws.UB, (size_t)M * cols_pad * Ks * sizeof(float2), "UB")) ||
+            (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
+            (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
+            (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * P * sizeof(float), "D")) ||
+            (st = ensure_ws(h, (void **)&ws.X, (size_t)M * W_rows * W_cols * sizeof(float2), "X")) ||
+            (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||
+            (st = ensure_ws(h, (void **)&ws.sqp, (size_t)cols_pad * sizeof(float), "sqp")) ||
+            (st = ensure_ws(h, (void **)&ws.shifts, (size_t)ns * 2 * sizeof(float) + 64, "shifts")) ||
+            (st = ensure_ws(h, (void **)&ws.cand_ref, (size_t)cols_pad * sizeof(int) + (size_t)P * sizeof(int), "perm")))
+            return st;
+        ws.nrs_pad = rows_pad; ws.np_pad = cols_pad; ws.nshifts = ns; ws.M = M; ws.nrs = nrs;
+        ws.X_elems = (size_t)M * W_rows * W_cols;
+    }
+    int *d_perm = ws.cand_ref;
+    int *d_rev = ws.cand_ref + cols_pad;
+    // the stage-2 kernel writes input j at slab position digit_rev(j)
+    std::vector<int> rev(P);
+    for (int j = 0; j < P; ++j) rev[j] = digit_rev(plan, P, j);
+    cudaError_t e;
+#define CKE(x, w) do { e = (x); if (e != cudaSuccess) return cuda_err(h, e, w); } while (0)
+    CKE(cudaMemcpyAsync(d_perm, perm.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->stream), "perm");
+    CKE(cudaMemcpyAsync(d_rev, rev.data(), P * sizeof(int), cudaMemcpyHostToDevice, h->stream), "rev");
+    std::vector<float> sh(2 * ns, 0.f);
+    if (nshifts_in > 0) std::copy(shifts_host, shifts_host + 2 * ns, sh.begin());
+    CKE(cudaMemcpyAsync(ws.shifts, sh.data(), sh.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream), "shifts");
+    const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
+    // particle spectra and CTF^2 spectra
+    {
+        const size_t smem = N * sizeof(float2) + (size_t)Ks * P * (sizeof(float2) + sizeof(float));
+        CKE(cudaFuncSetAttribute(k_spec_ptcl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+        PFTCC_LAUNCH(h);
+        KTimer kt(h, PFTCC_K_SPEC_PTCL);
+        k_spec_ptcl<<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, d_perm, np, cols_pad, ws.UB, ws.CV,
+                                                                 ws.sqp, h->sqsums);
+        CKE(cudaGetLastError(), "spec_ptcl");
+        PFTCC_LAUNCH(h);
+        k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
+        CKE(cudaGetLastError(), "cand_init");
+    }
+    const size_t smem_ref = N * sizeof(float2) + (size_t)Ks * P * sizeof(float2);
+    CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
+    const size_t smem_s1 = 2 * (size_t)Ks * S1_TILE * sizeof(float2);
+    CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");
+    const size_t smem_norm = ((size_t)NORM_COLS * J + P) * sizeof(double2);
+    CKE(cudaFuncSetAttribute(k_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_norm), "attr");
+    int T = 128;
+    while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
+    const size_t smem_s2 = 2 * (size_t)P * sizeof(float2) + (size_t)P * T * sizeof(float2) +
+                           (size_t)(W_rows + 8) * (sizeof(float) + sizeof(int));
+    CKE(cudaFuncSetAttribute(k_stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s2), "attr");
+    S2Params sp{};
+    sp.N = N; sp.P = P; sp.nf = plan.nf; sp.T = T;
+    for (int i = 0; i < plan.nf; ++i) sp.f[i] = plan.f[i];
+    sp.nshifts = ns;
+    for (int grp = 0; grp < 2; ++grp) {
+        const int gc0 = grp == 0 ? 0 : n_even, gc1 = grp == 0 ? n_even : np;
+        if (gc1 <= gc0) continue;
+        const float2 *refs = grp == 0 ? h->refs_even : h->refs_odd;
+        PFTCC_LAUNCH(h);
+        { KTimer kt(h, PFTCC_K_SPEC_REF);
+        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
+        CKE(cudaGetLastError(), "spec_r2");
+        PFTCC_LAUNCH(h);
+        k_spec_ref<<<rows_pad, SPEC_THREADS, smem_ref, h->stream>>>(g, ns, refs, ws.shifts, h->argtransf, h->argtransf1,
+                                                                    0, nrs, rows_pad, ws.UA); }
+        CKE(cudaGetLastError(), "spec_ref");
+        if (precision == PFTCC_PREC_BF16X3) {
+            int st = umma_stage1(h, M, Ks, ws.UA, 0, nrs, rows_pad, ws.UB, gc0, gc1 - gc0, cols_pad, nullptr, 1, grp);
+            if (st != PFTCC_OK) return st;
+        }
+        for (int row0 = 0; row0 < nrs; row0 += W_rows) {
+            const int rows = std::min(W_rows, nrs - row0);
+            const int rows_t = (rows + S1_TILE - 1) / S1_TILE * S1_TILE;
+            const int r_lo = row0 / ns, r_hi = (row0 + rows - 1) / ns;
+            for (int c0 = gc0; c0 < gc1; c0 += W_cols) {
+                const int cols = std::min(W_cols, gc1 - c0);
+                const int cols_t = (cols + COL_TILE - 1) / COL_TILE * COL_TILE;
+                if (precision == PFTCC_PREC_BF16X3) {
+                    int st = umma_stage1(h, M, Ks, ws.UA, row0, rows_t, rows_pad, ws.UB, c0, cols_t, cols_pad, ws.X, 0, grp);
+                    if (st != PFTCC_OK) return st;
+                } else {
+                    dim3 grid(rows_t / S1_TILE, cols_t / S1_TILE, M);
+                    PFTCC_LAUNCH(h);
+                    KTimer kt(h, PFTCC_K_STAGE1);
+                    k_stage1_fp32<<<grid, 256, smem_s1, h->stream>>>(Ks, ws.UA, rows_pad, row0, ws.UB, cols_pad, c0, ws.X,
+                                                                    rows_t, cols_t);
+                    CKE(cudaGetLastError(), "stage1");
+                }
+                dim3 gn(r_hi - r_lo + 1, (cols + NORM_COLS - 1) / NORM_COLS);
+                PFTCC_LAUNCH(h);
+                { KTimer kt(h, PFTCC_K_NORM);
+                k_norm<<<gn, 256, smem_norm, h->stream>>>(g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t, ws.D); }
+                CKE(cudaGetLastError(), "norm");
+                sp.rows = rows; sp.xrows = rows_t; sp.xcols = cols_t; sp.row0 = row0; sp.r0 = r_lo;
+                sp.dcols = cols_t; sp.col0 = c0;
+                PFTCC_LAUNCH(h);
+                KTimer kt(h, PFTCC_K_STAGE2);
+                k_stage2<<<cols, T, smem_s2, h->stream>>>(sp, ws.X, ws.D, ws.sqp, d_rev, ws.cand, ccall_dev, d_perm, nrs);
+                CKE(cudaGetLastError(), "stage2");
+            }
+        }
+    }
+    if (precision == PFTCC_PREC_BF16X3) {
+        int st = umma_check(h);
+        if (st != PFTCC_OK) return st;
+    }
+    // finish: top-1 or the exact re-score of the best ntop (ref, shift) per particle
+    if (!out_dev) return PFTCC_OK;
+    if (ntop == 0) {
+        PFTCC_LAUNCH(h);
+        k_finish<<<(np + 127) / 128, 128, 0, h->stream>>>(ws.cand, d_perm, np, N, ns, nshifts_in > 0, 0, out_dev, nullptr,
+                                                      nullptr);
+        CKE(cudaGetLastError(), "finish");
+        return PFTCC_OK;
+    }
+    int st = ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)np * ntop * sizeof(Work), 4096), "work");
+    if (st) return st;
+    st = ensure(h, (void **)&h->d_groups, &h->group_cap, std::max<size_t>((size_t)np * sizeof(Group), 256), "groups");
+    if (st) return st;
+    PFTCC_LAUNCH(h);
+    k_finish<<<(np + 127) / 128, 128, 0, h->stream>>>(ws.cand, d_perm, np, N, ns, nshifts_in > 0, ntop, out_dev,
+                                                      h->d_work, h->d_groups);
+    CKE(cudaGetLastError(), "finish");
+    CKE(launch_exact(h, h->d_groups, np, h->d_work, ws.shifts, MODE_BEST, h->cfg.ctf_frame, 1, nullptr, out_dev),
+        "rescore");
+#undef CKE
+    return PFTCC_OK;
+}
+
 }  // namespace pftcc

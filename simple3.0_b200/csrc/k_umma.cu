@@ -1,0 +1,490 @@
+// k_umma.cu -- stage 1 of the m-domain search on the tcgen05 tensor cores.
+//
+// For one angular frequency m, X[col][rs] = 4 sum_k UA(rs,k) conj(UB(col,k)) is
+// computed as a real GEMM with the particles on the UMMA M side and the (ref, shift)
+// rows on the N side:
+//   particle row  : [Br(k) | Bi(k) | 0]                       (K = Kp reals)
+//   N row 2i      : [Ar(k) | Ai(k) | 0]   -> column 2i   = Re X
+//   N row 2i+1    : [Ai(k) | -Ar(k) | 0]  -> column 2i+1 = Im X
+// so the accumulator's column pair (2i, 2i+1) is the complex X of rs = i.  Every
+// FP32 operand value v is split into bf16 hi = rn(v) and lo = rn(v - hi); the
+// product is accumulated in FP32 TMEM as hi*hi + hi*lo + lo*hi (three
+// kind::f16 MMAs per 16-wide K step).  Operands are pre-tiled in global memory in
+// the canonical no-swizzle K-major layout ([chunk of 8 K][row][8 K]) so that one
+// 4-D TMA tile copy per tile lands them ready for the UMMA descriptors.
+//
+// Kernel roles (192 threads, one persistent CTA per SM):
+//   warp 0   TMA producer: particle tile once per work item (m, particle tile),
+//            then the ring of N tiles (64 (ref, shift) rows each)
+//   warp 1   TMEM allocation and the single MMA-issuing thread; accumulators are
+//            double buffered (2 x 128 TMEM columns)
+//   warps 2-5 epilogue: tcgen05.ld of the 128 x 128 accumulator (each warp its
+//            32-lane quadrant), scale by 4, store float2 X[m][col][rs]
+// Every mbarrier wait is bounded; on timeout the kernel records an error code,
+// drains its own outstanding copies (bounded), frees its TMEM and returns.
+#include "pftcc_internal.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdio>
+
+namespace pftcc {
+
+constexpr int U_BM = 128;        // particles per tile (UMMA M)
+constexpr int U_BN = 128;        // N columns per tile = 64 rs x (re, im)
+constexpr int U_RS = 64;         // (ref, shift) rows per tile
+constexpr int U_THREADS = 192;
+constexpr long long WAIT_LIMIT = 20000000;   // polls of a bounded wait (~seconds)
+
+struct UmmaParams {
+    int M;              // m planes of the wave
+    int Kp;             // padded real K per operand part (multiple of 16)
+    int KC;             // 8-element chunks per operand row: 2*Kp/8 (hi then lo)
+    int n_ptiles;       // particle tiles in the wave
+    int ptile0;         // first particle tile of the wave (group relative)
+    int ptiles_m;       // particle tiles per m plane in the packed particle operand
+    int n_rtiles;       // rs tiles in the wave
+    int rtile0;         // first rs tile of the wave
+    int rtiles_m;       // rs tiles per m plane in the packed row operand
+    int stages;         // N-tile ring depth
+    float2 *X;          // [M][xcols][xrows]
+    int xrows, xcols;
+    int *err;           // device error word (0 = ok)
+};
+
+// ---- PTX wrappers --------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait: false on timeout or when another role has aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
+{
+    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        :
+        : "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    // canonical K-major layout without swizzle: start >> 4, LBO (K direction) >> 4,
+    // SBO (8-row groups) >> 4, descriptor version 1, layout type 0
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---- the GEMM ------------------------------------------------------------------------
+__global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ CUtensorMap tmP,
+                                                              const __grid_constant__ CUtensorMap tmR, UmmaParams up)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const uint32_t a_bytes = (uint32_t)U_BM * up.KC * 16;
+    const uint32_t b_bytes = (uint32_t)U_BN * up.KC * 16;
+    unsigned char *sA = smem;
+    unsigned char *sB = smem + a_bytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + (size_t)up.stages * b_bytes);
+    uint64_t *full = bars;                    // [stages]
+    uint64_t *empty = bars + up.stages;       // [stages]
+    uint64_t *a_full = bars + 2 * up.stages;
+    uint64_t *a_empty = a_full + 1;
+    uint64_t *t_full = a_full + 2;            // [2]
+    uint64_t *t_empty = a_full + 4;           // [2]
+    uint64_t *mma_done = a_full + 6;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(a_full + 7);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(a_full + 8);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < up.stages; ++s) { mbar_init(full + s, 1); mbar_init(empty + s, 1); }
+        mbar_init(a_full, 1);
+        mbar_init(a_empty, 1);
+        mbar_init(t_full, 1); mbar_init(t_full + 1, 1);
+        mbar_init(t_empty, 128); mbar_init(t_empty + 1, 128);
+        mbar_init(mma_done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(256));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int nitems = up.M * up.n_ptiles;
+    auto fail = [&](int code) {
+        if (!*abort_flag) atomicCAS(up.err, 0, code);
+        *abort_flag = 1;
+    };
+
+    if (warp == 0 && lane == 0) {
+        // ------------------------------------------------------------ TMA producer
+        long long itb = 0;
+        int ii = 0;
+        bool ok = true;
+        for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
+            const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
+            if (ii > 0 && !mbar_wait(a_empty, (ii - 1) & 1, abort_flag)) { fail(1); ok = false; break; }
+            mbar_expect_tx(a_full, a_bytes);
+            tma_load_4d(sA, &tmP, 0, 0, 0, m * up.ptiles_m + up.ptile0 + pt, a_full);
+            for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
+                const int s = (int)(itb % up.stages);
+                if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag)) {
+                    fail(2); ok = false; break;
+                }
+                mbar_expect_tx(full + s, b_bytes);
+                tma_load_4d(sB + (size_t)s * b_bytes, &tmR, 0, 0, 0, m * up.rtiles_m + up.rtile0 + j, full + s);
+            }
+        }
+        // drain: every issued copy must land before the CTA exits
+        for (long long t = (itb > up.stages ? itb - up.stages : 0); t < itb; ++t) {
+            const int s = (int)(t % up.stages);
+            for (long long i = 0; i < WAIT_LIMIT && !mbar_try(full + s, (uint32_t)((t / up.stages) & 1)); ++i)
+                __nanosleep(64);
+        }
+        if (ii > 0)
+            for (long long i = 0; i < WAIT_LIMIT && !mbar_try(a_full, (uint32_t)((ii - 1) & 1)); ++i) __nanosleep(64);
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------------------ MMA issuer
+        // instruction descriptor: F32 accumulate, BF16 x BF16, both K-major, N=128, M=128
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(U_BN >> 3) << 17) |
+                               ((uint32_t)(U_BM >> 4) << 24);
+        const uint32_t a_base = smem_u32(sA), b_base0 = smem_u32(sB);
+        const int ksteps = up.Kp / 16, lo_off = up.Kp / 8;
+        long long itb = 0, tacc = 0;
+        int ii = 0;
+        bool ok = true;
+        for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
+            if (!mbar_wait(a_full, ii & 1, abort_flag)) { fail(3); ok = false; break; }
+            tc_fence_after();
+            for (int j = 0; j < up.n_rtiles; ++j, ++itb, ++tacc) {
+                const int s = (int)(itb % up.stages);
+                if (!mbar_wait(full + s, (uint32_t)((itb / up.stages) & 1), abort_flag)) { fail(4); ok = false; break; }
+                const int acc = (int)(tacc & 1);
+                if (tacc >= 2 && !mbar_wait(t_empty + acc, (uint32_t)((tacc / 2 - 1) & 1), abort_flag)) {
+                    fail(5); ok = false; break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * U_BN);
+                const uint32_t b_base = b_base0 + (uint32_t)s * b_bytes;
+                for (int ks = 0; ks < ksteps; ++ks) {
+#pragma unroll
+                    for (int prod = 0; prod < 3; ++prod) {
+                        const int ac = (prod == 2 ? lo_off : 0) + 2 * ks;   // lo(A) * hi(B)
+                        const int bc = (prod == 1 ? lo_off : 0) + 2 * ks;   // hi(A) * lo(B)
+                        const uint64_t ad = umma_desc(a_base + (uint32_t)ac * (U_BM * 16), U_BM * 16, 128);
+                        const uint64_t bd = umma_desc(b_base + (uint32_t)bc * (U_BN * 16), U_BN * 16, 128);
+                        umma_bf16(d_tmem, ad, bd, idesc, (ks > 0 || prod > 0) ? 1u : 0u);
+                    }
+                }
+                umma_commit(empty + s);      // N stage reusable once these MMAs finish
+                umma_commit(t_full + acc);   // accumulator ready for the epilogue
+            }
+            umma_commit(a_empty);            // particle tile reusable
+        }
+        umma_commit(mma_done);
+        for (long long i = 0; i < WAIT_LIMIT && !mbar_try(mma_done, 0); ++i) __nanosleep(64);
+    } else if (warp >= 2) {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;                       // TMEM lane quadrant of this warp
+        const int prow = 32 * q + lane;               // particle row within the tile
+        long long tacc = 0;
+        bool ok = true;
+        for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
+            const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
+            const int col = pt * U_BM + prow;
+            for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
+                const int acc = (int)(tacc & 1);
+                // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
+                const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
+                if (!got) { if (lane == 0) fail(6); ok = false; break; }
+                tc_fence_after();
+                float2 *dst = up.X + ((size_t)m * up.xcols + col) * up.xrows + (size_t)j * U_RS;
+#pragma unroll 1
+                for (int c = 0; c < U_BN / 32; ++c) {
+                    uint32_t r[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r);
+                    float4 *d4 = reinterpret_cast<float4 *>(dst + 16 * c);
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        d4[e] = make_float4(4.f * __uint_as_float(r[4 * e]), 4.f * __uint_as_float(r[4 * e + 1]),
+                                            4.f * __uint_as_float(r[4 * e + 2]), 4.f * __uint_as_float(r[4 * e + 3]));
+                }
+                tc_fence_before();
+                mbar_arrive(t_empty + acc);
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(256));
+    }
+}
+
+// ---- operand packing -------------------------------------------------------------------
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// (ref, shift) rows -> R16[m][rt][chunk][128][8]
+__global__ void k_pack_rows(int M, int Ks, int Kp, int KC, int rtiles, int rows_pad, const float2 *__restrict__ UA,
+                            __nv_bfloat16 *__restrict__ R16)
+{
+    const size_t per_tile = (size_t)KC * 128 * 8;
+    const size_t total = (size_t)M * rtiles * per_tile;
+    const int half = Kp / 8;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t tile = e / per_tile;
+        const int within = (int)(e - tile * per_tile);
+        const int c = within / (128 * 8), i = (within / 8) & 127, el = within & 7;
+        const int m = (int)(tile / rtiles), rt = (int)(tile - (size_t)m * rtiles);
+        const int part = c / half, kk = (c - part * half) * 8 + el;
+        const int rs = rt * U_RS + (i >> 1), kind = i & 1;
+        float v = 0.f;
+        if (kk < 2 * Ks && rs < rows_pad) {
+            const int k = kk < Ks ? kk : kk - Ks;
+            const float2 a = UA[((size_t)m * rows_pad + rs) * Ks + k];
+            if (kind == 0) v = kk < Ks ? a.x : a.y;
+            else v = kk < Ks ? a.y : -a.x;
+        }
+        __nv_bfloat16 hi, lo;
+        split_bf16(v, hi, lo);
+        R16[e] = part ? lo : hi;
+    }
+}
+
+// particle columns [c0, c0 + ptiles*128) -> P16[m][pt][chunk][128][8]
+__global__ void k_pack_cols(int M, int Ks, int Kp, int KC, int ptiles, int cols_pad, int c0,
+                            const float2 *__restrict__ UB, __nv_bfloat16 *__restrict__ P16)
+{
+    const size_t per_tile = (size_t)KC * 128 * 8;
+    const size_t total = (size_t)M * ptiles * per_tile;
+    const int half = Kp / 8;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const size_t tile = e / per_tile;
+        const int within = (int)(e - tile * per_tile);
+        const int c = within / (128 * 8), i = (within / 8) & 127, el = within & 7;
+        const int m = (int)(tile / ptiles), pt = (int)(tile - (size_t)m * ptiles);
+        const int part = c / half, kk = (c - part * half) * 8 + el;
+        const int col = c0 + pt * U_BM + i;
+        float v = 0.f;
+        if (kk < 2 * Ks && col < cols_pad) {
+            const float2 b = UB[((size_t)m * cols_pad + col) * Ks + (kk < Ks ? kk : kk - Ks)];
+            v = kk < Ks ? b.x : b.y;
+        }
+        __nv_bfloat16 hi, lo;
+        split_bf16(v, hi, lo);
+        P16[e] = part ? lo : hi;
+    }
+}
+
+// ---- host side --------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+static int make_map(pftcc_handle *h, CUtensorMap *map, void *base, int KC, long long ntiles)
+{
+    auto enc = get_encode();
+    if (!enc) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (((uintptr_t)base & 15) != 0) return set_err(h, PFTCC_ERR_ARG, "operand base not 16-byte aligned");
+    cuuint64_t dims[4] = {8, 128, (cuuint64_t)KC, (cuuint64_t)ntiles};
+    cuuint64_t strides[3] = {16, 128 * 16, (cuuint64_t)KC * 128 * 16};
+    cuuint32_t box[4] = {8, 128, (cuuint32_t)KC, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return PFTCC_OK;
+}
+
+static UmmaState &ustate(pftcc_handle *h) { return h->ws.umma; }
+
+int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int nrs_w, int rows_pad, const float2 *UB,
+                int c0, int ncols_w, int cols_pad, float2 *X, int prepare, int parity_group)
+{
+    (void)parity_group;
+    SearchWS &ws = h->ws;
+    UmmaState &us = ustate(h);
+    const int Kp = (2 * Ks + 15) / 16 * 16;
+    const int KC = 2 * Kp / 8;
+    cudaError_t e;
+    if (prepare) {
+        const int rtiles = rows_pad / U_RS;
+        const int ptiles = (ncols_w + U_BM - 1) / U_BM;
+        const size_t r16 = (size_t)M * rtiles * KC * 128 * 8, p16 = (size_t)M * ptiles * KC * 128 * 8;
+        int st = ensure(h, (void **)&ws.A16, &ws.A16_elems, r16 * sizeof(__nv_bfloat16), "packed rows");
+        if (st) return st;
+        st = ensure(h, (void **)&ws.B16, &ws.B16_elems, p16 * sizeof(__nv_bfloat16), "packed particles");
+        if (st) return st;
+        if (!us.err) {
+            st = dev_alloc(h, (void **)&us.err, sizeof(int), "umma error word");
+            if (st) return st;
+        }
+        us.Kp = Kp; us.KC = KC; us.rtiles = rtiles; us.ptiles = ptiles; us.group_c0 = c0;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&us.sms, cudaDevAttrMultiProcessorCount, dev);
+        PFTCC_LAUNCH(h);
+        KTimer kt(h, PFTCC_K_PACK);
+        k_pack_rows<<<us.sms * 8, 256, 0, h->stream>>>(M, Ks, Kp, KC, rtiles, rows_pad, UA, ws.A16);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "pack rows");
+        PFTCC_LAUNCH(h);
+        k_pack_cols<<<us.sms * 8, 256, 0, h->stream>>>(M, Ks, Kp, KC, ptiles, cols_pad, c0, UB, ws.B16);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "pack cols");
+        if ((e = cudaMemsetAsync(us.err, 0, sizeof(int), h->stream)) != cudaSuccess) return cuda_err(h, e, "err reset");
+        return PFTCC_OK;
+    }
+    if (rs0 % U_RS || nrs_w % U_RS || (c0 - us.group_c0) % U_BM || ncols_w % U_BM)
+        return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave not tile aligned");
+    const int rtile0 = rs0 / U_RS, n_rtiles = nrs_w / U_RS;
+    const int ptile0 = (c0 - us.group_c0) / U_BM, n_ptiles = ncols_w / U_BM;
+    if (rtile0 + n_rtiles > us.rtiles || ptile0 + n_ptiles > us.ptiles)
+        return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave outside the packed operands");
+    CUtensorMap tmP, tmR;
+    int st = make_map(h, &tmP, ws.B16, KC, (long long)M * us.ptiles);
+    if (st) return st;
+    st = make_map(h, &tmR, ws.A16, KC, (long long)M * us.rtiles);
+    if (st) return st;
+    UmmaParams up{};
+    up.M = M; up.Kp = Kp; up.KC = KC;
+    up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
+    up.n_rtiles = n_rtiles; up.rtile0 = rtile0; up.rtiles_m = us.rtiles;
+    const size_t a_bytes = (size_t)U_BM * KC * 16, b_bytes = (size_t)U_BN * KC * 16;
+    // 1 KiB alignment slack, the particle tile, the N ring, 256 B of barriers, and a
+    // 32 KiB tail so that every address an MMA descriptor can form stays inside the
+    // CTA's own shared memory
+    const size_t tail = 32 * 1024;
+    int stages = 3;
+    while (stages > 2 && 1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024) --stages;
+    if (1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
+    up.stages = stages;
+    up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
+    up.err = us.err;
+    const size_t smem = 1024 + a_bytes + stages * b_bytes + 256 + tail;
+    if ((e = cudaFuncSetAttribute(k_umma_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return cuda_err(h, e, "umma attr");
+    const int nitems = M * n_ptiles;
+    const int grid = std::min(nitems, us.sms);
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_STAGE1);
+    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmP, tmR, up);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "umma stage 1 launch");
+    return PFTCC_OK;
+}
+
+int umma_check(pftcc_handle *h)
+{
+    UmmaState &us = ustate(h);
+    if (!us.err) return PFTCC_OK;
+    int v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, us.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, "umma error word");
+    if (v != 0) return set_err(h, PFTCC_ERR_TIMEOUT, "tcgen05 stage 1: bounded wait expired (code " + std::to_string(v) + ")");
+    return PFTCC_OK;
+}
+
+void umma_free(pftcc_handle *h)
+{
+    UmmaState &us = ustate(h);
+    if (us.err) cudaFree(us.err);
+    us.err = nullptr;
+}
+
+}  // namespace pftcc

@@ -51,6 +51,23 @@ int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *wha
     return st;
 }
 
+KTimer::KTimer(pftcc_handle *h_, int cls_) : h(h_), cls(cls_)
+{
+    if (!h->prof) return;
+    for (cudaEvent_t *e : {&a, &b}) {
+        if (!h->prof_pool.empty()) { *e = h->prof_pool.back(); h->prof_pool.pop_back(); }
+        else if (cudaEventCreate(e) != cudaSuccess) { *e = nullptr; }
+    }
+    if (a) cudaEventRecord(a, h->stream);
+}
+
+KTimer::~KTimer()
+{
+    if (!a || !b) return;
+    cudaEventRecord(b, h->stream);
+    h->prof_pending.push_back(pftcc_handle::ProfEv{cls, a, b});
+}
+
 }  // namespace pftcc
 
 #define CK(expr, what)                                             \
@@ -208,7 +225,11 @@ static void free_all(pftcc_handle *h)
                     h->ws.cand_ref};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    umma_free(h);
+    for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
+    cudaStream_t own = h->own_stream ? h->own_stream : h->stream;
+    if (own) cudaStreamDestroy(own);
 }
 
 static int alloc_ptcl_arrays(pftcc_handle *h)
@@ -740,6 +761,23 @@ int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
     return PFTCC_OK;
 }
 
+int pftcc_corr_all_prec(pftcc_handle *h, int nshifts, const float *shifts, int precision, float *cc)
+{
+    if (!h || !cc || nshifts < 0 || (nshifts > 0 && !shifts)) return set_err(h, PFTCC_ERR_ARG, "corr_all_prec: bad arguments");
+    if (precision == PFTCC_PREC_EXACT) return pftcc_corr_all(h, nshifts, shifts, cc);
+    if (precision != PFTCC_PREC_FP32 && precision != PFTCC_PREC_BF16X3)
+        return set_err(h, PFTCC_ERR_ARG, "corr_all_prec: unknown precision");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    const size_t n = (size_t)h->nptcls * h->nrefs * std::max(1, nshifts) * h->g.N;
+    ST(ensure(h, (void **)&h->d_out, &h->out_cap, n * sizeof(float), "corr_all_prec out"));
+    ST(search_mdomain(h, nshifts, shifts, precision, 0, nullptr, h->d_out));
+    CK(cudaMemcpyAsync(cc, h->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "corr_all_prec download");
+    CK(cudaStreamSynchronize(h->stream), "corr_all_prec");
+    return PFTCC_OK;
+}
+
 static int search_exact(pftcc_handle *h, int nshifts, const float *shifts, pftcc_best *out_dev)
 {
     const int ns = std::max(1, nshifts);
@@ -773,7 +811,7 @@ int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int
     if (precision == PFTCC_PREC_EXACT) {
         ST(search_exact(h, nshifts, shifts, (pftcc_best *)out_dev));
     } else if (precision == PFTCC_PREC_FP32 || precision == PFTCC_PREC_BF16X3) {
-        ST(search_mdomain(h, nshifts, shifts, precision, ntop, (pftcc_best *)out_dev));
+        ST(search_mdomain(h, nshifts, shifts, precision, ntop, (pftcc_best *)out_dev, nullptr));
     } else {
         return set_err(h, PFTCC_ERR_ARG, "search_best: unknown precision");
     }
@@ -932,6 +970,63 @@ int pftcc_synchronize(pftcc_handle *h)
     if (!h) return PFTCC_ERR_ARG;
     cudaSetDevice(h->dev);
     CK(cudaStreamSynchronize(h->stream), "synchronize");
+    return PFTCC_OK;
+}
+
+int pftcc_set_stream(pftcc_handle *h, void *stream)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    CK(cudaStreamSynchronize(h->stream), "set_stream");
+    if (!h->own_stream) h->own_stream = h->stream;
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+    return PFTCC_OK;
+}
+
+static void prof_collect(pftcc_handle *h)
+{
+    if (h->prof_pending.empty()) return;
+    cudaStreamSynchronize(h->stream);
+    for (auto &p : h->prof_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            h->prof_ms[p.cls] += ms;
+            h->prof_n[p.cls] += 1;
+        }
+        h->prof_pool.push_back(p.a);
+        h->prof_pool.push_back(p.b);
+    }
+    h->prof_pending.clear();
+    cudaGetLastError();
+}
+
+int pftcc_prof_enable(pftcc_handle *h, int on)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    h->prof = on ? 1 : 0;
+    return PFTCC_OK;
+}
+
+int pftcc_prof_read(pftcc_handle *h, int cls, double *ms, long long *n)
+{
+    if (!h || !ms || !n || cls < 0 || cls >= PFTCC_K_COUNT) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    prof_collect(h);
+    *ms = h->prof_ms[cls];
+    *n = h->prof_n[cls];
+    return PFTCC_OK;
+}
+
+int pftcc_prof_reset(pftcc_handle *h)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    prof_collect(h);
+    for (int i = 0; i < PFTCC_K_COUNT; ++i) { h->prof_ms[i] = 0.0; h->prof_n[i] = 0; }
     return PFTCC_OK;
 }
 

@@ -39,6 +39,12 @@ struct Group {          // all work items of one particle slot
 
 enum { MODE_FULL = 0, MODE_BEST = 1 };
 
+// state of the tcgen05 stage 1 (packed operand geometry, device error word)
+struct UmmaState {
+    int Kp = 0, KC = 0, rtiles = 0, ptiles = 0, group_c0 = 0, sms = 0;
+    int *err = nullptr;
+};
+
 // m-domain search workspace (sized on first use, reused across calls)
 struct SearchWS {
     int nshifts = 0, nrs = 0, nrs_pad = 0, np_pad = 0, M = 0, Mpad = 0;
@@ -58,6 +64,7 @@ struct SearchWS {
     pftcc_best *best = nullptr;  // [np_pad]
     int *cand_ref = nullptr;
     int ptcl_spectra_valid = 0;  // particle spectra current for this handle state
+    UmmaState umma;
 };
 
 }  // namespace pftcc
@@ -105,7 +112,27 @@ struct pftcc_handle {
     std::mutex mtx;
     std::string last_err;
     long long launches = 0;
+    cudaStream_t own_stream = nullptr;
+    // per-kernel-class event timing
+    int prof = 0;
+    struct ProfEv { int cls; cudaEvent_t a, b; };
+    std::vector<ProfEv> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    double prof_ms[PFTCC_K_COUNT] = {};
+    long long prof_n[PFTCC_K_COUNT] = {};
 };
+
+namespace pftcc {
+// records a start event on construction and a stop event on destruction when the
+// handle's profiling is on; wrap one kernel launch of class cls
+struct KTimer {
+    pftcc_handle *h;
+    int cls;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KTimer(pftcc_handle *h_, int cls_);
+    ~KTimer();
+};
+}  // namespace pftcc
 
 namespace pftcc {
 
@@ -128,9 +155,13 @@ cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, co
                               double *out4);
 cudaError_t launch_zero_beyond_kstop(pftcc_handle *h);
 
+// tcgen05 stage 1 (k_umma.cu)
+int umma_check(pftcc_handle *h);
+void umma_free(pftcc_handle *h);
+
 // m-domain search (k_search.cu)
 int search_mdomain(pftcc_handle *h, int nshifts, const float *shifts_host, int precision, int ntop,
-                   pftcc_best *out_dev);
+                   pftcc_best *out_dev, float *ccall_dev);
 
 }  // namespace pftcc
 

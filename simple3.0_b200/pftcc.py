@@ -246,6 +246,16 @@ class polarft_corrcalc:
         self._check(self._L.pftcc_corr_all(self._h, ns, None if sh is None else _f32p(sh), _f32p(out)))
         return out
 
+    def corr_all_prec(self, shifts=None, precision="fp32") -> np.ndarray:
+        """all correlations through the m-domain path (particle frame), same layout as corr_all"""
+        n = self.get_nptcls()
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        out = np.zeros((n, self.cfg.nrefs, max(1, ns), self.cfg.nrots), np.float32)
+        self._check(self._L.pftcc_corr_all_prec(self._h, ns, None if sh is None else _f32p(sh), _PRECS[precision],
+                                                _f32p(out)))
+        return out
+
     def search_best(self, shifts=None, precision="exact", ntop: int = 0) -> np.ndarray:
         """structured array (iref, irot, ishift, corr) per held particle slot"""
         n = self.get_nptcls()
@@ -338,3 +348,22 @@ class polarft_corrcalc:
 
     def synchronize(self):
         self._check(self._L.pftcc_synchronize(self._h))
+
+    def set_stream(self, stream_handle: int | None):
+        """run on a caller's cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)"""
+        self._check(self._L.pftcc_set_stream(self._h, None if not stream_handle else C.c_void_p(stream_handle)))
+
+    def prof_enable(self, on: bool = True):
+        self._check(self._L.pftcc_prof_enable(self._h, int(bool(on))))
+
+    def prof_reset(self):
+        self._check(self._L.pftcc_prof_reset(self._h))
+
+    def prof_read(self) -> dict:
+        """{kernel class: (total ms, launches)} from the CUDA events around each launch"""
+        out = {}
+        for i, name in enumerate(_lib.KERNEL_CLASSES):
+            ms, n = C.c_double(), C.c_longlong()
+            self._check(self._L.pftcc_prof_read(self._h, i, C.byref(ms), C.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
