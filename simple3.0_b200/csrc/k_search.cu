@@ -39,6 +39,14 @@ namespace pftcc {
 
 int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int nrs_w, int rows_pad,
                 const float2 *UB, int c0, int ncols_w, int cols_pad, float2 *X, int prepare, int parity_group);
+bool stage2_fast_supported(int P);
+cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
+                               int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
+                               float2 *cand, float *ccall, const int *perm);
+cudaError_t launch_rescore_md(pftcc_handle *h, int P, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
+                              const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
+                              const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
+                              pftcc_best *out);
 
 static constexpr int MAXF = 12;
 struct FFTPlan {
@@ -286,13 +294,15 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, const float2 *__res
 }
 
 // ---------------------------------------------------------------------------
-// rotation-dependent normaliser D[rl][col][rho] = (1/P) sum_j Y(j) w_P^{j rho} with
-// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k], all in FP64; a block handles one
-// reference and NORM_COLS particle columns.
+// rotation-dependent normaliser D(rho) = (1/P) sum_j Y(j) w_P^{j rho} with
+// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k], all in FP64; stored as the factor
+// Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col)) the correlations are scaled
+// by.  A block handles one reference and NORM_COLS particle columns.
 constexpr int NORM_COLS = 8;
 
 __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
-                                              int r0, int nr, int c0, int ncols, int cols_pad, float *__restrict__ D)
+                                              int r0, int nr, int c0, int ncols, int cols_pad,
+                                              const float *__restrict__ sqp, float *__restrict__ D)
 {
     extern __shared__ double2 sd[];
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
@@ -334,7 +344,7 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
             acc += 2.0 * (y[j].x * tw[idx].x - y[j].y * tw[idx].y);
         }
         if (peven) acc += y[P / 2].x * ((rho & 1) ? -1.0 : 1.0);
-        D[((size_t)rl * cols_pad + (cb + cl)) * P + rho] = (float)(acc / P);
+        D[((size_t)rl * cols_pad + (cb + cl)) * P + rho] = (float)(1.0 / sqrt((acc / P) * (double)sqp[c0 + cb + cl]));
     }
 }
 
@@ -382,8 +392,8 @@ __global__ void k_stage2(S2Params sp, const float2 *__restrict__ X, const float 
     __syncthreads();
     const size_t plane = (size_t)sp.xcols * sp.xrows;
     const float2 *Xc = X + (size_t)cl * sp.xrows;
-    const float sq = sqp[sp.col0 + cl];
-    const float scale = 2.0f / (float)N;
+    // X carries the factor 4 of the half-circle transforms; y/(2N) is the correlation sum
+    const float scale = 1.0f / (2.0f * (float)N);
     for (int row = t; row < sp.rows; row += T) {
         // packed Hermitian input, digit-reversed into the slab
         for (int j = 0; j <= P / 2; ++j) {
@@ -451,8 +461,8 @@ __global__ void k_stage2(S2Params sp, const float2 *__restrict__ X, const float 
         for (int l = 0; l < P; ++l) {
             const float2 z = buf[(size_t)l * T + t];
             const int r0 = 2 * l, r1 = 2 * l + 1;
-            const float c0 = scale * z.x * rsqrtf(Dr[r0 % P] * sq);
-            const float c1 = scale * z.y * rsqrtf(Dr[r1 % P] * sq);
+            const float c0 = scale * z.x * Dr[r0 % P];
+            const float c1 = scale * z.y * Dr[r1 % P];
             if (cc_out) { cc_out[r0] = c0; cc_out[r1] = c1; }
             if (c0 > best) { best = c0; brot = r0; }
             if (c1 > best) { best = c1; brot = r1; }
@@ -644,6 +654,11 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     sp.N = N; sp.P = P; sp.nf = plan.nf; sp.T = T;
     for (int i = 0; i < plan.nf; ++i) sp.f[i] = plan.f[i];
     sp.nshifts = ns;
+    // compile-time transforms for the common lengths; the generic radix loop otherwise
+    const bool fast_s2 = stage2_fast_supported(P);
+    // the top-ntop re-score: FP32 m-domain in the particle frame, the exact kernel in
+    // the reference frame
+    const bool md_rescore = ntop > 0 && fast_s2 && h->cfg.ctf_frame == PFTCC_FRAME_PTCL;
     for (int grp = 0; grp < 2; ++grp) {
         const int gc0 = grp == 0 ? 0 : n_even, gc1 = grp == 0 ? n_even : np;
         if (gc1 <= gc0) continue;
@@ -681,23 +696,34 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                 dim3 gn(r_hi - r_lo + 1, (cols + NORM_COLS - 1) / NORM_COLS);
                 PFTCC_LAUNCH(h);
                 { KTimer kt(h, PFTCC_K_NORM);
-                k_norm<<<gn, 256, smem_norm, h->stream>>>(g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t, ws.D); }
+                k_norm<<<gn, 256, smem_norm, h->stream>>>(g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
+                                                          ws.sqp, ws.D); }
                 CKE(cudaGetLastError(), "norm");
-                sp.rows = rows; sp.xrows = rows_t; sp.xcols = cols_t; sp.row0 = row0; sp.r0 = r_lo;
-                sp.dcols = cols_t; sp.col0 = c0;
-                PFTCC_LAUNCH(h);
-                KTimer kt(h, PFTCC_K_STAGE2);
-                k_stage2<<<cols, T, smem_s2, h->stream>>>(sp, ws.X, ws.D, ws.sqp, d_rev, ws.cand, ccall_dev, d_perm, nrs);
-                CKE(cudaGetLastError(), "stage2");
+                if (fast_s2) {
+                    CKE(launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
+                                           ws.cand, ccall_dev, d_perm), "stage2");
+                } else {
+                    sp.rows = rows; sp.xrows = rows_t; sp.xcols = cols_t; sp.row0 = row0; sp.r0 = r_lo;
+                    sp.dcols = cols_t; sp.col0 = c0;
+                    PFTCC_LAUNCH(h);
+                    KTimer kt(h, PFTCC_K_STAGE2);
+                    k_stage2<<<cols, T, smem_s2, h->stream>>>(sp, ws.X, ws.D, ws.sqp, d_rev, ws.cand, ccall_dev, d_perm, nrs);
+                    CKE(cudaGetLastError(), "stage2");
+                }
             }
         }
+        // particle-frame re-score from this group's FP32 spectra (before the next group
+        // overwrites them)
+        if (md_rescore && out_dev)
+            CKE(launch_rescore_md(h, P, gc1 - gc0, ntop, Ks, ns, nshifts_in > 0, ws.UA, rows_pad, ws.UB, cols_pad,
+                                  ws.RU, ws.CV, ws.sqp, ws.cand, d_perm, gc0, out_dev), "rescore");
     }
     if (precision == PFTCC_PREC_BF16X3) {
         int st = umma_check(h);
         if (st != PFTCC_OK) return st;
     }
     // finish: top-1 or the exact re-score of the best ntop (ref, shift) per particle
-    if (!out_dev) return PFTCC_OK;
+    if (!out_dev || md_rescore) return PFTCC_OK;
     if (ntop == 0) {
         PFTCC_LAUNCH(h);
         k_finish<<<(np + 127) / 128, 128, 0, h->stream>>>(ws.cand, d_perm, np, N, ns, nshifts_in > 0, 0, out_dev, nullptr,

@@ -1,0 +1,437 @@
+// k_stage2.cu -- per-(particle, reference x shift) inverse transform of the m-domain
+// spectrum, the correlation over all in-plane rotations, its argmax and the
+// particle's running top-8; and the FP32 m-domain re-score of the final candidates.
+//
+// For one triple the spectrum X(m), m = 0..P (Hermitian over the full circle of
+// N = 2P rotations) is packed into Z(j) = [X(j) + conj X(P-j)] + i [X(j) - conj X(P-j)]
+// w_N^{-j}, j < P, whose length-P forward DFT z(l) = y(2l) + i y(2l+1) gives every
+// rotation's correlation sum y(rot) = sum_{m<N} X(m) w_N^{-m rot} (the real-output
+// half-length transform; the reference runs the equivalent FFTW c2r per shell in
+// calc_corrs_over_k, simple_polarft_corrcalc.f90:1156).  The length-P DFT is one
+// Cooley-Tukey split P = P1 * P2 evaluated entirely in registers with compile-time
+// unrolled radix-2/3/4/5 butterflies:
+//   pass A: for each residue class j1 < P1 a length-P2 DFT over j2 of Z(j1 + P1 j2),
+//           times w_P^{-j1 l2}, into a thread-private shared-memory slab;
+//   pass B: for each l2 < P2 a length-P1 DFT over j1 -> z(l2 + P2 l1).
+// Classes j1 and P1 - j1 are processed together so that every X element is loaded
+// exactly once (Z(j) needs X(j) and X(P - j), which lie in the mirror class).
+#include "pftcc_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace pftcc {
+
+constexpr int TW_MAX = 320;
+struct TwTables {
+    float2 wP[TW_MAX];   // w_P^{-e} = exp(-2 pi i e / P), e < P
+    float2 wN[TW_MAX];   // w_N^{-e} = exp(-2 pi i e / N), e < P
+};
+
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 c_mi(float2 a) { return make_float2(a.y, -a.x); }   // -i * a
+
+// forward radix butterflies (textbook radix-2/3/4/5 DFT formulas)
+template <int F> struct Bfly;
+template <> struct Bfly<2> {
+    __device__ static void run(float2 *v) { const float2 a = v[0], b = v[1]; v[0] = c_add(a, b); v[1] = c_sub(a, b); }
+};
+template <> struct Bfly<4> {
+    __device__ static void run(float2 *v)
+    {
+        const float2 t0 = c_add(v[0], v[2]), t1 = c_sub(v[0], v[2]);
+        const float2 t2 = c_add(v[1], v[3]), t3 = c_mi(c_sub(v[1], v[3]));
+        v[0] = c_add(t0, t2);
+        v[2] = c_sub(t0, t2);
+        v[1] = c_add(t1, t3);
+        v[3] = c_sub(t1, t3);
+    }
+};
+template <> struct Bfly<3> {
+    __device__ static void run(float2 *v)
+    {
+        const float s3 = 0.86602540378443865f;   // sin(2 pi / 3)
+        const float2 a = v[0], t1 = c_add(v[1], v[2]);
+        const float2 t2 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+        const float2 d = c_sub(v[1], v[2]);
+        const float2 t3 = make_float2(s3 * d.y, -s3 * d.x);   // -i sin(2pi/3) (b - c)
+        v[0] = c_add(a, t1);
+        v[1] = c_add(t2, t3);
+        v[2] = c_sub(t2, t3);
+    }
+};
+template <> struct Bfly<5> {
+    __device__ static void run(float2 *v)
+    {
+        const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;   // cos(2pi/5), cos(4pi/5)
+        const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;    // sin(2pi/5), sin(4pi/5)
+        const float2 a = v[0];
+        const float2 t1 = c_add(v[1], v[4]), t2 = c_add(v[2], v[3]);
+        const float2 t3 = c_sub(v[1], v[4]), t4 = c_sub(v[2], v[3]);
+        const float2 m1 = make_float2(a.x + c1 * t1.x + c2 * t2.x, a.y + c1 * t1.y + c2 * t2.y);
+        const float2 m2 = make_float2(a.x + c2 * t1.x + c1 * t2.x, a.y + c2 * t1.y + c1 * t2.y);
+        const float2 n1 = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+        const float2 n2 = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+        v[0] = make_float2(a.x + t1.x + t2.x, a.y + t1.y + t2.y);
+        v[1] = c_add(m1, c_mi(n1));
+        v[4] = c_sub(m1, c_mi(n1));
+        v[2] = c_add(m2, c_mi(n2));
+        v[3] = c_sub(m2, c_mi(n2));
+    }
+};
+
+// length-L forward DFT in registers, natural order in and out; w_L^e = wP[e * STEP]
+template <int L, int STEP> struct SFFT {
+    static constexpr int F = (L % 4 == 0) ? 4 : (L % 2 == 0) ? 2 : (L % 3 == 0) ? 3 : (L % 5 == 0) ? 5 : 0;
+    static_assert(F != 0, "transform length must factor into 2, 3, 5");
+    static constexpr int M = L / F;
+    __device__ static void run(float2 *x, const TwTables &tw)
+    {
+        float2 s[F][M];
+#pragma unroll
+        for (int q = 0; q < F; ++q)
+#pragma unroll
+            for (int j = 0; j < M; ++j) s[q][j] = x[q + F * j];
+#pragma unroll
+        for (int q = 0; q < F; ++q) SFFT<M, STEP * F>::run(s[q], tw);
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            float2 v[F];
+#pragma unroll
+            for (int q = 0; q < F; ++q) v[q] = (q * k == 0) ? s[q][k] : c_mul(s[q][k], tw.wP[q * k * STEP]);
+            Bfly<F>::run(v);
+#pragma unroll
+            for (int r = 0; r < F; ++r) x[k + M * r] = v[r];
+        }
+    }
+};
+template <int STEP> struct SFFT<1, STEP> {
+    __device__ static void run(float2 *, const TwTables &) {}
+};
+
+// Z(j) from a = X(j) and b = X(P - j)
+__device__ __forceinline__ float2 make_z(float2 a, float2 b, float2 wn)
+{
+    const float2 E = make_float2(a.x + b.x, a.y - b.y);
+    const float2 O = c_mul(make_float2(a.x - b.x, a.y + b.y), wn);
+    return make_float2(E.x - O.y, E.y + O.x);
+}
+
+// the whole per-triple transform; getx(j) returns X(j) for j = 0..P; dinv(rot) the
+// normalising factor; slab is this thread's shared-memory slab with element stride T
+template <int P1, int P2, class GetX, class Dinv>
+__device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, float2 *slab, int T, const TwTables &tw,
+                                            float scale, float *cc_out, float &best, int &brot)
+{
+    constexpr int P = P1 * P2;
+    // ---- pass A: class 0 (mirror of itself, X(P) closes it)
+    {
+        float2 xa[P2 + 1];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) xa[j2] = getx(P1 * j2);
+        xa[P2] = getx(P);
+        xa[0].y = 0.f;       // X(0) and X(P) are real
+        xa[P2].y = 0.f;
+        float2 z[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) z[j2] = make_z(xa[j2], xa[P2 - j2], tw.wN[P1 * j2]);
+        SFFT<P2, P1>::run(z, tw);
+#pragma unroll
+        for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1) * T] = z[l2];
+    }
+    // ---- pass A: class pairs (c, P1 - c)
+#pragma unroll
+    for (int c = 1; c < (P1 + 1) / 2; ++c) {
+        float2 xa[P2], xb[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) {
+            xa[j2] = getx(c + P1 * j2);
+            xb[j2] = getx(P1 - c + P1 * j2);
+        }
+        float2 za[P2], zb[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) {
+            za[j2] = make_z(xa[j2], xb[P2 - 1 - j2], tw.wN[c + P1 * j2]);
+            zb[j2] = make_z(xb[j2], xa[P2 - 1 - j2], tw.wN[P1 - c + P1 * j2]);
+        }
+        SFFT<P2, P1>::run(za, tw);
+        SFFT<P2, P1>::run(zb, tw);
+#pragma unroll
+        for (int l2 = 0; l2 < P2; ++l2) {
+            slab[(l2 * P1 + c) * T] = l2 == 0 ? za[l2] : c_mul(za[l2], tw.wP[(c * l2) % P]);
+            slab[(l2 * P1 + P1 - c) * T] = l2 == 0 ? zb[l2] : c_mul(zb[l2], tw.wP[((P1 - c) * l2) % P]);
+        }
+    }
+    // ---- pass A: the self-mirrored class P1/2
+    if constexpr ((P1 & 1) == 0) {
+        constexpr int c = P1 / 2;
+        float2 xa[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) xa[j2] = getx(c + P1 * j2);
+        float2 z[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) z[j2] = make_z(xa[j2], xa[P2 - 1 - j2], tw.wN[c + P1 * j2]);
+        SFFT<P2, P1>::run(z, tw);
+#pragma unroll
+        for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1 + c) * T] = l2 == 0 ? z[l2] : c_mul(z[l2], tw.wP[(c * l2) % P]);
+    }
+    // ---- pass B: length-P1 DFTs, correlations, argmax (lowest rotation on ties)
+#pragma unroll 1
+    for (int l2 = 0; l2 < P2; ++l2) {
+        float2 v[P1];
+#pragma unroll
+        for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
+        SFFT<P1, P2>::run(v, tw);
+#pragma unroll
+        for (int l1 = 0; l1 < P1; ++l1) {
+            const int l = l2 + P2 * l1;
+            const int r0 = 2 * l, r1 = 2 * l + 1;
+            const float c0 = scale * v[l1].x * dinv(r0 < P ? r0 : r0 - P);
+            const float c1 = scale * v[l1].y * dinv(r1 < P ? r1 : r1 - P);
+            if (cc_out) { cc_out[r0] = c0; cc_out[r1] = c1; }
+            if (c0 > best || (c0 == best && r0 < brot)) { best = c0; brot = r0; }
+            if (c1 > best || (c1 == best && r1 < brot)) { best = c1; brot = r1; }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+struct S2Fast {
+    int rows, xrows, xcols, row0, nshifts, r0, dcols, col0, N, nrs_total;
+};
+
+template <int P1, int P2>
+__global__ void __launch_bounds__(128) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
+                                                     const float *__restrict__ Dinv, float2 *__restrict__ cand,
+                                                     float *__restrict__ ccall, const int *__restrict__ perm)
+{
+    constexpr int P = P1 * P2;
+    extern __shared__ float4 smem4[];
+    const int T = blockDim.x, t = threadIdx.x;
+    float2 *slab = reinterpret_cast<float2 *>(smem4) + t;       // [P][T]
+    float *ccs = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * T);
+    int *ids = reinterpret_cast<int *>(ccs + sp.rows + 8);
+    const int cl = blockIdx.x;
+    const size_t plane = (size_t)sp.xcols * sp.xrows;
+    const float2 *Xc = X + (size_t)cl * sp.xrows;
+    const float scale = 1.0f / (2.0f * (float)sp.N);    // X carries the factor 4 of the half-circle transforms
+    for (int row = t; row < sp.rows; row += T) {
+        const int grow = sp.row0 + row;
+        const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * P;
+        const float2 *xr = Xc + row;
+        auto getx = [&](int j) { return __ldg(xr + (size_t)j * plane); };
+        auto dinv = [&](int rho) { return __ldg(Dr + rho); };
+        float best = -INFINITY;
+        int brot = 0;
+        float *cc_out = ccall ? ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N : nullptr;
+        triple_corr<P1, P2>(getx, dinv, slab, T, tw, scale, cc_out, best, brot);
+        ccs[row] = best;
+        ids[row] = grow * sp.N + brot;
+    }
+    // merge with the particle's running top-8 (lowest id among equal correlations)
+    float2 *cp = cand + (size_t)(sp.col0 + cl) * 8;
+    if (t < 8) {
+        const float2 c = cp[t];
+        ccs[sp.rows + t] = c.x;
+        ids[sp.rows + t] = __float_as_int(c.y);
+    }
+    __syncthreads();
+    if (t < 32) {
+        const int n = sp.rows + 8;
+        float keep_c = -INFINITY;
+        int keep_i = -1;
+        for (int it = 0; it < 8; ++it) {
+            float bc = -INFINITY;
+            int bi = 0x7fffffff, bpos = -1;
+            for (int e = t; e < n; e += 32) {
+                const float c = ccs[e];
+                const int id = ids[e];
+                if (c != -INFINITY && (c > bc || (c == bc && id < bi))) { bc = c; bi = id; bpos = e; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
+                if (oc > bc || (oc == bc && oi < bi)) { bc = oc; bi = oi; bpos = op; }
+            }
+            if (t == it) { keep_c = bc; keep_i = bc == -INFINITY ? -1 : bi; }
+            if (bpos >= 0 && t == (bpos & 31)) ccs[bpos] = -INFINITY;
+            __syncwarp();
+        }
+        if (t < 8) cp[t] = make_float2(keep_c, __int_as_float(keep_i));
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// FP32 m-domain re-score of the top-ntop candidates of each particle (particle frame):
+// X(m) = 4 sum_k UA[m][rs][k] conj(UB[m][col][k]) from the FP32 spectra, the FP64
+// normaliser from the |ref|^2 and CTF^2 spectra, the same transform and argmax.  A
+// thread per (particle, candidate); RS_PER_BLOCK threads of a particle reduce to its best.
+template <int P1, int P2>
+__global__ void __launch_bounds__(64) k_rescore_md(int ncols, int ntop, int Ks, int N, int nshifts, int has_shifts,
+                                                   const TwTables tw, const float2 *__restrict__ UA, int rows_pad,
+                                                   const float2 *__restrict__ UB, int cols_pad,
+                                                   const double2 *__restrict__ RU, const double2 *__restrict__ CV,
+                                                   const float *__restrict__ sqp, const float2 *__restrict__ cand,
+                                                   const int *__restrict__ perm, int c0, pftcc_best *__restrict__ out)
+{
+    constexpr int P = P1 * P2, J = P / 2 + 1;
+    extern __shared__ float4 smem4[];
+    const int T = blockDim.x, t = threadIdx.x;
+    float2 *slab = reinterpret_cast<float2 *>(smem4) + t;                                   // [P][T]
+    float *dtab = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * T) + t;   // [P][T]
+    __shared__ float bc_s[64];
+    __shared__ int bi_s[64];
+    const int per_block = T / ntop;
+    const int cl = c0 + blockIdx.x * per_block + t / ntop, ci = t % ntop;
+    float best = -INFINITY;
+    int brot = 0, rs = -1;
+    if (t < per_block * ntop && cl < c0 + ncols) {
+        const int id = __float_as_int(cand[(size_t)cl * 8 + ci].y);
+        if (id >= 0) {
+            rs = id / N;
+            const int r = rs / nshifts;
+            // normaliser: Y(j) = sum_k conj(RU) CV and D(rho) = (1/P) sum_j Y(j) w_P^{+j rho},
+            // accumulated in FP64 in the (still unused) slab, P doubles = P float2
+            double *dacc = reinterpret_cast<double *>(slab);
+            const double sq = (double)sqp[cl];
+            for (int rho = 0; rho < P; ++rho) dacc[rho * T] = 0.0;
+            for (int j = 0; j <= P / 2; ++j) {
+                double yr = 0.0, yi = 0.0;
+                const double2 *ru = RU + ((size_t)r * J + j) * Ks;
+                const double2 *cv = CV + ((size_t)cl * J + j) * Ks;
+                for (int k = 0; k < Ks; ++k) {
+                    const double2 u = ru[k], v = cv[k];
+                    yr += u.x * v.x + u.y * v.y;
+                    yi += u.x * v.y - u.y * v.x;
+                }
+                const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
+                int idx = 0;
+                for (int rho = 0; rho < P; ++rho) {
+                    // w_P^{+e} = conj(wP[e])
+                    const float2 w = tw.wP[idx];
+                    dacc[rho * T] += wgt * (yr * (double)w.x + yi * (double)w.y);
+                    idx += j;
+                    if (idx >= P) idx -= P;
+                }
+            }
+            for (int rho = 0; rho < P; ++rho) dtab[rho * T] = (float)(1.0 / sqrt(dacc[rho * T] * sq));
+            const float2 *ua = UA + (size_t)rs * Ks;
+            const float2 *ub = UB + (size_t)cl * Ks;
+            const size_t pa = (size_t)rows_pad * Ks, pb = (size_t)cols_pad * Ks;
+            auto getx = [&](int j) {
+                const float2 *a = ua + (size_t)j * pa, *b = ub + (size_t)j * pb;
+                float xr = 0.f, xi = 0.f;
+                for (int k = 0; k < Ks; ++k) {
+                    const float2 av = a[k], bv = b[k];
+                    xr = fmaf(av.x, bv.x, fmaf(av.y, bv.y, xr));
+                    xi = fmaf(av.y, bv.x, fmaf(-av.x, bv.y, xi));
+                }
+                return make_float2(4.f * xr, 4.f * xi);
+            };
+            auto dinv = [&](int rho) { return dtab[rho * T]; };
+            triple_corr<P1, P2>(getx, dinv, slab, T, tw, 1.0f / (2.0f * (float)N), nullptr, best, brot);
+        }
+    }
+    bc_s[t] = best;
+    bi_s[t] = rs < 0 ? 0x7fffffff : rs * N + brot;
+    __syncthreads();
+    if (t < per_block && c0 + blockIdx.x * per_block + t < c0 + ncols) {
+        const int col = c0 + blockIdx.x * per_block + t;
+        float b = -INFINITY;
+        int bid = 0x7fffffff;
+        for (int i = 0; i < ntop; ++i) {
+            const float c = bc_s[t * ntop + i];
+            const int id = bi_s[t * ntop + i];
+            if (id != 0x7fffffff && (c > b || (c == b && id < bid))) { b = c; bid = id; }
+        }
+        pftcc_best o;
+        if (bid == 0x7fffffff) { o.iref = 0; o.irot = 0; o.ishift = -1; o.corr = -INFINITY; }
+        else {
+            const int rs2 = bid / N, rot = bid - rs2 * N;
+            o.iref = rs2 / nshifts + 1;
+            o.ishift = has_shifts ? rs2 % nshifts : -1;
+            o.irot = rot + 1;
+            o.corr = b;
+        }
+        out[perm[col]] = o;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+static void fill_tw(TwTables &tw, int P)
+{
+    for (int e = 0; e < P; ++e) {
+        const double a = -2.0 * M_PI * e / P, b = -2.0 * M_PI * e / (2.0 * P);
+        tw.wP[e] = make_float2((float)cos(a), (float)sin(a));
+        tw.wN[e] = make_float2((float)cos(b), (float)sin(b));
+    }
+}
+
+bool stage2_fast_supported(int P) { return P == 64 || P == 180 || P == 300; }
+
+template <int P1, int P2>
+static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
+                             float2 *cand, float *ccall, const int *perm)
+{
+    TwTables tw;
+    fill_tw(tw, P1 * P2);
+    const int T = 128;
+    const size_t smem = (size_t)P1 * P2 * T * sizeof(float2) + (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
+    cudaError_t e = cudaFuncSetAttribute(k_stage2_fast<P1, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_STAGE2);
+    k_stage2_fast<P1, P2><<<cols, T, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
+                               int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
+                               float2 *cand, float *ccall, const int *perm)
+{
+    S2Fast sp{rows, xrows, xcols, row0, nshifts, r0, dcols, col0, 2 * P, nrs_total};
+    switch (P) {
+    case 64: return launch_s2<8, 8>(h, sp, cols, X, Dinv, cand, ccall, perm);
+    case 180: return launch_s2<12, 15>(h, sp, cols, X, Dinv, cand, ccall, perm);
+    case 300: return launch_s2<15, 20>(h, sp, cols, X, Dinv, cand, ccall, perm);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int P1, int P2>
+static cudaError_t launch_rs(pftcc_handle *h, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
+                             const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
+                             const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
+                             pftcc_best *out)
+{
+    constexpr int P = P1 * P2;
+    TwTables tw;
+    fill_tw(tw, P);
+    const int T = 64, per_block = T / ntop;
+    const size_t smem = (size_t)P * T * (sizeof(float2) + sizeof(float));
+    cudaError_t e = cudaFuncSetAttribute(k_rescore_md<P1, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_EXACT);
+    k_rescore_md<P1, P2><<<(ncols + per_block - 1) / per_block, T, smem, h->stream>>>(
+        ncols, ntop, Ks, 2 * P, nshifts, has_shifts, tw, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rescore_md(pftcc_handle *h, int P, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
+                              const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
+                              const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
+                              pftcc_best *out)
+{
+    switch (P) {
+    case 64: return launch_rs<8, 8>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    case 180: return launch_rs<12, 15>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    case 300: return launch_rs<15, 20>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace pftcc

@@ -177,3 +177,26 @@ def test_bf16x3_parity_groups(pkg):
     ex = pc.search_best(shifts, "exact")
     bf = pc.search_best(shifts, "bf16x3", ntop=3)
     assert np.array_equal(bf["iref"], ex["iref"]) and np.array_equal(bf["corr"], ex["corr"])
+
+
+def test_generic_transform_length(pkg, O):
+    """nrots/2 = 50 has no compile-time transform: the generic radix loop serves it"""
+    w = pkg.synth.config0(nrefs=3, nptcls=5, nrots=100)
+    pc, refs, parts = build(pkg, w)
+    shifts = np.array([[0.0, 0.0], [1.0, 1.0]], np.float32)
+    cc = pc.corr_all_prec(shifts, "fp32")
+    g = O.geom(w.nrots, w.kfrom, w.kto, w.box)
+    t = O.tables(g)
+    worst = 0.0
+    for i in range(w.nptcls):
+        c = O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]), float(parts.dfy[i]),
+                                      float(parts.angast[i])))
+        pft = pc.get_ptcl_pft(i + 1)
+        for r in range(3):
+            for s in range(2):
+                worst = max(worst, relerr(cc[i, r, s], O.gencorrs_ptclframe(g, t, refs[r], pft, c,
+                                                                            shifts[s].astype(np.float64))))
+    assert worst < TOL_FP32, worst
+    ex = pc.search_best(shifts, "exact")
+    md = pc.search_best(shifts, "fp32", ntop=2)
+    assert np.array_equal(md["iref"], ex["iref"]) and np.array_equal(md["irot"], ex["irot"])
