@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1;
-    float2 *tw = reinterpret_cast<float2 *>(smem4);     // [N] w_N^{-e}
-    float2 *a = tw + N;                                  // [Ks][P]
+    double2 *tw = reinterpret_cast<double2 *>(smem4);   // [N] w_N^{-e}
+    float2 *a = reinterpret_cast<float2 *>(tw + N);      // [Ks][P]
     const int row = blockIdx.x;                          // local row
     const int rs = rs0 + row;
     float2 *dst = UA;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
         double sn, cs;
         sincospi(-2.0 * e / N, &sn, &cs);
-        tw[e] = make_float2((float)cs, (float)sn);
+        tw[e] = make_double2(cs, sn);
     }
     const float2 *R = refs + (size_t)r * g.K * P;
     const double sx = shifts ? (double)shifts[2 * s] : 0.0, sy = shifts ? (double)shifts[2 * s + 1] : 0.0;
@@ -128,24 +128,25 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
     for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
         const int m = e / Ks, k = e - m * Ks;
         const float2 *ak = a + k * P;
-        float ur = 0.f, ui = 0.f;
+        // FP64 twiddles and accumulation: the spectra carry no more than the operands' FP32 rounding
+        double ur = 0.0, ui = 0.0;
         int idx = 0;
         if (m & 1) {
             for (int n = 0; n < P; ++n) {
-                const float v = ak[n].y;
-                ur = fmaf(v, tw[idx].x, ur);
-                ui = fmaf(v, tw[idx].y, ui);
+                const double v = ak[n].y;
+                ur = fma(v, tw[idx].x, ur);
+                ui = fma(v, tw[idx].y, ui);
                 idx += m; if (idx >= N) idx -= N;
             }
         } else {
             for (int n = 0; n < P; ++n) {
-                const float v = ak[n].x;
-                ur = fmaf(v, tw[idx].x, ur);
-                ui = fmaf(v, tw[idx].y, ui);
+                const double v = ak[n].x;
+                ur = fma(v, tw[idx].x, ur);
+                ui = fma(v, tw[idx].y, ui);
                 idx += m; if (idx >= N) idx -= N;
             }
         }
-        dst[((size_t)m * rows_pad + row) * Ks + k] = make_float2(ur, ui);
+        dst[((size_t)m * rows_pad + row) * Ks + k] = make_float2((float)ur, (float)ui);
     }
 }
 
@@ -158,9 +159,9 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
-    float2 *tw = reinterpret_cast<float2 *>(smem4);   // [N]
-    float2 *b = tw + N;                                // [Ks][P]
-    float *c2 = reinterpret_cast<float *>(b + Ks * P); // [Ks][P]
+    double2 *tw = reinterpret_cast<double2 *>(smem4);  // [N]
+    float2 *b = reinterpret_cast<float2 *>(tw + N);     // [Ks][P]
+    float *c2 = reinterpret_cast<float *>(b + Ks * P);  // [Ks][P]
     const int col = blockIdx.x;
     if (col >= ncols) {
         for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     for (int e = threadIdx.x; e < N; e += blockDim.x) {
         double sn, cs;
         sincospi(-2.0 * e / N, &sn, &cs);
-        tw[e] = make_float2((float)cs, (float)sn);
+        tw[e] = make_double2(cs, sn);
     }
     const float2 *Q = ptcls + (size_t)slot * g.K * P;
     const float *C = ctfmats ? ctfmats + (size_t)slot * g.K * P : nullptr;
@@ -190,15 +191,15 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
         const int m = e / Ks, k = e - m * Ks;
         const float2 *bk = b + k * P;
-        float ur = 0.f, ui = 0.f;
+        double ur = 0.0, ui = 0.0;
         int idx = 0;
         for (int n = 0; n < P; ++n) {
-            const float v = (m & 1) ? bk[n].y : bk[n].x;
-            ur = fmaf(v, tw[idx].x, ur);
-            ui = fmaf(v, tw[idx].y, ui);
+            const double v = (m & 1) ? bk[n].y : bk[n].x;
+            ur = fma(v, tw[idx].x, ur);
+            ui = fma(v, tw[idx].y, ui);
             idx += m; if (idx >= N) idx -= N;
         }
-        UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2(ur, ui);
+        UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2((float)ur, (float)ui);
     }
     // CTF^2 spectra over P points in FP64: w_P^{-jn} = w_N^{-2jn}
     for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
@@ -588,9 +589,9 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     const int cols_pad = (np + COL_TILE - 1) / COL_TILE * COL_TILE + COL_TILE;
     const int rows_pad = (nrs + S1_TILE - 1) / S1_TILE * S1_TILE;
     // wave sizes: rows x cols per stage-1/stage-2 round, X scratch ~ 3 GiB max
-    int W_rows = std::min(rows_pad, 1024);
+    int W_rows = std::min(rows_pad, 4096);
     int W_cols = std::min(cols_pad - COL_TILE, 4096);
-    while ((size_t)M * W_rows * W_cols * sizeof(float2) > (3ull << 30) && W_cols > COL_TILE) W_cols /= 2;
+    while ((size_t)M * W_rows * W_cols * sizeof(float2) > (8ull << 30) && W_cols > COL_TILE) W_cols /= 2;
     const int nr_wave_max = (W_rows + ns - 1) / ns + 2;
     // (re)allocate the workspace when the geometry or counts change
     const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M;
@@ -628,7 +629,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
     // particle spectra and CTF^2 spectra
     {
-        const size_t smem = N * sizeof(float2) + (size_t)Ks * P * (sizeof(float2) + sizeof(float));
+        const size_t smem = N * sizeof(double2) + (size_t)Ks * P * (sizeof(float2) + sizeof(float));
         CKE(cudaFuncSetAttribute(k_spec_ptcl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
         PFTCC_LAUNCH(h);
         KTimer kt(h, PFTCC_K_SPEC_PTCL);
@@ -639,7 +640,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
         CKE(cudaGetLastError(), "cand_init");
     }
-    const size_t smem_ref = N * sizeof(float2) + (size_t)Ks * P * sizeof(float2);
+    const size_t smem_ref = N * sizeof(double2) + (size_t)Ks * P * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
     const size_t smem_s1 = 2 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");

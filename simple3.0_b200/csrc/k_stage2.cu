@@ -221,7 +221,18 @@ __global__ void __launch_bounds__(128) k_stage2_fast(S2Fast sp, const TwTables t
         const int grow = sp.row0 + row;
         const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * P;
         const float2 *xr = Xc + row;
-        auto getx = [&](int j) { return __ldg(xr + (size_t)j * plane); };
+        if (row + T < sp.rows) {
+            // the next row of this thread: pull its spectrum towards L2 while this one is transformed
+            const float2 *xn = xr + T;
+            for (int j = 0; j <= P; ++j) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
+        }
+        auto getx = [&](int j) {
+            float2 v;
+            asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
+                         : "=f"(v.x), "=f"(v.y)
+                         : "l"(xr + (size_t)j * plane));
+            return v;
+        };
         auto dinv = [&](int rho) { return __ldg(Dr + rho); };
         float best = -INFINITY;
         int brot = 0;
@@ -378,7 +389,8 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
 {
     TwTables tw;
     fill_tw(tw, P1 * P2);
-    const int T = 128;
+    // thread-private slabs of P complex: 128 threads up to P = 200, 64 beyond
+    const int T = P1 * P2 <= 200 ? 128 : 64;
     const size_t smem = (size_t)P1 * P2 * T * sizeof(float2) + (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
     cudaError_t e = cudaFuncSetAttribute(k_stage2_fast<P1, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

@@ -445,11 +445,9 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
     up.n_rtiles = n_rtiles; up.rtile0 = rtile0; up.rtiles_m = us.rtiles;
     const size_t a_bytes = (size_t)U_BM * KC * 16, b_bytes = (size_t)U_BN * KC * 16;
-    // 1 KiB alignment slack, the particle tile, the N ring, 256 B of barriers, and a
-    // 32 KiB tail so that every address an MMA descriptor can form stays inside the
-    // CTA's own shared memory
-    const size_t tail = 32 * 1024;
-    int stages = 3;
+    // 1 KiB alignment slack, the particle tile, the N ring and 256 B of barriers
+    const size_t tail = 0;
+    int stages = 4;
     while (stages > 2 && 1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024) --stages;
     if (1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
