@@ -298,54 +298,58 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, const float2 *__res
 // rotation-dependent normaliser D(rho) = (1/P) sum_j Y(j) w_P^{j rho} with
 // Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k], all in FP64; stored as the factor
 // Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col)) the correlations are scaled
-// by.  A block handles one reference and NORM_COLS particle columns.
-constexpr int NORM_COLS = 8;
-
+// by.  One block per particle column: the column's CTF^2 spectra are staged in
+// shared memory once and reused for every reference of the wave (the |ref|^2
+// spectra of the wave's references stay in L2); Y(j) is reduced by warps over the
+// shells, the inverse transform runs per rotation with an FP64 angle-addition
+// recurrence for w_P^{j rho}.
 __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
-                                              int r0, int nr, int c0, int ncols, int cols_pad,
+                                              int r0, int nr, int c0, int ncols, int dcols,
                                               const float *__restrict__ sqp, float *__restrict__ D)
 {
     extern __shared__ double2 sd[];
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
-    double2 *Y = sd;                       // [NORM_COLS][J]
-    double2 *tw = Y + NORM_COLS * J;       // [P] w_P^{+e}
-    const int rl = blockIdx.x, r = r0 + rl;
-    const int cb = blockIdx.y * NORM_COLS;
-    for (int e = threadIdx.x; e < P; e += blockDim.x) {
-        double sn, cs;
-        sincospi(2.0 * e / P, &sn, &cs);
-        tw[e] = make_double2(cs, sn);
-    }
-    for (int e = threadIdx.x; e < NORM_COLS * J; e += blockDim.x) {
-        const int cl = e / J, j = e - cl * J;
-        const int col = c0 + cb + cl;
-        double yr = 0.0, yi = 0.0;
-        if (cb + cl < ncols) {
+    double2 *cvs = sd;                     // [J][Ks]
+    double2 *Y = cvs + (size_t)J * Ks;     // [J]
+    const int cl = blockIdx.x;
+    if (cl >= ncols) return;
+    const int col = c0 + cl;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) cvs[e] = CV[(size_t)col * J * Ks + e];
+    const double sq = (double)sqp[col];
+    __syncthreads();
+    for (int rl = 0; rl < nr; ++rl) {
+        const int r = r0 + rl;
+        for (int j = warp; j < J; j += nwarps) {
+            double yr = 0.0, yi = 0.0;
             const double2 *ru = RU + ((size_t)r * J + j) * Ks;
-            const double2 *cv = CV + ((size_t)col * J + j) * Ks;
-            for (int k = 0; k < Ks; ++k) {
-                const double2 u = ru[k], v = cv[k];
+            for (int k = lane; k < Ks; k += 32) {
+                const double2 u = ru[k], v = cvs[j * Ks + k];
                 yr += u.x * v.x + u.y * v.y;     // conj(u) * v
                 yi += u.x * v.y - u.y * v.x;
             }
+            for (int o = 16; o > 0; o >>= 1) {
+                yr += __shfl_xor_sync(0xffffffffu, yr, o);
+                yi += __shfl_xor_sync(0xffffffffu, yi, o);
+            }
+            if (lane == 0) Y[j] = make_double2(yr, yi);
         }
-        Y[e] = make_double2(yr, yi);
-    }
-    __syncthreads();
-    const bool peven = (P & 1) == 0;
-    for (int e = threadIdx.x; e < NORM_COLS * P; e += blockDim.x) {
-        const int cl = e / P, rho = e - cl * P;
-        if (cb + cl >= ncols) continue;
-        const double2 *y = Y + cl * J;
-        double acc = y[0].x;
-        const int jmax = peven ? P / 2 - 1 : (P - 1) / 2;
-        int idx = 0;
-        for (int j = 1; j <= jmax; ++j) {
-            idx += rho; if (idx >= P) idx -= P;
-            acc += 2.0 * (y[j].x * tw[idx].x - y[j].y * tw[idx].y);
+        __syncthreads();
+        for (int rho = threadIdx.x; rho < P; rho += blockDim.x) {
+            double sr, cr;
+            sincospi(2.0 * rho / P, &sr, &cr);
+            double c = 1.0, s = 0.0, acc = 0.0;
+            for (int j = 0; j < J; ++j) {
+                const double2 y = Y[j];
+                const double wgt = (j == 0 || 2 * j == P) ? 1.0 : 2.0;
+                acc = fma(wgt, y.x * c - y.y * s, acc);
+                const double nc = c * cr - s * sr;
+                s = c * sr + s * cr;
+                c = nc;
+            }
+            D[((size_t)rl * dcols + cl) * P + rho] = (float)(1.0 / sqrt((acc / P) * sq));
         }
-        if (peven) acc += y[P / 2].x * ((rho & 1) ? -1.0 : 1.0);
-        D[((size_t)rl * cols_pad + (cb + cl)) * P + rho] = (float)(1.0 / sqrt((acc / P) * (double)sqp[c0 + cb + cl]));
+        __syncthreads();
     }
 }
 
@@ -644,7 +648,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
     const size_t smem_s1 = 2 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");
-    const size_t smem_norm = ((size_t)NORM_COLS * J + P) * sizeof(double2);
+    const size_t smem_norm = ((size_t)J * Ks + J) * sizeof(double2);
     CKE(cudaFuncSetAttribute(k_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_norm), "attr");
     int T = 128;
     while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
@@ -694,7 +698,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                                                                     rows_t, cols_t);
                     CKE(cudaGetLastError(), "stage1");
                 }
-                dim3 gn(r_hi - r_lo + 1, (cols + NORM_COLS - 1) / NORM_COLS);
+                const int gn = cols;
                 PFTCC_LAUNCH(h);
                 { KTimer kt(h, PFTCC_K_NORM);
                 k_norm<<<gn, 256, smem_norm, h->stream>>>(g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,

@@ -37,6 +37,8 @@ constexpr int U_BN = 128;        // N columns per tile = 64 rs x (re, im)
 constexpr int U_RS = 64;         // (ref, shift) rows per tile
 constexpr int U_THREADS = 192;
 constexpr long long WAIT_LIMIT = 20000000;   // polls of a bounded wait (~seconds)
+constexpr int STAGE_ROW = 36;                 // floats per staged epilogue row: 128 B + 16 B pad
+constexpr int STAGE_BYTES = 4 * 32 * STAGE_ROW * 4;   // four epilogue warps x 32 rows
 
 struct UmmaParams {
     int M;              // m planes of the wave
@@ -268,28 +270,38 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     } else if (warp >= 2) {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                       // TMEM lane quadrant of this warp
-        const int prow = 32 * q + lane;               // particle row within the tile
+        float *stage = reinterpret_cast<float *>(bars + 64) + (warp - 2) * 32 * STAGE_ROW;
         long long tacc = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
             const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
-            const int col = pt * U_BM + prow;
             for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
                 const int acc = (int)(tacc & 1);
                 // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
                 const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
                 if (!got) { if (lane == 0) fail(6); ok = false; break; }
                 tc_fence_after();
-                float2 *dst = up.X + ((size_t)m * up.xcols + col) * up.xrows + (size_t)j * U_RS;
+                // rows of this warp: particles 32q .. 32q+31 of the tile; each 32-column TMEM
+                // chunk is 16 complex X per row, staged through a padded shared tile so that
+                // each warp store writes four whole 128-byte row segments
+                float2 *dst0 = up.X + ((size_t)m * up.xcols + (size_t)pt * U_BM + 32 * q) * up.xrows + (size_t)j * U_RS;
 #pragma unroll 1
                 for (int c = 0; c < U_BN / 32; ++c) {
                     uint32_t r[32];
                     tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r);
-                    float4 *d4 = reinterpret_cast<float4 *>(dst + 16 * c);
+                    float4 *mine = reinterpret_cast<float4 *>(stage + lane * STAGE_ROW);
 #pragma unroll
                     for (int e = 0; e < 8; ++e)
-                        d4[e] = make_float4(4.f * __uint_as_float(r[4 * e]), 4.f * __uint_as_float(r[4 * e + 1]),
-                                            4.f * __uint_as_float(r[4 * e + 2]), 4.f * __uint_as_float(r[4 * e + 3]));
+                        mine[e] = make_float4(4.f * __uint_as_float(r[4 * e]), 4.f * __uint_as_float(r[4 * e + 1]),
+                                              4.f * __uint_as_float(r[4 * e + 2]), 4.f * __uint_as_float(r[4 * e + 3]));
+                    __syncwarp();
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int row = 4 * i + (lane >> 3), qv = lane & 7;
+                        const float4 v = reinterpret_cast<const float4 *>(stage + row * STAGE_ROW)[qv];
+                        reinterpret_cast<float4 *>(dst0 + (size_t)row * up.xrows + 16 * c)[qv] = v;
+                    }
+                    __syncwarp();
                 }
                 tc_fence_before();
                 mbar_arrive(t_empty + acc);
@@ -445,16 +457,17 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
     up.n_rtiles = n_rtiles; up.rtile0 = rtile0; up.rtiles_m = us.rtiles;
     const size_t a_bytes = (size_t)U_BM * KC * 16, b_bytes = (size_t)U_BN * KC * 16;
-    // 1 KiB alignment slack, the particle tile, the N ring and 256 B of barriers
-    const size_t tail = 0;
+    // 1 KiB alignment slack, the particle tile, the N ring, 512 B of barriers and the
+    // epilogue's staging tiles
+    const size_t tail = 512 + STAGE_BYTES;
     int stages = 4;
-    while (stages > 2 && 1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024) --stages;
-    if (1024 + a_bytes + stages * b_bytes + 256 + tail > 227 * 1024)
+    while (stages > 2 && 1024 + a_bytes + stages * b_bytes + tail > 227 * 1024) --stages;
+    if (1024 + a_bytes + stages * b_bytes + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
     up.stages = stages;
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
-    const size_t smem = 1024 + a_bytes + stages * b_bytes + 256 + tail;
+    const size_t smem = 1024 + a_bytes + stages * b_bytes + tail;
     if ((e = cudaFuncSetAttribute(k_umma_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
     const int nitems = M * n_ptiles;
