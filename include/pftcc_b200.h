@@ -154,6 +154,18 @@ int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int
  * the particle's CTF evaluated at defocus + ddf; the shift part is
  * gencorr_grad_for_rot_8 (:1863-1925) in the branch cfg.match_filt selects */
 int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);
+/* continuous refinement: for each request maximise corr over x = (shift_x, shift_y,
+ * defocus offset in microns) inside the box [lb, ub] at the fixed (iref, iptcl, irot),
+ * starting from x0 -- the role of pftcc_shsrch_grad%minimize with the reference's
+ * L-BFGS-B (simple_pftcc_shsrch_grad.f90:254-338, simple_opt_lbfgsb.f90:103-129)
+ * extended to the defocus.  All problems advance together; every round's pending
+ * function+gradient evaluations go to the GPU in one adjoint launch.  maxits bounds
+ * the iterations, pgtol/factr are L-BFGS-B's stopping tolerances (1e-5 / 1e7 in the
+ * reference's defaults). */
+typedef struct { int iref, iptcl, irot, pad; double x0[3]; } pftcc_refine_req;
+typedef struct { double x[3]; double f; int nevals, niter, converged, pad; } pftcc_refine_out;
+int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub,
+                       int maxits, double pgtol, double factr, pftcc_refine_out *out);
 
 /* ---- getters (:597-710) ----------------------------------------------------------- */
 int pftcc_get_nrots(const pftcc_handle *h, int *nrots);

@@ -36,6 +36,16 @@ class GradReq(C.Structure):
                 ("sx", C.c_double), ("sy", C.c_double), ("ddf", C.c_double)]
 
 
+class RefineReq(C.Structure):
+    _fields_ = [("iref", C.c_int), ("iptcl", C.c_int), ("irot", C.c_int), ("pad", C.c_int),
+                ("x0", C.c_double * 3)]
+
+
+class RefineOut(C.Structure):
+    _fields_ = [("x", C.c_double * 3), ("f", C.c_double), ("nevals", C.c_int), ("niter", C.c_int),
+                ("converged", C.c_int), ("pad", C.c_int)]
+
+
 # every exported entry point with its argument types (restype is int unless noted)
 _h = C.c_void_p
 _fp, _dp, _ip, _vp = C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
@@ -69,6 +79,8 @@ SIGNATURES = {
     "pftcc_search_best": [_h, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],
     "pftcc_search_best_dev": [_h, C.c_int, _fp, C.c_int, C.c_int, _vp],
     "pftcc_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
+    "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
+                           C.POINTER(RefineOut)],
     "pftcc_get_nrots": [_h, _ip],
     "pftcc_get_pftsz": [_h, _ip],
     "pftcc_get_pdim": [_h, _ip],

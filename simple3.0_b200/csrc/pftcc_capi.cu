@@ -841,6 +841,30 @@ int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, doubl
     if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "the adjoint is served in the reference frame");
     ST(check_ctf_state(h));
+    return grad_batch_host(h, nreq, req, f, grad3);
+}
+
+int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub,
+                       int maxits, double pgtol, double factr, pftcc_refine_out *out)
+{
+    if (!h || n < 0 || (n > 0 && (!req || !lb || !ub || !out)) || maxits < 1 || !(pgtol >= 0) || !(factr >= 0))
+        return set_err(h, PFTCC_ERR_ARG, "refine_batch: bad arguments");
+    for (int v = 0; v < 3; ++v)
+        if (!(lb[v] <= ub[v])) return set_err(h, PFTCC_ERR_ARG, "refine_batch: empty box");
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the adjoint is served in the reference frame");
+    ST(check_ctf_state(h));
+    return refine_batch(h, n, req, lb, ub, maxits, pgtol, factr, out);
+}
+
+}  // extern "C"
+
+// pending requests of the adjoint, evaluated in one launch (the caller holds the lock)
+int pftcc::grad_batch_host(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3)
+{
     std::vector<int> slots(nreq);
     for (int i = 0; i < nreq; ++i) {
         if (req[i].iref < 1 || req[i].iref > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "grad_batch: iref");
@@ -872,6 +896,8 @@ int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, doubl
     }
     return PFTCC_OK;
 }
+
+extern "C" {
 
 // ---- getters -------------------------------------------------------------------------------
 int pftcc_get_nrots(const pftcc_handle *h, int *v) { if (!h || !v) return PFTCC_ERR_ARG; *v = h->g.N; return PFTCC_OK; }

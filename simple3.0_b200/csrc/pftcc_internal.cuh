@@ -155,6 +155,12 @@ cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, co
                               double *out4);
 cudaError_t launch_zero_beyond_kstop(pftcc_handle *h);
 
+// adjoint requests served in one launch (pftcc_capi.cu; caller holds the handle lock)
+int grad_batch_host(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);
+// batched bound-constrained quasi-Newton refinement (refine.cu)
+int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub, int maxits,
+                 double pgtol, double factr, pftcc_refine_out *out);
+
 // tcgen05 stage 1 (k_umma.cu)
 int umma_check(pftcc_handle *h);
 void umma_free(pftcc_handle *h);

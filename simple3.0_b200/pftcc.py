@@ -31,6 +31,11 @@ _PRECS = {"exact": PREC_EXACT, "fp32": PREC_FP32, "bf16x3": PREC_BF16X3,
           PREC_EXACT: PREC_EXACT, PREC_FP32: PREC_FP32, PREC_BF16X3: PREC_BF16X3}
 
 
+_GRAD_REQ = np.dtype([("iref", "<i4"), ("iptcl", "<i4"), ("irot", "<i4"), ("pad", "<i4"),
+                      ("sx", "<f8"), ("sy", "<f8"), ("ddf", "<f8")])
+assert _GRAD_REQ.itemsize == C.sizeof(_lib.GradReq)
+
+
 class PftccError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"pftcc error {status}: {msg}")
@@ -277,15 +282,39 @@ class polarft_corrcalc:
         """f and grad3 = d f / d(shift_x, shift_y, defocus) for arrays of requests"""
         iref, iptcl, irot, sx, sy, ddf = np.broadcast_arrays(*(np.asarray(v) for v in (iref, iptcl, irot, sx, sy, ddf)))
         n = iref.size
-        req = (_lib.GradReq * n)()
-        for i in range(n):
-            req[i] = _lib.GradReq(int(iref.flat[i]), int(iptcl.flat[i]), int(irot.flat[i]), 0, float(sx.flat[i]),
-                                  float(sy.flat[i]), float(ddf.flat[i]))
+        # pftcc_grad_req records built as a numpy structured array (40 bytes each)
+        req = np.zeros(n, dtype=_GRAD_REQ)
+        req["iref"], req["iptcl"], req["irot"] = iref.ravel(), iptcl.ravel(), irot.ravel()
+        req["sx"], req["sy"], req["ddf"] = sx.ravel(), sy.ravel(), ddf.ravel()
         f = np.zeros(n, np.float64)
         g = np.zeros((n, 3), np.float64)
-        self._check(self._L.pftcc_grad_batch(self._h, n, req, f.ctypes.data_as(C.POINTER(C.c_double)),
+        self._check(self._L.pftcc_grad_batch(self._h, n, req.ctypes.data_as(C.POINTER(_lib.GradReq)),
+                                             f.ctypes.data_as(C.POINTER(C.c_double)),
                                              g.ctypes.data_as(C.POINTER(C.c_double))))
         return f, g
+
+    def refine_batch(self, iref, iptcl, irot, x0, lb, ub, maxits: int = 100, pgtol: float = 1e-5,
+                     factr: float = 1e7):
+        """maximise corr over (shift_x, shift_y, defocus offset) per problem in the box [lb, ub];
+        returns (x (n,3), corr (n,), nevals (n,), niter (n,), converged (n,))"""
+        iref, iptcl, irot = (np.atleast_1d(np.asarray(v)) for v in (iref, iptcl, irot))
+        x0 = np.asarray(x0, np.float64).reshape(-1, 3)
+        n = x0.shape[0]
+        req = (_lib.RefineReq * n)()
+        for i in range(n):
+            req[i].iref, req[i].iptcl, req[i].irot = int(iref.flat[i % iref.size]), int(iptcl.flat[i % iptcl.size]), \
+                int(irot.flat[i % irot.size])
+            for v in range(3):
+                req[i].x0[v] = float(x0[i, v])
+        out = (_lib.RefineOut * n)()
+        lb = np.ascontiguousarray(lb, np.float64)
+        ub = np.ascontiguousarray(ub, np.float64)
+        self._check(self._L.pftcc_refine_batch(self._h, n, req, lb.ctypes.data_as(C.POINTER(C.c_double)),
+                                               ub.ctypes.data_as(C.POINTER(C.c_double)), int(maxits), float(pgtol),
+                                               float(factr), out))
+        x = np.array([[o.x[v] for v in range(3)] for o in out])
+        return (x, np.array([o.f for o in out]), np.array([o.nevals for o in out]),
+                np.array([o.niter for o in out]), np.array([o.converged for o in out], bool))
 
     # ---- GETTERS ----------------------------------------------------------------------------
     def get_nrots(self) -> int:
