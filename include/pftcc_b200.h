@@ -167,6 +167,20 @@ typedef struct { double x[3]; double f; int nevals, niter, converged, pad; } pft
 int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub,
                        int maxits, double pgtol, double factr, pftcc_refine_out *out);
 
+/* gencorrs for npairs (reference, particle, shift) pairs that allocates no memory, for
+ * callers that cannot let a library call cudaMalloc (work being captured into a CUDA
+ * graph, applications that budget all device memory in their own pool, services
+ * that must not grow after start-up).  No counterpart in the reference.  The work
+ * descriptors live in a fixed 256 KiB device array that every GPU loading the library
+ * holds until exit, so npairs is limited to 6553 (larger batches are rejected with
+ * PFTCC_ERR_ARG -- split them).  iref/iptcl are 1-based as in pftcc_gencorrs, shifts is
+ * [npairs][2] or NULL (gencorrs_cc_1), cc_dev a device buffer of npairs*nrots floats
+ * written as cc_dev[pair*nrots + irot-1].  The first call on a device resolves the
+ * array's device address (make it before any stream capture); calls that overlap on
+ * the GPU race on the shared array -- order them on one stream. */
+int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *iref, const int *iptcl, const float *shifts,
+                           float *cc_dev);
+
 /* ---- getters (:597-710) ----------------------------------------------------------- */
 int pftcc_get_nrots(const pftcc_handle *h, int *nrots);
 int pftcc_get_pftsz(const pftcc_handle *h, int *pftsz);

@@ -81,6 +81,7 @@ SIGNATURES = {
     "pftcc_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
     "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
                            C.POINTER(RefineOut)],
+    "pftcc_gencorrs_noalloc": [_h, C.c_int, _ip, _ip, _fp, _vp],
     "pftcc_get_nrots": [_h, _ip],
     "pftcc_get_pftsz": [_h, _ip],
     "pftcc_get_pdim": [_h, _ip],

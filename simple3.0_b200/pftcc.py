@@ -211,6 +211,16 @@ class polarft_corrcalc:
         self._check(self._L.pftcc_gencorrs(self._h, int(iref), int(iptcl), None if sh is None else _f32p(sh), _f32p(cc)))
         return cc
 
+    def gencorrs_noalloc(self, iref, iptcl, shifts, cc_dev_ptr: int):
+        """gencorrs for many pairs into a caller's device buffer (npairs * nrots floats) without
+        any allocation by the library (fixed device scratch; see include/pftcc_b200.h)"""
+        ir = np.ascontiguousarray(iref, np.int32)
+        ip = np.ascontiguousarray(iptcl, np.int32)
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        self._check(self._L.pftcc_gencorrs_noalloc(self._h, ir.size, ir.ctypes.data_as(C.POINTER(C.c_int)),
+                                                   ip.ctypes.data_as(C.POINTER(C.c_int)),
+                                                   None if sh is None else _f32p(sh), C.c_void_p(cc_dev_ptr)))
+
     def gencorr_for_rot(self, iref: int, iptcl: int, shvec, irot: int) -> float:
         out = C.c_float()
         sh = np.ascontiguousarray(shvec, np.float32)
