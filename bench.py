@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--ntop", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--report", default="", choices=["", "precision"],
+                    help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
+                         "kernel over a particle sample (prints a report line instead of the bench line)")
+    ap.add_argument("--report-ptcls", type=int, default=256, help="particles in the precision sample")
     return ap.parse_args()
 
 
@@ -342,8 +346,83 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ precision report
+def run_precision_report(args):
+    """Every correlation of a particle sample of the workload (all references x all
+    shifts x all rotations) through the FP32 and BF16-split m-domain paths, against
+    the direct kernel with FP64 accumulation (the same objective, particle-frame CTF):
+    max / mean |dcc|, max / mean relative error with |cc| floored at 1e-3, the
+    agreement of the best (ref, shift, rot) per particle, and of the BF16-split search
+    with its FP32 re-score of the top 8.  A disagreement is excused where the exact
+    scores of the two poses differ by less than the path's tolerance."""
+    pkg = entry.load_package()
+    w = workload(pkg, args)
+    shifts = shifts_of(w)
+    ns = len(shifts)
+    refs, R = pkg.synth.make_refs(w)
+    r_host = refs.numpy()
+    chunk = 16
+    nsub = min(args.report_ptcls, w.nptcls)
+    tol = {"fp32": 1e-5, "bf16x3": 1e-4}
+    acc = {p: {"max_abs": 0.0, "sum_abs": 0.0, "max_rel": 0.0, "sum_rel": 0.0, "agree": 0, "excused": 0}
+           for p in ("fp32", "bf16x3")}
+    srch = {"agree": 0, "excused": 0}
+    count = 0
+    t0 = time.time()
+    for first in range(0, nsub, chunk):
+        n = min(chunk, nsub - first)
+        parts = pkg.synth.make_particles(w, R, first=first, count=n)
+        pc = pkg.polarft_corrcalc()
+        pc.new(w.nrefs, (1, n), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True, ctf_frame="ptcl")
+        pc.set_refs(1, r_host, True)
+        pc.set_refs(1, r_host, False)
+        pc.polarize_ptcls(0, parts.cmat.numpy())
+        pc.create_polar_absctfmats(pkg.ctfparams_array(n, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                       dfx=parts.dfx, dfy=parts.dfy, angast=parts.angast))
+        ex = pc.corr_all_prec(shifts, "exact").reshape(n, -1).astype(np.float64)
+        best_ex = ex.argmax(1)
+        count += ex.size
+        for prec in ("fp32", "bf16x3"):
+            cc = pc.corr_all_prec(shifts, prec).reshape(n, -1).astype(np.float64)
+            d = np.abs(cc - ex)
+            rel = d / np.maximum(np.abs(ex), 1e-3)
+            a = acc[prec]
+            a["max_abs"] = max(a["max_abs"], float(d.max()))
+            a["sum_abs"] += float(d.sum())
+            a["max_rel"] = max(a["max_rel"], float(rel.max()))
+            a["sum_rel"] += float(rel.sum())
+            bi = cc.argmax(1)
+            same = bi == best_ex
+            a["agree"] += int(same.sum())
+            gap = ex[np.arange(n), best_ex] - ex[np.arange(n), bi]
+            a["excused"] += int(((~same) & (gap < tol[prec])).sum())
+        sb = pc.search_best(shifts, "bf16x3", ntop=8)
+        pose = (sb["iref"].astype(np.int64) - 1) * ns * w.nrots + sb["ishift"].astype(np.int64) * w.nrots + \
+            sb["irot"].astype(np.int64) - 1
+        same = pose == best_ex
+        srch["agree"] += int(same.sum())
+        gap = ex[np.arange(n), best_ex] - ex[np.arange(n), pose]
+        srch["excused"] += int(((~same) & (gap < tol["bf16x3"])).sum())
+        pc.kill()
+    out = {"report": "precision", "workload": w.name, "oracle": "direct kernel, FP64 accumulation, particle-frame CTF",
+           "sample": f"{nsub} particles x {w.nrefs} refs x {ns} shifts x {w.nrots} rots", "correlations": count,
+           "seconds": round(time.time() - t0, 1)}
+    for prec, a in acc.items():
+        out[prec] = {"max_abs_dcc": a["max_abs"], "mean_abs_dcc": a["sum_abs"] / count,
+                     "max_rel_err_floor1e-3": a["max_rel"], "mean_rel_err_floor1e-3": a["sum_rel"] / count,
+                     "best_pose_agreement": a["agree"] / nsub,
+                     "best_pose_agreement_with_excused": (a["agree"] + a["excused"]) / nsub, "tolerance": tol[prec]}
+    out["search_bf16x3_fp32_rescore_top8"] = {"best_pose_agreement": srch["agree"] / nsub,
+                                              "best_pose_agreement_with_excused":
+                                                  (srch["agree"] + srch["excused"]) / nsub}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.report == "precision":
+        run_precision_report(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -134,6 +134,18 @@ int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, cons
                                       double *grad);
 
 /* ---- batched entry points (no single reference counterpart) ---------------------- */
+/* genfrc (:1417-1441) / calc_frc (:1443-1484): the per-shell correlation at irot,
+ * frc[k - kfrom] for k = kfrom..kstop, each shell normalised by
+ * sqrt(sum|ptcl_k|^2 * sum|ref_k|^2) and 0 where that is below 1e-12; the reference
+ * is prepared in the reference frame (ref * ctf, times the shift phases when shvec is
+ * given).  specscore_1/_2 (:2190-2205): max(0, median of those values), the median
+ * of median_nocopy (simple_math.f90:2111-2130).  The batch serves n (iref, iptcl, irot)
+ * requests in one launch; shifts is [n][2] or NULL, frcs [n][kstop-kfrom+1] or NULL. */
+int pftcc_genfrc(pftcc_handle *h, int iref, int iptcl, int irot, const float *shvec, float *frc);
+int pftcc_specscore(pftcc_handle *h, int iref, int iptcl, int irot, const float *shvec, float *score);
+int pftcc_specscore_batch(pftcc_handle *h, int n, const int *iref, const int *iptcl, const int *irot,
+                          const float *shifts, float *scores, float *frcs);
+
 /* all correlations: cc[slot][iref-1][ishift][irot-1] for every held particle,
  * reference and shift (the loop strategy2D_greedy :42 runs over gencorrs) */
 int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc);
@@ -154,8 +166,10 @@ int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int
  * the particle's CTF evaluated at defocus + ddf; the shift part is
  * gencorr_grad_for_rot_8 (:1863-1925) in the branch cfg.match_filt selects */
 int pftcc_grad_batch(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);
-/* continuous refinement: for each request maximise corr over x = (shift_x, shift_y,
- * defocus offset in microns) inside the box [lb, ub] at the fixed (iref, iptcl, irot),
+/* continuous refinement: for each request i maximise corr over x = (shift_x, shift_y,
+ * defocus offset in microns) inside its own box [lb[i], ub[i]] (lb, ub are [n][3], as the
+ * reference bounds each particle's search, simple_pftcc_shsrch_grad.f90:44-68) at the
+ * fixed (iref, iptcl, irot),
  * starting from x0 -- the role of pftcc_shsrch_grad%minimize with the reference's
  * L-BFGS-B (simple_pftcc_shsrch_grad.f90:254-338, simple_opt_lbfgsb.f90:103-129)
  * extended to the defocus.  All problems advance together; every round's pending

@@ -70,6 +70,9 @@ def lib():
         L.orc_gencorr_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, C.c_int, dp, dp]
         L.orc_gencorr_for_rot.restype = C.c_double
         L.orc_gencorr_grad3.argtypes = [G, fp, fp, dp, dp, dp, C.c_int, C.c_int, dp, dp, dp, dp]
+        L.orc_genfrc.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp]
+        L.orc_specscore.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp]
+        L.orc_specscore.restype = C.c_double
         L.orc_polarize.argtypes = [G, fp, fp, C.c_int, dp]
         L.orc_kb_apod.argtypes = [C.c_double]
         L.orc_kb_apod.restype = C.c_double
@@ -174,6 +177,22 @@ def gencorr_grad3(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, dctf=None,
                             int(irot), int(bool(match_filt)), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
                             _P(f, C.c_double), _P(g3, C.c_double))
     return float(f[0]), g3
+
+
+def genfrc(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=None) -> np.ndarray:
+    """shell FRCs k = kfrom..kstop at one rotation (genfrc / calc_frc), FP64"""
+    frc = np.zeros(g.kstop - g.kfrom + 1, np.float64)
+    lib().orc_genfrc(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float), _P(_ctf_arg(ctf), C.c_double),
+                     _P(_shv(shvec), C.c_double), int(irot), _P(t.argtransf, C.c_double),
+                     _P(t.argtransf1, C.c_double), _P(frc, C.c_double))
+    return frc
+
+
+def specscore(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=None) -> float:
+    """specscore_1 (shvec None) / specscore_2: max(0, median shell FRC), FP64"""
+    return lib().orc_specscore(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                               _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double), int(irot),
+                               _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double))
 
 
 def polarize(g: Geom, t: Tables, cmat, griddev=False) -> np.ndarray:

@@ -215,6 +215,37 @@ void orc_gencorrs(const orc_geom *g, const float *ref, const float *ptcl, const 
     free(pr);
 }
 
+void orc_genfrc(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat, const double *shvec,
+                int irot, const double *argtransf, const double *argtransf_shellone, double *frc)
+{
+    const int P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double den = sqrt(sqsum_kf(P, ptcl + 2 * ik * P) * sqsum_k(P, pr + 2 * ik * P));
+        frc[ik] = den < 1e-12 ? 0.0 : corrk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot) / den;
+    }
+    free(pr);
+}
+
+static int cmp_double(const void *a, const void *b)
+{
+    const double x = *(const double *)a, y = *(const double *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+double orc_specscore(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                     const double *shvec, int irot, const double *argtransf, const double *argtransf_shellone)
+{
+    const int Ks = g->kstop - g->kfrom + 1;
+    double *frc = (double *)malloc(sizeof(double) * Ks);
+    orc_genfrc(g, ref, ptcl, ctfmat, shvec, irot, argtransf, argtransf_shellone, frc);
+    qsort(frc, Ks, sizeof(double), cmp_double);
+    const double med = (Ks % 2) ? frc[Ks / 2] : 0.5 * (frc[Ks / 2 - 1] + frc[Ks / 2]);
+    free(frc);
+    return med > 0.0 ? med : 0.0;
+}
+
 /* gencorr_cc_for_rot_8 (:1690-1733).  match_filt: unweighted sums normalised by
  * sqsum over kfrom..kstop (:1729-1731).  Otherwise the shell-weighted ("jacobian")
  * form sum_k k*corr_k / sqrt(sum_k k|ref_k|^2 * sum_k k|ptcl_k|^2) (:1717-1727). */

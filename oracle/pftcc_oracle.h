@@ -86,6 +86,19 @@ void orc_gencorr_grad3(const orc_geom *g, const float *ref, const float *ptcl, c
                        const double *argtransf, const double *argtransf_shellone,
                        double *f, double *grad3);
 
+/* per-shell correlation coefficient at one rotation, k = kfrom..kstop into frc[Ks]:
+ * genfrc (:1417-1441) when shvec == NULL, calc_frc (:1443-1484) otherwise --
+ * kcorrs(irot) / sqrt(sum_n |ptcl(n,k)|^2 * sum_n |ref_prep(n,k)|^2), 0 when that
+ * denominator is below 1e-12 (no shell normalisation or filter: l_pssnr and
+ * l_match_filt off) */
+void orc_genfrc(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat, const double *shvec,
+                int irot, const double *argtransf, const double *argtransf_shellone, double *frc);
+/* specscore_1/_2 (:2190-2205): max(0, median of the shell FRCs), median as
+ * median_nocopy (simple_math.f90:2111-2130): the middle order statistic for an odd
+ * count, the mean of the two middle ones for an even count */
+double orc_specscore(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                     const double *shvec, int irot, const double *argtransf, const double *argtransf_shellone);
+
 /* d|CTF|/d(mean defocus) in 1/micron, with dfx and dfy both moved by the same amount */
 void orc_dctfmat_ddf(const orc_geom *g, const float *polar, const orc_ctf *c, double *dctfmat);
 

@@ -74,6 +74,9 @@ SIGNATURES = {
     "pftcc_gencorr_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp],
     "pftcc_gencorr_grad_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
     "pftcc_gencorr_grad_only_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp],
+    "pftcc_genfrc": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
+    "pftcc_specscore": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
+    "pftcc_specscore_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp],
     "pftcc_corr_all": [_h, C.c_int, _fp, _fp],
     "pftcc_corr_all_prec": [_h, C.c_int, _fp, C.c_int, _fp],
     "pftcc_search_best": [_h, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],

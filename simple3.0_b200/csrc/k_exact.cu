@@ -551,6 +551,100 @@ cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, doubl
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// genfrc / calc_frc (:1417-1484) and specscore_1/_2 (:2190-2205): for each shell
+// k <= kstop the correlation at irot over sqrt(sum_n |ptcl(n,k)|^2 * sum_n |ref(n,k)|^2),
+// the reference prepared as ref * ctf * shmat (reference frame, as prep_ref4corr and
+// calc_frc do; FP64 like the single-rotation correlators), 0 where that denominator is
+// below 1e-12; the score is max(0, median) with median_nocopy's rule
+// (simple_math.f90:2111-2130).  One block per request: threads over the polar angles,
+// warps reduce their per-shell partial sums into the block's FP64 accumulators.
+__global__ void __launch_bounds__(FR_THREADS) k_specscore(
+    Geom g, const FrcReq *__restrict__ reqs, const float2 *__restrict__ refs_even, const float2 *__restrict__ refs_odd,
+    const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const uint8_t *__restrict__ iseven,
+    const double *__restrict__ argtransf, const double *__restrict__ argtransf1, int with_ctf,
+    float *__restrict__ frc_out /* [nreq][Ks] or null */, float *__restrict__ score_out)
+{
+    extern __shared__ double acc[];   // [3][Ks]: correlation, |ref|^2, |ptcl|^2
+    const FrcReq rq = reqs[blockIdx.x];
+    const int N = g.N, P = g.P, Ks = g.Ks, lane = threadIdx.x & 31;
+    for (int e = threadIdx.x; e < 3 * Ks; e += blockDim.x) acc[e] = 0.0;
+    __syncthreads();
+    const float2 *q = ptcls + (long long)rq.slot * g.K * P;
+    const float2 *r = (iseven[rq.slot] ? refs_even : refs_odd) + (long long)rq.iref * g.K * P;
+    const int s = rq.irot - 1;
+    for (int n0 = 0; n0 < P; n0 += blockDim.x) {
+        const int n = n0 + threadIdx.x;
+        const bool on = n < P;
+        double st_r = 1.0, st_i = 0.0, v_r = 1.0, v_i = 0.0, qs = 1.0;
+        int jp = 0;
+        if (on) {
+            if (rq.has_shift) {
+                const double a = argtransf[n] * rq.sx + argtransf[P + n] * rq.sy;
+                const double a1 = argtransf1[n] * rq.sx + argtransf1[P + n] * rq.sy;
+                sincos(a, &st_i, &st_r);
+                sincos(a1, &v_i, &v_r);
+            }
+            int j = s + n;
+            if (j >= N) j -= N;
+            jp = j < P ? j : j - P;
+            qs = j < P ? 1.0 : -1.0;
+        }
+        for (int ik = 0; ik < Ks; ++ik) {
+            double cr = 0.0, r2 = 0.0, p2 = 0.0;
+            if (on) {
+                const double c = with_ctf ? (double)ctfmats[((long long)rq.slot * g.K + ik) * P + n] : 1.0;
+                const float2 rv = r[(long long)ik * P + n];
+                const double rr = (double)rv.x * c, ri = (double)rv.y * c;
+                const double ar = rr * st_r - ri * st_i, ai = rr * st_i + ri * st_r;
+                const float2 qv = q[(long long)ik * P + jp];
+                const double qr = qv.x, qi = qs * qv.y;
+                cr = ar * qr + ai * qi;
+                r2 = ar * ar + ai * ai;
+                p2 = (double)qv.x * qv.x + (double)qv.y * qv.y;
+                const double nr = st_r * v_r - st_i * v_i, ni = st_r * v_i + st_i * v_r;
+                st_r = nr; st_i = ni;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                cr += __shfl_xor_sync(0xffffffffu, cr, o);
+                r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+                p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+            }
+            if (lane == 0) {
+                atomicAdd(acc + ik, cr);
+                atomicAdd(acc + Ks + ik, r2);
+                atomicAdd(acc + 2 * Ks + ik, p2);
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ik = 0; ik < Ks; ++ik) {
+            const double den = sqrt(acc[2 * Ks + ik] * acc[Ks + ik]);
+            acc[ik] = den < 1e-12 ? 0.0 : acc[ik] / den;
+            if (frc_out) frc_out[(long long)blockIdx.x * Ks + ik] = (float)acc[ik];
+        }
+        for (int a = 1; a < Ks; ++a) {      // insertion sort of the Ks shell values
+            const double v = acc[a];
+            int b = a - 1;
+            while (b >= 0 && acc[b] > v) { acc[b + 1] = acc[b]; --b; }
+            acc[b + 1] = v;
+        }
+        const double med = (Ks & 1) ? acc[Ks / 2] : 0.5 * (acc[Ks / 2 - 1] + acc[Ks / 2]);
+        score_out[blockIdx.x] = (float)(med > 0.0 ? med : 0.0);
+    }
+}
+
+cudaError_t launch_specscore(pftcc_handle *h, const FrcReq *reqs_dev, int nreq, float *frc_dev, float *score_dev)
+{
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_EXACT);
+    k_specscore<<<nreq, FR_THREADS, 3 * h->g.Ks * sizeof(double), h->stream>>>(
+        h->g, reqs_dev, h->refs_even, h->refs_odd, h->ptcls, h->ctfmats, h->d_iseven, h->argtransf, h->argtransf1,
+        h->cfg.with_ctf && h->ctf_ready, frc_dev, score_dev);
+    return cudaGetLastError();
+}
+
 __global__ void k_grad_reqs(const pftcc_grad_req *__restrict__ in, const int *__restrict__ slots, int n,
                             RotReq *__restrict__ out)
 {

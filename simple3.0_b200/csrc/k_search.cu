@@ -40,6 +40,7 @@ namespace pftcc {
 int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int nrs_w, int rows_pad,
                 const float2 *UB, int c0, int ncols_w, int cols_pad, float2 *X, int prepare, int parity_group);
 bool stage2_fast_supported(int P);
+int stage2_fast_p2(int P);
 cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
                                int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
                                float2 *cand, float *ccall, const int *perm);
@@ -215,9 +216,10 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     }
 }
 
-// |ref|^2 spectra over P points (FP64): RU[r][j][k]
+// |ref|^2 spectra over P points (FP64): RU[r][j][k], and the same values j-fastest in
+// RUt[r][k][j] (the normaliser's coalesced layout)
 __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *__restrict__ refs,
-                                                          double2 *__restrict__ RU)
+                                                          double2 *__restrict__ RU, double2 *__restrict__ RUt)
 {
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
     const int r = blockIdx.x;
@@ -234,6 +236,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *
             ui += u * sn;
         }
         RU[(size_t)r * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
+        RUt[(size_t)r * J * Ks + (size_t)k * J + j] = make_double2(ur, ui);
     }
 }
 
@@ -295,62 +298,153 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, const float2 *__res
 }
 
 // ---------------------------------------------------------------------------
-// rotation-dependent normaliser D(rho) = (1/P) sum_j Y(j) w_P^{j rho} with
-// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k], all in FP64; stored as the factor
-// Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col)) the correlations are scaled
-// by.  One block per particle column: the column's CTF^2 spectra are staged in
-// shared memory once and reused for every reference of the wave (the |ref|^2
-// spectra of the wave's references stay in L2); Y(j) is reduced by warps over the
-// shells, the inverse transform runs per rotation with an FP64 angle-addition
-// recurrence for w_P^{j rho}.
-__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
+// rotation-dependent normaliser D(rho) = (1/P) sum_j wgt_j Re[Y(j) w_P^{+j rho}] with
+// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k] (wgt_j = 1 at j = 0 and j = P/2, else 2),
+// all in FP64; stored as the factor Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col))
+// the correlations are scaled by.  One block per particle column: the column's CTF^2
+// spectra are staged in shared memory once, k-major, and reused for every reference of
+// the wave (whose |ref|^2 spectra, read j-fastest from RUt, stay in L2).  References are
+// taken NORM_RB = 32 at a time:
+//   phase Y: threads over (reference, j), j fastest, contract the Ks shells with
+//            coalesced global and conflict-free shared loads;
+//   phase D: lane = reference, each thread NORM_GPT residues g < P/Q, and for each g
+//            the Q rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q}
+//            Y(j) w_P^{j g}, D(g + q P/Q) = Re sum_r i_Q^{q r} S_r (i_Q = exp(2 pi i/Q));
+//            the twiddles w_P^{j g} come from an FP64 table in shared memory and are
+//            the same for the whole warp (broadcast reads).
+// Layouts of the stored factor: p2 == 0, natural Dinv[rl][col][rho] (P values); p2 > 0,
+// the order in which the split-radix stage 2 (P = P1 x p2) visits the rotations,
+// Dinv[rl][col][l2][l1][b] for rot = 2 (l2 + p2 l1) + b (2P values, rho = rot mod P),
+// multiplied by dscale.
+constexpr int NORM_RB = 32;
+constexpr int NORM_GPT = 3;
+
+template <int Q>
+__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RUt, const double2 *__restrict__ CV,
                                               int r0, int nr, int c0, int ncols, int dcols,
-                                              const float *__restrict__ sqp, float *__restrict__ D)
+                                              const float *__restrict__ sqp, float *__restrict__ D, int p2,
+                                              double dscale)
 {
     extern __shared__ double2 sd[];
-    const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
-    double2 *cvs = sd;                     // [J][Ks]
-    double2 *Y = cvs + (size_t)J * Ks;     // [J]
+    const int P = g.P, Ks = g.Ks, J = P / 2 + 1, G = P / Q, Jp = J | 1;
+    const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 2 * P : P;
+    double2 *cvs = sd;                          // [Ks][J]
+    double2 *Y = cvs + (size_t)J * Ks;          // [NORM_RB][Jp], scaled by wgt_j / P
+    double2 *tw = Y + (size_t)NORM_RB * Jp;     // [P] w_P^{+e}
     const int cl = blockIdx.x;
     if (cl >= ncols) return;
     const int col = c0 + cl;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) cvs[e] = CV[(size_t)col * J * Ks + e];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
+        const int j = e / Ks, k = e - j * Ks;
+        cvs[(size_t)k * J + j] = CV[(size_t)col * J * Ks + e];
+    }
+    for (int e = threadIdx.x; e < P; e += blockDim.x) {
+        double s, c;
+        sincospi(2.0 * e / P, &s, &c);
+        tw[e] = make_double2(c, s);
+    }
     const double sq = (double)sqp[col];
+    const double invP = 1.0 / P;
     __syncthreads();
-    for (int rl = 0; rl < nr; ++rl) {
-        const int r = r0 + rl;
-        for (int j = warp; j < J; j += nwarps) {
+    for (int rb0 = 0; rb0 < nr; rb0 += NORM_RB) {
+        const int nb = min(NORM_RB, nr - rb0);
+        for (int it = threadIdx.x; it < nb * J; it += blockDim.x) {
+            const int rb = it / J, j = it - rb * J;
+            const double2 *ru = RUt + (size_t)(r0 + rb0 + rb) * J * Ks + j;
             double yr = 0.0, yi = 0.0;
-            const double2 *ru = RU + ((size_t)r * J + j) * Ks;
-            for (int k = lane; k < Ks; k += 32) {
-                const double2 u = ru[k], v = cvs[j * Ks + k];
-                yr += u.x * v.x + u.y * v.y;     // conj(u) * v
-                yi += u.x * v.y - u.y * v.x;
+            for (int k = 0; k < Ks; ++k) {
+                const double2 u = __ldg(ru + (size_t)k * J), v = cvs[(size_t)k * J + j];
+                yr = fma(u.x, v.x, fma(u.y, v.y, yr));     // conj(u) * v
+                yi = fma(u.x, v.y, fma(-u.y, v.x, yi));
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                yr += __shfl_xor_sync(0xffffffffu, yr, o);
-                yi += __shfl_xor_sync(0xffffffffu, yi, o);
-            }
-            if (lane == 0) Y[j] = make_double2(yr, yi);
+            const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
+            Y[(size_t)rb * Jp + j] = make_double2(wgt * yr, wgt * yi);
         }
         __syncthreads();
-        for (int rho = threadIdx.x; rho < P; rho += blockDim.x) {
-            double sr, cr;
-            sincospi(2.0 * rho / P, &sr, &cr);
-            double c = 1.0, s = 0.0, acc = 0.0;
-            for (int j = 0; j < J; ++j) {
-                const double2 y = Y[j];
-                const double wgt = (j == 0 || 2 * j == P) ? 1.0 : 2.0;
-                acc = fma(wgt, y.x * c - y.y * s, acc);
-                const double nc = c * cr - s * sr;
-                s = c * sr + s * cr;
-                c = nc;
+        if (lane < nb) {
+            const double2 *y = Y + (size_t)lane * Jp;
+            float *dst = D + ((size_t)(rb0 + lane) * dcols + cl) * dlen;
+            for (int g0 = warp * NORM_GPT; g0 < G; g0 += nwarps * NORM_GPT) {
+                double sr[NORM_GPT][Q], si[NORM_GPT][Q];
+                int idx[NORM_GPT];
+#pragma unroll
+                for (int t = 0; t < NORM_GPT; ++t) {
+                    idx[t] = 0;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) sr[t][q] = si[t][q] = 0.0;
+                }
+                for (int j0 = 0; j0 < J; j0 += Q) {
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        const int j = j0 + q;
+                        if (j < J) {
+                            const double2 a = y[j];
+#pragma unroll
+                            for (int t = 0; t < NORM_GPT; ++t) {
+                                const double2 w = tw[idx[t]];
+                                sr[t][q] = fma(a.x, w.x, fma(-a.y, w.y, sr[t][q]));
+                                si[t][q] = fma(a.x, w.y, fma(a.y, w.x, si[t][q]));
+                                idx[t] += g0 + t;                 // (j * g) mod P
+                                if (idx[t] >= P) idx[t] -= P;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < NORM_GPT; ++t) {
+                    const int gg = g0 + t;
+                    if (gg >= G) continue;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) {
+                        // Re sum_r i_Q^{q r} S_r
+                        double d = 0.0;
+#pragma unroll
+                        for (int r = 0; r < Q; ++r) {
+                            const int e = (q * r) % Q;   // i_Q^e in {1, i, -1, -i} (Q = 4), {1, -1} (Q = 2)
+                            if (Q == 1 || e == 0) d += sr[t][r];
+                            else if (2 * e == Q) d -= sr[t][r];
+                            else if (4 * e == Q) d -= si[t][r];
+                            else d += si[t][r];            // 4 e == 3 Q
+                        }
+                        const int rho = gg + q * G;
+                        if (p2 == 0) {
+                            dst[rho] = (float)(1.0 / sqrt(d * sq));
+                        } else {
+                            const float v = (float)(dscale / sqrt(d * sq));
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {   // rot = rho and rho + P
+                                const int rot = rho + h * P, l = rot >> 1;
+                                dst[((l % p2) * p1 + l / p2) * 2 + (rot & 1)] = v;
+                            }
+                        }
+                    }
+                }
             }
-            D[((size_t)rl * dcols + cl) * P + rho] = (float)(1.0 / sqrt((acc / P) * sq));
         }
         __syncthreads();
     }
+}
+
+static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RUt, const double2 *CV, int r0, int nr,
+                               int c0, int ncols, int dcols, const float *sqp, float *D, int p2, double dscale)
+{
+    const int J = g.P / 2 + 1;
+    const size_t smem = ((size_t)J * g.Ks + (size_t)NORM_RB * (J | 1) + g.P) * sizeof(double2);
+    cudaError_t e;
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_NORM);
+    if (g.P % 4 == 0) {
+        if ((e = cudaFuncSetAttribute(k_norm<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k_norm<4><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    } else if (g.P % 2 == 0) {
+        if ((e = cudaFuncSetAttribute(k_norm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k_norm<2><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    } else {
+        if ((e = cudaFuncSetAttribute(k_norm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        k_norm<1><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    }
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -606,9 +700,9 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         int st;
         if ((st = ensure_ws(h, (void **)&ws.UA, (size_t)M * rows_pad * Ks * sizeof(float2), "UA")) ||
             (st = ensure_ws(h, (void **)&ws.UB, (size_t)M * cols_pad * Ks * sizeof(float2), "UB")) ||
-            (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
+            (st = ensure_ws(h, (void **)&ws.RU, 2 * (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
             (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
-            (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * P * sizeof(float), "D")) ||
+            (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * 2 * P * sizeof(float), "D")) ||
             (st = ensure_ws(h, (void **)&ws.X, (size_t)M * W_rows * W_cols * sizeof(float2), "X")) ||
             (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||
             (st = ensure_ws(h, (void **)&ws.sqp, (size_t)cols_pad * sizeof(float), "sqp")) ||
@@ -648,8 +742,6 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
     const size_t smem_s1 = 2 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");
-    const size_t smem_norm = ((size_t)J * Ks + J) * sizeof(double2);
-    CKE(cudaFuncSetAttribute(k_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_norm), "attr");
     int T = 128;
     while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
     const size_t smem_s2 = 2 * (size_t)P * sizeof(float2) + (size_t)P * T * sizeof(float2) +
@@ -670,7 +762,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         const float2 *refs = grp == 0 ? h->refs_even : h->refs_odd;
         PFTCC_LAUNCH(h);
         { KTimer kt(h, PFTCC_K_SPEC_REF);
-        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
+        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU, ws.RU + (size_t)h->nrefs * J * Ks);
         CKE(cudaGetLastError(), "spec_r2");
         PFTCC_LAUNCH(h);
         k_spec_ref<<<rows_pad, SPEC_THREADS, smem_ref, h->stream>>>(g, ns, refs, ws.shifts, h->argtransf, h->argtransf1,
@@ -698,12 +790,9 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                                                                     rows_t, cols_t);
                     CKE(cudaGetLastError(), "stage1");
                 }
-                const int gn = cols;
-                PFTCC_LAUNCH(h);
-                { KTimer kt(h, PFTCC_K_NORM);
-                k_norm<<<gn, 256, smem_norm, h->stream>>>(g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
-                                                          ws.sqp, ws.D); }
-                CKE(cudaGetLastError(), "norm");
+                // the split-radix stage 2 reads the factor in its visiting order, times 1/(2N)
+                CKE(launch_norm(h, g, ws.RU + (size_t)h->nrefs * J * Ks, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
+                                ws.sqp, ws.D, fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N)), "norm");
                 if (fast_s2) {
                     CKE(launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
                                            ws.cand, ccall_dev, d_perm), "stage2");

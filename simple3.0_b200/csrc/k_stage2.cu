@@ -119,31 +119,34 @@ __device__ __forceinline__ float2 make_z(float2 a, float2 b, float2 wn)
     return make_float2(E.x - O.y, E.y + O.x);
 }
 
-// the whole per-triple transform; getx(j) returns X(j) for j = 0..P; dinv(rot) the
-// normalising factor; slab is this thread's shared-memory slab with element stride T
-template <int P1, int P2, class GetX, class Dinv>
-__device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, float2 *slab, int T, const TwTables &tw,
-                                            float scale, float *cc_out, float &best, int &brot)
+// Pass A, split into the pieces the two halves of a row's transform take: class 0 (its
+// own mirror, X(P) closes it), the class pairs (c, P1 - c) for C0 <= c < C1, and for even
+// P1 the self-mirrored class P1/2.  Outputs, times w_P^{-j1 l2}, go to the row's slab
+// (element stride T).
+template <int P1, int P2, class GetX>
+__device__ __forceinline__ void passA_class0(const GetX &getx, float2 *slab, int T, const TwTables &tw)
 {
     constexpr int P = P1 * P2;
-    // ---- pass A: class 0 (mirror of itself, X(P) closes it)
-    {
-        float2 xa[P2 + 1];
+    float2 xa[P2 + 1];
 #pragma unroll
-        for (int j2 = 0; j2 < P2; ++j2) xa[j2] = getx(P1 * j2);
-        xa[P2] = getx(P);
-        xa[0].y = 0.f;       // X(0) and X(P) are real
-        xa[P2].y = 0.f;
-        float2 z[P2];
+    for (int j2 = 0; j2 < P2; ++j2) xa[j2] = getx(P1 * j2);
+    xa[P2] = getx(P);
+    xa[0].y = 0.f;       // X(0) and X(P) are real
+    xa[P2].y = 0.f;
+    float2 z[P2];
 #pragma unroll
-        for (int j2 = 0; j2 < P2; ++j2) z[j2] = make_z(xa[j2], xa[P2 - j2], tw.wN[P1 * j2]);
-        SFFT<P2, P1>::run(z, tw);
+    for (int j2 = 0; j2 < P2; ++j2) z[j2] = make_z(xa[j2], xa[P2 - j2], tw.wN[P1 * j2]);
+    SFFT<P2, P1>::run(z, tw);
 #pragma unroll
-        for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1) * T] = z[l2];
-    }
-    // ---- pass A: class pairs (c, P1 - c)
+    for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1) * T] = z[l2];
+}
+
+template <int P1, int P2, int C0, int C1, class GetX>
+__device__ __forceinline__ void passA_pairs(const GetX &getx, float2 *slab, int T, const TwTables &tw)
+{
+    constexpr int P = P1 * P2;
 #pragma unroll
-    for (int c = 1; c < (P1 + 1) / 2; ++c) {
+    for (int c = C0; c < C1; ++c) {
         float2 xa[P2], xb[P2];
 #pragma unroll
         for (int j2 = 0; j2 < P2; ++j2) {
@@ -164,7 +167,12 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
             slab[(l2 * P1 + P1 - c) * T] = l2 == 0 ? zb[l2] : c_mul(zb[l2], tw.wP[((P1 - c) * l2) % P]);
         }
     }
-    // ---- pass A: the self-mirrored class P1/2
+}
+
+template <int P1, int P2, class GetX>
+__device__ __forceinline__ void passA_mid(const GetX &getx, float2 *slab, int T, const TwTables &tw)
+{
+    constexpr int P = P1 * P2;
     if constexpr ((P1 & 1) == 0) {
         constexpr int c = P1 / 2;
         float2 xa[P2];
@@ -177,9 +185,16 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
 #pragma unroll
         for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1 + c) * T] = l2 == 0 ? z[l2] : c_mul(z[l2], tw.wP[(c * l2) % P]);
     }
-    // ---- pass B: length-P1 DFTs, correlations, argmax (lowest rotation on ties)
+}
+
+// pass B for l2 in [L0, L1): length-P1 DFTs, correlations, argmax (lowest rotation on ties)
+template <int P1, int P2, int L0, int L1, class Dinv>
+__device__ __forceinline__ void passB(const float2 *slab, int T, const TwTables &tw, const Dinv &dinv, float scale,
+                                      float *cc_out, float &best, int &brot)
+{
+    constexpr int P = P1 * P2;
 #pragma unroll 1
-    for (int l2 = 0; l2 < P2; ++l2) {
+    for (int l2 = L0; l2 < L1; ++l2) {
         float2 v[P1];
 #pragma unroll
         for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
@@ -197,34 +212,163 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
     }
 }
 
+// the normalising factors of pass-B block l2, stored in visiting order: d[2 l1 + b]
+// belongs to rot = 2 (l2 + P2 l1) + b (and already carries the 1/(2N) scale)
+template <int P1>
+__device__ __forceinline__ void load_dblock(const float *Dp, int l2, float (&d)[2 * P1])
+{
+    if constexpr (P1 % 2 == 0) {
+        const float4 *d4 = reinterpret_cast<const float4 *>(Dp + (size_t)l2 * 2 * P1);
+#pragma unroll
+        for (int i = 0; i < P1 / 2; ++i) {
+            const float4 t = __ldg(d4 + i);
+            d[4 * i] = t.x; d[4 * i + 1] = t.y; d[4 * i + 2] = t.z; d[4 * i + 3] = t.w;
+        }
+    } else {
+        const float2 *d2 = reinterpret_cast<const float2 *>(Dp + (size_t)l2 * 2 * P1);
+#pragma unroll
+        for (int i = 0; i < P1; ++i) {
+            const float2 t = __ldg(d2 + i);
+            d[2 * i] = t.x; d[2 * i + 1] = t.y;
+        }
+    }
+}
+
+// pass B of the search for l2 in [L0, L1): the maximum correlation and its rotation
+// (lowest rotation among equal maxima).  Each block's 2 P1 values are reduced with
+// fmaxf; afterwards the winning block -- every block when another one reached the same
+// maximum -- is evaluated again by the same loop body (identical values) and scanned
+// for the lowest rotation holding the maximum.
+template <int P1, int P2, int L0, int L1>
+__device__ __forceinline__ void passB_search(const float2 *slab, int T, const TwTables &tw, const float *Dp,
+                                             float &best, int &brot)
+{
+    float bv = -INFINITY;
+    int bl2 = -1, l2 = L0, lend = L1, stage = 0, rmin = 0x7fffffff;
+    bool tie = false;
+#pragma unroll 1
+    while (true) {
+        float2 v[P1];
+#pragma unroll
+        for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
+        SFFT<P1, P2>::run(v, tw);
+        float d[2 * P1];
+        load_dblock<P1>(Dp, l2, d);
+        float c[2 * P1];
+#pragma unroll
+        for (int l1 = 0; l1 < P1; ++l1) {
+            c[2 * l1] = v[l1].x * d[2 * l1];
+            c[2 * l1 + 1] = v[l1].y * d[2 * l1 + 1];
+        }
+        if (stage == 0) {
+            float m = c[0];
+#pragma unroll
+            for (int e = 1; e < 2 * P1; ++e) m = fmaxf(m, c[e]);
+            if (m > bv) { bv = m; bl2 = l2; tie = false; }
+            else if (m == bv) tie = true;
+            if (++l2 < L1) continue;
+            if (bl2 < 0) break;
+            stage = 1;
+            l2 = tie ? L0 : bl2;
+            lend = tie ? L1 : bl2 + 1;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 2 * P1; ++e)
+                if (c[e] == bv) rmin = min(rmin, 2 * (l2 + P2 * (e >> 1)) + (e & 1));
+            if (++l2 >= lend) break;
+        }
+    }
+    best = bv;
+    brot = bl2 < 0 ? 0 : rmin;
+}
+
+// pass B writing every correlation (corr_all), with the per-rotation argmax
+template <int P1, int P2, int L0, int L1>
+__device__ __forceinline__ void passB_all(const float2 *slab, int T, const TwTables &tw, const float *Dp,
+                                          float *cc_out, float &best, int &brot)
+{
+#pragma unroll 1
+    for (int l2 = L0; l2 < L1; ++l2) {
+        float2 v[P1];
+#pragma unroll
+        for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
+        SFFT<P1, P2>::run(v, tw);
+        float d[2 * P1];
+        load_dblock<P1>(Dp, l2, d);
+#pragma unroll
+        for (int l1 = 0; l1 < P1; ++l1) {
+            const int l = l2 + P2 * l1;
+            const int r0 = 2 * l, r1 = 2 * l + 1;
+            const float c0 = v[l1].x * d[2 * l1], c1 = v[l1].y * d[2 * l1 + 1];
+            cc_out[r0] = c0;
+            cc_out[r1] = c1;
+            if (c0 > best || (c0 == best && r0 < brot)) { best = c0; brot = r0; }
+            if (c1 > best || (c1 == best && r1 < brot)) { best = c1; brot = r1; }
+        }
+    }
+}
+
+// how a row's transform is split between two threads: role 0 takes class 0, the class
+// pairs c < PAIRS_A + 1 and the middle class, role 1 the other pairs (P1 length-P2 DFTs
+// in all, split as evenly as the classes allow); pass B splits at l2 = LB
+template <int P1, int P2> struct RowSplit {
+    static constexpr int SELFS = 1 + ((P1 & 1) == 0);
+    static constexpr int PAIRS_A = (P1 - 2 * SELFS) / 4;
+    static constexpr int NPAIRS = (P1 - 1) / 2;
+    static constexpr int LB = (P2 + 1) / 2;
+};
+
+// the whole per-triple transform in one thread; getx(j) returns X(j) for j = 0..P;
+// dinv(rot) the normalising factor; slab is this thread's shared-memory slab with
+// element stride T
+template <int P1, int P2, class GetX, class Dinv>
+__device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, float2 *slab, int T, const TwTables &tw,
+                                            float scale, float *cc_out, float &best, int &brot)
+{
+    passA_class0<P1, P2>(getx, slab, T, tw);
+    passA_pairs<P1, P2, 1, (P1 + 1) / 2>(getx, slab, T, tw);
+    passA_mid<P1, P2>(getx, slab, T, tw);
+    passB<P1, P2, 0, P2>(slab, T, tw, dinv, scale, cc_out, best, brot);
+}
+
 // ---------------------------------------------------------------------------------------
 struct S2Fast {
     int rows, xrows, xcols, row0, nshifts, r0, dcols, col0, N, nrs_total;
 };
 
-template <int P1, int P2>
-__global__ void __launch_bounds__(128) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
-                                                     const float *__restrict__ Dinv, float2 *__restrict__ cand,
-                                                     float *__restrict__ ccall, const int *__restrict__ perm)
+// ROWS rows in flight per block, two threads per row: warp w < ROWS/32 (role 0) and warp
+// w + ROWS/32 (role 1) share the rows' slabs and meet at named barrier 1 + w twice per row
+// (after pass A; after pass B, when role 1 hands its argmax over).
+template <int P1, int P2, int ROWS, bool WRITE>
+__global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
+                                                            const float *__restrict__ Dinv, float2 *__restrict__ cand,
+                                                            float *__restrict__ ccall, const int *__restrict__ perm)
 {
     constexpr int P = P1 * P2;
+    using SP = RowSplit<P1, P2>;
     extern __shared__ float4 smem4[];
-    const int T = blockDim.x, t = threadIdx.x;
-    float2 *slab = reinterpret_cast<float2 *>(smem4) + t;       // [P][T]
-    float *ccs = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * T);
+    const int t = threadIdx.x;
+    const int role = t >= ROWS, lr = t - role * ROWS;
+    const int bar = 1 + (lr >> 5);
+    float2 *slab = reinterpret_cast<float2 *>(smem4) + lr;                       // [P][ROWS]
+    float *xfer_c = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * ROWS);   // [ROWS]
+    int *xfer_r = reinterpret_cast<int *>(xfer_c + ROWS);                                             // [ROWS]
+    float *ccs = reinterpret_cast<float *>(xfer_r + ROWS);                                            // [rows + 8]
     int *ids = reinterpret_cast<int *>(ccs + sp.rows + 8);
     const int cl = blockIdx.x;
     const size_t plane = (size_t)sp.xcols * sp.xrows;
     const float2 *Xc = X + (size_t)cl * sp.xrows;
-    const float scale = 1.0f / (2.0f * (float)sp.N);    // X carries the factor 4 of the half-circle transforms
-    for (int row = t; row < sp.rows; row += T) {
+    for (int base = 0; base < sp.rows; base += ROWS) {
+        const int row = base + lr;
+        const bool active = row < sp.rows;
         const int grow = sp.row0 + row;
-        const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * P;
+        // this row's reference: its factors in visiting order, 2P per (reference, column)
+        const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * (2 * P);
         const float2 *xr = Xc + row;
-        if (row + T < sp.rows) {
+        if (active && row + ROWS < sp.rows) {
             // the next row of this thread: pull its spectrum towards L2 while this one is transformed
-            const float2 *xn = xr + T;
-            for (int j = 0; j <= P; ++j) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
+            const float2 *xn = xr + ROWS;
+            for (int j = role; j <= P; j += 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
         }
         auto getx = [&](int j) {
             float2 v;
@@ -233,13 +377,37 @@ __global__ void __launch_bounds__(128) k_stage2_fast(S2Fast sp, const TwTables t
                          : "l"(xr + (size_t)j * plane));
             return v;
         };
-        auto dinv = [&](int rho) { return __ldg(Dr + rho); };
+        if (active) {
+            if (role == 0) {
+                passA_class0<P1, P2>(getx, slab, ROWS, tw);
+                passA_pairs<P1, P2, 1, SP::PAIRS_A + 1>(getx, slab, ROWS, tw);
+                passA_mid<P1, P2>(getx, slab, ROWS, tw);
+            } else {
+                passA_pairs<P1, P2, SP::PAIRS_A + 1, SP::NPAIRS + 1>(getx, slab, ROWS, tw);
+            }
+        }
+        asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
         float best = -INFINITY;
         int brot = 0;
-        float *cc_out = ccall ? ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N : nullptr;
-        triple_corr<P1, P2>(getx, dinv, slab, T, tw, scale, cc_out, best, brot);
-        ccs[row] = best;
-        ids[row] = grow * sp.N + brot;
+        if (active) {
+            if constexpr (WRITE) {
+                float *cc_out = ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N;
+                if (role == 0) passB_all<P1, P2, 0, SP::LB>(slab, ROWS, tw, Dr, cc_out, best, brot);
+                else passB_all<P1, P2, SP::LB, P2>(slab, ROWS, tw, Dr, cc_out, best, brot);
+            } else {
+                if (role == 0) passB_search<P1, P2, 0, SP::LB>(slab, ROWS, tw, Dr, best, brot);
+                else passB_search<P1, P2, SP::LB, P2>(slab, ROWS, tw, Dr, best, brot);
+            }
+            if (role == 1) { xfer_c[lr] = best; xfer_r[lr] = brot; }
+        }
+        asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
+        if (active && role == 0) {
+            const float oc = xfer_c[lr];
+            const int orot = xfer_r[lr];
+            if (oc > best || (oc == best && orot < brot)) { best = oc; brot = orot; }
+            ccs[row] = best;
+            ids[row] = grow * sp.N + brot;
+        }
     }
     // merge with the particle's running top-8 (lowest id among equal correlations)
     float2 *cp = cand + (size_t)(sp.col0 + cl) * 8;
@@ -383,20 +551,25 @@ static void fill_tw(TwTables &tw, int P)
 
 bool stage2_fast_supported(int P) { return P == 64 || P == 180 || P == 300; }
 
+// the inner factor P2 of the split P = P1 x P2 used for each supported length
+int stage2_fast_p2(int P) { return P == 64 ? 8 : P == 180 ? 15 : P == 300 ? 20 : 0; }
+
 template <int P1, int P2>
 static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
                              float2 *cand, float *ccall, const int *perm)
 {
     TwTables tw;
     fill_tw(tw, P1 * P2);
-    // thread-private slabs of P complex: 128 threads up to P = 200, 64 beyond
-    const int T = P1 * P2 <= 200 ? 128 : 64;
-    const size_t smem = (size_t)P1 * P2 * T * sizeof(float2) + (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_stage2_fast<P1, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // row slabs of P complex: 128 rows in flight up to P = 200, 64 beyond; two threads per row
+    constexpr int ROWS = P1 * P2 <= 200 ? 128 : 64;
+    const size_t smem = (size_t)P1 * P2 * ROWS * sizeof(float2) + (size_t)ROWS * (sizeof(float) + sizeof(int)) +
+                        (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
+    auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, true> : k_stage2_fast<P1, P2, ROWS, false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE2);
-    k_stage2_fast<P1, P2><<<cols, T, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
+    kern<<<cols, 2 * ROWS, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
     return cudaGetLastError();
 }
 

@@ -19,7 +19,11 @@
 //   warp 1   TMEM allocation and the single MMA-issuing thread; accumulators are
 //            double buffered (2 x 128 TMEM columns)
 //   warps 2-5 epilogue: tcgen05.ld of the 128 x 128 accumulator (each warp its
-//            32-lane quadrant), scale by 4, store float2 X[m][col][rs]
+//            32-lane quadrant, 32 columns = 16 complex X per particle at a time)
+//            into a 128B-swizzled staging tile, written out with one TMA bulk
+//            store per 32 x 16 block of X[m][col][rs]; two staging tiles per warp
+//            so the next block is staged while the previous store reads its tile
+// The factor 4 of X is carried by the packed particle operand (exact in BF16).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code,
 // drains its own outstanding copies (bounded), frees its TMEM and returns.
 #include "pftcc_internal.cuh"
@@ -37,8 +41,8 @@ constexpr int U_BN = 128;        // N columns per tile = 64 rs x (re, im)
 constexpr int U_RS = 64;         // (ref, shift) rows per tile
 constexpr int U_THREADS = 192;
 constexpr long long WAIT_LIMIT = 20000000;   // polls of a bounded wait (~seconds)
-constexpr int STAGE_ROW = 36;                 // floats per staged epilogue row: 128 B + 16 B pad
-constexpr int STAGE_BYTES = 4 * 32 * STAGE_ROW * 4;   // four epilogue warps x 32 rows
+constexpr int STAGE_TILE = 32 * 128;          // one staged 32-row x 128-byte block
+constexpr int STAGE_BYTES = 4 * 2 * STAGE_TILE;   // four epilogue warps x two blocks
 
 struct UmmaParams {
     int M;              // m planes of the wave
@@ -109,6 +113,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// TMA bulk store of a 2-D box from shared memory (bulk-group completion)
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, const void *src, int c0, int c1)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+                 :
+                 : "l"((uint64_t)map), "r"(smem_u32(src)), "r"(c0), "r"(c1)
+                 : "memory");
+}
+
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
     // canonical K-major layout without swizzle: start >> 4, LBO (K direction) >> 4,
@@ -156,7 +169,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 
 // ---- the GEMM ------------------------------------------------------------------------
 __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ CUtensorMap tmP,
-                                                              const __grid_constant__ CUtensorMap tmR, UmmaParams up)
+                                                              const __grid_constant__ CUtensorMap tmR,
+                                                              const __grid_constant__ CUtensorMap tmX, UmmaParams up)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -164,7 +178,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     const uint32_t b_bytes = (uint32_t)U_BN * up.KC * 16;
     unsigned char *sA = smem;
     unsigned char *sB = smem + a_bytes;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + (size_t)up.stages * b_bytes);
+    unsigned char *stg = sB + (size_t)up.stages * b_bytes;     // [4 warps][2][32][128 B], 1024-B aligned
+    uint64_t *bars = reinterpret_cast<uint64_t *>(stg + STAGE_BYTES);
     uint64_t *full = bars;                    // [stages]
     uint64_t *empty = bars + up.stages;       // [stages]
     uint64_t *a_full = bars + 2 * up.stages;
@@ -270,43 +285,49 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     } else if (warp >= 2) {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                       // TMEM lane quadrant of this warp
-        float *stage = reinterpret_cast<float *>(bars + 64) + (warp - 2) * 32 * STAGE_ROW;
+        unsigned char *stg_w = stg + (size_t)(warp - 2) * 2 * STAGE_TILE;
+        int sbuf = 0;
         long long tacc = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
             const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
+            // rows of this warp: particles 32q .. 32q+31 of the tile = box rows of X's tensor map
+            const int y0 = m * up.xcols + pt * U_BM + 32 * q;
             for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
                 const int acc = (int)(tacc & 1);
                 // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
                 const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
                 if (!got) { if (lane == 0) fail(6); ok = false; break; }
                 tc_fence_after();
-                // rows of this warp: particles 32q .. 32q+31 of the tile; each 32-column TMEM
-                // chunk is 16 complex X per row, staged through a padded shared tile so that
-                // each warp store writes four whole 128-byte row segments
-                float2 *dst0 = up.X + ((size_t)m * up.xcols + (size_t)pt * U_BM + 32 * q) * up.xrows + (size_t)j * U_RS;
 #pragma unroll 1
                 for (int c = 0; c < U_BN / 32; ++c) {
                     uint32_t r[32];
                     tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r);
-                    float4 *mine = reinterpret_cast<float4 *>(stage + lane * STAGE_ROW);
+                    // the staging tile written two stores ago must have been read out
+                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                    __syncwarp();
+                    // row `lane` of the box, 16-byte chunk e at position e ^ (lane & 7) (128B swizzle)
+                    float4 *row = reinterpret_cast<float4 *>(stg_w + sbuf * STAGE_TILE + lane * 128);
 #pragma unroll
                     for (int e = 0; e < 8; ++e)
-                        mine[e] = make_float4(4.f * __uint_as_float(r[4 * e]), 4.f * __uint_as_float(r[4 * e + 1]),
-                                              4.f * __uint_as_float(r[4 * e + 2]), 4.f * __uint_as_float(r[4 * e + 3]));
+                        row[e ^ (lane & 7)] = make_float4(__uint_as_float(r[4 * e]), __uint_as_float(r[4 * e + 1]),
+                                                          __uint_as_float(r[4 * e + 2]), __uint_as_float(r[4 * e + 3]));
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     __syncwarp();
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int row = 4 * i + (lane >> 3), qv = lane & 7;
-                        const float4 v = reinterpret_cast<const float4 *>(stage + row * STAGE_ROW)[qv];
-                        reinterpret_cast<float4 *>(dst0 + (size_t)row * up.xrows + 16 * c)[qv] = v;
+                    if (lane == 0) {
+                        // x in floats: complex rs = j * U_RS + 16 c, two floats each (a multiple of 32)
+                        tma_store_2d(&tmX, stg_w + sbuf * STAGE_TILE, 2 * (j * U_RS + 16 * c), y0);
+                        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
-                    __syncwarp();
+                    sbuf ^= 1;
                 }
                 tc_fence_before();
                 mbar_arrive(t_empty + acc);
             }
         }
+        // every store has finished reading shared memory and writing X before the CTA exits
+        if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        __syncwarp();
     }
     __syncthreads();
     if (warp == 1) {
@@ -366,7 +387,7 @@ __global__ void k_pack_cols(int M, int Ks, int Kp, int KC, int ptiles, int cols_
         float v = 0.f;
         if (kk < 2 * Ks && col < cols_pad) {
             const float2 b = UB[((size_t)m * cols_pad + col) * Ks + (kk < Ks ? kk : kk - Ks)];
-            v = kk < Ks ? b.x : b.y;
+            v = 4.f * (kk < Ks ? b.x : b.y);      // X = 4 sum_k ...: the power of two splits exactly
         }
         __nv_bfloat16 hi, lo;
         split_bf16(v, hi, lo);
@@ -401,6 +422,25 @@ static int make_map(pftcc_handle *h, CUtensorMap *map, void *base, int KC, long 
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return PFTCC_OK;
+}
+
+// X[M][xcols][xrows] float2 as a 2-D FP32 tensor: x = 2 * rs + (re, im), y = m * xcols + col;
+// boxes of 32 floats (128 B) x 32 rows, 128-byte swizzle (the staging layout of the epilogue)
+static int make_xmap(pftcc_handle *h, CUtensorMap *map, void *X, int xrows, int xcols, int M)
+{
+    auto enc = get_encode();
+    if (!enc) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (((uintptr_t)X & 15) != 0) return set_err(h, PFTCC_ERR_ARG, "X base not 16-byte aligned");
+    if (xrows % 64 != 0 || (long long)xcols * M >= (1LL << 31))
+        return set_err(h, PFTCC_ERR_ARG, "umma stage 1: X extents outside the tensor-map limits");
+    cuuint64_t dims[2] = {(cuuint64_t)2 * xrows, (cuuint64_t)xcols * M};
+    cuuint64_t strides[1] = {(cuuint64_t)xrows * sizeof(float2)};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, X, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled (X) failed: " + std::to_string((int)r));
     return PFTCC_OK;
 }
 
@@ -452,6 +492,9 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     if (st) return st;
     st = make_map(h, &tmR, ws.A16, KC, (long long)M * us.rtiles);
     if (st) return st;
+    CUtensorMap tmX;
+    st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M);
+    if (st) return st;
     UmmaParams up{};
     up.M = M; up.Kp = Kp; up.KC = KC;
     up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
@@ -474,7 +517,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     const int grid = std::min(nitems, us.sms);
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE1);
-    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmP, tmR, up);
+    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmP, tmR, tmX, up);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "umma stage 1 launch");
     return PFTCC_OK;
 }

@@ -723,6 +723,53 @@ int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, cons
     return pftcc_gencorr_grad_for_rot_8(h, iref, iptcl, shvec, irot, &f, grad);
 }
 
+int pftcc_specscore_batch(pftcc_handle *h, int n, const int *iref, const int *iptcl, const int *irot,
+                          const float *shifts, float *scores, float *frcs)
+{
+    if (!h || n < 0 || (n > 0 && (!iref || !iptcl || !irot || !scores)))
+        return set_err(h, PFTCC_ERR_ARG, "specscore: bad arguments");
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    std::vector<FrcReq> rq(n);
+    for (int i = 0; i < n; ++i) {
+        if (iref[i] < 1 || iref[i] > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "specscore: iref out of range");
+        if (irot[i] < 1 || irot[i] > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "specscore: irot out of range");
+        const int sl = slot_of(h, iptcl[i]);
+        if (sl < 0) return set_err(h, PFTCC_ERR_INDEX, "specscore: particle not held");
+        rq[i] = FrcReq{iref[i] - 1, sl, irot[i], shifts ? 1 : 0, shifts ? (double)shifts[2 * i] : 0.0,
+                       shifts ? (double)shifts[2 * i + 1] : 0.0};
+    }
+    const int Ks = h->g.Ks;
+    const size_t rq_bytes = (size_t)n * sizeof(FrcReq), out_floats = (size_t)n * (1 + Ks);
+    ST(ensure(h, (void **)&h->d_dout, &h->dout_cap, rq_bytes + out_floats * sizeof(float) + 256, "specscore"));
+    char *base = (char *)h->d_dout;
+    FrcReq *drq = (FrcReq *)base;
+    float *dscore = (float *)(base + rq_bytes);
+    float *dfrc = dscore + n;
+    CK(cudaMemcpyAsync(drq, rq.data(), rq_bytes, cudaMemcpyHostToDevice, h->stream), "specscore upload");
+    CK(launch_specscore(h, drq, n, frcs ? dfrc : nullptr, dscore), "specscore kernel");
+    CK(cudaMemcpyAsync(scores, dscore, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "specscore");
+    if (frcs)
+        CK(cudaMemcpyAsync(frcs, dfrc, (size_t)n * Ks * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "genfrc");
+    CK(cudaStreamSynchronize(h->stream), "specscore");
+    return PFTCC_OK;
+}
+
+int pftcc_specscore(pftcc_handle *h, int iref, int iptcl, int irot, const float *shvec, float *score)
+{
+    if (!h || !score) return set_err(h, PFTCC_ERR_ARG, "specscore: bad arguments");
+    return pftcc_specscore_batch(h, 1, &iref, &iptcl, &irot, shvec, score, nullptr);
+}
+
+int pftcc_genfrc(pftcc_handle *h, int iref, int iptcl, int irot, const float *shvec, float *frc)
+{
+    if (!h || !frc) return set_err(h, PFTCC_ERR_ARG, "genfrc: bad arguments");
+    float score;
+    return pftcc_specscore_batch(h, 1, &iref, &iptcl, &irot, shvec, &score, frc);
+}
+
 int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
 {
     if (!h || !cc || nshifts < 0 || (nshifts > 0 && !shifts)) return set_err(h, PFTCC_ERR_ARG, "corr_all: bad arguments");
@@ -849,8 +896,8 @@ int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, cons
 {
     if (!h || n < 0 || (n > 0 && (!req || !lb || !ub || !out)) || maxits < 1 || !(pgtol >= 0) || !(factr >= 0))
         return set_err(h, PFTCC_ERR_ARG, "refine_batch: bad arguments");
-    for (int v = 0; v < 3; ++v)
-        if (!(lb[v] <= ub[v])) return set_err(h, PFTCC_ERR_ARG, "refine_batch: empty box");
+    for (long long e = 0; e < 3LL * n; ++e)
+        if (!(lb[e] <= ub[e])) return set_err(h, PFTCC_ERR_ARG, "refine_batch: empty box");
     if (n == 0) return PFTCC_OK;
     std::lock_guard<std::mutex> lk(h->mtx);
     cudaSetDevice(h->dev);

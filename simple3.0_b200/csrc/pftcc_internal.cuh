@@ -50,7 +50,7 @@ struct SearchWS {
     int nshifts = 0, nrs = 0, nrs_pad = 0, np_pad = 0, M = 0, Mpad = 0;
     float2 *UA = nullptr;        // [M][nrs_pad][Ks] ref-side spectra (FP32 path)
     float2 *UB = nullptr;        // [M][np_pad][Ks] particle-side spectra (FP32 path)
-    double2 *RU = nullptr;       // [nrefs][J][Ks] spectra of |ref|^2, J = P/2+1
+    double2 *RU = nullptr;       // [nrefs][J][Ks] spectra of |ref|^2, J = P/2+1; then the same as [nrefs][Ks][J]
     double2 *CV = nullptr;       // [np_pad][J][Ks] spectra of CTF^2
     float *D = nullptr;          // [wave refs][np_pad][P] rotation-dependent normaliser
     float2 *X = nullptr;         // [M][wave rows][wave cols] stage-1 output of one wave
@@ -157,6 +157,9 @@ cudaError_t launch_zero_beyond_kstop(pftcc_handle *h);
 
 // adjoint requests served in one launch (pftcc_capi.cu; caller holds the handle lock)
 int grad_batch_host(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);
+// one genfrc / specscore request (reference frame); iref 0-based, slot = particle slot
+struct FrcReq { int iref, slot, irot, has_shift; double sx, sy; };
+cudaError_t launch_specscore(pftcc_handle *h, const FrcReq *reqs_dev, int nreq, float *frc_dev, float *score_dev);
 // batched bound-constrained quasi-Newton refinement (refine.cu)
 int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub, int maxits,
                  double pgtol, double factr, pftcc_refine_out *out);

@@ -1,279 +1,51 @@
 // refine.cu -- batched continuous refinement of (shift_x, shift_y, defocus) per
-// (reference, particle, rotation) problem by a bound-constrained limited-memory BFGS
-// method, driven on the host, with every round's pending function+gradient requests
-// of all problems served by ONE launch of the adjoint kernel.
-//
-// The reference minimises -corr over the shift with L-BFGS-B in reverse communication
-// (simple_opt_lbfgsb.f90:103-129 drives setulb; the cost is -gencorr_for_rot_8 and the
-// gradient -gencorr_grad_for_rot_8, simple_pftcc_shsrch_grad.f90:85-131), with the
-// defaults factr = 1e7, pgtol = 1e-5, m = 15 (simple_opt_spec.f90:23-24,271).  This
-// driver follows the published algorithm of Byrd, Lu, Nocedal & Zhu (1995, "A limited
-// memory algorithm for bound constrained optimization"): the quasi-Newton matrix B is
-// the BFGS update of theta*I by the stored correction pairs; each iteration finds the
-// generalised Cauchy point along the projected steepest-descent path, minimises the
-// quadratic model over the free variables (direct primal method, backtracked into the
-// box), and line-searches along the resulting direction (here with backtracking on the
-// Armijo condition).  Convergence: projected gradient max-norm <= pgtol, or relative
-// reduction (f_k - f_k+1)/max(|f_k|,|f_k+1|,1) <= factr * machine epsilon.
+// (reference, particle, rotation) problem: the bound-constrained L-BFGS of lbfgsb.h
+// minimises -corr, and every round's pending function+gradient requests of all
+// unfinished problems are served by ONE launch of the adjoint kernel (grad_batch_host).
+// Each problem has its own box, as the reference bounds every particle's shift search
+// around its own prior (simple_pftcc_shsrch_grad.f90:44-68).
 #include "pftcc_internal.cuh"
+#include "lbfgsb.h"
 
-#include <algorithm>
-#include <cfloat>
-#include <cmath>
 #include <vector>
 
 namespace pftcc {
 
-namespace {
-
-constexpr int NV = 3;   // (shift_x, shift_y, defocus)
-
-struct Prob {
-    double x[NV], f = 0, g[NV];
-    double lb[NV], ub[NV];
-    double xt[NV];                        // trial point being evaluated
-    double d[NV], dg0 = 0, alpha = 1;     // line search state
-    int ls_iter = 0;
-    std::vector<double> S, Y;             // stored pairs, NV each
-    double theta = 1.0;
-    int iter = 0, nevals = 0, state = 0;  // 0 start, 1 line search, 2 done
-    int converged = 0;
-};
-
-double proj_grad_norm(const Prob &p)
-{
-    double m = 0;
-    for (int i = 0; i < NV; ++i) {
-        double v = p.x[i] - p.g[i];
-        v = std::min(std::max(v, p.lb[i]), p.ub[i]);
-        m = std::max(m, std::fabs(v - p.x[i]));
-    }
-    return m;
-}
-
-// dense B = BFGS updates of theta*I with the stored pairs (oldest first)
-void form_B(const Prob &p, double B[NV][NV])
-{
-    for (int i = 0; i < NV; ++i)
-        for (int j = 0; j < NV; ++j) B[i][j] = i == j ? p.theta : 0.0;
-    const int np = (int)p.S.size() / NV;
-    for (int q = 0; q < np; ++q) {
-        const double *s = &p.S[q * NV], *y = &p.Y[q * NV];
-        double Bs[NV] = {0, 0, 0}, sBs = 0, ys = 0;
-        for (int i = 0; i < NV; ++i) {
-            for (int j = 0; j < NV; ++j) Bs[i] += B[i][j] * s[j];
-            ys += y[i] * s[i];
-        }
-        for (int i = 0; i < NV; ++i) sBs += s[i] * Bs[i];
-        if (sBs <= 0 || ys <= 0) continue;
-        for (int i = 0; i < NV; ++i)
-            for (int j = 0; j < NV; ++j) B[i][j] += -Bs[i] * Bs[j] / sBs + y[i] * y[j] / ys;
-    }
-}
-
-// generalised Cauchy point, then the subspace minimiser backtracked into the box
-void direction(const Prob &p, double d[NV])
-{
-    double B[NV][NV];
-    form_B(p, B);
-    // breakpoints of the projected path x(t) = P(x - t g)
-    double tb[NV];
-    for (int i = 0; i < NV; ++i) {
-        if (p.g[i] < 0) tb[i] = (p.x[i] - p.ub[i]) / p.g[i];
-        else if (p.g[i] > 0) tb[i] = (p.x[i] - p.lb[i]) / p.g[i];
-        else tb[i] = DBL_MAX;
-        if (tb[i] < 0) tb[i] = 0;
-    }
-    int order[NV] = {0, 1, 2};
-    std::sort(order, order + NV, [&](int a, int b) { return tb[a] < tb[b]; });
-    double xc[NV], dir[NV];
-    bool fixed[NV];
-    for (int i = 0; i < NV; ++i) {
-        xc[i] = p.x[i];
-        fixed[i] = tb[i] == 0;
-        dir[i] = fixed[i] ? 0.0 : -p.g[i];
-    }
-    double tprev = 0;
-    for (int seg = 0; seg <= NV; ++seg) {
-        const double tnext = seg < NV ? tb[order[seg]] : DBL_MAX;
-        if (tnext <= tprev && seg < NV) { fixed[order[seg]] = true; dir[order[seg]] = 0; continue; }
-        // model derivative along dir from xc: f' = g.dir + (xc - x)^T B dir, f'' = dir^T B dir
-        double z[NV], Bd[NV] = {0, 0, 0};
-        for (int i = 0; i < NV; ++i) z[i] = xc[i] - p.x[i];
-        for (int i = 0; i < NV; ++i)
-            for (int j = 0; j < NV; ++j) Bd[i] += B[i][j] * dir[j];
-        double f1 = 0, f2 = 0;
-        for (int i = 0; i < NV; ++i) { f1 += p.g[i] * dir[i] + z[i] * Bd[i]; f2 += dir[i] * Bd[i]; }
-        if (f1 >= 0) break;
-        const double dt = f2 > 0 ? -f1 / f2 : DBL_MAX;
-        if (tprev + dt < tnext) {
-            for (int i = 0; i < NV; ++i) xc[i] += dt * dir[i];
-            break;
-        }
-        if (seg == NV) break;
-        const double step = tnext - tprev;
-        for (int i = 0; i < NV; ++i) xc[i] += step * dir[i];
-        const int v = order[seg];
-        xc[v] = dir[v] < 0 ? p.lb[v] : p.ub[v];
-        fixed[v] = true;
-        dir[v] = 0;
-        tprev = tnext;
-    }
-    for (int i = 0; i < NV; ++i) xc[i] = std::min(std::max(xc[i], p.lb[i]), p.ub[i]);
-    // subspace minimisation over the free variables at the Cauchy point
-    int fr[NV], nf = 0;
-    for (int i = 0; i < NV; ++i)
-        if (xc[i] > p.lb[i] && xc[i] < p.ub[i]) fr[nf++] = i;
-    double xbar[NV] = {xc[0], xc[1], xc[2]};
-    if (nf > 0) {
-        double r[NV];
-        for (int i = 0; i < NV; ++i) {
-            r[i] = p.g[i];
-            for (int j = 0; j < NV; ++j) r[i] += B[i][j] * (xc[j] - p.x[j]);
-        }
-        // solve B_FF du = -r_F (Gaussian elimination with partial pivoting, nf <= 3)
-        double A[NV][NV + 1];
-        for (int a = 0; a < nf; ++a) {
-            for (int b = 0; b < nf; ++b) A[a][b] = B[fr[a]][fr[b]];
-            A[a][nf] = -r[fr[a]];
-        }
-        bool ok = true;
-        for (int c = 0; c < nf && ok; ++c) {
-            int piv = c;
-            for (int a = c + 1; a < nf; ++a)
-                if (std::fabs(A[a][c]) > std::fabs(A[piv][c])) piv = a;
-            if (std::fabs(A[piv][c]) < 1e-300) { ok = false; break; }
-            for (int b = 0; b <= nf; ++b) std::swap(A[c][b], A[piv][b]);
-            for (int a = 0; a < nf; ++a)
-                if (a != c) {
-                    const double fct = A[a][c] / A[c][c];
-                    for (int b = c; b <= nf; ++b) A[a][b] -= fct * A[c][b];
-                }
-        }
-        if (ok) {
-            double du[NV];
-            for (int a = 0; a < nf; ++a) du[a] = A[a][nf] / A[a][a];
-            double amax = 1.0;
-            for (int a = 0; a < nf; ++a) {
-                const int i = fr[a];
-                if (du[a] > 0) amax = std::min(amax, (p.ub[i] - xc[i]) / du[a]);
-                else if (du[a] < 0) amax = std::min(amax, (p.lb[i] - xc[i]) / du[a]);
-            }
-            amax = std::max(amax, 0.0);
-            for (int a = 0; a < nf; ++a) xbar[fr[a]] = xc[fr[a]] + amax * du[a];
-        }
-    }
-    for (int i = 0; i < NV; ++i) d[i] = xbar[i] - p.x[i];
-}
-
-}  // namespace
-
 int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub, int maxits,
                  double pgtol, double factr, pftcc_refine_out *out)
 {
-    const double eps = DBL_EPSILON, ftol = 1e-3;
-    const int mem = 15;
-    std::vector<Prob> P(n);
-    for (int i = 0; i < n; ++i) {
-        for (int v = 0; v < NV; ++v) {
-            P[i].lb[v] = lb[v];
-            P[i].ub[v] = ub[v];
-            P[i].x[v] = std::min(std::max(req[i].x0[v], lb[v]), ub[v]);
-            P[i].xt[v] = P[i].x[v];
-        }
-    }
+    using lbfgsb::NV;
+    std::vector<double> x0((size_t)n * NV);
+    for (int i = 0; i < n; ++i)
+        for (int v = 0; v < NV; ++v) x0[(size_t)i * NV + v] = req[i].x0[v];
     std::vector<pftcc_grad_req> batch;
-    std::vector<int> who;
-    std::vector<double> f, g3;
-    for (int round = 0; round < 64 * std::max(1, maxits); ++round) {
-        batch.clear();
-        who.clear();
-        for (int i = 0; i < n; ++i) {
-            if (P[i].state == 2) continue;
-            batch.push_back(pftcc_grad_req{req[i].iref, req[i].iptcl, req[i].irot, 0, P[i].xt[0], P[i].xt[1], P[i].xt[2]});
-            who.push_back(i);
+    std::vector<double> corr, g3;
+    auto eval = [&](int nb, const int *idx, const double *xt, double *f, double *g) -> int {
+        batch.resize(nb);
+        for (int b = 0; b < nb; ++b) {
+            const pftcc_refine_req &r = req[idx[b]];
+            batch[b] = pftcc_grad_req{r.iref, r.iptcl, r.irot, 0, xt[NV * b], xt[NV * b + 1], xt[NV * b + 2]};
         }
-        if (batch.empty()) break;
-        f.assign(batch.size(), 0.0);
-        g3.assign(3 * batch.size(), 0.0);
-        int st = grad_batch_host(h, (int)batch.size(), batch.data(), f.data(), g3.data());
+        corr.assign(nb, 0.0);
+        g3.assign((size_t)NV * nb, 0.0);
+        const int st = grad_batch_host(h, nb, batch.data(), corr.data(), g3.data());
         if (st != PFTCC_OK) return st;
-        for (size_t b = 0; b < who.size(); ++b) {
-            Prob &p = P[who[b]];
-            const double ft = -f[b];                       // cost = -corr
-            const double gt[NV] = {-g3[3 * b], -g3[3 * b + 1], -g3[3 * b + 2]};
-            ++p.nevals;
-            if (p.state == 0) {
-                p.f = ft;
-                for (int v = 0; v < NV; ++v) p.g[v] = gt[v];
-            } else {
-                // line search: Armijo test at xt = x + alpha d
-                if (ft <= p.f + ftol * p.alpha * p.dg0 || p.ls_iter >= 20) {
-                    if (ft > p.f) {                      // no decrease at all: stop here
-                        p.state = 2;
-                        p.converged = 0;
-                        continue;
-                    }
-                    double s[NV], y[NV], sy = 0, yy = 0;
-                    for (int v = 0; v < NV; ++v) {
-                        s[v] = p.xt[v] - p.x[v];
-                        y[v] = gt[v] - p.g[v];
-                        sy += s[v] * y[v];
-                        yy += y[v] * y[v];
-                    }
-                    const double fold = p.f;
-                    for (int v = 0; v < NV; ++v) { p.x[v] = p.xt[v]; p.g[v] = gt[v]; }
-                    p.f = ft;
-                    ++p.iter;
-                    if (sy > eps * yy) {
-                        p.S.insert(p.S.end(), s, s + NV);
-                        p.Y.insert(p.Y.end(), y, y + NV);
-                        if ((int)p.S.size() > mem * NV) {
-                            p.S.erase(p.S.begin(), p.S.begin() + NV);
-                            p.Y.erase(p.Y.begin(), p.Y.begin() + NV);
-                        }
-                        p.theta = yy / sy;
-                    }
-                    if ((fold - p.f) / std::max(std::max(std::fabs(fold), std::fabs(p.f)), 1.0) <= factr * eps) {
-                        p.state = 2;
-                        p.converged = 1;
-                        continue;
-                    }
-                } else {
-                    // backtrack: safeguarded quadratic interpolation
-                    const double a = p.alpha;
-                    double an = -p.dg0 * a * a / (2.0 * (ft - p.f - p.dg0 * a));
-                    if (!(an > 0.1 * a)) an = 0.1 * a;
-                    if (an > 0.5 * a) an = 0.5 * a;
-                    p.alpha = an;
-                    ++p.ls_iter;
-                    for (int v = 0; v < NV; ++v)
-                        p.xt[v] = std::min(std::max(p.x[v] + p.alpha * p.d[v], p.lb[v]), p.ub[v]);
-                    continue;
-                }
-            }
-            // new iterate: test convergence, compute the next direction
-            if (proj_grad_norm(p) <= pgtol) { p.state = 2; p.converged = 1; continue; }
-            if (p.iter >= maxits) { p.state = 2; p.converged = 0; continue; }
-            direction(p, p.d);
-            p.dg0 = 0;
-            double dn = 0;
-            for (int v = 0; v < NV; ++v) { p.dg0 += p.g[v] * p.d[v]; dn += p.d[v] * p.d[v]; }
-            if (!(p.dg0 < 0) || dn == 0) { p.state = 2; p.converged = proj_grad_norm(p) <= 10 * pgtol; continue; }
-            // first iteration: unit step along the gradient scaled to length one
-            p.alpha = (p.iter == 0 && p.S.empty()) ? std::min(1.0, 1.0 / std::sqrt(dn)) : 1.0;
-            p.ls_iter = 0;
-            for (int v = 0; v < NV; ++v) p.xt[v] = std::min(std::max(p.x[v] + p.alpha * p.d[v], p.lb[v]), p.ub[v]);
-            p.state = 1;
+        for (int b = 0; b < nb; ++b) {             // cost = -corr
+            f[b] = -corr[b];
+            for (int v = 0; v < NV; ++v) g[NV * b + v] = -g3[(size_t)NV * b + v];
         }
-    }
+        return 0;
+    };
+    std::vector<lbfgsb::Result> res(n);
+    const int st = lbfgsb::minimize_batch(n, x0.data(), lb, ub, maxits, pgtol, factr, eval, res.data());
+    if (st != 0) return st;
     for (int i = 0; i < n; ++i) {
         pftcc_refine_out &o = out[i];
-        for (int v = 0; v < NV; ++v) o.x[v] = P[i].x[v];
-        o.f = -P[i].f;
-        o.nevals = P[i].nevals;
-        o.niter = P[i].iter;
-        o.converged = P[i].converged;
+        for (int v = 0; v < NV; ++v) o.x[v] = res[i].x[v];
+        o.f = -res[i].f;
+        o.nevals = res[i].nevals;
+        o.niter = res[i].niter;
+        o.converged = res[i].converged;
         o.pad = 0;
     }
     return PFTCC_OK;

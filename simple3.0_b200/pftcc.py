@@ -221,6 +221,36 @@ class polarft_corrcalc:
                                                    ip.ctypes.data_as(C.POINTER(C.c_int)),
                                                    None if sh is None else _f32p(sh), C.c_void_p(cc_dev_ptr)))
 
+    def genfrc(self, iref: int, iptcl: int, irot: int, shvec=None) -> np.ndarray:
+        """per-shell correlations k = kfrom..kstop at irot (genfrc, or calc_frc with shvec)"""
+        frc = np.zeros(self.cfg.kstop - self.cfg.kfromto[0] + 1, np.float32)
+        sh = None if shvec is None else np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_genfrc(self._h, int(iref), int(iptcl), int(irot), None if sh is None else _f32p(sh),
+                                         _f32p(frc)))
+        return frc
+
+    def specscore(self, iref: int, iptcl: int, irot: int, shvec=None) -> float:
+        """max(0, median shell correlation) at irot (specscore_1, or specscore_2 with shvec)"""
+        out = C.c_float()
+        sh = None if shvec is None else np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_specscore(self._h, int(iref), int(iptcl), int(irot),
+                                            None if sh is None else _f32p(sh), C.byref(out)))
+        return out.value
+
+    def specscore_batch(self, iref, iptcl, irot, shifts=None, want_frc: bool = False):
+        """specscores of many (iref, iptcl, irot) requests in one launch; with want_frc also
+        their shell correlations (n, kstop-kfrom+1)"""
+        ir, ip, ro = (np.ascontiguousarray(np.atleast_1d(v), np.int32) for v in (iref, iptcl, irot))
+        n = ir.size
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(n, 2)
+        scores = np.zeros(n, np.float32)
+        frcs = np.zeros((n, self.cfg.kstop - self.cfg.kfromto[0] + 1), np.float32) if want_frc else None
+        ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self._L.pftcc_specscore_batch(self._h, n, ptr(ir), ptr(ip), ptr(ro),
+                                                  None if sh is None else _f32p(sh), _f32p(scores),
+                                                  None if frcs is None else _f32p(frcs)))
+        return (scores, frcs) if want_frc else scores
+
     def gencorr_for_rot(self, iref: int, iptcl: int, shvec, irot: int) -> float:
         out = C.c_float()
         sh = np.ascontiguousarray(shvec, np.float32)
@@ -305,7 +335,8 @@ class polarft_corrcalc:
 
     def refine_batch(self, iref, iptcl, irot, x0, lb, ub, maxits: int = 100, pgtol: float = 1e-5,
                      factr: float = 1e7):
-        """maximise corr over (shift_x, shift_y, defocus offset) per problem in the box [lb, ub];
+        """maximise corr over (shift_x, shift_y, defocus offset) per problem in its box [lb, ub]
+        (each (3,) for all problems or (n, 3) per problem);
         returns (x (n,3), corr (n,), nevals (n,), niter (n,), converged (n,))"""
         iref, iptcl, irot = (np.atleast_1d(np.asarray(v)) for v in (iref, iptcl, irot))
         x0 = np.asarray(x0, np.float64).reshape(-1, 3)
@@ -317,8 +348,8 @@ class polarft_corrcalc:
             for v in range(3):
                 req[i].x0[v] = float(x0[i, v])
         out = (_lib.RefineOut * n)()
-        lb = np.ascontiguousarray(lb, np.float64)
-        ub = np.ascontiguousarray(ub, np.float64)
+        lb = np.ascontiguousarray(np.broadcast_to(np.asarray(lb, np.float64), (n, 3)))
+        ub = np.ascontiguousarray(np.broadcast_to(np.asarray(ub, np.float64), (n, 3)))
         self._check(self._L.pftcc_refine_batch(self._h, n, req, lb.ctypes.data_as(C.POINTER(C.c_double)),
                                                ub.ctypes.data_as(C.POINTER(C.c_double)), int(maxits), float(pgtol),
                                                float(factr), out))

@@ -76,6 +76,42 @@ def test_gencorrs_matches_oracle(pkg, O, cfgname, frame):
                 assert relerr(got, want) < TOL, (i, r, sh)
 
 
+@pytest.mark.parametrize("cfgname", ["config0", "config1"])
+def test_specscore_matches_oracle(pkg, O, cfgname):
+    """genfrc / calc_frc shell correlations and specscore against the oracle, single
+    and batched, with and without a shift; a reference with itself scores 1"""
+    w = getattr(pkg.synth, cfgname)(nrefs=3, nptcls=3)
+    pc, refs, parts = setup(pkg, w)
+    reqs = []
+    for i in range(3):
+        g, t, c = oracle_ctx(O, w, parts, i)
+        pft = pc.get_ptcl_pft(i + 1)
+        for r in range(3):
+            for irot in (1, 17, w.nrots - 3):
+                for sh in (None, [1.25, -0.75]):
+                    shv = None if sh is None else np.asarray(sh, np.float64)
+                    want_frc = O.genfrc(g, t, refs[r], pft, irot, c, shv)
+                    got_frc = pc.genfrc(r + 1, i + 1, irot, sh)
+                    assert np.max(np.abs(got_frc - want_frc)) < 1e-5, (i, r, irot, sh)
+                    want = O.specscore(g, t, refs[r], pft, irot, c, shv)
+                    assert abs(pc.specscore(r + 1, i + 1, irot, sh) - want) < 1e-5
+                    if sh is not None:
+                        reqs.append((r + 1, i + 1, irot, sh, want, want_frc))
+    scores, frcs = pc.specscore_batch([q[0] for q in reqs], [q[1] for q in reqs], [q[2] for q in reqs],
+                                      np.array([q[3] for q in reqs]), want_frc=True)
+    assert np.max(np.abs(scores - np.array([q[4] for q in reqs]))) < 1e-5
+    assert np.max(np.abs(frcs - np.array([q[5] for q in reqs]))) < 1e-5
+    # self-correlation without CTF: a particle slot holding the reference itself
+    pc2 = pkg.polarft_corrcalc()
+    pc2.new(1, (1, 1), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=False)
+    pc2.set_refs(1, refs[:1], True)
+    pc2.set_ptcl_pft(1, refs[0])
+    assert abs(pc2.specscore(1, 1, 1) - 1.0) < 1e-6
+    with pytest.raises(pkg.PftccError):
+        pc2.specscore(1, 1, w.nrots + 1)
+    pc2.kill()
+
+
 def test_corr_all_and_search_exact(pkg, O):
     w = pkg.synth.config0(nrefs=5, nptcls=7)
     pc, refs, parts = setup(pkg, w)

@@ -1,9 +1,19 @@
 """GPU tests of the adjoint and the continuous refinement (reference frame):
 
 * torch.autograd.gradcheck of the hand-written d corr / d(shift_x, shift_y, defocus)
-  against FP64 finite differences (step 1e-4 px / 1e-4 micron) on 64 particles;
-* the batched bound-constrained quasi-Newton refinement recovers perturbed shifts
-  and defocus offsets, and takes a fraction of the time of an exhaustive GPU grid.
+  against FP64 finite differences (step 1e-4 px / 1e-4 micron) on 64 particles.  The
+  correlation uses |CTF| (the reference's absctfmats), which has a corner at every CTF
+  zero: across a particle's polar samples there are about 1e4 such corners per micron,
+  so a +-1e-4 micron central difference often straddles one and no longer measures the
+  derivative.  The defocus column is therefore gradchecked on the particles whose
+  difference interval contains no corner (found from the oracle's |CTF| and its
+  derivative at both ends); every particle's defocus derivative is compared with the
+  oracle's analytic one in test_gpu_exact.py::test_grad_batch_defocus.
+* the batched bound-constrained quasi-Newton refinement, each problem in its own box,
+  recovers perturbed shifts and reaches the maximum of an exhaustive grid over the box,
+  in a fraction of the grid's time.  The generator's defocus is not the maximiser of the
+  correlation at the nearest discrete rotation (the residual in-plane angle moves it by
+  up to ~0.3 micron), so defocus is judged by the grid, not by the generator.
 """
 import math
 import time
@@ -37,7 +47,21 @@ def true_pose(w, parts, i):
     return irot, sh
 
 
-def test_gradcheck_shift_defocus(pkg):
+def ctf_corner_free(O, w, parts, i, ddf, eps):
+    """True when no polar sample's CTF crosses zero for defocus offsets in [ddf-eps, ddf+eps]:
+    d|CTF|/d(defocus) keeps its sign at every sample where |CTF| is small"""
+    g = O.geom(w.nrots, w.kfrom, w.kto, w.box)
+    t = O.tables(g)
+    ends = []
+    for s in (-1.0, 1.0):
+        cp = O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]) + ddf + s * eps,
+                        float(parts.dfy[i]) + ddf + s * eps, float(parts.angast[i]))
+        ends.append((O.ctfmat(g, t, cp), O.dctfmat_ddf(g, t, cp)))
+    (c0, d0), (c1, d1) = ends
+    return not np.any((np.sign(d0) != np.sign(d1)) & (c0 < 0.5) & (c1 < 0.5))
+
+
+def test_gradcheck_shift_defocus(pkg, O):
     import torch
     from simple3_0_b200.autograd import ShiftDefocusCorr
     n = 64
@@ -46,10 +70,19 @@ def test_gradcheck_shift_defocus(pkg):
     iref = parts.ref + 1
     iptcl = np.arange(1, n + 1)
     irot = rng.integers(1, w.nrots + 1, n)
-    x = torch.tensor(np.c_[rng.uniform(-2, 2, (n, 2)), rng.uniform(-0.1, 0.1, n)], dtype=torch.float64,
-                     requires_grad=True)
-    fn = lambda x_: ShiftDefocusCorr.apply(x_, pc, iref, iptcl, irot)
-    assert torch.autograd.gradcheck(fn, (x,), eps=1e-4, atol=2e-5, rtol=1e-3)
+    x = np.c_[rng.uniform(-2, 2, (n, 2)), rng.uniform(-0.1, 0.1, n)]
+    # shifts: all particles, defocus held
+    xs = torch.tensor(x[:, :2], dtype=torch.float64, requires_grad=True)
+    ddf = torch.tensor(x[:, 2:], dtype=torch.float64)
+    fs = lambda xs_: ShiftDefocusCorr.apply(torch.cat([xs_, ddf], 1), pc, iref, iptcl, irot)
+    assert torch.autograd.gradcheck(fs, (xs,), eps=1e-4, atol=2e-5, rtol=1e-3)
+    # defocus: the particles whose difference interval straddles no |CTF| corner
+    sub = np.array([i for i in range(n) if ctf_corner_free(O, w, parts, i, x[i, 2], 1e-4)])
+    assert sub.size >= 16
+    sh = torch.tensor(x[sub, :2], dtype=torch.float64)
+    xd = torch.tensor(x[sub, 2:], dtype=torch.float64, requires_grad=True)
+    fd = lambda xd_: ShiftDefocusCorr.apply(torch.cat([sh, xd_], 1), pc, iref[sub], iptcl[sub], irot[sub])
+    assert torch.autograd.gradcheck(fd, (xd,), eps=1e-4, atol=2e-5, rtol=1e-3)
 
 
 def test_refine_recovers_shift_and_defocus(pkg):
@@ -73,13 +106,23 @@ def test_refine_recovers_shift_and_defocus(pkg):
     print(f"refine: median shift error {np.median(dsh):.3f} px, median defocus error {np.median(ddf):.4f} um, "
           f"median evaluations {np.median(nev):.0f}, converged {conv.mean():.2f}")
     assert np.median(dsh) < 0.25 and np.mean(dsh < 0.5) > 0.8
-    assert np.median(ddf) < 0.02
+    # the refined point is the best of a local exhaustive grid (0.05 px, 0.01 micron) around it
+    gx = np.arange(-2, 3) * 0.05
+    gd = np.arange(-2, 3) * 0.01
+    for i in range(n):
+        SX, SY, DD = np.meshgrid(x[i, 0] + gx, x[i, 1] + gx, x[i, 2] + gd, indexing="ij")
+        keep = (SX >= lb[0]) & (SX <= ub[0]) & (SY >= lb[1]) & (SY <= ub[1]) & (DD >= lb[2]) & (DD <= ub[2])
+        fg, _ = pc.grad_batch(np.full(keep.sum(), parts.ref[i] + 1), np.full(keep.sum(), i + 1),
+                              np.full(keep.sum(), irot[i]), SX[keep], SY[keep], DD[keep])
+        assert f[i] >= fg.max() - 1e-5, (i, f[i], fg.max())
 
 
 def test_refine_faster_than_exhaustive_grid(pkg):
     """the same problems on an exhaustive GPU grid (0.1 px, 0.02 micron) of the same box
     around the start: the refinement must reach at least the grid's best value in a
-    quarter of its time"""
+    quarter of its time.  The correlation has several maxima in defocus (about 0.09
+    micron apart at these shells), so each problem is refined from four defocus starts
+    spread over the box, all in the same batch, and keeps its best end point."""
     n = 16
     rng = np.random.default_rng(9)
     delta = rng.uniform(-0.1, 0.1, n)
@@ -101,10 +144,17 @@ def test_refine_faster_than_exhaustive_grid(pkg):
                              SX.ravel(), SY.ravel(), DD.ravel())
         best_grid[i] = f.max()
     t_grid = time.perf_counter() - t0
+    starts = np.array([-0.15, -0.05, 0.05, 0.15])
+    ns0 = starts.size
+    xs = np.repeat(x0, ns0, axis=0)
+    xs[:, 2] += np.tile(starts, n)
     t0 = time.perf_counter()
-    x, f, nev, nit, conv = pc.refine_batch(parts.ref + 1, np.arange(1, n + 1), irot, x0, x0 - half, x0 + half,
-                                           maxits=100)
+    xa, fa, neva, nit, conv = pc.refine_batch(np.repeat(parts.ref + 1, ns0), np.repeat(np.arange(1, n + 1), ns0),
+                                              np.repeat(irot, ns0), xs, np.repeat(x0 - half, ns0, axis=0),
+                                              np.repeat(x0 + half, ns0, axis=0), maxits=100)
     t_ref = time.perf_counter() - t0
+    f = fa.reshape(n, ns0).max(1)
+    nev = neva.reshape(n, ns0).sum(1)
     print(f"exhaustive grid {t_grid:.3f} s ({gx.size ** 2 * gd.size} points/problem), refinement {t_ref:.3f} s "
           f"(median {np.median(nev):.0f} evaluations/problem)")
     assert np.mean(f >= best_grid - 1e-4) > 0.9

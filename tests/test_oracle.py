@@ -212,3 +212,50 @@ def test_cpu_search_finds_best(O):
         r, s, rot = np.unravel_index(np.argmax(allcc), allcc.shape)
         assert (br[i], bs[i], bro[i]) == (r, s, rot + 1)
         assert abs(bcc[i] - allcc.max()) < 1e-5
+
+
+@pytest.mark.parametrize("geom", GEOMS)
+def test_specscore_self_is_one(O, geom):
+    """genfrc of a reference with itself at irot = 1: every shell FRC is 1, specscore 1"""
+    g = O.geom(*geom)
+    t = O.tables(g)
+    ref = rand_pft(np.random.default_rng(21), g.K, g.pftsz)
+    frc = O.genfrc(g, t, ref, ref, 1)
+    assert np.allclose(frc, 1.0, atol=1e-12)
+    assert abs(O.specscore(g, t, ref, ref, 1) - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("geom", GEOMS)
+def test_genfrc_shells_recombine_to_gencorrs(O, geom):
+    """sum_k frc_k sqrt(|p_k|^2 |r_k|^2) / sqrt(sum|p|^2 sum|r|^2) = gencorrs at that rotation
+    (both are the same per-shell sums, calc_k_corrs / calc_corrs_over_k), with CTF and shift"""
+    g = O.geom(*geom)
+    t = O.tables(g)
+    rng = np.random.default_rng(22)
+    ref = rand_pft(rng, g.K, g.pftsz)
+    ptcl = (0.5 * ref + rand_pft(rng, g.K, g.pftsz)).astype(np.complex64)
+    ctf = O.ctfmat(g, t, O.make_ctf(dfx=1.9, dfy=1.7, angast=10.0))
+    sh = [0.6, -0.9]
+    cc = O.gencorrs(g, t, ref, ptcl, ctf, sh)
+    prep = ref.astype(np.complex128) * ctf * O.shmat(g, t, *sh)
+    sp = np.sum(np.abs(ptcl.astype(np.complex128)) ** 2, axis=1)
+    sr = np.sum(np.abs(prep) ** 2, axis=1)
+    for irot in (1, 7, g.nrots // 2 + 3):
+        frc = O.genfrc(g, t, ref, ptcl, irot, ctf, sh)
+        rec = np.sum(frc * np.sqrt(sp * sr)) / math.sqrt(sp.sum() * sr.sum())
+        assert abs(rec - cc[irot - 1]) < 1e-12
+
+
+@pytest.mark.parametrize("kto", [20, 21])
+def test_specscore_is_clamped_median(O, kto):
+    """odd and even shell counts: the middle value / the mean of the two middle values
+    (median_nocopy), clamped at zero"""
+    g = O.geom(128, 2, kto, 64)
+    t = O.tables(g)
+    rng = np.random.default_rng(23 + kto)
+    ref = rand_pft(rng, g.K, g.pftsz)
+    for mix in (0.8, 0.0):
+        ptcl = (mix * ref + rand_pft(rng, g.K, g.pftsz)).astype(np.complex64)
+        for irot in (1, 40):
+            frc = O.genfrc(g, t, ref, ptcl, irot)
+            assert abs(O.specscore(g, t, ref, ptcl, irot) - max(0.0, float(np.median(frc)))) < 1e-14
