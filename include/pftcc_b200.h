@@ -181,6 +181,26 @@ typedef struct { double x[3]; double f; int nevals, niter, converged, pad; } pft
 int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub,
                        int maxits, double pgtol, double factr, pftcc_refine_out *out);
 
+/* stochastic neighbourhood hill climbing over the references for every held particle
+ * (strategy2D_snhc srch_snhc, simple_strategy2D_snhc.f90:33-93, with shcloc,
+ * simple_rnd.f90:273-295): order is [nptcls][nrefs] (slot order; each row the particle's
+ * 1-based reference visiting order, s2D%srch_order), prev_corr [nptcls] the particle's
+ * previous best correlation, cls_pops [nrefs] the class populations (0 = empty, skipped
+ * after being counted) or NULL, nrefs_bound the visit limit (the reference's
+ * max(2, min(nrefs, nint(nrefs * (1 - stoch_bound))))).  Every visited reference is
+ * correlated over all rotations without shift (gencorrs); shcloc's uniform pick among the
+ * rotations with corr >= prev_corr ends the search (found_better = 1), otherwise the
+ * greedy best of the visited references is returned.  The random draw of visit isample
+ * of particle iptcl is splitmix64(seed + iptcl * 0x9E3779B97F4A7C15 + isample *
+ * 0xD1B54A32D192ED03) -> u in [0,1), selecting the floor(u * count)-th improving
+ * rotation in rotation order.  precision: PFTCC_PREC_EXACT (the exact kernel, handle's
+ * CTF frame) or the m-domain FP32 / BF16X3 paths (particle frame only).  The correlations
+ * of all held particles are kept on the device (nptcls * nrefs * nrots floats, at most
+ * 32 GiB). */
+typedef struct { int iref, irot, found_better, nrefs_eval; float corr; int pad[3]; } pftcc_snhc_out;
+int pftcc_search_snhc(pftcc_handle *h, const int *order, const float *prev_corr, const int *cls_pops, int nrefs_bound,
+                      unsigned long long seed, int precision, pftcc_snhc_out *out);
+
 /* gencorrs for npairs (reference, particle, shift) pairs that allocates no memory, for
  * callers that cannot let a library call cudaMalloc (work being captured into a CUDA
  * graph, applications that budget all device memory in their own pool, services

@@ -73,6 +73,10 @@ def lib():
         L.orc_genfrc.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp]
         L.orc_specscore.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp]
         L.orc_specscore.restype = C.c_double
+        L.orc_snhc_select.argtypes = [C.c_int, C.c_int, fp, ip, ip, C.c_int, C.c_double, C.c_ulonglong, C.c_int, ip]
+        L.orc_snhc_select.restype = C.c_double
+        L.orc_snhc_uniform.argtypes = [C.c_ulonglong, C.c_int, C.c_int]
+        L.orc_snhc_uniform.restype = C.c_double
         L.orc_polarize.argtypes = [G, fp, fp, C.c_int, dp]
         L.orc_kb_apod.argtypes = [C.c_double]
         L.orc_kb_apod.restype = C.c_double
@@ -193,6 +197,22 @@ def specscore(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=None) ->
     return lib().orc_specscore(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
                                _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double), int(irot),
                                _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double))
+
+
+def snhc_select(corrs, order, prev_corr: float, nrefs_bound: int, seed: int, iptcl: int, pops=None):
+    """srch_snhc + shcloc over corrs[nrefs, nrots] for one particle: (iref, irot, found_better,
+    nrefs_eval, corr), iref/irot 1-based"""
+    c = np.ascontiguousarray(corrs, np.float32)
+    o = np.ascontiguousarray(order, np.int32)
+    pp = None if pops is None else np.ascontiguousarray(pops, np.int32)
+    out = np.zeros(4, np.int32)
+    v = lib().orc_snhc_select(c.shape[1], c.shape[0], _P(c, C.c_float), _P(o, C.c_int), _P(pp, C.c_int),
+                              int(nrefs_bound), float(prev_corr), int(seed), int(iptcl), _P(out, C.c_int))
+    return int(out[0]), int(out[1]), int(out[2]), int(out[3]), float(v)
+
+
+def snhc_uniform(seed: int, iptcl: int, isample: int) -> float:
+    return lib().orc_snhc_uniform(int(seed), int(iptcl), int(isample))
 
 
 def polarize(g: Geom, t: Tables, cmat, griddev=False) -> np.ndarray:

@@ -246,6 +246,57 @@ double orc_specscore(const orc_geom *g, const float *ref, const float *ptcl, con
     return med > 0.0 ? med : 0.0;
 }
 
+double orc_snhc_uniform(unsigned long long seed, int iptcl, int isample)
+{
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(unsigned)iptcl +
+                           0xD1B54A32D192ED03ULL * (unsigned long long)(unsigned)isample;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+double orc_snhc_select(int nrots, int nrefs, const float *corrs, const int *order, const int *pops, int nrefs_bound,
+                       double prev_corr, unsigned long long seed, int iptcl, int *out4)
+{
+    const float pf = (float)prev_corr;
+    double cc_glob = -HUGE_VAL;
+    int class_glob = 0, inpl_glob = 0, neval = 0, found = 0, best_ref = 0, best_rot = 0;
+    double best_corr = 0.0;
+    for (int isample = 1; isample <= nrefs; ++isample) {
+        const int iref = order[isample - 1];
+        ++neval;
+        if (neval > nrefs_bound) break;
+        if (pops && pops[iref - 1] == 0) continue;
+        const float *c = corrs + (size_t)(iref - 1) * nrots;
+        /* shcloc: the rotations whose difference to the previous best is not negative */
+        int navail = 0;
+        for (int r = 0; r < nrots; ++r) navail += !(c[r] < pf);
+        int inpl;
+        double inpl_corr;
+        if (navail == 0) {
+            inpl = 0;   /* maxloc: the first maximum */
+            for (int r = 1; r < nrots; ++r)
+                if (c[r] > c[inpl]) inpl = r;
+            inpl_corr = c[inpl];
+        } else {
+            int k = (int)(orc_snhc_uniform(seed, iptcl, isample) * navail);
+            if (k >= navail) k = navail - 1;
+            inpl = -1;
+            for (int r = 0; r < nrots; ++r)
+                if (!(c[r] < pf) && k-- == 0) { inpl = r; break; }
+            inpl_corr = c[inpl];
+            best_ref = iref; best_rot = inpl + 1; best_corr = inpl_corr;
+            found = 1;
+        }
+        if (inpl_corr > cc_glob) { cc_glob = inpl_corr; class_glob = iref; inpl_glob = inpl + 1; }
+        if (found) break;
+    }
+    if (!found) { best_ref = class_glob; best_rot = inpl_glob; best_corr = class_glob ? cc_glob : 0.0; }
+    out4[0] = best_ref; out4[1] = best_rot; out4[2] = found; out4[3] = neval;
+    return best_corr;
+}
+
 /* gencorr_cc_for_rot_8 (:1690-1733).  match_filt: unweighted sums normalised by
  * sqsum over kfrom..kstop (:1729-1731).  Otherwise the shell-weighted ("jacobian")
  * form sum_k k*corr_k / sqrt(sum_k k|ref_k|^2 * sum_k k|ptcl_k|^2) (:1717-1727). */

@@ -99,6 +99,23 @@ void orc_genfrc(const orc_geom *g, const float *ref, const float *ptcl, const do
 double orc_specscore(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
                      const double *shvec, int irot, const double *argtransf, const double *argtransf_shellone);
 
+/* stochastic neighbourhood hill climbing for one particle (strategy2D_snhc srch_snhc,
+ * simple_strategy2D_snhc.f90:33-93) over given per-rotation correlations
+ * corrs[nrefs][nrots] (reference iref at row iref-1): references visited in order[]
+ * (1-based), counting every visit against nrefs_bound (empty classes, pops[iref-1] == 0,
+ * are skipped after being counted); for each, shcloc (simple_rnd.f90:273-295): a uniformly
+ * random rotation among those with corr >= prev_corr -- the k-th such rotation in rotation
+ * order, k = floor(u * count) with u = orc_snhc_uniform(seed, iptcl, isample) -- ending the
+ * search (found_better = 1); otherwise the greedy best rotation, tracked as the global best
+ * returned when no reference improves.  The comparison corr - prev_corr < 0 of the
+ * reference's single precision is corr < prev_corr with prev_corr rounded to float.
+ * out4 = {iref, irot (1-based), found_better, nrefs_eval}; the return value is the chosen
+ * correlation. */
+double orc_snhc_select(int nrots, int nrefs, const float *corrs, const int *order, const int *pops, int nrefs_bound,
+                       double prev_corr, unsigned long long seed, int iptcl, int *out4);
+/* the uniform deviate of draw isample for particle iptcl: splitmix64 of a Weyl sequence */
+double orc_snhc_uniform(unsigned long long seed, int iptcl, int isample);
+
 /* d|CTF|/d(mean defocus) in 1/micron, with dfx and dfy both moved by the same amount */
 void orc_dctfmat_ddf(const orc_geom *g, const float *polar, const orc_ctf *c, double *dctfmat);
 

@@ -46,6 +46,11 @@ class RefineOut(C.Structure):
                 ("converged", C.c_int), ("pad", C.c_int)]
 
 
+class SnhcOut(C.Structure):
+    _fields_ = [("iref", C.c_int), ("irot", C.c_int), ("found_better", C.c_int), ("nrefs_eval", C.c_int),
+                ("corr", C.c_float), ("pad", C.c_int * 3)]
+
+
 # every exported entry point with its argument types (restype is int unless noted)
 _h = C.c_void_p
 _fp, _dp, _ip, _vp = C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
@@ -85,6 +90,7 @@ SIGNATURES = {
     "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
                            C.POINTER(RefineOut)],
     "pftcc_gencorrs_noalloc": [_h, C.c_int, _ip, _ip, _fp, _vp],
+    "pftcc_search_snhc": [_h, _ip, _fp, _ip, C.c_int, C.c_ulonglong, C.c_int, C.POINTER(SnhcOut)],
     "pftcc_get_nrots": [_h, _ip],
     "pftcc_get_pftsz": [_h, _ip],
     "pftcc_get_pdim": [_h, _ip],

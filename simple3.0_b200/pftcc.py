@@ -312,6 +312,22 @@ class polarft_corrcalc:
         dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("ishift", np.int32), ("corr", np.float32)])
         return np.frombuffer(out, dtype=dt).copy()
 
+    def search_snhc(self, order, prev_corr, nrefs_bound: int, seed: int, cls_pops=None, precision="exact"):
+        """stochastic neighbourhood hill climbing (srch_snhc + shcloc) for every held particle:
+        order (nptcls, nrefs) 1-based visiting orders, prev_corr (nptcls,); returns a structured
+        array (iref, irot, found_better, nrefs_eval, corr) per particle slot"""
+        n = self.get_nptcls()
+        o = np.ascontiguousarray(order, np.int32).reshape(n, self.cfg.nrefs)
+        pv = np.ascontiguousarray(prev_corr, np.float32).reshape(n)
+        pops = None if cls_pops is None else np.ascontiguousarray(cls_pops, np.int32).reshape(self.cfg.nrefs)
+        out = (_lib.SnhcOut * n)()
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self._L.pftcc_search_snhc(self._h, ip(o), _f32p(pv), None if pops is None else ip(pops),
+                                              int(nrefs_bound), int(seed) & ((1 << 64) - 1), _PRECS[precision], out))
+        dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("found_better", np.int32), ("nrefs_eval", np.int32),
+                       ("corr", np.float32), ("pad", np.int32, 3)])
+        return np.frombuffer(out, dtype=dt).copy()
+
     def search_best_dev(self, shifts, precision, ntop: int, out_dev_ptr: int):
         sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
         ns = 0 if sh is None else sh.shape[0]

@@ -259,3 +259,41 @@ def test_specscore_is_clamped_median(O, kto):
         for irot in (1, 40):
             frc = O.genfrc(g, t, ref, ptcl, irot)
             assert abs(O.specscore(g, t, ref, ptcl, irot) - max(0.0, float(np.median(frc)))) < 1e-14
+
+
+def test_snhc_first_improvement_and_greedy_fallback(O):
+    """srch_snhc + shcloc: with prev_corr below everything the first visited (non-empty)
+    reference improves and its rotation is the draw's pick among all rotations; with
+    prev_corr above everything no reference improves and the greedy best over the first
+    nrefs_bound visited references is kept; empty classes count against the bound"""
+    rng = np.random.default_rng(31)
+    nrefs, nrots = 12, 40
+    corrs = rng.uniform(-0.2, 0.9, (nrefs, nrots)).astype(np.float32)
+    order = rng.permutation(nrefs) + 1
+    iref, irot, found, neval, cc = O.snhc_select(corrs, order, -1.0, 6, 7, 5)
+    k = int(O.snhc_uniform(7, 5, 1) * nrots)
+    assert (iref, irot, found, neval) == (order[0], k + 1, 1, 1) and cc == corrs[order[0] - 1, k]
+    iref, irot, found, neval, cc = O.snhc_select(corrs, order, 2.0, 6, 7, 5)
+    sub = corrs[order[:6] - 1]
+    best_row = int(np.argmax(sub.max(1)))
+    assert (iref, irot, found, neval) == (order[best_row], int(np.argmax(sub[best_row])) + 1, 0, 7)
+    pops = np.ones(nrefs, np.int32)
+    pops[order[0] - 1] = 0
+    iref, irot, found, neval, cc = O.snhc_select(corrs, order, -1.0, 6, 7, 5, pops)
+    k = int(O.snhc_uniform(7, 5, 2) * nrots)
+    assert (iref, irot, found, neval) == (order[1], k + 1, 1, 2)
+
+
+def test_snhc_pick_is_uniform_over_improving_rotations(O):
+    """shcloc draws uniformly among the rotations with corr >= prev_corr"""
+    nrots = 20
+    corrs = np.full((1, nrots), 0.1, np.float32)
+    good = [2, 5, 11, 17]
+    corrs[0, good] = 0.5
+    counts = np.zeros(nrots, int)
+    for seed in range(4000):
+        iref, irot, found, neval, cc = O.snhc_select(corrs, [1], 0.3, 1, seed, 3)
+        assert found == 1 and cc == np.float32(0.5)
+        counts[irot - 1] += 1
+    assert set(np.flatnonzero(counts)) == set(good)
+    assert np.all(np.abs(counts[good] - 1000) < 120)
