@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1;
     double2 *tw = reinterpret_cast<double2 *>(smem4);   // [N] w_N^{-e}
-    float2 *a = reinterpret_cast<float2 *>(tw + N);      // [Ks][P]
+    float2 *a = reinterpret_cast<float2 *>(tw + N);      // [P][Ks]: the threads of a DFT step read consecutive k
     const int row = blockIdx.x;                          // local row
     const int rs = rs0 + row;
     float2 *dst = UA;
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
         for (int k = 0; k < Ks; ++k) {
             const float2 x = R[(size_t)k * P + n];
             const float fr = (float)sr, fi = (float)si;
-            a[k * P + n] = make_float2(x.x * fr - x.y * fi, x.x * fi + x.y * fr);
+            a[n * Ks + k] = make_float2(x.x * fr - x.y * fi, x.x * fi + x.y * fr);
             const double nr = sr * vr - si * vi, ni = sr * vi + si * vr;
             sr = nr; si = ni;
         }
@@ -128,20 +128,20 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref(
     __syncthreads();
     for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
         const int m = e / Ks, k = e - m * Ks;
-        const float2 *ak = a + k * P;
+        const float2 *ak = a + k;
         // FP64 twiddles and accumulation: the spectra carry no more than the operands' FP32 rounding
         double ur = 0.0, ui = 0.0;
         int idx = 0;
         if (m & 1) {
             for (int n = 0; n < P; ++n) {
-                const double v = ak[n].y;
+                const double v = ak[n * Ks].y;
                 ur = fma(v, tw[idx].x, ur);
                 ui = fma(v, tw[idx].y, ui);
                 idx += m; if (idx >= N) idx -= N;
             }
         } else {
             for (int n = 0; n < P; ++n) {
-                const double v = ak[n].x;
+                const double v = ak[n * Ks].x;
                 ur = fma(v, tw[idx].x, ur);
                 ui = fma(v, tw[idx].y, ui);
                 idx += m; if (idx >= N) idx -= N;
@@ -161,8 +161,8 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
     double2 *tw = reinterpret_cast<double2 *>(smem4);  // [N]
-    float2 *b = reinterpret_cast<float2 *>(tw + N);     // [Ks][P]
-    float *c2 = reinterpret_cast<float *>(b + Ks * P);  // [Ks][P]
+    float2 *b = reinterpret_cast<float2 *>(tw + N);     // [P][Ks]: DFT steps read consecutive k
+    float *c2 = reinterpret_cast<float *>(b + Ks * P);  // [P][Ks]
     const int col = blockIdx.x;
     if (col >= ncols) {
         for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
@@ -184,33 +184,35 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     for (int e = threadIdx.x; e < Ks * P; e += blockDim.x) {
         const float c = C ? C[e] : 1.f;
         const float2 q = Q[e];
-        b[e] = make_float2(c * q.x, c * q.y);
-        c2[e] = c * c;
+        const int k = e / P, n = e - k * P;
+        b[n * Ks + k] = make_float2(c * q.x, c * q.y);
+        c2[n * Ks + k] = c * c;
     }
     if (threadIdx.x == 0) sqp_out[col] = sqsums[slot];
     __syncthreads();
     for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
         const int m = e / Ks, k = e - m * Ks;
-        const float2 *bk = b + k * P;
+        const float2 *bk = b + k;
         double ur = 0.0, ui = 0.0;
         int idx = 0;
         for (int n = 0; n < P; ++n) {
-            const double v = (m & 1) ? bk[n].y : bk[n].x;
+            const double v = (m & 1) ? bk[n * Ks].y : bk[n * Ks].x;
             ur = fma(v, tw[idx].x, ur);
             ui = fma(v, tw[idx].y, ui);
             idx += m; if (idx >= N) idx -= N;
         }
         UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2((float)ur, (float)ui);
     }
-    // CTF^2 spectra over P points in FP64: w_P^{-jn} = w_N^{-2jn}
+    // CTF^2 spectra over P points in FP64: w_P^{-jn} = w_N^{-2jn}, read from the w_N table
     for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
         const int j = e / Ks, k = e - j * Ks;
         double ur = 0.0, ui = 0.0;
+        int idx = 0;
         for (int n = 0; n < P; ++n) {
-            double sn, cs;
-            sincospi(-2.0 * (double)((j * n) % P) / P, &sn, &cs);
-            ur += (double)c2[k * P + n] * cs;
-            ui += (double)c2[k * P + n] * sn;
+            const double v = (double)c2[n * Ks + k];
+            ur = fma(v, tw[idx].x, ur);
+            ui = fma(v, tw[idx].y, ui);
+            idx += 2 * j; if (idx >= N) idx -= N;
         }
         CV[(size_t)col * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
     }

@@ -141,12 +141,14 @@ __device__ __forceinline__ void passA_class0(const GetX &getx, float2 *slab, int
     for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1) * T] = z[l2];
 }
 
-template <int P1, int P2, int C0, int C1, class GetX>
-__device__ __forceinline__ void passA_pairs(const GetX &getx, float2 *slab, int T, const TwTables &tw)
+// the class-pair loop runs over a runtime range (one copy of its code for both halves of
+// a row's transform); c * l2 < P1 * P2 for every class and pass-B index, so the twiddle
+// indices need no reduction
+template <int P1, int P2, class GetX>
+__device__ __forceinline__ void passA_pairs(int c0, int c1, const GetX &getx, float2 *slab, int T, const TwTables &tw)
 {
-    constexpr int P = P1 * P2;
-#pragma unroll
-    for (int c = C0; c < C1; ++c) {
+#pragma unroll 1
+    for (int c = c0; c < c1; ++c) {
         float2 xa[P2], xb[P2];
 #pragma unroll
         for (int j2 = 0; j2 < P2; ++j2) {
@@ -163,8 +165,8 @@ __device__ __forceinline__ void passA_pairs(const GetX &getx, float2 *slab, int 
         SFFT<P2, P1>::run(zb, tw);
 #pragma unroll
         for (int l2 = 0; l2 < P2; ++l2) {
-            slab[(l2 * P1 + c) * T] = l2 == 0 ? za[l2] : c_mul(za[l2], tw.wP[(c * l2) % P]);
-            slab[(l2 * P1 + P1 - c) * T] = l2 == 0 ? zb[l2] : c_mul(zb[l2], tw.wP[((P1 - c) * l2) % P]);
+            slab[(l2 * P1 + c) * T] = l2 == 0 ? za[l2] : c_mul(za[l2], tw.wP[c * l2]);
+            slab[(l2 * P1 + P1 - c) * T] = l2 == 0 ? zb[l2] : c_mul(zb[l2], tw.wP[(P1 - c) * l2]);
         }
     }
 }
@@ -188,9 +190,9 @@ __device__ __forceinline__ void passA_mid(const GetX &getx, float2 *slab, int T,
 }
 
 // pass B for l2 in [L0, L1): length-P1 DFTs, correlations, argmax (lowest rotation on ties)
-template <int P1, int P2, int L0, int L1, class Dinv>
-__device__ __forceinline__ void passB(const float2 *slab, int T, const TwTables &tw, const Dinv &dinv, float scale,
-                                      float *cc_out, float &best, int &brot)
+template <int P1, int P2, class Dinv>
+__device__ __forceinline__ void passB(int L0, int L1, const float2 *slab, int T, const TwTables &tw, const Dinv &dinv,
+                                      float scale, float *cc_out, float &best, int &brot)
 {
     constexpr int P = P1 * P2;
 #pragma unroll 1
@@ -239,9 +241,9 @@ __device__ __forceinline__ void load_dblock(const float *Dp, int l2, float (&d)[
 // fmaxf; afterwards the winning block -- every block when another one reached the same
 // maximum -- is evaluated again by the same loop body (identical values) and scanned
 // for the lowest rotation holding the maximum.
-template <int P1, int P2, int L0, int L1>
-__device__ __forceinline__ void passB_search(const float2 *slab, int T, const TwTables &tw, const float *Dp,
-                                             float &best, int &brot)
+template <int P1, int P2>
+__device__ __forceinline__ void passB_search(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
+                                             const float *Dp, float &best, int &brot)
 {
     float bv = -INFINITY;
     int bl2 = -1, l2 = L0, lend = L1, stage = 0, rmin = 0x7fffffff;
@@ -283,9 +285,9 @@ __device__ __forceinline__ void passB_search(const float2 *slab, int T, const Tw
 }
 
 // pass B writing every correlation (corr_all), with the per-rotation argmax
-template <int P1, int P2, int L0, int L1>
-__device__ __forceinline__ void passB_all(const float2 *slab, int T, const TwTables &tw, const float *Dp,
-                                          float *cc_out, float &best, int &brot)
+template <int P1, int P2>
+__device__ __forceinline__ void passB_all(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
+                                          const float *Dp, float *cc_out, float &best, int &brot)
 {
 #pragma unroll 1
     for (int l2 = L0; l2 < L1; ++l2) {
@@ -326,9 +328,9 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
                                             float scale, float *cc_out, float &best, int &brot)
 {
     passA_class0<P1, P2>(getx, slab, T, tw);
-    passA_pairs<P1, P2, 1, (P1 + 1) / 2>(getx, slab, T, tw);
+    passA_pairs<P1, P2>(1, (P1 + 1) / 2, getx, slab, T, tw);
     passA_mid<P1, P2>(getx, slab, T, tw);
-    passB<P1, P2, 0, P2>(slab, T, tw, dinv, scale, cc_out, best, brot);
+    passB<P1, P2>(0, P2, slab, T, tw, dinv, scale, cc_out, best, brot);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -378,25 +380,22 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
             return v;
         };
         if (active) {
-            if (role == 0) {
-                passA_class0<P1, P2>(getx, slab, ROWS, tw);
-                passA_pairs<P1, P2, 1, SP::PAIRS_A + 1>(getx, slab, ROWS, tw);
-                passA_mid<P1, P2>(getx, slab, ROWS, tw);
-            } else {
-                passA_pairs<P1, P2, SP::PAIRS_A + 1, SP::NPAIRS + 1>(getx, slab, ROWS, tw);
-            }
+            // both halves share the class-pair and pass-B code; only their ranges differ
+            if (role == 0) passA_class0<P1, P2>(getx, slab, ROWS, tw);
+            passA_pairs<P1, P2>(role == 0 ? 1 : SP::PAIRS_A + 1, role == 0 ? SP::PAIRS_A + 1 : SP::NPAIRS + 1, getx,
+                                slab, ROWS, tw);
+            if (role == 0) passA_mid<P1, P2>(getx, slab, ROWS, tw);
         }
         asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
         float best = -INFINITY;
         int brot = 0;
         if (active) {
+            const int l0 = role == 0 ? 0 : SP::LB, l1 = role == 0 ? SP::LB : P2;
             if constexpr (WRITE) {
                 float *cc_out = ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N;
-                if (role == 0) passB_all<P1, P2, 0, SP::LB>(slab, ROWS, tw, Dr, cc_out, best, brot);
-                else passB_all<P1, P2, SP::LB, P2>(slab, ROWS, tw, Dr, cc_out, best, brot);
+                passB_all<P1, P2>(l0, l1, slab, ROWS, tw, Dr, cc_out, best, brot);
             } else {
-                if (role == 0) passB_search<P1, P2, 0, SP::LB>(slab, ROWS, tw, Dr, best, brot);
-                else passB_search<P1, P2, SP::LB, P2>(slab, ROWS, tw, Dr, best, brot);
+                passB_search<P1, P2>(l0, l1, slab, ROWS, tw, Dr, best, brot);
             }
             if (role == 1) { xfer_c[lr] = best; xfer_r[lr] = brot; }
         }
