@@ -51,9 +51,12 @@ def parse():
     ap.add_argument("--ntop", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
-    ap.add_argument("--report", default="", choices=["", "precision"],
+    ap.add_argument("--report", default="", choices=["", "precision", "refine"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
-                         "kernel over a particle sample (prints a report line instead of the bench line)")
+                         "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
+                         "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
+                         "prints a report line instead of the bench line)")
+    ap.add_argument("--grid-ptcls", type=int, default=200, help="particles whose problems also run the exhaustive grid")
     ap.add_argument("--report-ptcls", type=int, default=256, help="particles in the precision sample")
     return ap.parse_args()
 
@@ -418,10 +421,100 @@ def run_precision_report(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------ refinement report
+def refine_problems(pkg, w, seed=3):
+    """Continuous-refinement problems of the workload: every particle against its own
+    reference at the 11 in-plane indices around its pose, the shift started U[-2,2] px
+    away from the one that undoes the particle's shift, the CTF handed to the search
+    off by U[-0.1,0.1] microns of defocus.  Returns (handle, iref, iptcl, irot, x0)."""
+    import math
+    refs, R = pkg.synth.make_refs(w)
+    parts = pkg.synth.make_particles(w, R, device="cuda")
+    rng = np.random.default_rng(seed)
+    delta = rng.uniform(-0.1, 0.1, w.nptcls)
+    pc = pkg.polarft_corrcalc()
+    pc.new(w.nrefs, (1, w.nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True)
+    r_host = refs.numpy()
+    pc.set_refs(1, r_host, True)
+    pc.set_refs(1, r_host, False)
+    pc.polarize_ptcls_dev(0, w.nptcls, parts.cmat.contiguous().data_ptr())
+    pc.create_polar_absctfmats(pkg.ctfparams_array(w.nptcls, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                   dfx=parts.dfx + delta, dfy=parts.dfy + delta,
+                                                   angast=parts.angast))
+    iref, iptcl, irot, x0, truth = [], [], [], [], []
+    for i in range(w.nptcls):
+        psi = math.radians(parts.psi[i])
+        tx, ty = parts.shift[i]
+        r0 = int(round(parts.psi[i] * w.nrots / 360.0))
+        sh = (-(math.cos(psi) * tx + math.sin(psi) * ty), -(-math.sin(psi) * tx + math.cos(psi) * ty))
+        start = (sh[0] + rng.uniform(-2, 2), sh[1] + rng.uniform(-2, 2))
+        for d in range(-5, 6):
+            iref.append(parts.ref[i] + 1)
+            iptcl.append(i + 1)
+            irot.append((r0 + d) % w.nrots + 1)
+            x0.append((start[0], start[1], 0.0))
+            truth.append((sh[0], sh[1], -delta[i]))
+    return (pc, np.array(iref), np.array(iptcl), np.array(irot), np.array(x0, np.float64),
+            np.array(truth, np.float64))
+
+
+def run_refine_report(args):
+    """Config-3 style measurement: all problems refined in shift and defocus together; on
+    the problems of the first --grid-ptcls particles, the shift-only refinement against the
+    exhaustive shift grid (0.1 px over the same +-2 px box, defocus held) evaluated by the
+    same adjoint kernel, both timed as wall time of the library calls."""
+    pkg = entry.load_package()
+    w = workload(pkg, args)
+    pc, iref, iptcl, irot, x0, truth = refine_problems(pkg, w)
+    n = iref.size
+    half = np.array([2.0, 2.0, 0.2])
+    lb, ub = x0 - half, x0 + half
+    t0 = time.perf_counter()
+    x, f, nev, nit, conv = pc.refine_batch(iref, iptcl, irot, x0, lb, ub, maxits=100)
+    t_all = time.perf_counter() - t0
+    centre = np.arange(n) % 11 == 5                    # the problems at the particle's own pose index
+    dsh = np.hypot(*(x[centre, :2] - truth[centre, :2]).T)
+    ns = min(args.grid_ptcls, w.nptcls) * 11
+    lb0, ub0 = lb[:ns].copy(), ub[:ns].copy()
+    lb0[:, 2] = ub0[:, 2] = 0.0
+    t0 = time.perf_counter()
+    xs, fs, nevs, _, _ = pc.refine_batch(iref[:ns], iptcl[:ns], irot[:ns], x0[:ns], lb0, ub0, maxits=100)
+    t_ref = time.perf_counter() - t0
+    g = np.arange(-20, 21) * 0.1
+    GX, GY = (a.ravel() for a in np.meshgrid(g, g, indexing="ij"))
+    npts = GX.size
+    best = np.full(ns, -np.inf)
+    chunk = max(1, 250000 // npts)
+    t0 = time.perf_counter()
+    for p0 in range(0, ns, chunk):
+        p1 = min(ns, p0 + chunk)
+        k = p1 - p0
+        fg, _ = pc.grad_batch(np.repeat(iref[p0:p1], npts), np.repeat(iptcl[p0:p1], npts), np.repeat(irot[p0:p1], npts),
+                              (x0[p0:p1, 0][:, None] + GX[None, :]).ravel(), (x0[p0:p1, 1][:, None] + GY[None, :]).ravel(),
+                              np.zeros(k * npts))
+        best[p0:p1] = fg.reshape(k, npts).max(1)
+    t_grid = time.perf_counter() - t0
+    out = {"report": "refine", "workload": w.name,
+           "problems": int(n), "problem": "one particle vs its own reference at one of 11 in-plane indices around "
+                                          "its pose; start U[-2,2] px off, CTF defocus off by U[-0.1,0.1] um",
+           "all_shift_defocus": {"seconds": round(t_all, 3), "problems_per_s": n / t_all,
+                                 "median_evaluations": float(np.median(nev)), "converged": float(conv.mean()),
+                                 "median_shift_error_px_at_pose": float(np.median(dsh))},
+           "sample": {"problems": int(ns), "grid_points_per_problem": int(npts), "grid_seconds": round(t_grid, 3),
+                      "refine_shift_seconds": round(t_ref, 3), "refine_over_grid_time": t_ref / t_grid,
+                      "median_refine_evaluations": float(np.median(nevs)),
+                      "reaching_grid_best_within_1e-4": float(np.mean(fs >= best - 1e-4))}}
+    print(json.dumps(out), flush=True)
+    pc.kill()
+
+
 def main():
     args = parse()
     if args.report == "precision":
         run_precision_report(args)
+        return
+    if args.report == "refine":
+        run_refine_report(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -10,8 +10,9 @@
 // FP32 operand value v is split into bf16 hi = rn(v) and lo = rn(v - hi); the
 // product is accumulated in FP32 TMEM as hi*hi + hi*lo + lo*hi (three
 // kind::f16 MMAs per 16-wide K step).  Operands are pre-tiled in global memory in
-// the canonical no-swizzle K-major layout ([chunk of 8 K][row][8 K]) so that one
-// 4-D TMA tile copy per tile lands them ready for the UMMA descriptors.
+// the canonical no-swizzle K-major layout ([chunk of 8 K][row][8 K]), each tile one
+// contiguous block, so that one bulk copy (cp.async.bulk) per tile lands it ready for
+// the UMMA descriptors (a tiled tensor copy of this layout would move 16-byte rows).
 //
 // Kernel roles (192 threads, one persistent CTA per SM):
 //   warp 0   TMA producer: particle tile once per work item (m, particle tile),
@@ -55,6 +56,8 @@ struct UmmaParams {
     int rtile0;         // first rs tile of the wave
     int rtiles_m;       // rs tiles per m plane in the packed row operand
     int stages;         // N-tile ring depth
+    const __nv_bfloat16 *P16;   // packed particle operand, one contiguous tile per (m, particle tile)
+    const __nv_bfloat16 *R16;   // packed row operand, one contiguous tile per (m, rs tile)
     float2 *X;          // [M][xcols][xrows]
     int xrows, xcols;
     int *err;           // device error word (0 = ok)
@@ -102,15 +105,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     return false;
 }
 
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                            uint64_t *bar)
+// bulk copy of one pre-tiled operand tile (contiguous in global memory, already in the
+// UMMA canonical layout) into shared memory, completing on the mbarrier's transaction count;
+// both addresses 16-byte aligned, size a multiple of 16
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%3, %4, %5, %6}], [%2];"
-        :
-        : "r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-        : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :
+                 : "r"(smem_u32(dst)), "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // TMA bulk store of a 2-D box from shared memory (bulk-group completion)
@@ -164,13 +167,13 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// completes every tcgen05.ld this thread issued before it
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // ---- the GEMM ------------------------------------------------------------------------
-__global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ CUtensorMap tmP,
-                                                              const __grid_constant__ CUtensorMap tmR,
-                                                              const __grid_constant__ CUtensorMap tmX, UmmaParams up)
+__global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ CUtensorMap tmX, UmmaParams up)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -224,14 +227,15 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
             if (ii > 0 && !mbar_wait(a_empty, (ii - 1) & 1, abort_flag)) { fail(1); ok = false; break; }
             mbar_expect_tx(a_full, a_bytes);
-            tma_load_4d(sA, &tmP, 0, 0, 0, m * up.ptiles_m + up.ptile0 + pt, a_full);
+            bulk_load(sA, up.P16 + (size_t)(m * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
             for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
                 const int s = (int)(itb % up.stages);
                 if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag)) {
                     fail(2); ok = false; break;
                 }
                 mbar_expect_tx(full + s, b_bytes);
-                tma_load_4d(sB + (size_t)s * b_bytes, &tmR, 0, 0, 0, m * up.rtiles_m + up.rtile0 + j, full + s);
+                bulk_load(sB + (size_t)s * b_bytes, up.R16 + (size_t)(m * up.rtiles_m + up.rtile0 + j) * (b_bytes / 2),
+                          b_bytes, full + s);
             }
         }
         // drain: every issued copy must land before the CTA exits
@@ -299,10 +303,18 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                 const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
                 if (!got) { if (lane == 0) fail(6); ok = false; break; }
                 tc_fence_after();
-#pragma unroll 1
+                // all four 32-column loads in flight at once, one wait; the accumulator is
+                // handed back to the MMA issuer before the stores start
+                uint32_t r4[U_BN / 32][32];
+#pragma unroll
+                for (int c = 0; c < U_BN / 32; ++c)
+                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r4[c]);
+                tmem_wait_ld();
+                tc_fence_before();
+                mbar_arrive(t_empty + acc);
+#pragma unroll
                 for (int c = 0; c < U_BN / 32; ++c) {
-                    uint32_t r[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r);
+                    const uint32_t (&r)[32] = r4[c];
                     // the staging tile written two stores ago must have been read out
                     if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
                     __syncwarp();
@@ -321,8 +333,6 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                     }
                     sbuf ^= 1;
                 }
-                tc_fence_before();
-                mbar_arrive(t_empty + acc);
             }
         }
         // every store has finished reading shared memory and writing X before the CTA exits
@@ -409,22 +419,6 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
     return fn;
 }
 
-static int make_map(pftcc_handle *h, CUtensorMap *map, void *base, int KC, long long ntiles)
-{
-    auto enc = get_encode();
-    if (!enc) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    if (((uintptr_t)base & 15) != 0) return set_err(h, PFTCC_ERR_ARG, "operand base not 16-byte aligned");
-    cuuint64_t dims[4] = {8, 128, (cuuint64_t)KC, (cuuint64_t)ntiles};
-    cuuint64_t strides[3] = {16, 128 * 16, (cuuint64_t)KC * 128 * 16};
-    cuuint32_t box[4] = {8, 128, (cuuint32_t)KC, 1};
-    cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
-    return PFTCC_OK;
-}
-
 // X[M][xcols][xrows] float2 as a 2-D FP32 tensor: x = 2 * rs + (re, im), y = m * xcols + col;
 // boxes of 32 floats (128 B) x 32 rows, 128-byte swizzle (the staging layout of the epilogue)
 static int make_xmap(pftcc_handle *h, CUtensorMap *map, void *X, int xrows, int xcols, int M)
@@ -487,13 +481,10 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     const int ptile0 = (c0 - us.group_c0) / U_BM, n_ptiles = ncols_w / U_BM;
     if (rtile0 + n_rtiles > us.rtiles || ptile0 + n_ptiles > us.ptiles)
         return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave outside the packed operands");
-    CUtensorMap tmP, tmR;
-    int st = make_map(h, &tmP, ws.B16, KC, (long long)M * us.ptiles);
-    if (st) return st;
-    st = make_map(h, &tmR, ws.A16, KC, (long long)M * us.rtiles);
-    if (st) return st;
+    if (((uintptr_t)ws.A16 & 15) != 0 || ((uintptr_t)ws.B16 & 15) != 0)
+        return set_err(h, PFTCC_ERR_ARG, "umma stage 1: packed operands not 16-byte aligned");
     CUtensorMap tmX;
-    st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M);
+    int st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M);
     if (st) return st;
     UmmaParams up{};
     up.M = M; up.Kp = Kp; up.KC = KC;
@@ -508,6 +499,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     if (1024 + a_bytes + stages * b_bytes + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
     up.stages = stages;
+    up.P16 = ws.B16; up.R16 = ws.A16;
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
     const size_t smem = 1024 + a_bytes + stages * b_bytes + tail;
@@ -517,7 +509,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     const int grid = std::min(nitems, us.sms);
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE1);
-    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmP, tmR, tmX, up);
+    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmX, up);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "umma stage 1 launch");
     return PFTCC_OK;
 }
