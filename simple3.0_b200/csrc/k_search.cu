@@ -244,58 +244,84 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *
 
 // ---------------------------------------------------------------------------
 // stage 1 on CUDA cores: X[m][col][row] = 4 * sum_k UA[m][row][k] * conj(UB[m][col][k])
-// block tile 64 cols x 64 rows, 256 threads with 4 x 4 complex micro-tiles, the whole
-// shell range staged in shared memory (Ks <= 64).
+// for the plane pair (m, P - m) of blockIdx.z (m = 0 pairs with P; m = P/2 with itself),
+// stored as the packed spectrum of stage 2, Z(m) and Z(P - m) (make_z).  Block tile 64
+// cols x 64 rows, 256 threads with 4 x 4 complex micro-tiles per plane, the whole shell
+// range of both planes staged in shared memory (Ks <= 64).
 constexpr int S1_TILE = 64;
 constexpr int COL_TILE = 128;
 
-__global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, const float2 *__restrict__ UA, int rows_pad, int row0,
-                                                     const float2 *__restrict__ UB, int cols_pad, int col0,
-                                                     float2 *__restrict__ X, int xrows, int xcols)
+__global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2 *__restrict__ UA, int rows_pad,
+                                                     int row0, const float2 *__restrict__ UB, int cols_pad, int col0,
+                                                     float2 *__restrict__ Z, int xrows, int xcols)
 {
     extern __shared__ float4 smem4[];
-    float2 *sa = reinterpret_cast<float2 *>(smem4);   // [Ks][64] rows
-    float2 *sb = sa + Ks * S1_TILE;                    // [Ks][64] cols
-    const int m = blockIdx.z;
+    float2 *sa = reinterpret_cast<float2 *>(smem4);   // [2 planes][Ks][64] rows
+    float2 *sb = sa + 2 * Ks * S1_TILE;                // [2 planes][Ks][64] cols
+    const int mp = blockIdx.z;
+    const int mA = mp, mB = mp == 0 ? P : P - mp;
     const int rt = blockIdx.x * S1_TILE, ct = blockIdx.y * S1_TILE;
-    const float2 *A = UA + ((size_t)m * rows_pad + row0 + rt) * Ks;
-    const float2 *B = UB + ((size_t)m * cols_pad + col0 + ct) * Ks;
-    for (int e = threadIdx.x; e < S1_TILE * Ks; e += blockDim.x) {
-        const int i = e / Ks, k = e - i * Ks;
-        sa[k * S1_TILE + i] = A[e];
-        sb[k * S1_TILE + i] = B[e];
+    for (int h = 0; h < 2; ++h) {
+        const int m = h == 0 ? mA : mB;
+        const float2 *A = UA + ((size_t)m * rows_pad + row0 + rt) * Ks;
+        const float2 *B = UB + ((size_t)m * cols_pad + col0 + ct) * Ks;
+        for (int e = threadIdx.x; e < S1_TILE * Ks; e += blockDim.x) {
+            const int i = e / Ks, k = e - i * Ks;
+            sa[(h * Ks + k) * S1_TILE + i] = A[e];
+            sb[(h * Ks + k) * S1_TILE + i] = B[e];
+        }
     }
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;   // rows 4*tx.., cols 4*ty..
-    float accr[4][4], acci[4][4];
+    float accr[2][4][4], acci[2][4][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) { accr[i][j] = 0.f; acci[i][j] = 0.f; }
-    for (int k = 0; k < Ks; ++k) {
-        const float4 a01 = *reinterpret_cast<const float4 *>(sa + k * S1_TILE + 4 * tx);
-        const float4 a23 = *reinterpret_cast<const float4 *>(sa + k * S1_TILE + 4 * tx + 2);
-        const float4 b01 = *reinterpret_cast<const float4 *>(sb + k * S1_TILE + 4 * ty);
-        const float4 b23 = *reinterpret_cast<const float4 *>(sb + k * S1_TILE + 4 * ty + 2);
-        const float ar[4] = {a01.x, a01.z, a23.x, a23.z}, ai[4] = {a01.y, a01.w, a23.y, a23.w};
-        const float br[4] = {b01.x, b01.z, b23.x, b23.z}, bi[4] = {b01.y, b01.w, b23.y, b23.w};
+    for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                // a * conj(b)
-                accr[i][j] = fmaf(ar[i], br[j], fmaf(ai[i], bi[j], accr[i][j]));
-                acci[i][j] = fmaf(ai[i], br[j], fmaf(-ar[i], bi[j], acci[i][j]));
-            }
+            for (int j = 0; j < 4; ++j) { accr[h][i][j] = 0.f; acci[h][i][j] = 0.f; }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float2 *sah = sa + h * Ks * S1_TILE, *sbh = sb + h * Ks * S1_TILE;
+        for (int k = 0; k < Ks; ++k) {
+            const float4 a01 = *reinterpret_cast<const float4 *>(sah + k * S1_TILE + 4 * tx);
+            const float4 a23 = *reinterpret_cast<const float4 *>(sah + k * S1_TILE + 4 * tx + 2);
+            const float4 b01 = *reinterpret_cast<const float4 *>(sbh + k * S1_TILE + 4 * ty);
+            const float4 b23 = *reinterpret_cast<const float4 *>(sbh + k * S1_TILE + 4 * ty + 2);
+            const float ar[4] = {a01.x, a01.z, a23.x, a23.z}, ai[4] = {a01.y, a01.w, a23.y, a23.w};
+            const float br[4] = {b01.x, b01.z, b23.x, b23.z}, bi[4] = {b01.y, b01.w, b23.y, b23.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    // a * conj(b)
+                    accr[h][i][j] = fmaf(ar[i], br[j], fmaf(ai[i], bi[j], accr[h][i][j]));
+                    acci[h][i][j] = fmaf(ai[i], br[j], fmaf(-ar[i], bi[j], acci[h][i][j]));
+                }
+        }
     }
+    const int N = 2 * P;
+    const float2 wA = wn_of(mA, N), wB = wn_of(mB, N);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int col = ct + 4 * ty + j;
         if (col >= xcols) continue;
-        float2 *dst = X + ((size_t)m * xcols + col) * xrows + rt + 4 * tx;
+        float2 *dA = Z + ((size_t)mA * xcols + col) * xrows + rt + 4 * tx;
+        float2 *dB = Z + ((size_t)(mB < P ? mB : 0) * xcols + col) * xrows + rt + 4 * tx;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-            if (rt + 4 * tx + i < xrows) dst[i] = make_float2(4.f * accr[i][j], 4.f * acci[i][j]);
+        for (int i = 0; i < 4; ++i) {
+            if (rt + 4 * tx + i >= xrows) continue;
+            float2 xa = make_float2(4.f * accr[0][i][j], 4.f * acci[0][i][j]);
+            float2 xb = make_float2(4.f * accr[1][i][j], 4.f * acci[1][i][j]);
+            if (mp == 0) {              // X(0) and X(P) are real
+                xa.y = 0.f;
+                xb.y = 0.f;
+                dA[i] = make_z(xa, xb, wA);
+            } else {
+                dA[i] = make_z(xa, xb, wA);
+                if (mB != mA) dB[i] = make_z(xb, xa, wB);
+            }
+        }
     }
 }
 
@@ -496,28 +522,8 @@ __global__ void k_stage2(S2Params sp, const float2 *__restrict__ X, const float 
     // X carries the factor 4 of the half-circle transforms; y/(2N) is the correlation sum
     const float scale = 1.0f / (2.0f * (float)N);
     for (int row = t; row < sp.rows; row += T) {
-        // packed Hermitian input, digit-reversed into the slab
-        for (int j = 0; j <= P / 2; ++j) {
-            const float2 a = Xc[(size_t)j * plane + row];
-            const float2 b = Xc[(size_t)(P - j) * plane + row];
-            if (j == 0) {
-                // X(0), X(P) are real
-                buf[(size_t)rev[0] * T + t] = make_float2(a.x + b.x, a.x - b.x);
-                continue;
-            }
-            // Z(j) from a = X(j), conj b
-            {
-                const float2 E = make_float2(a.x + b.x, a.y - b.y);
-                const float2 O = cmul(make_float2(a.x - b.x, a.y + b.y), twN[j]);
-                buf[(size_t)rev[j] * T + t] = make_float2(E.x - O.y, E.y + O.x);
-            }
-            if (P - j != j) {
-                // Z(P-j) from b = X(P-j), conj a
-                const float2 E = make_float2(b.x + a.x, b.y - a.y);
-                const float2 O = cmul(make_float2(b.x - a.x, b.y + a.y), twN[P - j]);
-                buf[(size_t)rev[P - j] * T + t] = make_float2(E.x - O.y, E.y + O.x);
-            }
-        }
+        // the packed spectrum Z as stage 1 stored it, digit-reversed into the slab
+        for (int j = 0; j < P; ++j) buf[(size_t)rev[j] * T + t] = Xc[(size_t)j * plane + row];
         // in-place mixed-radix DIT passes, innermost radix first
         int span = 1;   // m_l of the current level
         for (int l = sp.nf - 1; l >= 0; --l) {
@@ -742,7 +748,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     }
     const size_t smem_ref = N * sizeof(double2) + (size_t)Ks * P * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
-    const size_t smem_s1 = 2 * (size_t)Ks * S1_TILE * sizeof(float2);
+    const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");
     int T = 128;
     while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
@@ -785,11 +791,11 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                     int st = umma_stage1(h, M, Ks, ws.UA, row0, rows_t, rows_pad, ws.UB, c0, cols_t, cols_pad, ws.X, 0, grp);
                     if (st != PFTCC_OK) return st;
                 } else {
-                    dim3 grid(rows_t / S1_TILE, cols_t / S1_TILE, M);
+                    dim3 grid(rows_t / S1_TILE, cols_t / S1_TILE, P / 2 + 1);
                     PFTCC_LAUNCH(h);
                     KTimer kt(h, PFTCC_K_STAGE1);
-                    k_stage1_fp32<<<grid, 256, smem_s1, h->stream>>>(Ks, ws.UA, rows_pad, row0, ws.UB, cols_pad, c0, ws.X,
-                                                                    rows_t, cols_t);
+                    k_stage1_fp32<<<grid, 256, smem_s1, h->stream>>>(Ks, P, ws.UA, rows_pad, row0, ws.UB, cols_pad, c0,
+                                                                    ws.X, rows_t, cols_t);
                     CKE(cudaGetLastError(), "stage1");
                 }
                 // the split-radix stage 2 reads the factor in its visiting order, times 1/(2N)

@@ -13,8 +13,10 @@
 //   pass A: for each residue class j1 < P1 a length-P2 DFT over j2 of Z(j1 + P1 j2),
 //           times w_P^{-j1 l2}, into a thread-private shared-memory slab;
 //   pass B: for each l2 < P2 a length-P1 DFT over j1 -> z(l2 + P2 l1).
-// Classes j1 and P1 - j1 are processed together so that every X element is loaded
-// exactly once (Z(j) needs X(j) and X(P - j), which lie in the mirror class).
+// The search (k_stage2_fast) reads Z as stage 1 stored it, P planes of [col][row]; the
+// FP32 re-score forms Z from X itself, processing classes j1 and P1 - j1 together so
+// that every X element is computed once (Z(j) needs X(j) and X(P - j), which lie in the
+// mirror class).
 #include "pftcc_internal.cuh"
 
 #include <algorithm>
@@ -111,12 +113,30 @@ template <int STEP> struct SFFT<1, STEP> {
     __device__ static void run(float2 *, const TwTables &) {}
 };
 
-// Z(j) from a = X(j) and b = X(P - j)
-__device__ __forceinline__ float2 make_z(float2 a, float2 b, float2 wn)
+// pass A over the packed spectrum Z itself (the search path, where stage 1 stores Z):
+// classes c in [c0, c1), each a length-P2 DFT over j2 of Z(c + P1 j2), times w_P^{-c l2},
+// into the row's slab; the next class's P2 loads are issued before this class's transform
+template <int P1, int P2, class GetZ>
+__device__ __forceinline__ void passA_z(int c0, int c1, const GetZ &getz, float2 *slab, int T, const TwTables &tw)
 {
-    const float2 E = make_float2(a.x + b.x, a.y - b.y);
-    const float2 O = c_mul(make_float2(a.x - b.x, a.y + b.y), wn);
-    return make_float2(E.x - O.y, E.y + O.x);
+    float2 zn[P2];
+    if (c0 < c1) {
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) zn[j2] = getz(c0 + P1 * j2);
+    }
+#pragma unroll 1
+    for (int c = c0; c < c1; ++c) {
+        float2 z[P2];
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) z[j2] = zn[j2];
+        if (c + 1 < c1) {
+#pragma unroll
+            for (int j2 = 0; j2 < P2; ++j2) zn[j2] = getz(c + 1 + P1 * j2);
+        }
+        SFFT<P2, P1>::run(z, tw);
+#pragma unroll
+        for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1 + c) * T] = l2 == 0 ? z[l2] : c_mul(z[l2], tw.wP[c * l2]);
+    }
 }
 
 // Pass A, split into the pieces the two halves of a row's transform take: class 0 (its
@@ -310,13 +330,9 @@ __device__ __forceinline__ void passB_all(int L0, int L1, const float2 *slab, in
     }
 }
 
-// how a row's transform is split between two threads: role 0 takes class 0, the class
-// pairs c < PAIRS_A + 1 and the middle class, role 1 the other pairs (P1 length-P2 DFTs
-// in all, split as evenly as the classes allow); pass B splits at l2 = LB
+// how a row's transform is split between two threads: pass A by classes, [0, P1/2) and
+// [P1/2, P1) of Z; pass B at l2 = LB
 template <int P1, int P2> struct RowSplit {
-    static constexpr int SELFS = 1 + ((P1 & 1) == 0);
-    static constexpr int PAIRS_A = (P1 - 2 * SELFS) / 4;
-    static constexpr int NPAIRS = (P1 - 1) / 2;
     static constexpr int LB = (P2 + 1) / 2;
 };
 
@@ -341,6 +357,7 @@ struct S2Fast {
 // ROWS rows in flight per block, two threads per row: warp w < ROWS/32 (role 0) and warp
 // w + ROWS/32 (role 1) share the rows' slabs and meet at named barrier 1 + w twice per row
 // (after pass A; after pass B, when role 1 hands its argmax over).
+// X here is the packed spectrum Z, P planes of [col][row].
 template <int P1, int P2, int ROWS, bool WRITE>
 __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
                                                             const float *__restrict__ Dinv, float2 *__restrict__ cand,
@@ -370,7 +387,7 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         if (active && row + ROWS < sp.rows) {
             // the next row of this thread: pull its spectrum towards L2 while this one is transformed
             const float2 *xn = xr + ROWS;
-            for (int j = role; j <= P; j += 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
+            for (int j = role; j < P; j += 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
         }
         auto getx = [&](int j) {
             float2 v;
@@ -381,10 +398,8 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         };
         if (active) {
             // both halves share the class-pair and pass-B code; only their ranges differ
-            if (role == 0) passA_class0<P1, P2>(getx, slab, ROWS, tw);
-            passA_pairs<P1, P2>(role == 0 ? 1 : SP::PAIRS_A + 1, role == 0 ? SP::PAIRS_A + 1 : SP::NPAIRS + 1, getx,
-                                slab, ROWS, tw);
-            if (role == 0) passA_mid<P1, P2>(getx, slab, ROWS, tw);
+            // the two halves of the row take the classes [0, P1/2) and [P1/2, P1) of Z
+            passA_z<P1, P2>(role == 0 ? 0 : P1 / 2, role == 0 ? P1 / 2 : P1, getx, slab, ROWS, tw);
         }
         asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
         float best = -INFINITY;

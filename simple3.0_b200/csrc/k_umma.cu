@@ -2,7 +2,8 @@
 //
 // For one angular frequency m, X[col][rs] = 4 sum_k UA(rs,k) conj(UB(col,k)) is
 // computed as a real GEMM with the particles on the UMMA M side and the (ref, shift)
-// rows on the N side:
+// rows on the N side, for the planes m and P - m of a pair together so that the
+// epilogue stores stage 2's packed spectrum Z(m), Z(P - m) (make_z) instead of X:
 //   particle row  : [Br(k) | Bi(k) | 0]                       (K = Kp reals)
 //   N row 2i      : [Ar(k) | Ai(k) | 0]   -> column 2i   = Re X
 //   N row 2i+1    : [Ai(k) | -Ar(k) | 0]  -> column 2i+1 = Im X
@@ -15,15 +16,15 @@
 // the UMMA descriptors (a tiled tensor copy of this layout would move 16-byte rows).
 //
 // Kernel roles (192 threads, one persistent CTA per SM):
-//   warp 0   TMA producer: particle tile once per work item (m, particle tile),
-//            then the ring of N tiles (64 (ref, shift) rows each)
+//   warp 0   producer: both planes' particle tiles once per work item (plane pair,
+//            particle tile), then the ring of row tiles (32 (ref, shift) rows of each
+//            plane per stage)
 //   warp 1   TMEM allocation and the single MMA-issuing thread; accumulators are
-//            double buffered (2 x 128 TMEM columns)
-//   warps 2-5 epilogue: tcgen05.ld of the 128 x 128 accumulator (each warp its
-//            32-lane quadrant, 32 columns = 16 complex X per particle at a time)
-//            into a 128B-swizzled staging tile, written out with one TMA bulk
-//            store per 32 x 16 block of X[m][col][rs]; two staging tiles per warp
-//            so the next block is staged while the previous store reads its tile
+//            double buffered, each buffer 2 x 64 TMEM columns (one per plane)
+//   warps 2-5 epilogue: tcgen05.ld of both planes' 128 x 64 accumulators (each warp
+//            its 32-lane quadrant), Z(m) and Z(P - m) for 16 rows at a time into two
+//            128B-swizzled staging tiles, written out with one TMA bulk store each
+//            to Z[plane][col][rs]
 // The factor 4 of X is carried by the packed particle operand (exact in BF16).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code,
 // drains its own outstanding copies (bounded), frees its TMEM and returns.
@@ -38,15 +39,15 @@
 namespace pftcc {
 
 constexpr int U_BM = 128;        // particles per tile (UMMA M)
-constexpr int U_BN = 128;        // N columns per tile = 64 rs x (re, im)
-constexpr int U_RS = 64;         // (ref, shift) rows per tile
+constexpr int U_BN = 64;         // N columns per plane and tile = 32 rs x (re, im)
+constexpr int U_RS = 32;         // (ref, shift) rows per tile
 constexpr int U_THREADS = 192;
 constexpr long long WAIT_LIMIT = 20000000;   // polls of a bounded wait (~seconds)
 constexpr int STAGE_TILE = 32 * 128;          // one staged 32-row x 128-byte block
-constexpr int STAGE_BYTES = 4 * 2 * STAGE_TILE;   // four epilogue warps x two blocks
+constexpr int STAGE_BYTES = 4 * 2 * STAGE_TILE;   // four epilogue warps x (Z(m), Z(P-m)) blocks
 
 struct UmmaParams {
-    int M;              // m planes of the wave
+    int M;              // m planes of the packed operands (P + 1)
     int Kp;             // padded real K per operand part (multiple of 16)
     int KC;             // 8-element chunks per operand row: 2*Kp/8 (hi then lo)
     int n_ptiles;       // particle tiles in the wave
@@ -55,10 +56,10 @@ struct UmmaParams {
     int n_rtiles;       // rs tiles in the wave
     int rtile0;         // first rs tile of the wave
     int rtiles_m;       // rs tiles per m plane in the packed row operand
-    int stages;         // N-tile ring depth
+    int stages;         // N-tile ring depth (each stage holds the row tiles of both planes)
     const __nv_bfloat16 *P16;   // packed particle operand, one contiguous tile per (m, particle tile)
     const __nv_bfloat16 *R16;   // packed row operand, one contiguous tile per (m, rs tile)
-    float2 *X;          // [M][xcols][xrows]
+    float2 *X;          // output Z: [P][xcols][xrows]
     int xrows, xcols;
     int *err;           // device error word (0 = ok)
 };
@@ -177,11 +178,11 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const uint32_t a_bytes = (uint32_t)U_BM * up.KC * 16;
-    const uint32_t b_bytes = (uint32_t)U_BN * up.KC * 16;
-    unsigned char *sA = smem;
-    unsigned char *sB = smem + a_bytes;
-    unsigned char *stg = sB + (size_t)up.stages * b_bytes;     // [4 warps][2][32][128 B], 1024-B aligned
+    const uint32_t a_bytes = (uint32_t)U_BM * up.KC * 16;     // one plane's particle tile
+    const uint32_t b_bytes = (uint32_t)U_BN * up.KC * 16;     // one plane's row tile
+    unsigned char *sA = smem;                                  // [2 planes] particle tiles
+    unsigned char *sB = smem + 2 * a_bytes;                    // [stages][2 planes] row tiles
+    unsigned char *stg = sB + (size_t)up.stages * 2 * b_bytes; // [4 warps][2][32][128 B], 1024-B aligned
     uint64_t *bars = reinterpret_cast<uint64_t *>(stg + STAGE_BYTES);
     uint64_t *full = bars;                    // [stages]
     uint64_t *empty = bars + up.stages;       // [stages]
@@ -212,7 +213,10 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int nitems = up.M * up.n_ptiles;
+    // work item = (plane pair mp, particle tile): planes mA = mp and mB = P - mp (mp = 0
+    // pairs plane 0 with plane P, mp = P/2 of an even P pairs the plane with itself)
+    const int P = up.M - 1, npairs = P / 2 + 1;
+    const int nitems = npairs * up.n_ptiles;
     auto fail = [&](int code) {
         if (!*abort_flag) atomicCAS(up.err, 0, code);
         *abort_flag = 1;
@@ -224,18 +228,22 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
         int ii = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
-            const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
+            const int mp = w / up.n_ptiles, pt = w - mp * up.n_ptiles;
+            const int pm[2] = {mp, mp == 0 ? P : P - mp};
             if (ii > 0 && !mbar_wait(a_empty, (ii - 1) & 1, abort_flag)) { fail(1); ok = false; break; }
-            mbar_expect_tx(a_full, a_bytes);
-            bulk_load(sA, up.P16 + (size_t)(m * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
+            mbar_expect_tx(a_full, 2 * a_bytes);
+            for (int h = 0; h < 2; ++h)
+                bulk_load(sA + (size_t)h * a_bytes,
+                          up.P16 + (size_t)(pm[h] * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
             for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
                 const int s = (int)(itb % up.stages);
                 if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag)) {
                     fail(2); ok = false; break;
                 }
-                mbar_expect_tx(full + s, b_bytes);
-                bulk_load(sB + (size_t)s * b_bytes, up.R16 + (size_t)(m * up.rtiles_m + up.rtile0 + j) * (b_bytes / 2),
-                          b_bytes, full + s);
+                mbar_expect_tx(full + s, 2 * b_bytes);
+                for (int h = 0; h < 2; ++h)
+                    bulk_load(sB + ((size_t)s * 2 + h) * b_bytes,
+                              up.R16 + (size_t)(pm[h] * up.rtiles_m + up.rtile0 + j) * (b_bytes / 2), b_bytes, full + s);
             }
         }
         // drain: every issued copy must land before the CTA exits
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             for (long long i = 0; i < WAIT_LIMIT && !mbar_try(a_full, (uint32_t)((ii - 1) & 1)); ++i) __nanosleep(64);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------------------ MMA issuer
-        // instruction descriptor: F32 accumulate, BF16 x BF16, both K-major, N=128, M=128
+        // instruction descriptor: F32 accumulate, BF16 x BF16, both K-major, N=64, M=128
         const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(U_BN >> 3) << 17) |
                                ((uint32_t)(U_BM >> 4) << 24);
         const uint32_t a_base = smem_u32(sA), b_base0 = smem_u32(sB);
@@ -267,16 +275,20 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                     fail(5); ok = false; break;
                 }
                 tc_fence_after();
-                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * U_BN);
-                const uint32_t b_base = b_base0 + (uint32_t)s * b_bytes;
-                for (int ks = 0; ks < ksteps; ++ks) {
+                // accumulator buffer acc: columns [0, 64) plane mA, [64, 128) plane mB
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(acc * 2 * U_BN + h * U_BN);
+                    const uint32_t ah = a_base + (uint32_t)h * a_bytes;
+                    const uint32_t b_base = b_base0 + ((uint32_t)s * 2 + h) * b_bytes;
+                    for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
-                    for (int prod = 0; prod < 3; ++prod) {
-                        const int ac = (prod == 2 ? lo_off : 0) + 2 * ks;   // lo(A) * hi(B)
-                        const int bc = (prod == 1 ? lo_off : 0) + 2 * ks;   // hi(A) * lo(B)
-                        const uint64_t ad = umma_desc(a_base + (uint32_t)ac * (U_BM * 16), U_BM * 16, 128);
-                        const uint64_t bd = umma_desc(b_base + (uint32_t)bc * (U_BN * 16), U_BN * 16, 128);
-                        umma_bf16(d_tmem, ad, bd, idesc, (ks > 0 || prod > 0) ? 1u : 0u);
+                        for (int prod = 0; prod < 3; ++prod) {
+                            const int ac = (prod == 2 ? lo_off : 0) + 2 * ks;   // lo(A) * hi(B)
+                            const int bc = (prod == 1 ? lo_off : 0) + 2 * ks;   // hi(A) * lo(B)
+                            const uint64_t ad = umma_desc(ah + (uint32_t)ac * (U_BM * 16), U_BM * 16, 128);
+                            const uint64_t bd = umma_desc(b_base + (uint32_t)bc * (U_BN * 16), U_BN * 16, 128);
+                            umma_bf16(d_tmem, ad, bd, idesc, (ks > 0 || prod > 0) ? 1u : 0u);
+                        }
                     }
                 }
                 umma_commit(empty + s);      // N stage reusable once these MMAs finish
@@ -289,49 +301,67 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     } else if (warp >= 2) {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                       // TMEM lane quadrant of this warp
-        unsigned char *stg_w = stg + (size_t)(warp - 2) * 2 * STAGE_TILE;
-        int sbuf = 0;
+        unsigned char *stg_w = stg + (size_t)(warp - 2) * 2 * STAGE_TILE;   // boxes of Z(mA), Z(mB)
         long long tacc = 0;
         bool ok = true;
+        const int N = 2 * P;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
-            const int m = w / up.n_ptiles, pt = w - m * up.n_ptiles;
-            // rows of this warp: particles 32q .. 32q+31 of the tile = box rows of X's tensor map
-            const int y0 = m * up.xcols + pt * U_BM + 32 * q;
+            const int mp = w / up.n_ptiles, pt = w - mp * up.n_ptiles;
+            const int mA = mp, mB = mp == 0 ? P : P - mp;
+            const bool two = mp != 0 && mB != mA;      // a second output plane
+            const float2 wA = wn_of(mA, N), wB = wn_of(mB, N);
+            // rows of this warp: particles 32q .. 32q+31 of the tile = box rows of Z's tensor map
+            const int yA = mA * up.xcols + pt * U_BM + 32 * q, yB = (two ? mB : 0) * up.xcols + pt * U_BM + 32 * q;
             for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
                 const int acc = (int)(tacc & 1);
                 // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
                 const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
                 if (!got) { if (lane == 0) fail(6); ok = false; break; }
                 tc_fence_after();
-                // all four 32-column loads in flight at once, one wait; the accumulator is
-                // handed back to the MMA issuer before the stores start
-                uint32_t r4[U_BN / 32][32];
+                // both planes' 64 columns in flight at once, one wait; the accumulator is handed
+                // back to the MMA issuer before Z is formed and stored
+                uint32_t r4[4][32];     // [plane * 2 + chunk][32 columns = 16 complex]
 #pragma unroll
-                for (int c = 0; c < U_BN / 32; ++c)
-                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * U_BN + 32 * c), r4[c]);
+                for (int c = 0; c < 4; ++c)
+                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * 2 * U_BN + 32 * c), r4[c]);
                 tmem_wait_ld();
                 tc_fence_before();
                 mbar_arrive(t_empty + acc);
 #pragma unroll
-                for (int c = 0; c < U_BN / 32; ++c) {
-                    const uint32_t (&r)[32] = r4[c];
-                    // the staging tile written two stores ago must have been read out
-                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                for (int c = 0; c < 2; ++c) {
+                    const uint32_t (&ra)[32] = r4[c];
+                    const uint32_t (&rb)[32] = r4[2 + c];
+                    // the staging boxes of the previous chunk must have been read out
+                    if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                     __syncwarp();
-                    // row `lane` of the box, 16-byte chunk e at position e ^ (lane & 7) (128B swizzle)
-                    float4 *row = reinterpret_cast<float4 *>(stg_w + sbuf * STAGE_TILE + lane * 128);
+                    // row `lane` of each box, 16-byte chunk e at position e ^ (lane & 7) (128B swizzle)
+                    float4 *rowA = reinterpret_cast<float4 *>(stg_w + lane * 128);
+                    float4 *rowB = reinterpret_cast<float4 *>(stg_w + STAGE_TILE + lane * 128);
 #pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        row[e ^ (lane & 7)] = make_float4(__uint_as_float(r[4 * e]), __uint_as_float(r[4 * e + 1]),
-                                                          __uint_as_float(r[4 * e + 2]), __uint_as_float(r[4 * e + 3]));
+                    for (int e = 0; e < 8; ++e) {
+                        float2 xa0 = make_float2(__uint_as_float(ra[4 * e]), __uint_as_float(ra[4 * e + 1]));
+                        float2 xa1 = make_float2(__uint_as_float(ra[4 * e + 2]), __uint_as_float(ra[4 * e + 3]));
+                        float2 xb0 = make_float2(__uint_as_float(rb[4 * e]), __uint_as_float(rb[4 * e + 1]));
+                        float2 xb1 = make_float2(__uint_as_float(rb[4 * e + 2]), __uint_as_float(rb[4 * e + 3]));
+                        if (mp == 0) {                 // X(0) and X(P) are real
+                            xa0.y = xa1.y = xb0.y = xb1.y = 0.f;
+                        }
+                        const float2 za0 = make_z(xa0, xb0, wA), za1 = make_z(xa1, xb1, wA);
+                        rowA[e ^ (lane & 7)] = make_float4(za0.x, za0.y, za1.x, za1.y);
+                        if (two) {
+                            const float2 zb0 = make_z(xb0, xa0, wB), zb1 = make_z(xb1, xa1, wB);
+                            rowB[e ^ (lane & 7)] = make_float4(zb0.x, zb0.y, zb1.x, zb1.y);
+                        }
+                    }
                     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                     __syncwarp();
                     if (lane == 0) {
                         // x in floats: complex rs = j * U_RS + 16 c, two floats each (a multiple of 32)
-                        tma_store_2d(&tmX, stg_w + sbuf * STAGE_TILE, 2 * (j * U_RS + 16 * c), y0);
+                        const int x = 2 * (j * U_RS + 16 * c);
+                        tma_store_2d(&tmX, stg_w, x, yA);
+                        if (two) tma_store_2d(&tmX, stg_w + STAGE_TILE, x, yB);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
-                    sbuf ^= 1;
                 }
             }
         }
@@ -353,17 +383,17 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 &hi, __nv_bflo
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
-// (ref, shift) rows -> R16[m][rt][chunk][128][8]
+// (ref, shift) rows -> R16[m][rt][chunk][U_BN][8]: U_RS rows = U_BN N-rows per tile
 __global__ void k_pack_rows(int M, int Ks, int Kp, int KC, int rtiles, int rows_pad, const float2 *__restrict__ UA,
                             __nv_bfloat16 *__restrict__ R16)
 {
-    const size_t per_tile = (size_t)KC * 128 * 8;
+    const size_t per_tile = (size_t)KC * U_BN * 8;
     const size_t total = (size_t)M * rtiles * per_tile;
     const int half = Kp / 8;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
         const size_t tile = e / per_tile;
         const int within = (int)(e - tile * per_tile);
-        const int c = within / (128 * 8), i = (within / 8) & 127, el = within & 7;
+        const int c = within / (U_BN * 8), i = (within / 8) & (U_BN - 1), el = within & 7;
         const int m = (int)(tile / rtiles), rt = (int)(tile - (size_t)m * rtiles);
         const int part = c / half, kk = (c - part * half) * 8 + el;
         const int rs = rt * U_RS + (i >> 1), kind = i & 1;
@@ -421,14 +451,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 
 // X[M][xcols][xrows] float2 as a 2-D FP32 tensor: x = 2 * rs + (re, im), y = m * xcols + col;
 // boxes of 32 floats (128 B) x 32 rows, 128-byte swizzle (the staging layout of the epilogue)
-static int make_xmap(pftcc_handle *h, CUtensorMap *map, void *X, int xrows, int xcols, int M)
+static int make_xmap(pftcc_handle *h, CUtensorMap *map, void *X, int xrows, int xcols, int nplanes)
 {
     auto enc = get_encode();
     if (!enc) return set_err(h, PFTCC_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     if (((uintptr_t)X & 15) != 0) return set_err(h, PFTCC_ERR_ARG, "X base not 16-byte aligned");
-    if (xrows % 64 != 0 || (long long)xcols * M >= (1LL << 31))
+    if (xrows % 64 != 0 || (long long)xcols * nplanes >= (1LL << 31))
         return set_err(h, PFTCC_ERR_ARG, "umma stage 1: X extents outside the tensor-map limits");
-    cuuint64_t dims[2] = {(cuuint64_t)2 * xrows, (cuuint64_t)xcols * M};
+    cuuint64_t dims[2] = {(cuuint64_t)2 * xrows, (cuuint64_t)xcols * nplanes};
     cuuint64_t strides[1] = {(cuuint64_t)xrows * sizeof(float2)};
     cuuint32_t box[2] = {32, 32};
     cuuint32_t estr[2] = {1, 1};
@@ -452,7 +482,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     if (prepare) {
         const int rtiles = rows_pad / U_RS;
         const int ptiles = (ncols_w + U_BM - 1) / U_BM;
-        const size_t r16 = (size_t)M * rtiles * KC * 128 * 8, p16 = (size_t)M * ptiles * KC * 128 * 8;
+        const size_t r16 = (size_t)M * rtiles * KC * U_BN * 8, p16 = (size_t)M * ptiles * KC * U_BM * 8;
         int st = ensure(h, (void **)&ws.A16, &ws.A16_elems, r16 * sizeof(__nv_bfloat16), "packed rows");
         if (st) return st;
         st = ensure(h, (void **)&ws.B16, &ws.B16_elems, p16 * sizeof(__nv_bfloat16), "packed particles");
@@ -484,7 +514,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     if (((uintptr_t)ws.A16 & 15) != 0 || ((uintptr_t)ws.B16 & 15) != 0)
         return set_err(h, PFTCC_ERR_ARG, "umma stage 1: packed operands not 16-byte aligned");
     CUtensorMap tmX;
-    int st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M);
+    int st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M - 1);   // Z has P = M - 1 planes
     if (st) return st;
     UmmaParams up{};
     up.M = M; up.Kp = Kp; up.KC = KC;
@@ -494,18 +524,19 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     // 1 KiB alignment slack, the particle tile, the N ring, 512 B of barriers and the
     // epilogue's staging tiles
     const size_t tail = 512 + STAGE_BYTES;
+    // both planes' particle tiles, and per ring stage both planes' row tiles
     int stages = 4;
-    while (stages > 2 && 1024 + a_bytes + stages * b_bytes + tail > 227 * 1024) --stages;
-    if (1024 + a_bytes + stages * b_bytes + tail > 227 * 1024)
+    while (stages > 1 && 1024 + 2 * a_bytes + stages * 2 * b_bytes + tail > 227 * 1024) --stages;
+    if (1024 + 2 * a_bytes + stages * 2 * b_bytes + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
     up.stages = stages;
     up.P16 = ws.B16; up.R16 = ws.A16;
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
-    const size_t smem = 1024 + a_bytes + stages * b_bytes + tail;
+    const size_t smem = 1024 + 2 * a_bytes + stages * 2 * b_bytes + tail;
     if ((e = cudaFuncSetAttribute(k_umma_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
-    const int nitems = M * n_ptiles;
+    const int nitems = ((M - 1) / 2 + 1) * n_ptiles;   // plane pairs x particle tiles
     const int grid = std::min(nitems, us.sms);
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE1);

@@ -25,6 +25,26 @@ struct Geom {
 
 // per-shift phase tables used by the exact kernels: shmat for a list of shifts is
 // generated on the device from argtransf in double precision (gen_shmat_8)
+// The packed spectrum the stage-2 transform consumes: for the Hermitian contraction
+// output X(m), m = 0..P, Z(j) = [X(j) + conj X(P-j)] + i [X(j) - conj X(P-j)] w_N^{-j}
+// (j < P; X(0) and X(P) taken as real), whose length-P DFT z(l) = y(2l) + i y(2l+1)
+// gives every rotation's correlation sum y(rot) = sum_{m<N} X(m) w_N^{-m rot}.
+__device__ __forceinline__ float2 make_z(float2 a, float2 b, float2 wn)   // a = X(j), b = X(P-j)
+{
+    const float2 E = make_float2(a.x + b.x, a.y - b.y);
+    const float ox = a.x - b.x, oy = a.y + b.y;
+    const float2 O = make_float2(ox * wn.x - oy * wn.y, ox * wn.y + oy * wn.x);
+    return make_float2(E.x - O.y, E.y + O.x);
+}
+
+// w_N^{-j} in single precision (FP64 angle, rounded once)
+__device__ __forceinline__ float2 wn_of(int j, int N)
+{
+    double s, c;
+    sincospi(-2.0 * j / N, &s, &c);
+    return make_float2((float)c, (float)s);
+}
+
 struct Work {           // one (reference, shift) correlation for the particle of a group
     int iref;           // 0-based
     int ishift;         // index into the shift list (-1 = no shift, gencorrs_cc_1)
