@@ -51,11 +51,13 @@ def parse():
     ap.add_argument("--ntop", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
-    ap.add_argument("--report", default="", choices=["", "precision", "refine"],
+    ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
+    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
                          "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
                          "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
-                         "prints a report line instead of the bench line)")
+                         "prints a report line instead of the bench line); batching: a queue of chunks of the "
+                         "three batching geometries, U[50,300] references x U[500,5000] particles each")
     ap.add_argument("--grid-ptcls", type=int, default=200, help="particles whose problems also run the exhaustive grid")
     ap.add_argument("--report-ptcls", type=int, default=256, help="particles in the precision sample")
     return ap.parse_args()
@@ -199,7 +201,7 @@ def algorithmic_costs(w, nshifts, kernel):
     if kernel == "stage1":
         return 3.0 * F * trip, 0.0               # BF16 hi+lo: three issued products
     if kernel == "stage2":
-        return 0.0, trip * (P + 1) * 8.0         # the contraction output read back once
+        return 0.0, trip * P * 8.0               # stage 1's packed spectrum Z (P planes) read back once
     if kernel == "polarize":
         return 0.0, w.nptcls * (w.box * (w.box // 2 + 1) * 8.0 + Ks * P * 8.0)
     return 0.0, 0.0
@@ -508,8 +510,46 @@ def run_refine_report(args):
     pc.kill()
 
 
+# ------------------------------------------------------------------ batching report
+def run_batching_report(args):
+    """The batching workload: --chunks chunks, each of a geometry drawn from box 64 /
+    nrots 128 / k 2..20, box 128 / nrots 360 / k 2..40 and box 200 / nrots 600 / k 2..60
+    with U[50,300] references and U[500,5000] particles, searched (BF16 split, FP32 re-score
+    of the top 8) through the chunk queue with one and with two worker streams; inputs are
+    resident on the device; every chunk's result must be the same in both runs."""
+    import torch
+    pkg = entry.load_package()
+    b = pkg.batching
+    rng = np.random.default_rng(2024)
+    spec = [(str(rng.choice(list("ABC"))), int(rng.integers(50, 301)), int(rng.integers(500, 5001)))
+            for _ in range(args.chunks)]
+    cache = {}
+    t0 = time.perf_counter()
+    chunks = [b.synthetic_chunk(g, nr, npt, seed=i, ref_cache=cache) for i, (g, nr, npt) in enumerate(spec)]
+    t_gen = time.perf_counter() - t0
+    evals = sum(ch.evals() for ch in chunks)
+    for g in "ABC":                                   # warm-up: one small chunk per geometry
+        b.search_chunk(b.synthetic_chunk(g, 20, 200, seed=999, ref_cache=cache))
+    out = {"report": "batching", "chunks": len(chunks),
+           "geometry_chunks": {g: sum(1 for s_ in spec if s_[0] == g) for g in "ABC"},
+           "particles": sum(s_[2] for s_ in spec), "evals": evals, "data_seconds": round(t_gen, 1)}
+    results = {}
+    for workers in (1, 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        results[workers] = b.SearchQueue(workers=workers).run(chunks)
+        t = time.perf_counter() - t0
+        out[f"workers_{workers}"] = {"seconds": round(t, 3), "evals_per_s": evals / t, "chunks_per_s": len(chunks) / t}
+    out["identical_results"] = all(np.array_equal(a.view(np.int32).reshape(len(a), -1), c.view(np.int32).reshape(len(c), -1))
+                                   for a, c in zip(results[1], results[2]))
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.report == "batching":
+        run_batching_report(args)
+        return
     if args.report == "precision":
         run_precision_report(args)
         return

@@ -66,7 +66,7 @@ cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int fir
     const Geom &g = h->g;
     const long long img_elems = (long long)g.box * (g.box / 2 + 1);
     const size_t smem = (size_t)img_elems * sizeof(float2);
-    cudaError_t e = cudaFuncSetAttribute(k_polarize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_polarize, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_POLARIZE);
@@ -393,7 +393,7 @@ cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, cons
     cudaError_t e;
     const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
     if (frame == PFTCC_FRAME_PTCL) {
-        e = cudaFuncSetAttribute(k_exact<PFTCC_FRAME_PTCL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = smem_limit((const void *)k_exact<PFTCC_FRAME_PTCL>, smem);
         if (e != cudaSuccess) return e;
         PFTCC_LAUNCH(h);
         KTimer kt(h, PFTCC_K_EXACT);
@@ -401,7 +401,7 @@ cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, cons
             h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
             h->argtransf1, groups, work, shifts, mode, cc1_kstop, out, best);
     } else {
-        e = cudaFuncSetAttribute(k_exact<PFTCC_FRAME_REF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = smem_limit((const void *)k_exact<PFTCC_FRAME_REF>, smem);
         if (e != cudaSuccess) return e;
         PFTCC_LAUNCH(h);
         KTimer kt(h, PFTCC_K_EXACT);

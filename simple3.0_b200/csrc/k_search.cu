@@ -463,13 +463,13 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_NORM);
     if (g.P % 4 == 0) {
-        if ((e = cudaFuncSetAttribute(k_norm<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = smem_limit((const void *)k_norm<4>, smem))) return e;
         k_norm<4><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     } else if (g.P % 2 == 0) {
-        if ((e = cudaFuncSetAttribute(k_norm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = smem_limit((const void *)k_norm<2>, smem))) return e;
         k_norm<2><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     } else {
-        if ((e = cudaFuncSetAttribute(k_norm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+        if ((e = smem_limit((const void *)k_norm<1>, smem))) return e;
         k_norm<1><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     }
     return cudaGetLastError();
@@ -736,7 +736,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     // particle spectra and CTF^2 spectra
     {
         const size_t smem = N * sizeof(double2) + (size_t)Ks * P * (sizeof(float2) + sizeof(float));
-        CKE(cudaFuncSetAttribute(k_spec_ptcl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+        CKE(smem_limit((const void *)k_spec_ptcl, smem), "attr");
         PFTCC_LAUNCH(h);
         KTimer kt(h, PFTCC_K_SPEC_PTCL);
         k_spec_ptcl<<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, d_perm, np, cols_pad, ws.UB, ws.CV,
@@ -747,14 +747,14 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         CKE(cudaGetLastError(), "cand_init");
     }
     const size_t smem_ref = N * sizeof(double2) + (size_t)Ks * P * sizeof(float2);
-    CKE(cudaFuncSetAttribute(k_spec_ref, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ref), "attr");
+    CKE(smem_limit((const void *)k_spec_ref, smem_ref), "attr");
     const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
-    CKE(cudaFuncSetAttribute(k_stage1_fp32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s1), "attr");
+    CKE(smem_limit((const void *)k_stage1_fp32, smem_s1), "attr");
     int T = 128;
     while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
     const size_t smem_s2 = 2 * (size_t)P * sizeof(float2) + (size_t)P * T * sizeof(float2) +
                            (size_t)(W_rows + 8) * (sizeof(float) + sizeof(int));
-    CKE(cudaFuncSetAttribute(k_stage2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s2), "attr");
+    CKE(smem_limit((const void *)k_stage2, smem_s2), "attr");
     S2Params sp{};
     sp.N = N; sp.P = P; sp.nf = plan.nf; sp.T = T;
     for (int i = 0; i < plan.nf; ++i) sp.f[i] = plan.f[i];
@@ -802,8 +802,12 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                 CKE(launch_norm(h, g, ws.RU + (size_t)h->nrefs * J * Ks, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
                                 ws.sqp, ws.D, fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N)), "norm");
                 if (fast_s2) {
-                    CKE(launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
-                                           ws.cand, ccall_dev, d_perm), "stage2");
+                    e = launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
+                                           ws.cand, ccall_dev, d_perm);
+                    if (e != cudaSuccess)
+                        return set_err(h, e == cudaErrorMemoryAllocation ? PFTCC_ERR_OOM : PFTCC_ERR_CUDA,
+                                       "stage2 (P " + std::to_string(P) + ", rows " + std::to_string(rows) + ", columns " +
+                                           std::to_string(cols) + "): " + cudaGetErrorString(e));
                 } else {
                     sp.rows = rows; sp.xrows = rows_t; sp.xcols = cols_t; sp.row0 = row0; sp.r0 = r_lo;
                     sp.dcols = cols_t; sp.col0 = c0;

@@ -20,6 +20,7 @@
 #include "pftcc_internal.cuh"
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 
 namespace pftcc {
@@ -579,7 +580,7 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
     const size_t smem = (size_t)P1 * P2 * ROWS * sizeof(float2) + (size_t)ROWS * (sizeof(float) + sizeof(int)) +
                         (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
     auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, true> : k_stage2_fast<P1, P2, ROWS, false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE2);
@@ -611,7 +612,7 @@ static cudaError_t launch_rs(pftcc_handle *h, int ncols, int ntop, int Ks, int n
     fill_tw(tw, P);
     const int T = 64, per_block = T / ntop;
     const size_t smem = (size_t)P * T * (sizeof(float2) + sizeof(float));
-    cudaError_t e = cudaFuncSetAttribute(k_rescore_md<P1, P2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit((const void *)k_rescore_md<P1, P2>, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_EXACT);

@@ -534,7 +534,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
     const size_t smem = 1024 + 2 * a_bytes + stages * 2 * b_bytes + tail;
-    if ((e = cudaFuncSetAttribute(k_umma_stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    if ((e = smem_limit((const void *)k_umma_stage1, smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
     const int nitems = ((M - 1) / 2 + 1) * n_ptiles;   // plane pairs x particle tiles
     const int grid = std::min(nitems, us.sms);

@@ -19,6 +19,27 @@ int set_err(pftcc_handle *h, int code, const std::string &msg)
     return code;
 }
 
+cudaError_t smem_limit(const void *kernel, size_t bytes)
+{
+    struct Limit { int dev; const void *fn; size_t max; };
+    static std::mutex mu;
+    static std::vector<Limit> known;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const Limit &l : known)
+        if (l.dev == dev && l.fn == kernel) return bytes <= l.max ? cudaSuccess : cudaErrorInvalidValue;
+    int optin = 0;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    if ((e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess) return e;
+    const int max = optin - (int)fa.sharedSizeBytes;
+    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max)) != cudaSuccess) return e;
+    known.push_back(Limit{dev, kernel, (size_t)max});
+    return bytes <= (size_t)max ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 int cuda_err(pftcc_handle *h, cudaError_t e, const char *what)
 {
     if (e == cudaSuccess) return PFTCC_OK;

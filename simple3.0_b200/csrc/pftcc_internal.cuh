@@ -156,6 +156,12 @@ struct KTimer {
 
 namespace pftcc {
 
+// Lets `kernel` use `bytes` of dynamic shared memory: its limit is raised once per device to
+// the device's opt-in maximum (less the kernel's static shared memory) -- one fixed value,
+// so concurrent callers that launch the kernel with different sizes never lower the limit
+// under each other; cudaErrorInvalidValue when `bytes` exceeds it.
+cudaError_t smem_limit(const void *kernel, size_t bytes);
+
 int set_err(pftcc_handle *h, int code, const std::string &msg);
 int cuda_err(pftcc_handle *h, cudaError_t e, const char *what);
 int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what);
