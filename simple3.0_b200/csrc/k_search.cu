@@ -702,8 +702,10 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     // (re)allocate the workspace when the geometry or counts change
     const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M;
     if (realloc) {
-        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref};
-        for (void *b : bufs) if (b) cudaFree(b);
+        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref,
+                        ws.A16, ws.B16, ws.best};
+        for (void *b : bufs) dev_free(h, b);
+        umma_free(h);
         ws = SearchWS{};
         int st;
         if ((st = ensure_ws(h, (void **)&ws.UA, (size_t)M * rows_pad * Ks * sizeof(float2), "UA")) ||

@@ -560,7 +560,7 @@ int umma_check(pftcc_handle *h)
 void umma_free(pftcc_handle *h)
 {
     UmmaState &us = ustate(h);
-    if (us.err) cudaFree(us.err);
+    dev_free(h, us.err);
     us.err = nullptr;
 }
 

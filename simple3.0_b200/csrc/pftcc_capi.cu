@@ -47,24 +47,52 @@ int cuda_err(pftcc_handle *h, cudaError_t e, const char *what)
     return set_err(h, code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device memory comes from the device's stream-ordered pool, which keeps up to 32 GB of freed
+// memory for reuse: handles created and killed one after another (a queue of chunks) reuse
+// the same memory instead of returning to the driver for every buffer.
+static cudaError_t pool_ready(int dev)
+{
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    for (int d : done)
+        if (d == dev) return cudaSuccess;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, dev);
+    if (e != cudaSuccess) return e;
+    unsigned long long keep = 32ull << 30;   // bytes of freed memory the pool holds on to
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    done.push_back(dev);
+    return cudaSuccess;
+}
+
 int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what)
 {
     *p = nullptr;
     if (bytes == 0) return PFTCC_OK;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = pool_ready(h->dev);
+    if (e == cudaSuccess) e = cudaMallocAsync(p, bytes, h->stream);
+    // the buffer may next be used on another stream (pftcc_set_stream): complete the allocation
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
-        return set_err(h, PFTCC_ERR_OOM, std::string("cudaMalloc failed for ") + what + " (" +
+        return set_err(h, PFTCC_ERR_OOM, std::string("device allocation failed for ") + what + " (" +
                                               std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
     }
     return PFTCC_OK;
 }
 
+// returns a buffer to the pool in the order of the handle's stream (after its last use there)
+void dev_free(pftcc_handle *h, void *p)
+{
+    if (p) cudaFreeAsync(p, h->stream);
+}
+
 int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *what)
 {
     if (*cap >= bytes && *p) return PFTCC_OK;
-    if (*p) cudaFree(*p);
+    if (*p) dev_free(h, *p);
     *p = nullptr;
     *cap = 0;
     int st = dev_alloc(h, p, bytes, what);
@@ -244,8 +272,7 @@ static void free_all(pftcc_handle *h)
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
                     h->ws.D, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
                     h->ws.cand_ref};
-    for (void *p : ptrs)
-        if (p) cudaFree(p);
+    for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
     for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
@@ -409,8 +436,7 @@ int pftcc_reallocate_ptcls(pftcc_handle *h, int nptcls, const int *pinds)
     if (nptcls != h->nptcls) {
         CK(cudaStreamSynchronize(h->stream), "sync");
         void *old[] = {h->ptcls, h->sqsums, h->d_iseven, h->d_ctfp, h->ctfmats};
-        for (void *p : old)
-            if (p) cudaFree(p);
+        for (void *p : old) dev_free(h, p);
         h->ptcls = nullptr; h->sqsums = nullptr; h->d_iseven = nullptr; h->d_ctfp = nullptr; h->ctfmats = nullptr;
         h->nptcls = nptcls;
         ST(alloc_ptcl_arrays(h));
@@ -632,7 +658,7 @@ int pftcc_polarize_refs(pftcc_handle *h, int first_iref, int n, const float *cma
     h->ptcls = save_p;
     h->sqsums = save_s;
     cudaError_t e2 = cudaStreamSynchronize(h->stream);
-    cudaFree(dummy);
+    dev_free(h, dummy);
     CK(e, "polarize refs");
     CK(e2, "polarize refs");
     return PFTCC_OK;

@@ -165,6 +165,7 @@ cudaError_t smem_limit(const void *kernel, size_t bytes);
 int set_err(pftcc_handle *h, int code, const std::string &msg);
 int cuda_err(pftcc_handle *h, cudaError_t e, const char *what);
 int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what);
+void dev_free(pftcc_handle *h, void *p);
 int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *what);
 
 // ---- kernels (launch wrappers return cudaError_t of the launch) ---------------------
