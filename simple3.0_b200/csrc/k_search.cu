@@ -218,10 +218,9 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
     }
 }
 
-// |ref|^2 spectra over P points (FP64): RU[r][j][k], and the same values j-fastest in
-// RUt[r][k][j] (the normaliser's coalesced layout)
+// |ref|^2 spectra over P points (FP64): RU[r][j][k]
 __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *__restrict__ refs,
-                                                          double2 *__restrict__ RU, double2 *__restrict__ RUt)
+                                                          double2 *__restrict__ RU)
 {
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
     const int r = blockIdx.x;
@@ -238,7 +237,6 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *
             ui += u * sn;
         }
         RU[(size_t)r * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
-        RUt[(size_t)r * J * Ks + (size_t)k * J + j] = make_double2(ur, ui);
     }
 }
 
@@ -329,65 +327,104 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 // rotation-dependent normaliser D(rho) = (1/P) sum_j wgt_j Re[Y(j) w_P^{+j rho}] with
 // Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k] (wgt_j = 1 at j = 0 and j = P/2, else 2),
 // all in FP64; stored as the factor Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col))
-// the correlations are scaled by.  One block per particle column: the column's CTF^2
-// spectra are staged in shared memory once, k-major, and reused for every reference of
-// the wave (whose |ref|^2 spectra, read j-fastest from RUt, stay in L2).  References are
-// taken NORM_RB = 32 at a time:
-//   phase Y: threads over (reference, j), j fastest, contract the Ks shells with
-//            coalesced global and conflict-free shared loads;
-//   phase D: lane = reference, each thread NORM_GPT residues g < P/Q, and for each g
-//            the Q rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q}
-//            Y(j) w_P^{j g}, D(g + q P/Q) = Re sum_r i_Q^{q r} S_r (i_Q = exp(2 pi i/Q));
-//            the twiddles w_P^{j g} come from an FP64 table in shared memory and are
-//            the same for the whole warp (broadcast reads).
+// the correlations are scaled by.  Two kernels per wave:
+//   k_norm_y: Y for every (reference, particle) pair of the wave as a batched complex
+//            GEMM over the shells -- a block takes 32 references x 64 particles and 8
+//            values of j, stages the j-th |ref|^2 and CTF^2 spectra of its tile in shared
+//            memory (k-major), and each thread accumulates 2 references x 4 particles;
+//            Y[rl][cl][j], scaled by wgt_j / P;
+//   k_norm:  D from Y, one block per particle column, NORM_RB = 32 references at a time:
+//            lane = reference, each thread NORM_GPT residues g < P/Q, and for each g the Q
+//            rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q} Y(j) w_P^{j g},
+//            D(g + q P/Q) = Re sum_r i_Q^{q r} S_r (i_Q = exp(2 pi i/Q)); the twiddles
+//            w_P^{j g} come from an FP64 table in shared memory and are the same for the
+//            whole warp (broadcast reads).
 // Layouts of the stored factor: p2 == 0, natural Dinv[rl][col][rho] (P values); p2 > 0,
 // the order in which the split-radix stage 2 (P = P1 x p2) visits the rotations,
 // Dinv[rl][col][l2][l1][b] for rot = 2 (l2 + p2 l1) + b (2P values, rho = rot mod P),
 // multiplied by dscale.
 constexpr int NORM_RB = 32;
 constexpr int NORM_GPT = 3;
+constexpr int NY_R = 32, NY_C = 64, NY_J = 8;
+
+__global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
+                                                int r0, int nr, int c0, int ncols, double2 *__restrict__ Y)
+{
+    extern __shared__ double2 sy[];
+    const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
+    double2 *sr = sy;                        // [Ks][NY_R] |ref|^2 spectra of the tile's references
+    double2 *sc = sy + (size_t)Ks * NY_R;    // [Ks][NY_C] CTF^2 spectra of the tile's particles
+    const int cb = blockIdx.x * NY_C, rb = blockIdx.y * NY_R, j0 = blockIdx.z * NY_J;
+    const int tc = threadIdx.x & 15, tr = threadIdx.x >> 4;   // particles tc + 16 q, references tr + 16 i
+    const double2 zero = make_double2(0.0, 0.0);
+    const double invP = 1.0 / P;
+    for (int j = j0; j < min(J, j0 + NY_J); ++j) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < NY_R * Ks; e += blockDim.x) {
+            const int r = e / Ks, k = e - r * Ks;
+            sr[(size_t)k * NY_R + r] = rb + r < nr ? RU[((size_t)(r0 + rb + r) * J + j) * Ks + k] : zero;
+        }
+        for (int e = threadIdx.x; e < NY_C * Ks; e += blockDim.x) {
+            const int c = e / Ks, k = e - c * Ks;
+            sc[(size_t)k * NY_C + c] = cb + c < ncols ? CV[((size_t)(c0 + cb + c) * J + j) * Ks + k] : zero;
+        }
+        __syncthreads();
+        double yr[2][4], yi[2][4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) yr[i][q] = yi[i][q] = 0.0;
+        for (int k = 0; k < Ks; ++k) {
+            double2 u[2], v[4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) u[i] = sr[(size_t)k * NY_R + tr + 16 * i];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v[q] = sc[(size_t)k * NY_C + tc + 16 * q];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    yr[i][q] = fma(u[i].x, v[q].x, fma(u[i].y, v[q].y, yr[i][q]));     // conj(u) * v
+                    yi[i][q] = fma(u[i].x, v[q].y, fma(-u[i].y, v[q].x, yi[i][q]));
+                }
+        }
+        const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = rb + tr + 16 * i, c = cb + tc + 16 * q;
+                if (r < nr && c < ncols) Y[((size_t)r * ncols + c) * J + j] = make_double2(wgt * yr[i][q], wgt * yi[i][q]);
+            }
+    }
+}
 
 template <int Q>
-__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ RUt, const double2 *__restrict__ CV,
-                                              int r0, int nr, int c0, int ncols, int dcols,
-                                              const float *__restrict__ sqp, float *__restrict__ D, int p2,
+__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ Yg, int nr, int c0, int ncols,
+                                              int dcols, const float *__restrict__ sqp, float *__restrict__ D, int p2,
                                               double dscale)
 {
     extern __shared__ double2 sd[];
-    const int P = g.P, Ks = g.Ks, J = P / 2 + 1, G = P / Q, Jp = J | 1;
+    const int P = g.P, J = P / 2 + 1, G = P / Q, Jp = J | 1;
     const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 2 * P : P;
-    double2 *cvs = sd;                          // [Ks][J]
-    double2 *Y = cvs + (size_t)J * Ks;          // [NORM_RB][Jp], scaled by wgt_j / P
+    double2 *Y = sd;                            // [NORM_RB][Jp], scaled by wgt_j / P
     double2 *tw = Y + (size_t)NORM_RB * Jp;     // [P] w_P^{+e}
     const int cl = blockIdx.x;
     if (cl >= ncols) return;
     const int col = c0 + cl;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
-        const int j = e / Ks, k = e - j * Ks;
-        cvs[(size_t)k * J + j] = CV[(size_t)col * J * Ks + e];
-    }
     for (int e = threadIdx.x; e < P; e += blockDim.x) {
         double s, c;
         sincospi(2.0 * e / P, &s, &c);
         tw[e] = make_double2(c, s);
     }
     const double sq = (double)sqp[col];
-    const double invP = 1.0 / P;
-    __syncthreads();
     for (int rb0 = 0; rb0 < nr; rb0 += NORM_RB) {
         const int nb = min(NORM_RB, nr - rb0);
+        __syncthreads();
         for (int it = threadIdx.x; it < nb * J; it += blockDim.x) {
             const int rb = it / J, j = it - rb * J;
-            const double2 *ru = RUt + (size_t)(r0 + rb0 + rb) * J * Ks + j;
-            double yr = 0.0, yi = 0.0;
-            for (int k = 0; k < Ks; ++k) {
-                const double2 u = __ldg(ru + (size_t)k * J), v = cvs[(size_t)k * J + j];
-                yr = fma(u.x, v.x, fma(u.y, v.y, yr));     // conj(u) * v
-                yi = fma(u.x, v.y, fma(-u.y, v.x, yi));
-            }
-            const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
-            Y[(size_t)rb * Jp + j] = make_double2(wgt * yr, wgt * yi);
+            Y[(size_t)rb * Jp + j] = Yg[((size_t)(rb0 + rb) * ncols + cl) * J + j];
         }
         __syncthreads();
         if (lane < nb) {
@@ -454,23 +491,32 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
     }
 }
 
-static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RUt, const double2 *CV, int r0, int nr,
-                               int c0, int ncols, int dcols, const float *sqp, float *D, int p2, double dscale)
+static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU, const double2 *CV, int r0, int nr,
+                               int c0, int ncols, int dcols, const float *sqp, double2 *Y, float *D, int p2,
+                               double dscale)
 {
     const int J = g.P / 2 + 1;
-    const size_t smem = ((size_t)J * g.Ks + (size_t)NORM_RB * (J | 1) + g.P) * sizeof(double2);
     cudaError_t e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_NORM);
+    {
+        const size_t smem = (size_t)g.Ks * (NY_R + NY_C) * sizeof(double2);
+        if ((e = smem_limit((const void *)k_norm_y, smem))) return e;
+        dim3 grid((ncols + NY_C - 1) / NY_C, (nr + NY_R - 1) / NY_R, (J + NY_J - 1) / NY_J);
+        k_norm_y<<<grid, 256, smem, h->stream>>>(g, RU, CV, r0, nr, c0, ncols, Y);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    PFTCC_LAUNCH(h);
+    const size_t smem = ((size_t)NORM_RB * (J | 1) + g.P) * sizeof(double2);
     if (g.P % 4 == 0) {
         if ((e = smem_limit((const void *)k_norm<4>, smem))) return e;
-        k_norm<4><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+        k_norm<4><<<ncols, 256, smem, h->stream>>>(g, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     } else if (g.P % 2 == 0) {
         if ((e = smem_limit((const void *)k_norm<2>, smem))) return e;
-        k_norm<2><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+        k_norm<2><<<ncols, 256, smem, h->stream>>>(g, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     } else {
         if ((e = smem_limit((const void *)k_norm<1>, smem))) return e;
-        k_norm<1><<<ncols, 256, smem, h->stream>>>(g, RUt, CV, r0, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+        k_norm<1><<<ncols, 256, smem, h->stream>>>(g, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
     }
     return cudaGetLastError();
 }
@@ -702,7 +748,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     // (re)allocate the workspace when the geometry or counts change
     const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M;
     if (realloc) {
-        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref,
+        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.Yn, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref,
                         ws.A16, ws.B16, ws.best};
         for (void *b : bufs) dev_free(h, b);
         umma_free(h);
@@ -710,9 +756,10 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         int st;
         if ((st = ensure_ws(h, (void **)&ws.UA, (size_t)M * rows_pad * Ks * sizeof(float2), "UA")) ||
             (st = ensure_ws(h, (void **)&ws.UB, (size_t)M * cols_pad * Ks * sizeof(float2), "UB")) ||
-            (st = ensure_ws(h, (void **)&ws.RU, 2 * (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
+            (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
             (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
             (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * 2 * P * sizeof(float), "D")) ||
+            (st = ensure_ws(h, (void **)&ws.Yn, (size_t)nr_wave_max * W_cols * J * sizeof(double2), "Y")) ||
             (st = ensure_ws(h, (void **)&ws.X, (size_t)M * W_rows * W_cols * sizeof(float2), "X")) ||
             (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||
             (st = ensure_ws(h, (void **)&ws.sqp, (size_t)cols_pad * sizeof(float), "sqp")) ||
@@ -772,7 +819,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         const float2 *refs = grp == 0 ? h->refs_even : h->refs_odd;
         PFTCC_LAUNCH(h);
         { KTimer kt(h, PFTCC_K_SPEC_REF);
-        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU, ws.RU + (size_t)h->nrefs * J * Ks);
+        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
         CKE(cudaGetLastError(), "spec_r2");
         PFTCC_LAUNCH(h);
         k_spec_ref<<<rows_pad, SPEC_THREADS, smem_ref, h->stream>>>(g, ns, refs, ws.shifts, h->argtransf, h->argtransf1,
@@ -801,8 +848,8 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                     CKE(cudaGetLastError(), "stage1");
                 }
                 // the split-radix stage 2 reads the factor in its visiting order, times 1/(2N)
-                CKE(launch_norm(h, g, ws.RU + (size_t)h->nrefs * J * Ks, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
-                                ws.sqp, ws.D, fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N)), "norm");
+                CKE(launch_norm(h, g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t, ws.sqp, ws.Yn, ws.D,
+                                fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N)), "norm");
                 if (fast_s2) {
                     e = launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
                                            ws.cand, ccall_dev, d_perm);

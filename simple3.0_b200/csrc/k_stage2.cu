@@ -385,11 +385,6 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         // this row's reference: its factors in visiting order, 2P per (reference, column)
         const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * (2 * P);
         const float2 *xr = Xc + row;
-        if (active && row + ROWS < sp.rows) {
-            // the next row of this thread: pull its spectrum towards L2 while this one is transformed
-            const float2 *xn = xr + ROWS;
-            for (int j = role; j < P; j += 2) asm volatile("prefetch.global.L2 [%0];" ::"l"(xn + (size_t)j * plane));
-        }
         auto getx = [&](int j) {
             float2 v;
             asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"

@@ -270,7 +270,7 @@ static void free_all(pftcc_handle *h)
     void *ptrs[] = {h->refs_even, h->refs_odd, h->ptcls, h->sqsums, h->ctfmats, h->d_iseven, h->d_ctfp, h->polar,
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
-                    h->ws.D, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
+                    h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
                     h->ws.cand_ref};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
