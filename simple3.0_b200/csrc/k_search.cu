@@ -41,6 +41,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
                 const float2 *UB, int c0, int ncols_w, int cols_pad, float2 *X, int prepare, int parity_group);
 bool stage2_fast_supported(int P);
 int stage2_fast_p2(int P);
+int stage2_fast_dlen(int P);
 cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
                                int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
                                float2 *cand, float *ccall, const int *perm);
@@ -340,9 +341,10 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 //            w_P^{j g} come from an FP64 table in shared memory and are the same for the
 //            whole warp (broadcast reads).
 // Layouts of the stored factor: p2 == 0, natural Dinv[rl][col][rho] (P values); p2 > 0,
-// the order in which the split-radix stage 2 (P = P1 x p2) visits the rotations,
-// Dinv[rl][col][l2][l1][b] for rot = 2 (l2 + p2 l1) + b (2P values, rho = rot mod P),
-// multiplied by dscale.
+// the order in which the split-radix stage 2 (P = P1 x p2) reads them, block pairs
+// (l2, l2 + 1) of its pass B: Dinv[rl][col][l2 >> 1][l1][b][l2 & 1] for
+// rot = 2 (l2 + p2 l1) + b (rho = rot mod P; for odd p2 lane 1 of the last pair repeats
+// l2 = p2 - 1; 4 P1 ceil(p2 / 2) values), multiplied by dscale.
 constexpr int NORM_RB = 32;
 constexpr int NORM_GPT = 3;
 constexpr int NY_R = 32, NY_C = 64, NY_J = 8;
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
 {
     extern __shared__ double2 sd[];
     const int P = g.P, J = P / 2 + 1, G = P / Q, Jp = J | 1;
-    const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 2 * P : P;
+    const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 4 * p1 * ((p2 + 1) / 2) : P;
     double2 *Y = sd;                            // [NORM_RB][Jp], scaled by wgt_j / P
     double2 *tw = Y + (size_t)NORM_RB * Jp;     // [P] w_P^{+e}
     const int cl = blockIdx.x;
@@ -479,8 +481,10 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
                             const float v = (float)(dscale / sqrt(d * sq));
 #pragma unroll
                             for (int h = 0; h < 2; ++h) {   // rot = rho and rho + P
-                                const int rot = rho + h * P, l = rot >> 1;
-                                dst[((l % p2) * p1 + l / p2) * 2 + (rot & 1)] = v;
+                                const int rot = rho + h * P, l = rot >> 1, l2 = l % p2;
+                                float *o = dst + ((((l2 >> 1) * p1 + l / p2) * 2 + (rot & 1)) * 2 + (l2 & 1));
+                                o[0] = v;
+                                if ((p2 & 1) && l2 == p2 - 1) o[1] = v;
                             }
                         }
                     }
@@ -758,7 +762,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
             (st = ensure_ws(h, (void **)&ws.UB, (size_t)M * cols_pad * Ks * sizeof(float2), "UB")) ||
             (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
             (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
-            (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * 2 * P * sizeof(float), "D")) ||
+            (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * std::max(2 * P, stage2_fast_dlen(P)) * sizeof(float), "D")) ||
             (st = ensure_ws(h, (void **)&ws.Yn, (size_t)nr_wave_max * W_cols * J * sizeof(double2), "Y")) ||
             (st = ensure_ws(h, (void **)&ws.X, (size_t)M * W_rows * W_cols * sizeof(float2), "X")) ||
             (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||

@@ -29,6 +29,8 @@ constexpr int TW_MAX = 320;
 struct TwTables {
     float2 wP[TW_MAX];   // w_P^{-e} = exp(-2 pi i e / P), e < P
     float2 wN[TW_MAX];   // w_N^{-e} = exp(-2 pi i e / N), e < P
+    // the same w_P^{-e} = (c, s) as lane pairs for the two-lane transforms: (c, c), (s, s), (-s, -s)
+    float2 pc[TW_MAX], ps[TW_MAX], pn[TW_MAX];
 };
 
 __device__ __forceinline__ float2 c_mul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -114,29 +116,172 @@ template <int STEP> struct SFFT<1, STEP> {
     __device__ static void run(float2 *, const TwTables &) {}
 };
 
-// pass A over the packed spectrum Z itself (the search path, where stage 1 stores Z):
-// classes c in [c0, c1), each a length-P2 DFT over j2 of Z(c + P1 j2), times w_P^{-c l2},
-// into the row's slab; the next class's P2 loads are issued before this class's transform
-template <int P1, int P2, class GetZ>
-__device__ __forceinline__ void passA_z(int c0, int c1, const GetZ &getz, float2 *slab, int T, const TwTables &tw)
+// ---------------------------------------------------------------------------------------
+// Two transforms at once with the packed two-lane FP32 instructions of sm_100 (one
+// add / mul / fma on a register pair): C2 holds two complex numbers as r = (re_a, re_b),
+// i = (im_a, im_b), so a butterfly of two independent transforms costs half the
+// instructions of two scalar ones.  Each lane is rounded exactly as the scalar operation.
+struct C2 { float2 r, i; };
+__device__ __forceinline__ float2 f2_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2_sub(float2 a, float2 b)
 {
-    float2 zn[P2];
-    if (c0 < c1) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(*reinterpret_cast<unsigned long long *>(&a)),
+        "l"(*reinterpret_cast<unsigned long long *>(&b)));
+    return *reinterpret_cast<float2 *>(&d);
+}
+__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2_s(float s) { return make_float2(s, s); }
+__device__ __forceinline__ C2 p_add(const C2 &a, const C2 &b) { return {f2_add(a.r, b.r), f2_add(a.i, b.i)}; }
+__device__ __forceinline__ C2 p_sub(const C2 &a, const C2 &b) { return {f2_sub(a.r, b.r), f2_sub(a.i, b.i)}; }
+// a * (c + i s) with c, s and -s given as lane pairs
+__device__ __forceinline__ C2 p_twid(const C2 &a, float2 c, float2 s, float2 ns)
+{
+    return {f2_fma(a.r, c, f2_mul(a.i, ns)), f2_fma(a.r, s, f2_mul(a.i, c))};
+}
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
+// the radix-2/3/4/5 butterflies above, on lane pairs (-i a = (a.i, -a.r) is folded into
+// the adds that follow it)
+template <int F> struct PBfly;
+template <> struct PBfly<2> {
+    __device__ static void run(C2 *v) { const C2 a = v[0], b = v[1]; v[0] = p_add(a, b); v[1] = p_sub(a, b); }
+};
+template <> struct PBfly<4> {
+    __device__ static void run(C2 *v)
+    {
+        const C2 t0 = p_add(v[0], v[2]), t1 = p_sub(v[0], v[2]);
+        const C2 t2 = p_add(v[1], v[3]), d = p_sub(v[1], v[3]);
+        v[0] = p_add(t0, t2);
+        v[2] = p_sub(t0, t2);
+        v[1] = {f2_add(t1.r, d.i), f2_sub(t1.i, d.r)};
+        v[3] = {f2_sub(t1.r, d.i), f2_add(t1.i, d.r)};
+    }
+};
+template <> struct PBfly<3> {
+    __device__ static void run(C2 *v)
+    {
+        const float s3 = 0.86602540378443865f;
+        const C2 a = v[0], t1 = p_add(v[1], v[2]), d = p_sub(v[1], v[2]);
+        const C2 t2 = {f2_fma(t1.r, f2_s(-0.5f), a.r), f2_fma(t1.i, f2_s(-0.5f), a.i)};
+        v[0] = p_add(a, t1);
+        v[1] = {f2_fma(d.i, f2_s(s3), t2.r), f2_fma(d.r, f2_s(-s3), t2.i)};
+        v[2] = {f2_fma(d.i, f2_s(-s3), t2.r), f2_fma(d.r, f2_s(s3), t2.i)};
+    }
+};
+template <> struct PBfly<5> {
+    __device__ static void run(C2 *v)
+    {
+        const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+        const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+        const C2 a = v[0];
+        const C2 t1 = p_add(v[1], v[4]), t2 = p_add(v[2], v[3]);
+        const C2 t3 = p_sub(v[1], v[4]), t4 = p_sub(v[2], v[3]);
+        const C2 m1 = {f2_fma(t2.r, f2_s(c2), f2_fma(t1.r, f2_s(c1), a.r)), f2_fma(t2.i, f2_s(c2), f2_fma(t1.i, f2_s(c1), a.i))};
+        const C2 m2 = {f2_fma(t2.r, f2_s(c1), f2_fma(t1.r, f2_s(c2), a.r)), f2_fma(t2.i, f2_s(c1), f2_fma(t1.i, f2_s(c2), a.i))};
+        const C2 n1 = {f2_fma(t4.r, f2_s(s2), f2_mul(t3.r, f2_s(s1))), f2_fma(t4.i, f2_s(s2), f2_mul(t3.i, f2_s(s1)))};
+        const C2 n2 = {f2_fma(t4.r, f2_s(-s1), f2_mul(t3.r, f2_s(s2))), f2_fma(t4.i, f2_s(-s1), f2_mul(t3.i, f2_s(s2)))};
+        v[0] = p_add(p_add(a, t1), t2);
+        v[1] = {f2_add(m1.r, n1.i), f2_sub(m1.i, n1.r)};
+        v[4] = {f2_sub(m1.r, n1.i), f2_add(m1.i, n1.r)};
+        v[2] = {f2_add(m2.r, n2.i), f2_sub(m2.i, n2.r)};
+        v[3] = {f2_sub(m2.r, n2.i), f2_add(m2.i, n2.r)};
+    }
+};
+
+// two length-L forward DFTs, one per lane, natural order in and out (SFFT's recursion)
+template <int L, int STEP> struct PFFT {
+    static constexpr int F = SFFT<L, STEP>::F;
+    static constexpr int M = L / F;
+    __device__ static void run(C2 *x, const TwTables &tw)
+    {
+        C2 s[F][M];
 #pragma unroll
-        for (int j2 = 0; j2 < P2; ++j2) zn[j2] = getz(c0 + P1 * j2);
+        for (int q = 0; q < F; ++q)
+#pragma unroll
+            for (int j = 0; j < M; ++j) s[q][j] = x[q + F * j];
+#pragma unroll
+        for (int q = 0; q < F; ++q) PFFT<M, STEP * F>::run(s[q], tw);
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            C2 v[F];
+#pragma unroll
+            for (int q = 0; q < F; ++q) {
+                const int e = q * k * STEP;
+                v[q] = (q * k == 0) ? s[q][k] : p_twid(s[q][k], tw.pc[e], tw.ps[e], tw.pn[e]);
+            }
+            PBfly<F>::run(v);
+#pragma unroll
+            for (int r = 0; r < F; ++r) x[k + M * r] = v[r];
+        }
+    }
+};
+template <int STEP> struct PFFT<1, STEP> {
+    __device__ static void run(C2 *, const TwTables &) {}
+};
+
+// Row slab of the search (two-lane layout): pass-A output (l2, j1) -- re and im as two
+// scalars -- sits in lane l2 & 1 of the float2 slots ((l2 >> 1) P1 + j1) 2 + part
+// (part 0 = re, 1 = im), element stride T, so that pass B reads the pair of blocks
+// (l2, l2 + 1) with one 8-byte load per part.  For odd P2 the last block l2 = P2 - 1 is
+// stored in both lanes.
+
+// pass A of the search over the packed spectrum Z, two classes per step: c and cb = c + 1
+// (c again for the last class of an odd range), one per lane -- a length-P2 DFT over j2
+// of Z(c + P1 j2), times w_P^{-c l2} (lane-pair twiddles twa / twb, entry c P2 + l2), into
+// the slab; the next pair's 2 P2 loads are issued before this pair's transform
+template <int P1, int P2, class GetZ>
+__device__ __forceinline__ void passA_pk(int c0, int c1, const GetZ &getz, float2 *slab, int T, const float4 *twa,
+                                         const float2 *twb, const TwTables &tw)
+{
+    float2 na[P2], nb[P2];
+    if (c0 < c1) {
+        const int cb = min(c0 + 1, c1 - 1);
+#pragma unroll
+        for (int j2 = 0; j2 < P2; ++j2) {
+            na[j2] = getz(c0 + P1 * j2);
+            nb[j2] = getz(cb + P1 * j2);
+        }
     }
 #pragma unroll 1
-    for (int c = c0; c < c1; ++c) {
-        float2 z[P2];
+    for (int c = c0; c < c1; c += 2) {
+        const int cb = min(c + 1, c1 - 1);
+        C2 z[P2];
 #pragma unroll
-        for (int j2 = 0; j2 < P2; ++j2) z[j2] = zn[j2];
-        if (c + 1 < c1) {
+        for (int j2 = 0; j2 < P2; ++j2) z[j2] = {make_float2(na[j2].x, nb[j2].x), make_float2(na[j2].y, nb[j2].y)};
+        if (c + 2 < c1) {
+            const int cn = c + 2, cnb = min(c + 3, c1 - 1);
 #pragma unroll
-            for (int j2 = 0; j2 < P2; ++j2) zn[j2] = getz(c + 1 + P1 * j2);
+            for (int j2 = 0; j2 < P2; ++j2) {
+                na[j2] = getz(cn + P1 * j2);
+                nb[j2] = getz(cnb + P1 * j2);
+            }
         }
-        SFFT<P2, P1>::run(z, tw);
+        PFFT<P2, P1>::run(z, tw);
+        float2 *sa = slab + (size_t)c * 2 * T, *sb = slab + (size_t)cb * 2 * T;
 #pragma unroll
-        for (int l2 = 0; l2 < P2; ++l2) slab[(l2 * P1 + c) * T] = l2 == 0 ? z[l2] : c_mul(z[l2], tw.wP[c * l2]);
+        for (int l2 = 0; l2 < P2; ++l2) {
+            C2 o = z[l2];
+            if (l2 > 0) {
+                const float4 w = twa[c * P2 + l2];
+                o = p_twid(o, make_float2(w.x, w.y), make_float2(w.z, w.w), twb[c * P2 + l2]);
+            }
+            const int q = (l2 >> 1) * P1 * 2;
+#pragma unroll
+            for (int ln = 0; ln < 2; ++ln) {
+                if (ln != (l2 & 1) && !((P2 & 1) && l2 == P2 - 1)) continue;
+                reinterpret_cast<float *>(sa + q * T)[ln] = o.r.x;
+                reinterpret_cast<float *>(sa + (q + 1) * T)[ln] = o.i.x;
+                reinterpret_cast<float *>(sb + q * T)[ln] = o.r.y;
+                reinterpret_cast<float *>(sb + (q + 1) * T)[ln] = o.i.y;
+            }
+        }
     }
 }
 
@@ -235,98 +380,98 @@ __device__ __forceinline__ void passB(int L0, int L1, const float2 *slab, int T,
     }
 }
 
-// the normalising factors of pass-B block l2, stored in visiting order: d[2 l1 + b]
-// belongs to rot = 2 (l2 + P2 l1) + b (and already carries the 1/(2N) scale)
-template <int P1>
-__device__ __forceinline__ void load_dblock(const float *Dp, int l2, float (&d)[2 * P1])
+// pass B on the block pair (l, l + 1), l even: two length-P1 DFTs (one per lane) of the
+// slab blocks, times the normalising factors -- stored in pair order, four per l1:
+// (l, re), (l + 1, re), (l, im), (l + 1, im), already carrying the 1/(2N) scale -- leaving
+// the correlation of rot = 2 (l + lane + P2 l1) + part in lane `lane` of v[l1].r / v[l1].i
+template <int P1, int P2>
+__device__ __forceinline__ void passB_pair(int l, const float2 *slab, int T, const TwTables &tw, const float4 *Dp,
+                                           C2 (&v)[P1])
 {
-    if constexpr (P1 % 2 == 0) {
-        const float4 *d4 = reinterpret_cast<const float4 *>(Dp + (size_t)l2 * 2 * P1);
+    const float2 *sq = slab + (size_t)(l >> 1) * P1 * 2 * T;
 #pragma unroll
-        for (int i = 0; i < P1 / 2; ++i) {
-            const float4 t = __ldg(d4 + i);
-            d[4 * i] = t.x; d[4 * i + 1] = t.y; d[4 * i + 2] = t.z; d[4 * i + 3] = t.w;
-        }
-    } else {
-        const float2 *d2 = reinterpret_cast<const float2 *>(Dp + (size_t)l2 * 2 * P1);
+    for (int j1 = 0; j1 < P1; ++j1) v[j1] = {sq[(2 * j1) * T], sq[(2 * j1 + 1) * T]};
+    PFFT<P1, P2>::run(v, tw);
+    const float4 *dq = Dp + (size_t)(l >> 1) * P1;
 #pragma unroll
-        for (int i = 0; i < P1; ++i) {
-            const float2 t = __ldg(d2 + i);
-            d[2 * i] = t.x; d[2 * i + 1] = t.y;
-        }
+    for (int l1 = 0; l1 < P1; ++l1) {
+        const float4 d = __ldg(dq + l1);
+        v[l1].r = f2_mul(v[l1].r, make_float2(d.x, d.y));
+        v[l1].i = f2_mul(v[l1].i, make_float2(d.z, d.w));
     }
 }
 
-// pass B of the search for l2 in [L0, L1): the maximum correlation and its rotation
-// (lowest rotation among equal maxima).  Each block's 2 P1 values are reduced with
-// fmaxf; afterwards the winning block -- every block when another one reached the same
-// maximum -- is evaluated again by the same loop body (identical values) and scanned
-// for the lowest rotation holding the maximum.
+// pass B of the search for the block pairs (l, l + 1), l = L0, L0 + 2, ... < L1 (L0 even;
+// for odd P2 the pair (P2 - 1, P2) holds block P2 - 1 twice): the maximum correlation and
+// its rotation (lowest rotation among equal maxima).  Each pair's 4 P1 values are reduced
+// with max; afterwards the winning pair -- every pair when another one reached the same
+// maximum -- is evaluated again by the same code (identical values) and scanned for the
+// lowest rotation holding the maximum.
 template <int P1, int P2>
 __device__ __forceinline__ void passB_search(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
-                                             const float *Dp, float &best, int &brot)
+                                             const float4 *Dp, float &best, int &brot)
 {
     float bv = -INFINITY;
-    int bl2 = -1, l2 = L0, lend = L1, stage = 0, rmin = 0x7fffffff;
+    int bl = -1, l = L0, lend = L1, stage = 0, rmin = 0x7fffffff;
     bool tie = false;
 #pragma unroll 1
     while (true) {
-        float2 v[P1];
-#pragma unroll
-        for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
-        SFFT<P1, P2>::run(v, tw);
-        float d[2 * P1];
-        load_dblock<P1>(Dp, l2, d);
-        float c[2 * P1];
-#pragma unroll
-        for (int l1 = 0; l1 < P1; ++l1) {
-            c[2 * l1] = v[l1].x * d[2 * l1];
-            c[2 * l1 + 1] = v[l1].y * d[2 * l1 + 1];
-        }
+        C2 v[P1];
+        passB_pair<P1, P2>(l, slab, T, tw, Dp, v);
         if (stage == 0) {
-            float m = c[0];
+            float m = fmaxf(v[0].r.x, v[0].r.y);
+            m = max3f(m, v[0].i.x, v[0].i.y);
 #pragma unroll
-            for (int e = 1; e < 2 * P1; ++e) m = fmaxf(m, c[e]);
-            if (m > bv) { bv = m; bl2 = l2; tie = false; }
+            for (int l1 = 1; l1 < P1; ++l1) {
+                m = max3f(m, v[l1].r.x, v[l1].r.y);
+                m = max3f(m, v[l1].i.x, v[l1].i.y);
+            }
+            if (m > bv) { bv = m; bl = l; tie = false; }
             else if (m == bv) tie = true;
-            if (++l2 < L1) continue;
-            if (bl2 < 0) break;
+            l += 2;
+            if (l < L1) continue;
+            if (bl < 0) break;
             stage = 1;
-            l2 = tie ? L0 : bl2;
-            lend = tie ? L1 : bl2 + 1;
+            l = tie ? L0 : bl;
+            lend = tie ? L1 : bl + 2;
         } else {
+            const int lb = min(l + 1, P2 - 1);
 #pragma unroll
-            for (int e = 0; e < 2 * P1; ++e)
-                if (c[e] == bv) rmin = min(rmin, 2 * (l2 + P2 * (e >> 1)) + (e & 1));
-            if (++l2 >= lend) break;
+            for (int l1 = 0; l1 < P1; ++l1) {
+                const int ra = 2 * (l + P2 * l1), rb = 2 * (lb + P2 * l1);
+                if (v[l1].r.x == bv) rmin = min(rmin, ra);
+                if (v[l1].i.x == bv) rmin = min(rmin, ra + 1);
+                if (v[l1].r.y == bv) rmin = min(rmin, rb);
+                if (v[l1].i.y == bv) rmin = min(rmin, rb + 1);
+            }
+            l += 2;
+            if (l >= lend) break;
         }
     }
     best = bv;
-    brot = bl2 < 0 ? 0 : rmin;
+    brot = bl < 0 ? 0 : rmin;
 }
 
 // pass B writing every correlation (corr_all), with the per-rotation argmax
 template <int P1, int P2>
 __device__ __forceinline__ void passB_all(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
-                                          const float *Dp, float *cc_out, float &best, int &brot)
+                                          const float4 *Dp, float *cc_out, float &best, int &brot)
 {
 #pragma unroll 1
-    for (int l2 = L0; l2 < L1; ++l2) {
-        float2 v[P1];
-#pragma unroll
-        for (int j1 = 0; j1 < P1; ++j1) v[j1] = slab[(l2 * P1 + j1) * T];
-        SFFT<P1, P2>::run(v, tw);
-        float d[2 * P1];
-        load_dblock<P1>(Dp, l2, d);
+    for (int l = L0; l < L1; l += 2) {
+        C2 v[P1];
+        passB_pair<P1, P2>(l, slab, T, tw, Dp, v);
+        const bool two = l + 1 < P2;
 #pragma unroll
         for (int l1 = 0; l1 < P1; ++l1) {
-            const int l = l2 + P2 * l1;
-            const int r0 = 2 * l, r1 = 2 * l + 1;
-            const float c0 = v[l1].x * d[2 * l1], c1 = v[l1].y * d[2 * l1 + 1];
-            cc_out[r0] = c0;
-            cc_out[r1] = c1;
-            if (c0 > best || (c0 == best && r0 < brot)) { best = c0; brot = r0; }
-            if (c1 > best || (c1 == best && r1 < brot)) { best = c1; brot = r1; }
+            const float cv[4] = {v[l1].r.x, v[l1].i.x, v[l1].r.y, v[l1].i.y};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                if (e >= 2 && !two) continue;
+                const int r = 2 * (l + (e >> 1) + P2 * l1) + (e & 1);
+                cc_out[r] = cv[e];
+                if (cv[e] > best || (cv[e] == best && r < brot)) { best = cv[e]; brot = r; }
+            }
         }
     }
 }
@@ -355,37 +500,61 @@ struct S2Fast {
     int rows, xrows, xcols, row0, nshifts, r0, dcols, col0, N, nrs_total;
 };
 
+// the normalising factors per (reference, particle) in the order the search's pass B
+// reads them: 4 P1 values per block pair, ceil(P2 / 2) pairs (the last pair of an odd P2
+// repeats block P2 - 1)
+template <int P1, int P2> __host__ __device__ constexpr int s2_dlen() { return 4 * P1 * ((P2 + 1) / 2); }
+
+// (c, id) ranks above (c2, id2): larger correlation, then lower id
+__device__ __forceinline__ bool ranks_above(float c, int id, float c2, int id2) { return c > c2 || (c == c2 && id < id2); }
+
 // ROWS rows in flight per block, two threads per row: warp w < ROWS/32 (role 0) and warp
 // w + ROWS/32 (role 1) share the rows' slabs and meet at named barrier 1 + w twice per row
-// (after pass A; after pass B, when role 1 hands its argmax over).
+// (after pass A; after pass B, when role 1 hands its argmax over).  Role 0 keeps its rows'
+// running top-8 in registers; at the end the block merges those lists with the
+// particle's running top-8.
 // X here is the packed spectrum Z, P planes of [col][row].
 template <int P1, int P2, int ROWS, bool WRITE>
 __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
                                                             const float *__restrict__ Dinv, float2 *__restrict__ cand,
                                                             float *__restrict__ ccall, const int *__restrict__ perm)
 {
-    constexpr int P = P1 * P2;
+    constexpr int P = P1 * P2, Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>();
     using SP = RowSplit<P1, P2>;
     extern __shared__ float4 smem4[];
     const int t = threadIdx.x;
     const int role = t >= ROWS, lr = t - role * ROWS;
     const int bar = 1 + (lr >> 5);
-    float2 *slab = reinterpret_cast<float2 *>(smem4) + lr;                       // [P][ROWS]
-    float *xfer_c = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * ROWS);   // [ROWS]
-    int *xfer_r = reinterpret_cast<int *>(xfer_c + ROWS);                                             // [ROWS]
-    float *ccs = reinterpret_cast<float *>(xfer_r + ROWS);                                            // [rows + 8]
-    int *ids = reinterpret_cast<int *>(ccs + sp.rows + 8);
+    float2 *slab = reinterpret_cast<float2 *>(smem4) + lr;                                      // [Q2 P1 2][ROWS]
+    float4 *twa = smem4 + (size_t)Q2 * P1 * ROWS;                                               // [P1 P2]
+    float2 *twb = reinterpret_cast<float2 *>(twa + P1 * P2);                                    // [P1 P2]
+    float *xfer_c = reinterpret_cast<float *>(twb + P1 * P2);                                   // [ROWS]
+    int *xfer_r = reinterpret_cast<int *>(xfer_c + ROWS);                                       // [ROWS]
+    // lane-pair twiddles of pass A: lane a class c, lane b class min(c + 1, end of c's half - 1)
+    for (int e = t; e < P1 * P2; e += blockDim.x) {
+        const int c = e / P2, l2 = e - c * P2;
+        const int cb = min(c + 1, (c < P1 / 2 ? P1 / 2 : P1) - 1);
+        const float2 wa = tw.wP[c * l2], wb = tw.wP[cb * l2];
+        twa[e] = make_float4(wa.x, wb.x, wa.y, wb.y);
+        twb[e] = make_float2(-wa.y, -wb.y);
+    }
+    __syncthreads();
     const int cl = blockIdx.x;
     const size_t plane = (size_t)sp.xcols * sp.xrows;
     const float2 *Xc = X + (size_t)cl * sp.xrows;
+    float kc[8];
+    int ki[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { kc[k] = -INFINITY; ki[k] = 0x7fffffff; }
     for (int base = 0; base < sp.rows; base += ROWS) {
         const int row = base + lr;
         const bool active = row < sp.rows;
         const int grow = sp.row0 + row;
-        // this row's reference: its factors in visiting order, 2P per (reference, column)
-        const float *Dr = Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * (2 * P);
+        // this row's reference: its factors in pass-B order
+        const float4 *Dr = reinterpret_cast<const float4 *>(
+            Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * DLEN);
         const float2 *xr = Xc + row;
-        auto getx = [&](int j) {
+        auto getz = [&](int j) {
             float2 v;
             asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
                          : "=f"(v.x), "=f"(v.y)
@@ -393,9 +562,8 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
             return v;
         };
         if (active) {
-            // both halves share the class-pair and pass-B code; only their ranges differ
             // the two halves of the row take the classes [0, P1/2) and [P1/2, P1) of Z
-            passA_z<P1, P2>(role == 0 ? 0 : P1 / 2, role == 0 ? P1 / 2 : P1, getx, slab, ROWS, tw);
+            passA_pk<P1, P2>(role == 0 ? 0 : P1 / 2, role == 0 ? P1 / 2 : P1, getz, slab, ROWS, twa, twb, tw);
         }
         asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
         float best = -INFINITY;
@@ -415,20 +583,39 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
             const float oc = xfer_c[lr];
             const int orot = xfer_r[lr];
             if (oc > best || (oc == best && orot < brot)) { best = oc; brot = orot; }
-            ccs[row] = best;
-            ids[row] = grow * sp.N + brot;
+            if (best != -INFINITY) {
+                // insert into the running top-8 (kept sorted)
+                float c = best;
+                int id = grow * sp.N + brot;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    if (ranks_above(c, id, kc[k], ki[k])) {
+                        const float tc = kc[k];
+                        const int ti = ki[k];
+                        kc[k] = c; ki[k] = id; c = tc; id = ti;
+                    }
+                }
+            }
         }
     }
-    // merge with the particle's running top-8 (lowest id among equal correlations)
+    // merge the role-0 lists with the particle's running top-8 (lowest id among equal
+    // correlations); the slab space holds the candidates now
+    __syncthreads();
+    float *ccs = reinterpret_cast<float *>(smem4);                 // [8 ROWS + 8]
+    int *ids = reinterpret_cast<int *>(ccs + 8 * ROWS + 8);
+    if (role == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { ccs[8 * lr + k] = kc[k]; ids[8 * lr + k] = ki[k]; }
+    }
     float2 *cp = cand + (size_t)(sp.col0 + cl) * 8;
     if (t < 8) {
         const float2 c = cp[t];
-        ccs[sp.rows + t] = c.x;
-        ids[sp.rows + t] = __float_as_int(c.y);
+        ccs[8 * ROWS + t] = c.x;
+        ids[8 * ROWS + t] = __float_as_int(c.y);
     }
     __syncthreads();
     if (t < 32) {
-        const int n = sp.rows + 8;
+        const int n = 8 * ROWS + 8;
         float keep_c = -INFINITY;
         int keep_i = -1;
         for (int it = 0; it < 8; ++it) {
@@ -437,13 +624,13 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
             for (int e = t; e < n; e += 32) {
                 const float c = ccs[e];
                 const int id = ids[e];
-                if (c != -INFINITY && (c > bc || (c == bc && id < bi))) { bc = c; bi = id; bpos = e; }
+                if (c != -INFINITY && ranks_above(c, id, bc, bi)) { bc = c; bi = id; bpos = e; }
             }
             for (int o = 16; o > 0; o >>= 1) {
                 const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
                 const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
                 const int op = __shfl_xor_sync(0xffffffffu, bpos, o);
-                if (oc > bc || (oc == bc && oi < bi)) { bc = oc; bi = oi; bpos = op; }
+                if (ranks_above(oc, oi, bc, bi)) { bc = oc; bi = oi; bpos = op; }
             }
             if (t == it) { keep_c = bc; keep_i = bc == -INFINITY ? -1 : bi; }
             if (bpos >= 0 && t == (bpos & 31)) ccs[bpos] = -INFINITY;
@@ -556,6 +743,9 @@ static void fill_tw(TwTables &tw, int P)
         const double a = -2.0 * M_PI * e / P, b = -2.0 * M_PI * e / (2.0 * P);
         tw.wP[e] = make_float2((float)cos(a), (float)sin(a));
         tw.wN[e] = make_float2((float)cos(b), (float)sin(b));
+        tw.pc[e] = make_float2(tw.wP[e].x, tw.wP[e].x);
+        tw.ps[e] = make_float2(tw.wP[e].y, tw.wP[e].y);
+        tw.pn[e] = make_float2(-tw.wP[e].y, -tw.wP[e].y);
     }
 }
 
@@ -564,16 +754,28 @@ bool stage2_fast_supported(int P) { return P == 64 || P == 180 || P == 300; }
 // the inner factor P2 of the split P = P1 x P2 used for each supported length
 int stage2_fast_p2(int P) { return P == 64 ? 8 : P == 180 ? 15 : P == 300 ? 20 : 0; }
 
+// floats of normalising factors per (reference, particle) the search's pass B reads
+int stage2_fast_dlen(int P)
+{
+    switch (P) {
+    case 64: return s2_dlen<8, 8>();
+    case 180: return s2_dlen<12, 15>();
+    case 300: return s2_dlen<15, 20>();
+    default: return P;
+    }
+}
+
 template <int P1, int P2>
 static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
                              float2 *cand, float *ccall, const int *perm)
 {
     TwTables tw;
     fill_tw(tw, P1 * P2);
-    // row slabs of P complex: 128 rows in flight up to P = 200, 64 beyond; two threads per row
+    // row slabs of P complex (the two-lane layout): 128 rows in flight up to P = 200, 64
+    // beyond; two threads per row
     constexpr int ROWS = P1 * P2 <= 200 ? 128 : 64;
-    const size_t smem = (size_t)P1 * P2 * ROWS * sizeof(float2) + (size_t)ROWS * (sizeof(float) + sizeof(int)) +
-                        (size_t)(sp.rows + 8) * (sizeof(float) + sizeof(int));
+    const size_t smem = (size_t)((P2 + 1) / 2) * P1 * 2 * ROWS * sizeof(float2) +
+                        (size_t)P1 * P2 * (sizeof(float4) + sizeof(float2)) + (size_t)ROWS * (sizeof(float) + sizeof(int));
     auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, true> : k_stage2_fast<P1, P2, ROWS, false>;
     cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
