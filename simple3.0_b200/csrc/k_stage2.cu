@@ -232,37 +232,33 @@ template <int STEP> struct PFFT<1, STEP> {
 // (l2, l2 + 1) with one 8-byte load per part.  For odd P2 the last block l2 = P2 - 1 is
 // stored in both lanes.
 
+// the loads of class pair (c, cb) of one row: Z(c + P1 j2) and Z(cb + P1 j2)
+template <int P1, int P2, class GetZ>
+__device__ __forceinline__ void load_pair(int c, int cb, const GetZ &getz, float2 (&na)[P2], float2 (&nb)[P2])
+{
+#pragma unroll
+    for (int j2 = 0; j2 < P2; ++j2) {
+        na[j2] = getz(c + P1 * j2);
+        nb[j2] = getz(cb + P1 * j2);
+    }
+}
+
 // pass A of the search over the packed spectrum Z, two classes per step: c and cb = c + 1
 // (c again for the last class of an odd range), one per lane -- a length-P2 DFT over j2
 // of Z(c + P1 j2), times w_P^{-c l2} (lane-pair twiddles twa / twb, entry c P2 + l2), into
-// the slab; the next pair's 2 P2 loads are issued before this pair's transform
+// the slab.  na / nb hold the first pair's loads on entry (issued by the caller during the
+// previous row's pass B); the next pair's 2 P2 loads are issued before each transform.
 template <int P1, int P2, class GetZ>
 __device__ __forceinline__ void passA_pk(int c0, int c1, const GetZ &getz, float2 *slab, int T, const float4 *twa,
-                                         const float2 *twb, const TwTables &tw)
+                                         const float2 *twb, const TwTables &tw, float2 (&na)[P2], float2 (&nb)[P2])
 {
-    float2 na[P2], nb[P2];
-    if (c0 < c1) {
-        const int cb = min(c0 + 1, c1 - 1);
-#pragma unroll
-        for (int j2 = 0; j2 < P2; ++j2) {
-            na[j2] = getz(c0 + P1 * j2);
-            nb[j2] = getz(cb + P1 * j2);
-        }
-    }
 #pragma unroll 1
     for (int c = c0; c < c1; c += 2) {
         const int cb = min(c + 1, c1 - 1);
         C2 z[P2];
 #pragma unroll
         for (int j2 = 0; j2 < P2; ++j2) z[j2] = {make_float2(na[j2].x, nb[j2].x), make_float2(na[j2].y, nb[j2].y)};
-        if (c + 2 < c1) {
-            const int cn = c + 2, cnb = min(c + 3, c1 - 1);
-#pragma unroll
-            for (int j2 = 0; j2 < P2; ++j2) {
-                na[j2] = getz(cn + P1 * j2);
-                nb[j2] = getz(cnb + P1 * j2);
-            }
-        }
+        if (c + 2 < c1) load_pair<P1, P2>(c + 2, min(c + 3, c1 - 1), getz, na, nb);
         PFFT<P2, P1>::run(z, tw);
         float2 *sa = slab + (size_t)c * 2 * T, *sb = slab + (size_t)cb * 2 * T;
 #pragma unroll
@@ -388,16 +384,18 @@ template <int P1, int P2>
 __device__ __forceinline__ void passB_pair(int l, const float2 *slab, int T, const TwTables &tw, const float4 *Dp,
                                            C2 (&v)[P1])
 {
+    const float4 *dq = Dp + (size_t)(l >> 1) * P1;
+    float4 d[P1];
+#pragma unroll
+    for (int l1 = 0; l1 < P1; ++l1) d[l1] = __ldg(dq + l1);   // issued ahead of the transform
     const float2 *sq = slab + (size_t)(l >> 1) * P1 * 2 * T;
 #pragma unroll
     for (int j1 = 0; j1 < P1; ++j1) v[j1] = {sq[(2 * j1) * T], sq[(2 * j1 + 1) * T]};
     PFFT<P1, P2>::run(v, tw);
-    const float4 *dq = Dp + (size_t)(l >> 1) * P1;
 #pragma unroll
     for (int l1 = 0; l1 < P1; ++l1) {
-        const float4 d = __ldg(dq + l1);
-        v[l1].r = f2_mul(v[l1].r, make_float2(d.x, d.y));
-        v[l1].i = f2_mul(v[l1].i, make_float2(d.z, d.w));
+        v[l1].r = f2_mul(v[l1].r, make_float2(d[l1].x, d[l1].y));
+        v[l1].i = f2_mul(v[l1].i, make_float2(d[l1].z, d[l1].w));
     }
 }
 
@@ -546,6 +544,20 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
     int ki[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { kc[k] = -INFINITY; ki[k] = 0x7fffffff; }
+    // the two halves of a row take the classes [0, P1/2) and [P1/2, P1) of Z
+    const int ca = role == 0 ? 0 : P1 / 2, ce = role == 0 ? P1 / 2 : P1;
+    auto zload = [&](int row) {
+        const float2 *xr = Xc + row;
+        return [=](int j) {
+            float2 v;
+            asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
+                         : "=f"(v.x), "=f"(v.y)
+                         : "l"(xr + (size_t)j * plane));
+            return v;
+        };
+    };
+    float2 na[P2], nb[P2];   // the first class pair of this thread's next row
+    if (lr < sp.rows) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(lr), na, nb);
     for (int base = 0; base < sp.rows; base += ROWS) {
         const int row = base + lr;
         const bool active = row < sp.rows;
@@ -553,19 +565,9 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         // this row's reference: its factors in pass-B order
         const float4 *Dr = reinterpret_cast<const float4 *>(
             Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * DLEN);
-        const float2 *xr = Xc + row;
-        auto getz = [&](int j) {
-            float2 v;
-            asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
-                         : "=f"(v.x), "=f"(v.y)
-                         : "l"(xr + (size_t)j * plane));
-            return v;
-        };
-        if (active) {
-            // the two halves of the row take the classes [0, P1/2) and [P1/2, P1) of Z
-            passA_pk<P1, P2>(role == 0 ? 0 : P1 / 2, role == 0 ? P1 / 2 : P1, getz, slab, ROWS, twa, twb, tw);
-        }
+        if (active) passA_pk<P1, P2>(ca, ce, zload(row), slab, ROWS, twa, twb, tw, na, nb);
         asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
+        if (row + ROWS < sp.rows) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(row + ROWS), na, nb);
         float best = -INFINITY;
         int brot = 0;
         if (active) {
