@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
                                                             const float *__restrict__ Dinv, float2 *__restrict__ cand,
                                                             float *__restrict__ ccall, const int *__restrict__ perm)
 {
-    constexpr int P = P1 * P2, Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>();
+    constexpr int Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>();
     using SP = RowSplit<P1, P2>;
     extern __shared__ float4 smem4[];
     const int t = threadIdx.x;
