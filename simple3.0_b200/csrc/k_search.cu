@@ -30,6 +30,7 @@
 //                 into the particle's running top-8 (cc, rs*N + rot)
 //   k_finish      top-1, or the exact FP32 re-score of the top-ntop (ref, shift)
 #include "pftcc_internal.cuh"
+#include "spec_fft.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -217,6 +218,217 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl(
         }
         CV[(size_t)col * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
     }
+}
+
+// The same spectra by FP64 transforms of length N = N1 * N2 (spec_fft.cuh), shells in
+// batches of sfft::KB: (reference, shift) rows UA[m][rs][k], one block per row.  The shifted
+// polar samples a(n, k) are formed exactly as in k_spec_ref (FP32 products with the
+// single-precision shift phases of the de Moivre recurrence), a batch of shells at a time
+// ([shell][n] in shared memory), the recurrence state kept per angular sample n.
+template <int N1, int N2>
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref_fft(
+    Geom g, int nshifts, const float2 *__restrict__ refs, const float *__restrict__ shifts,
+    const double *__restrict__ argtransf, const double *__restrict__ argtransf1, int rs0, int nrs, int rows_pad,
+    float2 *__restrict__ UA)
+{
+    constexpr int N = N1 * N2, P = N / 2, NPT = (P + SPEC_THREADS - 1) / SPEC_THREADS;
+    extern __shared__ float4 smem4[];
+    const int Ks = g.Ks, M = P + 1;
+    double2 *tw = reinterpret_cast<double2 *>(smem4);                              // [N] w_N^{-e}
+    double2 *buf = tw + N;                                                          // the transform buffer
+    float2 *a = reinterpret_cast<float2 *>(buf + sfft::buf_elems<N1, N2>());       // [KB][P]
+    const int row = blockIdx.x;
+    const int rs = rs0 + row;
+    if (rs >= nrs) {   // zero padding rows
+        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+            const int m = e / Ks, k = e - m * Ks;
+            UA[((size_t)m * rows_pad + row) * Ks + k] = make_float2(0.f, 0.f);
+        }
+        return;
+    }
+    const int r = rs / nshifts, s = rs - r * nshifts;
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / N, &sn, &cs);
+        tw[e] = make_double2(cs, sn);
+    }
+    const float2 *R = refs + (size_t)r * g.K * P;
+    const double sx = shifts ? (double)shifts[2 * s] : 0.0, sy = shifts ? (double)shifts[2 * s + 1] : 0.0;
+    // gen_shmat_8 per angular sample: analytic first shell, de Moivre recurrence over k
+    double pr[NPT], pi[NPT], qr[NPT], qi[NPT];
+#pragma unroll
+    for (int i = 0; i < NPT; ++i) {
+        const int n = threadIdx.x + i * SPEC_THREADS;
+        pr[i] = 1.0; pi[i] = 0.0; qr[i] = 1.0; qi[i] = 0.0;
+        if (n < P) {
+            sincos(argtransf[n] * sx + argtransf[P + n] * sy, &pi[i], &pr[i]);
+            sincos(argtransf1[n] * sx + argtransf1[P + n] * sy, &qi[i], &qr[i]);
+        }
+    }
+    for (int k0 = 0; k0 < Ks; k0 += sfft::KB) {
+        const int nk = min(sfft::KB, Ks - k0);
+#pragma unroll
+        for (int i = 0; i < NPT; ++i) {
+            const int n = threadIdx.x + i * SPEC_THREADS;
+            if (n >= P) continue;
+            for (int kl = 0; kl < nk; ++kl) {
+                const float2 x = R[(size_t)(k0 + kl) * P + n];
+                const float fr = (float)pr[i], fi = (float)pi[i];
+                a[kl * P + n] = make_float2(x.x * fr - x.y * fi, x.x * fi + x.y * fr);
+                const double nr = pr[i] * qr[i] - pi[i] * qi[i], ni = pr[i] * qi[i] + pi[i] * qr[i];
+                pr[i] = nr; pi[i] = ni;
+            }
+        }
+        auto getf = [&](int kl, int n) {
+            const float2 v = a[kl * P + (n < P ? n : n - P)];
+            return make_double2((double)v.x, n < P ? (double)v.y : -(double)v.y);
+        };
+        auto put = [&](int kl, int m, double2 F) {
+            if (m <= P) {
+                const float2 u = (m & 1) ? make_float2((float)(0.5 * F.y), (float)(-0.5 * F.x))
+                                         : make_float2((float)(0.5 * F.x), (float)(0.5 * F.y));
+                UA[((size_t)m * rows_pad + row) * Ks + k0 + kl] = u;
+            }
+        };
+        sfft::batch_fft<N1, N2>(nk, getf, put, buf, tw);
+    }
+}
+
+// particle-side spectra by the FP64 transforms: UB[m][col][k] of B = |CTF| * ptcl and the
+// CTF^2 spectra CV[col][j][k] = sum_{n<P} CTF^2(n, k) w_P^{-jn} (the even outputs F(2j) / 2
+// of the transform of the real sequence continued periodically over the full circle)
+template <int N1, int N2>
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl_fft(
+    Geom g, const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const int *__restrict__ perm,
+    int ncols, int cols_pad, float2 *__restrict__ UB, double2 *__restrict__ CV, float *__restrict__ sqp_out,
+    const float *__restrict__ sqsums)
+{
+    constexpr int N = N1 * N2, P = N / 2, J = P / 2 + 1;
+    extern __shared__ float4 smem4[];
+    const int Ks = g.Ks, M = P + 1;
+    double2 *tw = reinterpret_cast<double2 *>(smem4);                              // [N]
+    double2 *buf = tw + N;
+    float2 *b = reinterpret_cast<float2 *>(buf + sfft::buf_elems<N1, N2>());       // [KB][P]
+    float *c2 = reinterpret_cast<float *>(b + sfft::KB * P);                        // [KB][P]
+    const int col = blockIdx.x;
+    if (col >= ncols) {
+        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+            const int m = e / Ks, k = e - m * Ks;
+            UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2(0.f, 0.f);
+        }
+        for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) CV[(size_t)col * J * Ks + e] = make_double2(0.0, 0.0);
+        if (threadIdx.x == 0) sqp_out[col] = 1.f;
+        return;
+    }
+    const int slot = perm[col];
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / N, &sn, &cs);
+        tw[e] = make_double2(cs, sn);
+    }
+    const float2 *Q = ptcls + (size_t)slot * g.K * P;
+    const float *C = ctfmats ? ctfmats + (size_t)slot * g.K * P : nullptr;
+    if (threadIdx.x == 0) sqp_out[col] = sqsums[slot];
+    for (int k0 = 0; k0 < Ks; k0 += sfft::KB) {
+        const int nk = min(sfft::KB, Ks - k0);
+        for (int e = threadIdx.x; e < nk * P; e += blockDim.x) {   // e = kl P + n
+            const float c = C ? C[(size_t)k0 * P + e] : 1.f;
+            const float2 q = Q[(size_t)k0 * P + e];
+            b[e] = make_float2(c * q.x, c * q.y);
+            c2[e] = c * c;
+        }
+        auto getf = [&](int kl, int n) {
+            const float2 v = b[kl * P + (n < P ? n : n - P)];
+            return make_double2((double)v.x, n < P ? (double)v.y : -(double)v.y);
+        };
+        auto put = [&](int kl, int m, double2 F) {
+            if (m <= P) {
+                const float2 u = (m & 1) ? make_float2((float)(0.5 * F.y), (float)(-0.5 * F.x))
+                                         : make_float2((float)(0.5 * F.x), (float)(0.5 * F.y));
+                UB[((size_t)m * cols_pad + col) * Ks + k0 + kl] = u;
+            }
+        };
+        sfft::batch_fft<N1, N2>(nk, getf, put, buf, tw);
+        auto getc = [&](int kl, int n) { return make_double2((double)c2[kl * P + (n < P ? n : n - P)], 0.0); };
+        auto putc = [&](int kl, int m, double2 F) {
+            if (!(m & 1) && m <= P) CV[(size_t)col * J * Ks + (size_t)(m >> 1) * Ks + k0 + kl] = make_double2(0.5 * F.x, 0.5 * F.y);
+        };
+        sfft::batch_fft<N1, N2>(nk, getc, putc, buf, tw);
+    }
+}
+
+template <int N1, int N2> static size_t spec_ref_fft_smem(int)
+{
+    return (size_t)N1 * N2 * sizeof(double2) + (size_t)sfft::buf_elems<N1, N2>() * sizeof(double2) +
+           (size_t)sfft::KB * (N1 * N2 / 2) * sizeof(float2);
+}
+template <int N1, int N2> static size_t spec_ptcl_fft_smem(int)
+{
+    return spec_ref_fft_smem<N1, N2>(0) + (size_t)sfft::KB * (N1 * N2 / 2) * sizeof(float);
+}
+
+// launches of the spectra kernels: the FFT forms for the supported lengths, the direct
+// sums otherwise (identical spectra up to FP64 rounding before the final FP32 / FP64 store)
+template <int N1, int N2>
+static cudaError_t launch_spec_ref_fft(pftcc_handle *h, const Geom &g, int ns, const float2 *refs, const float *shifts,
+                                       int nrs, int rows_pad, float2 *UA)
+{
+    const size_t smem = spec_ref_fft_smem<N1, N2>(0);
+    cudaError_t e = smem_limit((const void *)k_spec_ref_fft<N1, N2>, smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    k_spec_ref_fft<N1, N2><<<rows_pad, SPEC_THREADS, smem, h->stream>>>(g, ns, refs, shifts, h->argtransf,
+                                                                         h->argtransf1, 0, nrs, rows_pad, UA);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_spec_ref(pftcc_handle *h, const Geom &g, int ns, const float2 *refs, const float *shifts,
+                                   int nrs, int rows_pad, float2 *UA)
+{
+    switch (g.P) {
+    case 64: return launch_spec_ref_fft<16, 8>(h, g, ns, refs, shifts, nrs, rows_pad, UA);
+    case 180: return launch_spec_ref_fft<24, 15>(h, g, ns, refs, shifts, nrs, rows_pad, UA);
+    case 300: return launch_spec_ref_fft<24, 25>(h, g, ns, refs, shifts, nrs, rows_pad, UA);
+    default: break;
+    }
+    const size_t smem = g.N * sizeof(double2) + (size_t)g.Ks * g.P * sizeof(float2);
+    cudaError_t e = smem_limit((const void *)k_spec_ref, smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    k_spec_ref<<<rows_pad, SPEC_THREADS, smem, h->stream>>>(g, ns, refs, shifts, h->argtransf, h->argtransf1, 0, nrs,
+                                                            rows_pad, UA);
+    return cudaGetLastError();
+}
+
+template <int N1, int N2>
+static cudaError_t launch_spec_ptcl_fft(pftcc_handle *h, const Geom &g, const float *ctf, const int *perm, int np,
+                                        int cols_pad, float2 *UB, double2 *CV, float *sqp)
+{
+    const size_t smem = spec_ptcl_fft_smem<N1, N2>(0);
+    cudaError_t e = smem_limit((const void *)k_spec_ptcl_fft<N1, N2>, smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    k_spec_ptcl_fft<N1, N2><<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, perm, np, cols_pad, UB, CV,
+                                                                          sqp, h->sqsums);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_spec_ptcl(pftcc_handle *h, const Geom &g, const float *ctf, const int *perm, int np,
+                                    int cols_pad, float2 *UB, double2 *CV, float *sqp)
+{
+    switch (g.P) {
+    case 64: return launch_spec_ptcl_fft<16, 8>(h, g, ctf, perm, np, cols_pad, UB, CV, sqp);
+    case 180: return launch_spec_ptcl_fft<24, 15>(h, g, ctf, perm, np, cols_pad, UB, CV, sqp);
+    case 300: return launch_spec_ptcl_fft<24, 25>(h, g, ctf, perm, np, cols_pad, UB, CV, sqp);
+    default: break;
+    }
+    const size_t smem = g.N * sizeof(double2) + (size_t)g.Ks * g.P * (sizeof(float2) + sizeof(float));
+    cudaError_t e = smem_limit((const void *)k_spec_ptcl, smem);
+    if (e != cudaSuccess) return e;
+    PFTCC_LAUNCH(h);
+    k_spec_ptcl<<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, perm, np, cols_pad, UB, CV, sqp,
+                                                             h->sqsums);
+    return cudaGetLastError();
 }
 
 // |ref|^2 spectra over P points (FP64): RU[r][j][k]
@@ -788,19 +1000,12 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
     // particle spectra and CTF^2 spectra
     {
-        const size_t smem = N * sizeof(double2) + (size_t)Ks * P * (sizeof(float2) + sizeof(float));
-        CKE(smem_limit((const void *)k_spec_ptcl, smem), "attr");
-        PFTCC_LAUNCH(h);
         KTimer kt(h, PFTCC_K_SPEC_PTCL);
-        k_spec_ptcl<<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, d_perm, np, cols_pad, ws.UB, ws.CV,
-                                                                 ws.sqp, h->sqsums);
-        CKE(cudaGetLastError(), "spec_ptcl");
+        CKE(launch_spec_ptcl(h, g, ctf, d_perm, np, cols_pad, ws.UB, ws.CV, ws.sqp), "spec_ptcl");
         PFTCC_LAUNCH(h);
         k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
         CKE(cudaGetLastError(), "cand_init");
     }
-    const size_t smem_ref = N * sizeof(double2) + (size_t)Ks * P * sizeof(float2);
-    CKE(smem_limit((const void *)k_spec_ref, smem_ref), "attr");
     const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(smem_limit((const void *)k_stage1_fp32, smem_s1), "attr");
     int T = 128;
@@ -825,10 +1030,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         { KTimer kt(h, PFTCC_K_SPEC_REF);
         k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
         CKE(cudaGetLastError(), "spec_r2");
-        PFTCC_LAUNCH(h);
-        k_spec_ref<<<rows_pad, SPEC_THREADS, smem_ref, h->stream>>>(g, ns, refs, ws.shifts, h->argtransf, h->argtransf1,
-                                                                    0, nrs, rows_pad, ws.UA); }
-        CKE(cudaGetLastError(), "spec_ref");
+        CKE(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref"); }
         if (precision == PFTCC_PREC_BF16X3) {
             int st = umma_stage1(h, M, Ks, ws.UA, 0, nrs, rows_pad, ws.UB, gc0, gc1 - gc0, cols_pad, nullptr, 1, grp);
             if (st != PFTCC_OK) return st;
