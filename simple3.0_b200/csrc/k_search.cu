@@ -707,6 +707,113 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
     }
 }
 
+// D from Y by an FP64 transform of length P/2 = N1 * N2 (spec_fft.cuh), the lengths with
+// that split; same inputs, outputs and layouts as k_norm.  With c_j = Y(j) (j <= P/2, already
+// scaled by wgt_j / P), D(rho) = sum_{j<P} H(j) w_P^{+j rho} for the Hermitian extension H
+// (H(0) = Re c_0, H(P/2) = Re c_{P/2}, H(j) = c_j / 2, H(P - j) = conj(c_j) / 2), and
+// z(l) = D(2l) + i D(2l + 1) is the length-P/2 inverse DFT of
+// Zh(j) = [H(j) + H(j + P/2)] + i [H(j) - H(j + P/2)] w_P^{+j}, computed as conj of the
+// forward transform of conj(Zh).  One block per particle column, NB references per batch:
+//   pass 1, task (reference, n1): a length-N2 DFT over n2 of conj Zh(n1 + N1 n2), times
+//           w_{P/2}^{-n1 k2}, into buf[reference][k2][n1];
+//   pass 2, task (reference, k2): a length-N1 DFT over n1 -> conj z(k2 + N2 k1).
+template <int N1, int N2>
+__global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg, int nr, int c0, int ncols, int dcols,
+                                                  const float *__restrict__ sqp, float *__restrict__ D, int p2,
+                                                  double dscale)
+{
+    constexpr int H = N1 * N2, P = 2 * H, J = H + 1;
+    constexpr int NB = 256 / (N1 > N2 ? N1 : N2);
+    extern __shared__ double2 sd[];
+    double2 *tw = sd;                 // [H] w_{P/2}^{-e}
+    double2 *wp = tw + H;             // [H] w_P^{+e}
+    double2 *buf = wp + H;            // [NB][N2][N1 + 1]
+    const int cl = blockIdx.x;
+    if (cl >= ncols) return;
+    const int col = c0 + cl;
+    for (int e = threadIdx.x; e < H; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / H, &sn, &cs);
+        tw[e] = make_double2(cs, sn);
+        sincospi(2.0 * e / P, &sn, &cs);
+        wp[e] = make_double2(cs, sn);
+    }
+    const double sq = (double)sqp[col];
+    const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 4 * p1 * ((p2 + 1) / 2) : P;
+    for (int rb0 = 0; rb0 < nr; rb0 += NB) {
+        const int nb = min(NB, nr - rb0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nb * N1; t += blockDim.x) {
+            const int kl = t / N1, n1 = t - kl * N1;
+            const double2 *y = Yg + ((size_t)(rb0 + kl) * ncols + cl) * J;
+            double2 x[N2];
+#pragma unroll
+            for (int n2 = 0; n2 < N2; ++n2) {
+                const int j = n1 + N1 * n2;
+                double2 hj, hh;
+                if (j == 0) {
+                    hj = make_double2(y[0].x, 0.0);
+                    hh = make_double2(y[H].x, 0.0);
+                } else {
+                    const double2 a = y[j], b = y[H - j];
+                    hj = make_double2(0.5 * a.x, 0.5 * a.y);
+                    hh = make_double2(0.5 * b.x, -0.5 * b.y);
+                }
+                const double2 ev = sfft::d_add(hj, hh), od = sfft::d_mul(sfft::d_sub(hj, hh), wp[j]);
+                x[n2] = make_double2(ev.x - od.y, -(ev.y + od.x));   // conj(ev + i od)
+            }
+            sfft::DFFT<N2, N1>::run(x, tw);
+            double2 *row = buf + (size_t)kl * N2 * (N1 + 1) + n1;
+#pragma unroll
+            for (int k2 = 0; k2 < N2; ++k2)
+                row[k2 * (N1 + 1)] = (k2 == 0 || n1 == 0) ? x[k2] : sfft::d_mul(x[k2], tw[n1 * k2]);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nb * N2; t += blockDim.x) {
+            const int kl = t / N2, k2 = t - kl * N2;
+            const double2 *row = buf + ((size_t)kl * N2 + k2) * (N1 + 1);
+            double2 x[N1];
+#pragma unroll
+            for (int n1 = 0; n1 < N1; ++n1) x[n1] = row[n1];
+            sfft::DFFT<N1, N2>::run(x, tw);
+            float *dst = D + ((size_t)(rb0 + kl) * dcols + cl) * dlen;
+#pragma unroll
+            for (int k1 = 0; k1 < N1; ++k1) {
+                const int l = k2 + N2 * k1;
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const double d = b == 0 ? x[k1].x : -x[k1].y;   // D(2l + b)
+                    const int rho = 2 * l + b;
+                    if (p2 == 0) {
+                        dst[rho] = (float)(1.0 / sqrt(d * sq));
+                    } else {
+                        const float v = (float)(dscale / sqrt(d * sq));
+#pragma unroll
+                        for (int hh = 0; hh < 2; ++hh) {   // rot = rho and rho + P
+                            const int rot = rho + hh * P, lr = rot >> 1, l2 = lr % p2;
+                            float *o = dst + ((((l2 >> 1) * p1 + lr / p2) * 2 + (rot & 1)) * 2 + (l2 & 1));
+                            o[0] = v;
+                            if ((p2 & 1) && l2 == p2 - 1) o[1] = v;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int N1, int N2>
+static cudaError_t launch_norm_fft(pftcc_handle *h, const double2 *Y, int nr, int c0, int ncols, int dcols,
+                                   const float *sqp, float *D, int p2, double dscale)
+{
+    constexpr int H = N1 * N2, NB = 256 / (N1 > N2 ? N1 : N2);
+    const size_t smem = (size_t)(2 * H + NB * N2 * (N1 + 1)) * sizeof(double2);
+    cudaError_t e = smem_limit((const void *)k_norm_fft<N1, N2>, smem);
+    if (e != cudaSuccess) return e;
+    k_norm_fft<N1, N2><<<ncols, 256, smem, h->stream>>>(Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    return cudaGetLastError();
+}
+
 static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU, const double2 *CV, int r0, int nr,
                                int c0, int ncols, int dcols, const float *sqp, double2 *Y, float *D, int p2,
                                double dscale)
@@ -723,6 +830,12 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     PFTCC_LAUNCH(h);
+    switch (g.P) {
+    case 64: return launch_norm_fft<8, 4>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    case 180: return launch_norm_fft<10, 9>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    case 300: return launch_norm_fft<15, 10>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    default: break;
+    }
     const size_t smem = ((size_t)NORM_RB * (J | 1) + g.P) * sizeof(double2);
     if (g.P % 4 == 0) {
         if ((e = smem_limit((const void *)k_norm<4>, smem))) return e;
