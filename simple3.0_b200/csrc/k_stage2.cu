@@ -18,6 +18,7 @@
 // that every X element is computed once (Z(j) needs X(j) and X(P - j), which lie in the
 // mirror class).
 #include "pftcc_internal.cuh"
+#include "spec_fft.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -645,84 +646,165 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
 // ---------------------------------------------------------------------------------------
 // FP32 m-domain re-score of the top-ntop candidates of each particle (particle frame):
 // X(m) = 4 sum_k UA[m][rs][k] conj(UB[m][col][k]) from the FP32 spectra, the FP64
-// normaliser from the |ref|^2 and CTF^2 spectra, the same transform and argmax.  A
-// thread per (particle, candidate); RS_PER_BLOCK threads of a particle reduce to its best.
-template <int P1, int P2>
-__global__ void __launch_bounds__(64) k_rescore_md(int ncols, int ntop, int Ks, int N, int nshifts, int has_shifts,
-                                                   const TwTables tw, const float2 *__restrict__ UA, int rows_pad,
-                                                   const float2 *__restrict__ UB, int cols_pad,
-                                                   const double2 *__restrict__ RU, const double2 *__restrict__ CV,
-                                                   const float *__restrict__ sqp, const float2 *__restrict__ cand,
-                                                   const int *__restrict__ perm, int c0, pftcc_best *__restrict__ out)
+// normaliser from the |ref|^2 and CTF^2 spectra, the same transform and argmax.  One block
+// per particle, its ntop <= 8 candidates in four phases:
+//   A  Y(c, j) = (wgt_j / P) sum_k conj(RU[r_c][j][k]) CV[col][j][k] in FP64, a thread per (c, j);
+//   B  D(c, rho) from Y by the length-P/2 FP64 transform of the packed half spectrum (the
+//      normaliser's k_norm_fft, split H1 x H2 = P/2), stored as 1/sqrt(D * sqsum_ptcl);
+//   C  X(c, m) in FP32, a thread per (c, m);
+//   D  the per-triple transform and argmax of each candidate (one thread each, triple_corr),
+//      then the particle's best (lowest id among equal correlations).
+template <int P> struct HalfSplit;
+template <> struct HalfSplit<64> { static constexpr int H1 = 8, H2 = 4; };
+template <> struct HalfSplit<180> { static constexpr int H1 = 10, H2 = 9; };
+template <> struct HalfSplit<300> { static constexpr int H1 = 15, H2 = 10; };
+constexpr int RS_MAX = 8;     // candidates per particle
+constexpr int RS_THREADS = 256;
+
+template <int P1, int P2> __host__ __device__ constexpr size_t rescore_smem_bytes()
 {
-    constexpr int P = P1 * P2, J = P / 2 + 1;
+    constexpr int P = P1 * P2, J = P / 2 + 1, H = P / 2;
+    constexpr int H1 = HalfSplit<P>::H1, H2 = HalfSplit<P>::H2;
+    return sizeof(double2) * ((size_t)2 * H + (size_t)RS_MAX * J + (size_t)RS_MAX * H2 * (H1 + 1)) +
+           sizeof(float2) * ((size_t)RS_MAX * (P + 1) + (size_t)P * RS_MAX) + sizeof(float) * (size_t)RS_MAX * P;
+}
+
+template <int P1, int P2>
+__global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, int Ks, int N, int nshifts,
+                                                           int has_shifts, const TwTables tw,
+                                                           const float2 *__restrict__ UA, int rows_pad,
+                                                           const float2 *__restrict__ UB, int cols_pad,
+                                                           const double2 *__restrict__ RU,
+                                                           const double2 *__restrict__ CV, const float *__restrict__ sqp,
+                                                           const float2 *__restrict__ cand, const int *__restrict__ perm,
+                                                           int c0, pftcc_best *__restrict__ out)
+{
+    constexpr int P = P1 * P2, J = P / 2 + 1, H = P / 2, M = P + 1;
+    constexpr int H1 = HalfSplit<P>::H1, H2 = HalfSplit<P>::H2;
     extern __shared__ float4 smem4[];
-    const int T = blockDim.x, t = threadIdx.x;
-    float2 *slab = reinterpret_cast<float2 *>(smem4) + t;                                   // [P][T]
-    float *dtab = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem4) + (size_t)P * T) + t;   // [P][T]
-    __shared__ float bc_s[64];
-    __shared__ int bi_s[64];
-    const int per_block = T / ntop;
-    const int cl = c0 + blockIdx.x * per_block + t / ntop, ci = t % ntop;
-    float best = -INFINITY;
-    int brot = 0, rs = -1;
-    if (t < per_block * ntop && cl < c0 + ncols) {
-        const int id = __float_as_int(cand[(size_t)cl * 8 + ci].y);
-        if (id >= 0) {
-            rs = id / N;
-            const int r = rs / nshifts;
-            // normaliser: Y(j) = sum_k conj(RU) CV and D(rho) = (1/P) sum_j Y(j) w_P^{+j rho},
-            // accumulated in FP64 in the (still unused) slab, P doubles = P float2
-            double *dacc = reinterpret_cast<double *>(slab);
-            const double sq = (double)sqp[cl];
-            for (int rho = 0; rho < P; ++rho) dacc[rho * T] = 0.0;
-            for (int j = 0; j <= P / 2; ++j) {
-                double yr = 0.0, yi = 0.0;
-                const double2 *ru = RU + ((size_t)r * J + j) * Ks;
-                const double2 *cv = CV + ((size_t)cl * J + j) * Ks;
-                for (int k = 0; k < Ks; ++k) {
-                    const double2 u = ru[k], v = cv[k];
-                    yr += u.x * v.x + u.y * v.y;
-                    yi += u.x * v.y - u.y * v.x;
-                }
-                const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
-                int idx = 0;
-                for (int rho = 0; rho < P; ++rho) {
-                    // w_P^{+e} = conj(wP[e])
-                    const float2 w = tw.wP[idx];
-                    dacc[rho * T] += wgt * (yr * (double)w.x + yi * (double)w.y);
-                    idx += j;
-                    if (idx >= P) idx -= P;
-                }
+    double2 *tw_h = reinterpret_cast<double2 *>(smem4);            // [H] w_{P/2}^{-e}
+    double2 *wp = tw_h + H;                                         // [H] w_P^{+e}
+    double2 *Ys = wp + H;                                           // [RS_MAX][J]
+    double2 *buf = Ys + RS_MAX * J;                                 // [RS_MAX][H2][H1 + 1]
+    float2 *Xs = reinterpret_cast<float2 *>(buf + RS_MAX * H2 * (H1 + 1));   // [RS_MAX][M]
+    float2 *slab = Xs + RS_MAX * M;                                 // [P][RS_MAX]
+    float *Ds = reinterpret_cast<float *>(slab + P * RS_MAX);       // [RS_MAX][P]
+    __shared__ int rs_s[RS_MAX];
+    __shared__ float bc_s[RS_MAX];
+    __shared__ int bi_s[RS_MAX];
+    const int cl = c0 + blockIdx.x;
+    if (cl >= c0 + ncols) return;
+    const int t = threadIdx.x;
+    const int nc = min(ntop, RS_MAX);
+    if (t < nc) {
+        const int id = __float_as_int(cand[(size_t)cl * 8 + t].y);
+        rs_s[t] = id >= 0 ? id / N : -1;
+    }
+    for (int e = t; e < H; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / H, &sn, &cs);
+        tw_h[e] = make_double2(cs, sn);
+        sincospi(2.0 * e / P, &sn, &cs);
+        wp[e] = make_double2(cs, sn);
+    }
+    __syncthreads();
+    // A: Y
+    for (int e = t; e < nc * J; e += blockDim.x) {
+        const int c = e / J, j = e - c * J;
+        const int rs = rs_s[c];
+        double yr = 0.0, yi = 0.0;
+        if (rs >= 0) {
+            const double2 *ru = RU + ((size_t)(rs / nshifts) * J + j) * Ks;
+            const double2 *cv = CV + ((size_t)cl * J + j) * Ks;
+            for (int k = 0; k < Ks; ++k) {
+                const double2 u = ru[k], v = cv[k];
+                yr += u.x * v.x + u.y * v.y;
+                yi += u.x * v.y - u.y * v.x;
             }
-            for (int rho = 0; rho < P; ++rho) dtab[rho * T] = (float)(1.0 / sqrt(dacc[rho * T] * sq));
-            const float2 *ua = UA + (size_t)rs * Ks;
-            const float2 *ub = UB + (size_t)cl * Ks;
-            const size_t pa = (size_t)rows_pad * Ks, pb = (size_t)cols_pad * Ks;
-            auto getx = [&](int j) {
-                const float2 *a = ua + (size_t)j * pa, *b = ub + (size_t)j * pb;
-                float xr = 0.f, xi = 0.f;
-                for (int k = 0; k < Ks; ++k) {
-                    const float2 av = a[k], bv = b[k];
-                    xr = fmaf(av.x, bv.x, fmaf(av.y, bv.y, xr));
-                    xi = fmaf(av.y, bv.x, fmaf(-av.x, bv.y, xi));
-                }
-                return make_float2(4.f * xr, 4.f * xi);
-            };
-            auto dinv = [&](int rho) { return dtab[rho * T]; };
-            triple_corr<P1, P2>(getx, dinv, slab, T, tw, 1.0f / (2.0f * (float)N), nullptr, best, brot);
+        }
+        const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
+        Ys[c * J + j] = make_double2(wgt * yr, wgt * yi);
+    }
+    __syncthreads();
+    // B: D, pass 1 (c, n1) then pass 2 (c, k2)
+    for (int e = t; e < nc * H1; e += blockDim.x) {
+        const int c = e / H1, n1 = e - c * H1;
+        const double2 *y = Ys + c * J;
+        double2 x[H2];
+#pragma unroll
+        for (int n2 = 0; n2 < H2; ++n2) {
+            const int j = n1 + H1 * n2;
+            double2 hj, hh;
+            if (j == 0) {
+                hj = make_double2(y[0].x, 0.0);
+                hh = make_double2(y[H].x, 0.0);
+            } else {
+                const double2 a = y[j], b = y[H - j];
+                hj = make_double2(0.5 * a.x, 0.5 * a.y);
+                hh = make_double2(0.5 * b.x, -0.5 * b.y);
+            }
+            const double2 ev = sfft::d_add(hj, hh), od = sfft::d_mul(sfft::d_sub(hj, hh), wp[j]);
+            x[n2] = make_double2(ev.x - od.y, -(ev.y + od.x));   // conj(ev + i od)
+        }
+        sfft::DFFT<H2, H1>::run(x, tw_h);
+        double2 *row = buf + (size_t)c * H2 * (H1 + 1) + n1;
+#pragma unroll
+        for (int k2 = 0; k2 < H2; ++k2)
+            row[k2 * (H1 + 1)] = (k2 == 0 || n1 == 0) ? x[k2] : sfft::d_mul(x[k2], tw_h[n1 * k2]);
+    }
+    __syncthreads();
+    const double sq = (double)sqp[cl];
+    for (int e = t; e < nc * H2; e += blockDim.x) {
+        const int c = e / H2, k2 = e - c * H2;
+        const double2 *row = buf + ((size_t)c * H2 + k2) * (H1 + 1);
+        double2 x[H1];
+#pragma unroll
+        for (int n1 = 0; n1 < H1; ++n1) x[n1] = row[n1];
+        sfft::DFFT<H1, H2>::run(x, tw_h);
+#pragma unroll
+        for (int k1 = 0; k1 < H1; ++k1) {
+            const int l = k2 + H2 * k1;
+            Ds[c * P + 2 * l] = (float)(1.0 / sqrt(x[k1].x * sq));
+            Ds[c * P + 2 * l + 1] = (float)(1.0 / sqrt(-x[k1].y * sq));
         }
     }
-    bc_s[t] = best;
-    bi_s[t] = rs < 0 ? 0x7fffffff : rs * N + brot;
+    // C: X
+    const size_t pa = (size_t)rows_pad * Ks, pb = (size_t)cols_pad * Ks;
+    for (int e = t; e < nc * M; e += blockDim.x) {
+        const int c = e / M, m = e - c * M;
+        const int rs = rs_s[c];
+        float xr = 0.f, xi = 0.f;
+        if (rs >= 0) {
+            const float2 *a = UA + (size_t)rs * Ks + (size_t)m * pa, *b = UB + (size_t)cl * Ks + (size_t)m * pb;
+            for (int k = 0; k < Ks; ++k) {
+                const float2 av = a[k], bv = b[k];
+                xr = fmaf(av.x, bv.x, fmaf(av.y, bv.y, xr));
+                xi = fmaf(av.y, bv.x, fmaf(-av.x, bv.y, xi));
+            }
+        }
+        Xs[c * M + m] = make_float2(4.f * xr, 4.f * xi);
+    }
     __syncthreads();
-    if (t < per_block && c0 + blockIdx.x * per_block + t < c0 + ncols) {
-        const int col = c0 + blockIdx.x * per_block + t;
+    // D: transform and argmax per candidate
+    if (t < nc) {
+        float best = -INFINITY;
+        int brot = 0;
+        const int rs = rs_s[t];
+        if (rs >= 0) {
+            auto getx = [&](int j) { return Xs[t * M + j]; };
+            auto dinv = [&](int rho) { return Ds[t * P + rho]; };
+            triple_corr<P1, P2>(getx, dinv, slab + t, RS_MAX, tw, 1.0f / (2.0f * (float)N), nullptr, best, brot);
+        }
+        bc_s[t] = best;
+        bi_s[t] = rs < 0 ? 0x7fffffff : rs * N + brot;
+    }
+    __syncthreads();
+    if (t == 0) {
         float b = -INFINITY;
         int bid = 0x7fffffff;
-        for (int i = 0; i < ntop; ++i) {
-            const float c = bc_s[t * ntop + i];
-            const int id = bi_s[t * ntop + i];
+        for (int i = 0; i < nc; ++i) {
+            const float c = bc_s[i];
+            const int id = bi_s[i];
             if (id != 0x7fffffff && (c > b || (c == b && id < bid))) { b = c; bid = id; }
         }
         pftcc_best o;
@@ -734,7 +816,7 @@ __global__ void __launch_bounds__(64) k_rescore_md(int ncols, int ntop, int Ks, 
             o.irot = rot + 1;
             o.corr = b;
         }
-        out[perm[col]] = o;
+        out[perm[cl]] = o;
     }
 }
 
@@ -809,13 +891,13 @@ static cudaError_t launch_rs(pftcc_handle *h, int ncols, int ntop, int Ks, int n
     constexpr int P = P1 * P2;
     TwTables tw;
     fill_tw(tw, P);
-    const int T = 64, per_block = T / ntop;
-    const size_t smem = (size_t)P * T * (sizeof(float2) + sizeof(float));
+    if (ntop < 1 || ntop > RS_MAX) return cudaErrorInvalidValue;
+    const size_t smem = rescore_smem_bytes<P1, P2>();
     cudaError_t e = smem_limit((const void *)k_rescore_md<P1, P2>, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_EXACT);
-    k_rescore_md<P1, P2><<<(ncols + per_block - 1) / per_block, T, smem, h->stream>>>(
+    k_rescore_md<P1, P2><<<ncols, RS_THREADS, smem, h->stream>>>(
         ncols, ntop, Ks, 2 * P, nshifts, has_shifts, tw, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
     return cudaGetLastError();
 }

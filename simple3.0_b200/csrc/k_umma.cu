@@ -383,55 +383,77 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16 &hi, __nv_bflo
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
-// (ref, shift) rows -> R16[m][rt][chunk][U_BN][8]: U_RS rows = U_BN N-rows per tile
+__device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat16 a, __nv_bfloat16 b)
+{
+    return (uint32_t)__bfloat16_as_ushort(a) | ((uint32_t)__bfloat16_as_ushort(b) << 16);
+}
+
+// one thread per 16-byte chunk pair: the 8 K values kk = 8c .. 8c + 7 (c < Kp / 8) of one
+// operand row, given by val(kk), split into the hi chunk c and the lo chunk c + Kp / 8 of the
+// tile layout [chunk][rows][8]
+template <class Val>
+__device__ __forceinline__ void pack_chunk(const Val &val, int c, int half, int nrows, int i, __nv_bfloat16 *tile)
+{
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int el = 0; el < 8; el += 2) {
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(val(8 * c + el), h0, l0);
+        split_bf16(val(8 * c + el + 1), h1, l1);
+        hw[el >> 1] = bf16x2_bits(h0, h1);
+        lw[el >> 1] = bf16x2_bits(l0, l1);
+    }
+    uint4 *t4 = reinterpret_cast<uint4 *>(tile);
+    t4[(size_t)c * nrows + i] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    t4[(size_t)(c + half) * nrows + i] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+// (ref, shift) rows -> R16[m][rt][chunk][U_BN][8]: U_RS rows = U_BN N-rows per tile, N-row
+// 2i + 0 = [Ar | Ai | 0], 2i + 1 = [Ai | -Ar | 0] of row i
 __global__ void k_pack_rows(int M, int Ks, int Kp, int KC, int rtiles, int rows_pad, const float2 *__restrict__ UA,
                             __nv_bfloat16 *__restrict__ R16)
 {
-    const size_t per_tile = (size_t)KC * U_BN * 8;
-    const size_t total = (size_t)M * rtiles * per_tile;
     const int half = Kp / 8;
+    const size_t per_tile = (size_t)KC * U_BN * 8;
+    const size_t total = (size_t)M * rtiles * half * U_BN;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        const size_t tile = e / per_tile;
-        const int within = (int)(e - tile * per_tile);
-        const int c = within / (U_BN * 8), i = (within / 8) & (U_BN - 1), el = within & 7;
+        const int i = (int)(e % U_BN);
+        const size_t q = e / U_BN;
+        const int c = (int)(q % half);
+        const size_t tile = q / half;
         const int m = (int)(tile / rtiles), rt = (int)(tile - (size_t)m * rtiles);
-        const int part = c / half, kk = (c - part * half) * 8 + el;
         const int rs = rt * U_RS + (i >> 1), kind = i & 1;
-        float v = 0.f;
-        if (kk < 2 * Ks && rs < rows_pad) {
-            const int k = kk < Ks ? kk : kk - Ks;
-            const float2 a = UA[((size_t)m * rows_pad + rs) * Ks + k];
-            if (kind == 0) v = kk < Ks ? a.x : a.y;
-            else v = kk < Ks ? a.y : -a.x;
-        }
-        __nv_bfloat16 hi, lo;
-        split_bf16(v, hi, lo);
-        R16[e] = part ? lo : hi;
+        const float2 *src = UA + ((size_t)m * rows_pad + rs) * Ks;
+        auto val = [&](int kk) {
+            if (kk >= 2 * Ks || rs >= rows_pad) return 0.f;
+            const float2 a = src[kk < Ks ? kk : kk - Ks];
+            return kind == 0 ? (kk < Ks ? a.x : a.y) : (kk < Ks ? a.y : -a.x);
+        };
+        pack_chunk(val, c, half, U_BN, i, R16 + tile * per_tile);
     }
 }
 
-// particle columns [c0, c0 + ptiles*128) -> P16[m][pt][chunk][128][8]
+// particle columns [c0, c0 + ptiles*128) -> P16[m][pt][chunk][128][8], row = [4 Br | 4 Bi | 0]
 __global__ void k_pack_cols(int M, int Ks, int Kp, int KC, int ptiles, int cols_pad, int c0,
                             const float2 *__restrict__ UB, __nv_bfloat16 *__restrict__ P16)
 {
-    const size_t per_tile = (size_t)KC * 128 * 8;
-    const size_t total = (size_t)M * ptiles * per_tile;
     const int half = Kp / 8;
+    const size_t per_tile = (size_t)KC * U_BM * 8;
+    const size_t total = (size_t)M * ptiles * half * U_BM;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        const size_t tile = e / per_tile;
-        const int within = (int)(e - tile * per_tile);
-        const int c = within / (128 * 8), i = (within / 8) & 127, el = within & 7;
+        const int i = (int)(e % U_BM);
+        const size_t q = e / U_BM;
+        const int c = (int)(q % half);
+        const size_t tile = q / half;
         const int m = (int)(tile / ptiles), pt = (int)(tile - (size_t)m * ptiles);
-        const int part = c / half, kk = (c - part * half) * 8 + el;
         const int col = c0 + pt * U_BM + i;
-        float v = 0.f;
-        if (kk < 2 * Ks && col < cols_pad) {
-            const float2 b = UB[((size_t)m * cols_pad + col) * Ks + (kk < Ks ? kk : kk - Ks)];
-            v = 4.f * (kk < Ks ? b.x : b.y);      // X = 4 sum_k ...: the power of two splits exactly
-        }
-        __nv_bfloat16 hi, lo;
-        split_bf16(v, hi, lo);
-        P16[e] = part ? lo : hi;
+        const float2 *src = UB + ((size_t)m * cols_pad + col) * Ks;
+        auto val = [&](int kk) {
+            if (kk >= 2 * Ks || col >= cols_pad) return 0.f;
+            const float2 b = src[kk < Ks ? kk : kk - Ks];
+            return 4.f * (kk < Ks ? b.x : b.y);      // X = 4 sum_k ...: the power of two splits exactly
+        };
+        pack_chunk(val, c, half, U_BM, i, P16 + tile * per_tile);
     }
 }
 
