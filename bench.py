@@ -208,6 +208,13 @@ def algorithmic_costs(w, nshifts, kernel):
     return 0.0, 0.0
 
 
+# DRAM bytes (read + write) per (reference, shift, particle) triple measured by ncu on one
+# launch of the same kernel (box 128 / nrots 360: 4096 rows x 512 columns, 3.0601 GB read +
+# 0.0043 GB written = 1461.2 B per triple against 1440 B algorithmic); the stage-2 traffic grows
+# with the triples processed, so the bench scales it to its own launches
+DRAM_BYTES_PER_TRIPLE = {("stage2", 180): (3.060076e9 + 0.004345e9) / (4096 * 512)}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -300,8 +307,12 @@ def run_ours(args):
     else:
         flops_b, byts_b = algorithmic_costs(w, ns, dom)
         ach = byts_b / n_launch_per_step / per_launch_s / 1e9 if byts_b else 0.0
+        per_trip = DRAM_BYTES_PER_TRIPLE.get((dom, w.pftsz))
+        trip_launch = float(w.nrefs) * ns * w.nptcls / n_launch_per_step
         roof = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
-                "traffic": None, "kernel": f"k_{dom}", "peak_source": f"{peak_src} hbm copy"}
+                "traffic": per_trip * trip_launch if per_trip else None,
+                "algorithmic_bytes": byts_b / n_launch_per_step,
+                "kernel": f"k_{dom}", "peak_source": f"{peak_src} hbm copy"}
     roof["kernel_ms_per_step"] = {k: round(v[0] / args.steps, 3) for k, v in prof.items() if v[1]}
     roof["kernel_share"] = shares
 
