@@ -196,17 +196,32 @@ template <> struct PBfly<5> {
     }
 };
 
-// two length-L forward DFTs, one per lane, natural order in and out (SFFT's recursion)
+__host__ __device__ constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+// the index o < F M with o = r (mod F) and o = k (mod M), gcd(F, M) = 1
+__host__ __device__ constexpr int crt_c(int r, int k, int F, int M)
+{
+    int o = k;
+    while (o % F != r) o += M;
+    return o;
+}
+
+// two length-L forward DFTs, one per lane, natural order in and out (SFFT's recursion).
+// When the radix F and the rest M = L / F are coprime (15 = 3 x 5, 12 = 4 x 3, 20 = 4 x 5)
+// the Good-Thomas prime-factor mapping needs no twiddles between the two stages: input
+// x((M q + F j) mod L) -> the M-point DFTs over j, the F-point butterflies over q, output
+// index o with o = r (mod F) and o = k (mod M); otherwise the Cooley-Tukey split with the
+// twiddles w_L^{qk}.
 template <int L, int STEP> struct PFFT {
     static constexpr int F = SFFT<L, STEP>::F;
     static constexpr int M = L / F;
+    static constexpr bool PFA = M > 1 && gcd_c(F, M) == 1;
     __device__ static void run(C2 *x, const TwTables &tw)
     {
         C2 s[F][M];
 #pragma unroll
         for (int q = 0; q < F; ++q)
 #pragma unroll
-            for (int j = 0; j < M; ++j) s[q][j] = x[q + F * j];
+            for (int j = 0; j < M; ++j) s[q][j] = PFA ? x[(M * q + F * j) % L] : x[q + F * j];
 #pragma unroll
         for (int q = 0; q < F; ++q) PFFT<M, STEP * F>::run(s[q], tw);
 #pragma unroll
@@ -215,11 +230,11 @@ template <int L, int STEP> struct PFFT {
 #pragma unroll
             for (int q = 0; q < F; ++q) {
                 const int e = q * k * STEP;
-                v[q] = (q * k == 0) ? s[q][k] : p_twid(s[q][k], tw.pc[e], tw.ps[e], tw.pn[e]);
+                v[q] = (PFA || q * k == 0) ? s[q][k] : p_twid(s[q][k], tw.pc[e], tw.ps[e], tw.pn[e]);
             }
             PBfly<F>::run(v);
 #pragma unroll
-            for (int r = 0; r < F; ++r) x[k + M * r] = v[r];
+            for (int r = 0; r < F; ++r) x[PFA ? crt_c(r, k, F, M) : k + M * r] = v[r];
         }
     }
 };
@@ -475,11 +490,10 @@ __device__ __forceinline__ void passB_all(int L0, int L1, const float2 *slab, in
     }
 }
 
-// how a row's transform is split between two threads: pass A by classes, [0, P1/2) and
-// [P1/2, P1) of Z; pass B at l2 = LB
-template <int P1, int P2> struct RowSplit {
-    static constexpr int LB = (P2 + 1) / 2;
-};
+// how a row's transform is split between its NT threads: thread (role) r takes the class
+// pairs [r n / NT, (r + 1) n / NT) of the n = ceil(P1 / 2) pairs (2k, 2k + 1) of pass A and the
+// block pairs likewise of the ceil(P2 / 2) pairs (2q, 2q + 1) of pass B
+__host__ __device__ constexpr int role_part(int n, int r, int nt) { return r * n / nt; }
 
 // the whole per-triple transform in one thread; getx(j) returns X(j) for j = 0..P;
 // dinv(rot) the normalising factor; slab is this thread's shared-memory slab with
@@ -504,35 +518,37 @@ struct S2Fast {
 // repeats block P2 - 1)
 template <int P1, int P2> __host__ __device__ constexpr int s2_dlen() { return 4 * P1 * ((P2 + 1) / 2); }
 
+// threads per row of the search's stage 2
+constexpr int S2_THREADS_PER_ROW = 2;
+
 // (c, id) ranks above (c2, id2): larger correlation, then lower id
 __device__ __forceinline__ bool ranks_above(float c, int id, float c2, int id2) { return c > c2 || (c == c2 && id < id2); }
 
-// ROWS rows in flight per block, two threads per row: warp w < ROWS/32 (role 0) and warp
-// w + ROWS/32 (role 1) share the rows' slabs and meet at named barrier 1 + w twice per row
-// (after pass A; after pass B, when role 1 hands its argmax over).  Role 0 keeps its rows'
-// running top-8 in registers; at the end the block merges those lists with the
-// particle's running top-8.
+// ROWS rows in flight per block, NT threads per row: warps w + r ROWS/32 (role r) share the
+// rows' slabs and meet at named barrier 1 + w twice per row (after pass A; after pass B, when
+// roles 1.. hand their argmax over).  Role 0 keeps its rows' running top-8 in registers; at
+// the end the block merges those lists with the particle's running top-8.
 // X here is the packed spectrum Z, P planes of [col][row].
-template <int P1, int P2, int ROWS, bool WRITE>
-__global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
+template <int P1, int P2, int ROWS, int NT, bool WRITE>
+__global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
                                                             const float *__restrict__ Dinv, float2 *__restrict__ cand,
                                                             float *__restrict__ ccall, const int *__restrict__ perm)
 {
-    constexpr int Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>();
-    using SP = RowSplit<P1, P2>;
+    constexpr int Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>(), NPA = (P1 + 1) / 2;
     extern __shared__ float4 smem4[];
     const int t = threadIdx.x;
-    const int role = t >= ROWS, lr = t - role * ROWS;
+    const int role = t / ROWS, lr = t - role * ROWS;
     const int bar = 1 + (lr >> 5);
     float2 *slab = reinterpret_cast<float2 *>(smem4) + lr;                                      // [Q2 P1 2][ROWS]
     float4 *twa = smem4 + (size_t)Q2 * P1 * ROWS;                                               // [P1 P2]
     float2 *twb = reinterpret_cast<float2 *>(twa + P1 * P2);                                    // [P1 P2]
-    float *xfer_c = reinterpret_cast<float *>(twb + P1 * P2);                                   // [ROWS]
-    int *xfer_r = reinterpret_cast<int *>(xfer_c + ROWS);                                       // [ROWS]
-    // lane-pair twiddles of pass A: lane a class c, lane b class min(c + 1, end of c's half - 1)
+    float *xfer_c = reinterpret_cast<float *>(twb + P1 * P2);                                   // [NT - 1][ROWS]
+    int *xfer_r = reinterpret_cast<int *>(xfer_c + (NT - 1) * ROWS);                            // [NT - 1][ROWS]
+    // lane-pair twiddles of pass A: lane a class c, lane b class min(c + 1, P1 - 1) (pairs
+    // start at even classes in every role's range)
     for (int e = t; e < P1 * P2; e += blockDim.x) {
         const int c = e / P2, l2 = e - c * P2;
-        const int cb = min(c + 1, (c < P1 / 2 ? P1 / 2 : P1) - 1);
+        const int cb = min(c + 1, P1 - 1);
         const float2 wa = tw.wP[c * l2], wb = tw.wP[cb * l2];
         twa[e] = make_float4(wa.x, wb.x, wa.y, wb.y);
         twb[e] = make_float2(-wa.y, -wb.y);
@@ -545,8 +561,9 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
     int ki[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { kc[k] = -INFINITY; ki[k] = 0x7fffffff; }
-    // the two halves of a row take the classes [0, P1/2) and [P1/2, P1) of Z
-    const int ca = role == 0 ? 0 : P1 / 2, ce = role == 0 ? P1 / 2 : P1;
+    // this role's classes [ca, ce) of Z and pass-B blocks [lb0, lb1)
+    const int ca = 2 * role_part(NPA, role, NT), ce = min(P1, 2 * role_part(NPA, role + 1, NT));
+    const int lb0 = 2 * role_part(Q2, role, NT), lb1 = min(P2, 2 * role_part(Q2, role + 1, NT));
     auto zload = [&](int row) {
         const float2 *xr = Xc + row;
         return [=](int j) {
@@ -558,7 +575,7 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         };
     };
     float2 na[P2], nb[P2];   // the first class pair of this thread's next row
-    if (lr < sp.rows) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(lr), na, nb);
+    if (lr < sp.rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(lr), na, nb);
     for (int base = 0; base < sp.rows; base += ROWS) {
         const int row = base + lr;
         const bool active = row < sp.rows;
@@ -567,25 +584,27 @@ __global__ void __launch_bounds__(2 * ROWS, 1) k_stage2_fast(S2Fast sp, const Tw
         const float4 *Dr = reinterpret_cast<const float4 *>(
             Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * DLEN);
         if (active) passA_pk<P1, P2>(ca, ce, zload(row), slab, ROWS, twa, twb, tw, na, nb);
-        asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
-        if (row + ROWS < sp.rows) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(row + ROWS), na, nb);
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(32 * NT) : "memory");
+        if (row + ROWS < sp.rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(row + ROWS), na, nb);
         float best = -INFINITY;
         int brot = 0;
         if (active) {
-            const int l0 = role == 0 ? 0 : SP::LB, l1 = role == 0 ? SP::LB : P2;
             if constexpr (WRITE) {
                 float *cc_out = ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N;
-                passB_all<P1, P2>(l0, l1, slab, ROWS, tw, Dr, cc_out, best, brot);
+                passB_all<P1, P2>(lb0, lb1, slab, ROWS, tw, Dr, cc_out, best, brot);
             } else {
-                passB_search<P1, P2>(l0, l1, slab, ROWS, tw, Dr, best, brot);
+                passB_search<P1, P2>(lb0, lb1, slab, ROWS, tw, Dr, best, brot);
             }
-            if (role == 1) { xfer_c[lr] = best; xfer_r[lr] = brot; }
+            if (role > 0) { xfer_c[(role - 1) * ROWS + lr] = best; xfer_r[(role - 1) * ROWS + lr] = brot; }
         }
-        asm volatile("bar.sync %0, 64;" ::"r"(bar) : "memory");
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(32 * NT) : "memory");
         if (active && role == 0) {
-            const float oc = xfer_c[lr];
-            const int orot = xfer_r[lr];
-            if (oc > best || (oc == best && orot < brot)) { best = oc; brot = orot; }
+#pragma unroll
+            for (int r = 1; r < NT; ++r) {
+                const float oc = xfer_c[(r - 1) * ROWS + lr];
+                const int orot = xfer_r[(r - 1) * ROWS + lr];
+                if (oc > best || (oc == best && orot < brot)) { best = oc; brot = orot; }
+            }
             if (best != -INFINITY) {
                 // insert into the running top-8 (kept sorted)
                 float c = best;
@@ -856,16 +875,18 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
     TwTables tw;
     fill_tw(tw, P1 * P2);
     // row slabs of P complex (the two-lane layout): 128 rows in flight up to P = 200, 64
-    // beyond; two threads per row
+    // beyond; NT threads per row
     constexpr int ROWS = P1 * P2 <= 200 ? 128 : 64;
+    constexpr int NT = S2_THREADS_PER_ROW;
     const size_t smem = (size_t)((P2 + 1) / 2) * P1 * 2 * ROWS * sizeof(float2) +
-                        (size_t)P1 * P2 * (sizeof(float4) + sizeof(float2)) + (size_t)ROWS * (sizeof(float) + sizeof(int));
-    auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, true> : k_stage2_fast<P1, P2, ROWS, false>;
+                        (size_t)P1 * P2 * (sizeof(float4) + sizeof(float2)) +
+                        (size_t)(NT - 1) * ROWS * (sizeof(float) + sizeof(int));
+    auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, NT, true> : k_stage2_fast<P1, P2, ROWS, NT, false>;
     cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE2);
-    kern<<<cols, 2 * ROWS, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
+    kern<<<cols, NT * ROWS, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
     return cudaGetLastError();
 }
 
