@@ -544,8 +544,9 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 //   k_norm_y: Y for every (reference, particle) pair of the wave as a batched complex
 //            GEMM over the shells -- a block takes 32 references x 64 particles and 8
 //            values of j, stages the j-th |ref|^2 and CTF^2 spectra of its tile in shared
-//            memory (k-major), and each thread accumulates 2 references x 4 particles;
-//            Y[rl][cl][j], scaled by wgt_j / P;
+//            memory (k-major, double buffered: the next j's tile arrives by asynchronous
+//            copies during this j's products), and each thread accumulates 2 references x
+//            4 particles; Y[rl][cl][j], scaled by wgt_j / P;
 //   k_norm:  D from Y, one block per particle column, NORM_RB = 32 references at a time:
 //            lane = reference, each thread NORM_GPT residues g < P/Q, and for each g the Q
 //            rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q} Y(j) w_P^{j g},
@@ -561,28 +562,51 @@ constexpr int NORM_RB = 32;
 constexpr int NORM_GPT = 3;
 constexpr int NY_R = 32, NY_C = 64, NY_J = 8;
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
                                                 int r0, int nr, int c0, int ncols, double2 *__restrict__ Y)
 {
     extern __shared__ double2 sy[];
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
-    double2 *sr = sy;                        // [Ks][NY_R] |ref|^2 spectra of the tile's references
-    double2 *sc = sy + (size_t)Ks * NY_R;    // [Ks][NY_C] CTF^2 spectra of the tile's particles
+    // two buffers, each [Ks][NY_R] |ref|^2 spectra then [Ks][NY_C] CTF^2 spectra of the tile; the
+    // next j's tile is copied asynchronously while this j's is used
+    const size_t bufsz = (size_t)Ks * (NY_R + NY_C);
     const int cb = blockIdx.x * NY_C, rb = blockIdx.y * NY_R, j0 = blockIdx.z * NY_J;
+    const int jend = min(J, j0 + NY_J);
     const int tc = threadIdx.x & 15, tr = threadIdx.x >> 4;   // particles tc + 16 q, references tr + 16 i
     const double2 zero = make_double2(0.0, 0.0);
     const double invP = 1.0 / P;
-    for (int j = j0; j < min(J, j0 + NY_J); ++j) {
-        __syncthreads();
+    auto stage = [&](int j, int buf) {
+        double2 *sr = sy + buf * bufsz, *sc = sr + (size_t)Ks * NY_R;
         for (int e = threadIdx.x; e < NY_R * Ks; e += blockDim.x) {
             const int r = e / Ks, k = e - r * Ks;
-            sr[(size_t)k * NY_R + r] = rb + r < nr ? RU[((size_t)(r0 + rb + r) * J + j) * Ks + k] : zero;
+            if (rb + r < nr) cp_async16(sr + (size_t)k * NY_R + r, RU + ((size_t)(r0 + rb + r) * J + j) * Ks + k);
+            else sr[(size_t)k * NY_R + r] = zero;
         }
         for (int e = threadIdx.x; e < NY_C * Ks; e += blockDim.x) {
             const int c = e / Ks, k = e - c * Ks;
-            sc[(size_t)k * NY_C + c] = cb + c < ncols ? CV[((size_t)(c0 + cb + c) * J + j) * Ks + k] : zero;
+            if (cb + c < ncols) cp_async16(sc + (size_t)k * NY_C + c, CV + ((size_t)(c0 + cb + c) * J + j) * Ks + k);
+            else sc[(size_t)k * NY_C + c] = zero;
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (j0 < jend) stage(j0, 0);
+    for (int j = j0; j < jend; ++j) {
+        const int b = (j - j0) & 1;
+        if (j + 1 < jend) {
+            stage(j + 1, b ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
+        const double2 *sr = sy + b * bufsz, *sc = sr + (size_t)Ks * NY_R;
         double yr[2][4], yi[2][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
@@ -602,6 +626,7 @@ __global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restric
                     yi[i][q] = fma(u[i].x, v[q].y, fma(-u[i].y, v[q].x, yi[i][q]));
                 }
         }
+        __syncthreads();   // buffer b is refilled by the stage of j + 2
         const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
 #pragma unroll
         for (int i = 0; i < 2; ++i)
@@ -784,10 +809,15 @@ __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg
                 for (int b = 0; b < 2; ++b) {
                     const double d = b == 0 ? x[k1].x : -x[k1].y;   // D(2l + b)
                     const int rho = 2 * l + b;
+                    // the FP32 factor 1/sqrt(D sqsum): D sqsum formed in FP64, its reciprocal square
+                    // root in FP32 by rsqrtf and one Newton-Raphson step y (3 - a y^2) / 2
+                    const float a = (float)(d * sq);
+                    float y = rsqrtf(a);
+                    y = y * fmaf(-0.5f * a, y * y, 1.5f);
                     if (p2 == 0) {
-                        dst[rho] = (float)(1.0 / sqrt(d * sq));
+                        dst[rho] = y;
                     } else {
-                        const float v = (float)(dscale / sqrt(d * sq));
+                        const float v = (float)dscale * y;
 #pragma unroll
                         for (int hh = 0; hh < 2; ++hh) {   // rot = rho and rho + P
                             const int rot = rho + hh * P, lr = rot >> 1, l2 = lr % p2;
@@ -823,7 +853,7 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_NORM);
     {
-        const size_t smem = (size_t)g.Ks * (NY_R + NY_C) * sizeof(double2);
+        const size_t smem = 2 * (size_t)g.Ks * (NY_R + NY_C) * sizeof(double2);
         if ((e = smem_limit((const void *)k_norm_y, smem))) return e;
         dim3 grid((ncols + NY_C - 1) / NY_C, (nr + NY_R - 1) / NY_R, (J + NY_J - 1) / NY_J);
         k_norm_y<<<grid, 256, smem, h->stream>>>(g, RU, CV, r0, nr, c0, ncols, Y);
