@@ -538,15 +538,17 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 
 // ---------------------------------------------------------------------------
 // rotation-dependent normaliser D(rho) = (1/P) sum_j wgt_j Re[Y(j) w_P^{+j rho}] with
-// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k] (wgt_j = 1 at j = 0 and j = P/2, else 2),
-// all in FP64; stored as the factor Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col))
-// the correlations are scaled by.  Two kernels per wave:
+// Y(j) = sum_k conj(RU[r][j][k]) CV[col][j][k] (wgt_j = 1 at j = 0 and j = P/2, else 2)
+// (spectra FP64, products FP32, transform FP64); stored as the FP32 factor
+// Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col)) the correlations are scaled by.
+// Two kernels per wave:
 //   k_norm_y: Y for every (reference, particle) pair of the wave as a batched complex
 //            GEMM over the shells -- a block takes 32 references x 64 particles and 8
 //            values of j, stages the j-th |ref|^2 and CTF^2 spectra of its tile in shared
-//            memory (k-major, double buffered: the next j's tile arrives by asynchronous
-//            copies during this j's products), and each thread accumulates 2 references x
-//            4 particles; Y[rl][cl][j], scaled by wgt_j / P;
+//            memory (k-major, FP32), and each thread accumulates 2 references x 4
+//            particles with two-lane FP32 FMAs (these factors rank the search's
+//            candidates; the re-score forms its own normaliser in FP64); Y[rl][cl][j],
+//            scaled by wgt_j / P, stored FP64 for the transform;
 //   k_norm:  D from Y, one block per particle column, NORM_RB = 32 references at a time:
 //            lane = reference, each thread NORM_GPT residues g < P/Q, and for each g the Q
 //            rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q} Y(j) w_P^{j g},
@@ -562,58 +564,48 @@ constexpr int NORM_RB = 32;
 constexpr int NORM_GPT = 3;
 constexpr int NY_R = 32, NY_C = 64, NY_J = 8;
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
-                 "l"(src)
-                 : "memory");
-}
-
 __global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
                                                 int r0, int nr, int c0, int ncols, double2 *__restrict__ Y)
 {
-    extern __shared__ double2 sy[];
+    extern __shared__ float4 sy4[];
     const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
-    // two buffers, each [Ks][NY_R] |ref|^2 spectra then [Ks][NY_C] CTF^2 spectra of the tile; the
-    // next j's tile is copied asynchronously while this j's is used
-    const size_t bufsz = (size_t)Ks * (NY_R + NY_C);
+    // the j-th spectra of the tile in FP32, laid out for the two-lane products:
+    // sr[k][r] = (u.x, u.x, u.y, u.y) of |ref|^2, sc[k][c] = (v.x, v.y, v.y, -v.x) of CTF^2, so that
+    // conj(u) v accumulates as fma2((u.x, u.x), (v.x, v.y)) + fma2((u.y, u.y), (v.y, -v.x))
+    float4 *sr = sy4;                        // [Ks][NY_R]
+    float4 *sc = sy4 + (size_t)Ks * NY_R;    // [Ks][NY_C]
     const int cb = blockIdx.x * NY_C, rb = blockIdx.y * NY_R, j0 = blockIdx.z * NY_J;
-    const int jend = min(J, j0 + NY_J);
     const int tc = threadIdx.x & 15, tr = threadIdx.x >> 4;   // particles tc + 16 q, references tr + 16 i
-    const double2 zero = make_double2(0.0, 0.0);
     const double invP = 1.0 / P;
-    auto stage = [&](int j, int buf) {
-        double2 *sr = sy + buf * bufsz, *sc = sr + (size_t)Ks * NY_R;
+    for (int j = j0; j < min(J, j0 + NY_J); ++j) {
+        __syncthreads();
         for (int e = threadIdx.x; e < NY_R * Ks; e += blockDim.x) {
             const int r = e / Ks, k = e - r * Ks;
-            if (rb + r < nr) cp_async16(sr + (size_t)k * NY_R + r, RU + ((size_t)(r0 + rb + r) * J + j) * Ks + k);
-            else sr[(size_t)k * NY_R + r] = zero;
+            float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (rb + r < nr) {
+                const double2 u = __ldg(RU + ((size_t)(r0 + rb + r) * J + j) * Ks + k);
+                w = make_float4((float)u.x, (float)u.x, (float)u.y, (float)u.y);
+            }
+            sr[(size_t)k * NY_R + r] = w;
         }
         for (int e = threadIdx.x; e < NY_C * Ks; e += blockDim.x) {
             const int c = e / Ks, k = e - c * Ks;
-            if (cb + c < ncols) cp_async16(sc + (size_t)k * NY_C + c, CV + ((size_t)(c0 + cb + c) * J + j) * Ks + k);
-            else sc[(size_t)k * NY_C + c] = zero;
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-    if (j0 < jend) stage(j0, 0);
-    for (int j = j0; j < jend; ++j) {
-        const int b = (j - j0) & 1;
-        if (j + 1 < jend) {
-            stage(j + 1, b ^ 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (cb + c < ncols) {
+                const double2 v = __ldg(CV + ((size_t)(c0 + cb + c) * J + j) * Ks + k);
+                w = make_float4((float)v.x, (float)v.y, (float)v.y, -(float)v.x);
+            }
+            sc[(size_t)k * NY_C + c] = w;
         }
         __syncthreads();
-        const double2 *sr = sy + b * bufsz, *sc = sr + (size_t)Ks * NY_R;
-        double yr[2][4], yi[2][4];
+        float2 acc[2][4];
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) yr[i][q] = yi[i][q] = 0.0;
+            for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
+#pragma unroll 4
         for (int k = 0; k < Ks; ++k) {
-            double2 u[2], v[4];
+            float4 u[2], v[4];
 #pragma unroll
             for (int i = 0; i < 2; ++i) u[i] = sr[(size_t)k * NY_R + tr + 16 * i];
 #pragma unroll
@@ -622,18 +614,18 @@ __global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restric
             for (int i = 0; i < 2; ++i)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    yr[i][q] = fma(u[i].x, v[q].x, fma(u[i].y, v[q].y, yr[i][q]));     // conj(u) * v
-                    yi[i][q] = fma(u[i].x, v[q].y, fma(-u[i].y, v[q].x, yi[i][q]));
+                    acc[i][q] = __ffma2_rn(make_float2(u[i].x, u[i].y), make_float2(v[q].x, v[q].y), acc[i][q]);
+                    acc[i][q] = __ffma2_rn(make_float2(u[i].z, u[i].w), make_float2(v[q].z, v[q].w), acc[i][q]);
                 }
         }
-        __syncthreads();   // buffer b is refilled by the stage of j + 2
         const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int r = rb + tr + 16 * i, c = cb + tc + 16 * q;
-                if (r < nr && c < ncols) Y[((size_t)r * ncols + c) * J + j] = make_double2(wgt * yr[i][q], wgt * yi[i][q]);
+                if (r < nr && c < ncols)
+                    Y[((size_t)r * ncols + c) * J + j] = make_double2(wgt * acc[i][q].x, wgt * acc[i][q].y);
             }
     }
 }
@@ -853,7 +845,7 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_NORM);
     {
-        const size_t smem = 2 * (size_t)g.Ks * (NY_R + NY_C) * sizeof(double2);
+        const size_t smem = (size_t)g.Ks * (NY_R + NY_C) * sizeof(float4);
         if ((e = smem_limit((const void *)k_norm_y, smem))) return e;
         dim3 grid((ncols + NY_C - 1) / NY_C, (nr + NY_R - 1) / NY_R, (J + NY_J - 1) / NY_J);
         k_norm_y<<<grid, 256, smem, h->stream>>>(g, RU, CV, r0, nr, c0, ncols, Y);
