@@ -15,16 +15,20 @@
 // contiguous block, so that one bulk copy (cp.async.bulk) per tile lands it ready for
 // the UMMA descriptors (a tiled tensor copy of this layout would move 16-byte rows).
 //
-// Kernel roles (192 threads, one persistent CTA per SM):
+// Kernel roles (320 threads, one persistent CTA per SM):
 //   warp 0   producer: both planes' particle tiles once per work item (plane pair,
-//            particle tile), then the ring of row tiles (32 (ref, shift) rows of each
-//            plane per stage)
+//            particle tile), one at a time through a single shared-memory tile, then the
+//            ring of row tiles (32 (ref, shift) rows of each plane per stage)
 //   warp 1   TMEM allocation and the single MMA-issuing thread; accumulators are
-//            double buffered, each buffer 2 x 64 TMEM columns (one per plane)
-//   warps 2-5 epilogue: tcgen05.ld of both planes' 128 x 64 accumulators (each warp
-//            its 32-lane quadrant), Z(m) and Z(P - m) for 16 rows at a time into two
-//            128B-swizzled staging tiles, written out with one TMA bulk store each
-//            to Z[plane][col][rs]
+//            double buffered, each buffer 2 x 64 TMEM columns (one per plane); each
+//            particle tile is copied into TMEM (tcgen05.cp, 8 columns per 16-wide K step)
+//            and the MMAs read their A operand from there, so shared memory holds one
+//            particle tile in transit and a deeper ring of row tiles; before an item's
+//            copies replace the particle tiles the previous item's MMAs are waited for
+//   warps 2-9 epilogue, two per TMEM lane quadrant (warp w: quadrant w mod 4, half
+//            (w - 2) / 4 of the tile): tcgen05.ld of its 16 (ref, shift) rows of both
+//            planes' accumulators, Z(m) and Z(P - m) into two 128B-swizzled staging tiles,
+//            written out with one TMA bulk store each to Z[plane][col][rs]
 // The factor 4 of X is carried by the packed particle operand (exact in BF16).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code,
 // drains its own outstanding copies (bounded), frees its TMEM and returns.
@@ -41,10 +45,12 @@ namespace pftcc {
 constexpr int U_BM = 128;        // particles per tile (UMMA M)
 constexpr int U_BN = 64;         // N columns per plane and tile = 32 rs x (re, im)
 constexpr int U_RS = 32;         // (ref, shift) rows per tile
-constexpr int U_THREADS = 192;
+constexpr int U_THREADS = 320;
+constexpr int ACC_COLS = 2 * 2 * U_BN;        // TMEM: two accumulator buffers x two planes x U_BN columns
+constexpr int TMEM_COLS = 512;                // accumulators, then both planes' particle tiles (A operands)
 constexpr long long WAIT_LIMIT = 20000000;   // polls of a bounded wait (~seconds)
 constexpr int STAGE_TILE = 32 * 128;          // one staged 32-row x 128-byte block
-constexpr int STAGE_BYTES = 4 * 2 * STAGE_TILE;   // four epilogue warps x (Z(m), Z(P-m)) blocks
+constexpr int STAGE_BYTES = 8 * 2 * STAGE_TILE;   // eight epilogue warps x (Z(m), Z(P-m)) blocks
 
 struct UmmaParams {
     int M;              // m planes of the packed operands (P + 1)
@@ -148,6 +154,25 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
         : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
 }
 
+// the same MMA with the A operand read from tensor memory (K-major, one row per lane)
+__device__ __forceinline__ void umma_bf16_at(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+// copy of a 128-row x 256-bit block (16 bf16 per row) from shared memory (matrix descriptor)
+// into tensor memory: row i to lane i, 8 columns
+__device__ __forceinline__ void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc)
+{
+    asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(taddr), "l"(sdesc));
+}
+
 __device__ __forceinline__ void umma_commit(uint64_t *bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -180,8 +205,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t a_bytes = (uint32_t)U_BM * up.KC * 16;     // one plane's particle tile
     const uint32_t b_bytes = (uint32_t)U_BN * up.KC * 16;     // one plane's row tile
-    unsigned char *sA = smem;                                  // [2 planes] particle tiles
-    unsigned char *sB = smem + 2 * a_bytes;                    // [stages][2 planes] row tiles
+    unsigned char *sA = smem;                                  // one plane's particle tile (on its way to TMEM)
+    unsigned char *sB = smem + a_bytes;                        // [stages][2 planes] row tiles
     unsigned char *stg = sB + (size_t)up.stages * 2 * b_bytes; // [4 warps][2][32][128 B], 1024-B aligned
     uint64_t *bars = reinterpret_cast<uint64_t *>(stg + STAGE_BYTES);
     uint64_t *full = bars;                    // [stages]
@@ -191,8 +216,9 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     uint64_t *t_full = a_full + 2;            // [2]
     uint64_t *t_empty = a_full + 4;           // [2]
     uint64_t *mma_done = a_full + 6;
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(a_full + 7);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(a_full + 8);
+    uint64_t *item_done = a_full + 7;          // an item's MMAs finished (its TMEM A may be replaced)
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(a_full + 8);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(a_full + 9);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -200,14 +226,15 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
         mbar_init(a_full, 1);
         mbar_init(a_empty, 1);
         mbar_init(t_full, 1); mbar_init(t_full + 1, 1);
-        mbar_init(t_empty, 128); mbar_init(t_empty + 1, 128);
+        mbar_init(t_empty, 256); mbar_init(t_empty + 1, 256);
         mbar_init(mma_done, 1);
+        mbar_init(item_done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(256));
+                     "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
@@ -224,17 +251,18 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
 
     if (warp == 0 && lane == 0) {
         // ------------------------------------------------------------ TMA producer
-        long long itb = 0;
-        int ii = 0;
+        long long itb = 0, na = 0;     // row-tile stages and particle tiles loaded
         bool ok = true;
-        for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
+        for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
             const int mp = w / up.n_ptiles, pt = w - mp * up.n_ptiles;
             const int pm[2] = {mp, mp == 0 ? P : P - mp};
-            if (ii > 0 && !mbar_wait(a_empty, (ii - 1) & 1, abort_flag)) { fail(1); ok = false; break; }
-            mbar_expect_tx(a_full, 2 * a_bytes);
-            for (int h = 0; h < 2; ++h)
-                bulk_load(sA + (size_t)h * a_bytes,
-                          up.P16 + (size_t)(pm[h] * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
+            // both planes' particle tiles, one at a time through sA (the MMA issuer copies each to TMEM)
+            for (int h = 0; h < 2; ++h, ++na) {
+                if (na > 0 && !mbar_wait(a_empty, (uint32_t)((na - 1) & 1), abort_flag)) { fail(1); ok = false; break; }
+                mbar_expect_tx(a_full, a_bytes);
+                bulk_load(sA, up.P16 + (size_t)(pm[h] * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
+            }
+            if (!ok) break;
             for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
                 const int s = (int)(itb % up.stages);
                 if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag)) {
@@ -252,8 +280,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             for (long long i = 0; i < WAIT_LIMIT && !mbar_try(full + s, (uint32_t)((t / up.stages) & 1)); ++i)
                 __nanosleep(64);
         }
-        if (ii > 0)
-            for (long long i = 0; i < WAIT_LIMIT && !mbar_try(a_full, (uint32_t)((ii - 1) & 1)); ++i) __nanosleep(64);
+        if (na > 0)
+            for (long long i = 0; i < WAIT_LIMIT && !mbar_try(a_full, (uint32_t)((na - 1) & 1)); ++i) __nanosleep(64);
     } else if (warp == 1 && lane == 0) {
         // ------------------------------------------------------------ MMA issuer
         // instruction descriptor: F32 accumulate, BF16 x BF16, both K-major, N=64, M=128
@@ -261,12 +289,25 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                                ((uint32_t)(U_BM >> 4) << 24);
         const uint32_t a_base = smem_u32(sA), b_base0 = smem_u32(sB);
         const int ksteps = up.Kp / 16, lo_off = up.Kp / 8;
-        long long itb = 0, tacc = 0;
+        const int acol = up.KC * 4;              // TMEM columns of one plane's particle tile (8 per 16-wide K step)
+        long long itb = 0, tacc = 0, na = 0;
         int ii = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
-            if (!mbar_wait(a_full, ii & 1, abort_flag)) { fail(3); ok = false; break; }
-            tc_fence_after();
+            if (ii > 0) {
+                // the previous item's MMAs read the TMEM particle tiles: let them finish first
+                umma_commit(item_done);
+                if (!mbar_wait(item_done, (uint32_t)((ii - 1) & 1), abort_flag)) { fail(7); ok = false; break; }
+            }
+            for (int h = 0; h < 2; ++h, ++na) {
+                if (!mbar_wait(a_full, (uint32_t)(na & 1), abort_flag)) { fail(3); ok = false; break; }
+                tc_fence_after();
+                const uint32_t tcol = tmem_base + ACC_COLS + (uint32_t)(h * acol);
+                for (int st = 0; st < up.KC / 2; ++st)
+                    tmem_cp_128x256b(tcol + 8 * st, umma_desc(a_base + (uint32_t)(2 * st) * (U_BM * 16), U_BM * 16, 128));
+                umma_commit(a_empty);            // sA reusable once the copies have read it
+            }
+            if (!ok) break;
             for (int j = 0; j < up.n_rtiles; ++j, ++itb, ++tacc) {
                 const int s = (int)(itb % up.stages);
                 if (!mbar_wait(full + s, (uint32_t)((itb / up.stages) & 1), abort_flag)) { fail(4); ok = false; break; }
@@ -278,29 +319,28 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                 // accumulator buffer acc: columns [0, 64) plane mA, [64, 128) plane mB
                 for (int h = 0; h < 2; ++h) {
                     const uint32_t d_tmem = tmem_base + (uint32_t)(acc * 2 * U_BN + h * U_BN);
-                    const uint32_t ah = a_base + (uint32_t)h * a_bytes;
+                    const uint32_t at = tmem_base + ACC_COLS + (uint32_t)(h * acol);   // this plane's particle tile
                     const uint32_t b_base = b_base0 + ((uint32_t)s * 2 + h) * b_bytes;
                     for (int ks = 0; ks < ksteps; ++ks) {
 #pragma unroll
                         for (int prod = 0; prod < 3; ++prod) {
                             const int ac = (prod == 2 ? lo_off : 0) + 2 * ks;   // lo(A) * hi(B)
                             const int bc = (prod == 1 ? lo_off : 0) + 2 * ks;   // hi(A) * lo(B)
-                            const uint64_t ad = umma_desc(ah + (uint32_t)ac * (U_BM * 16), U_BM * 16, 128);
                             const uint64_t bd = umma_desc(b_base + (uint32_t)bc * (U_BN * 16), U_BN * 16, 128);
-                            umma_bf16(d_tmem, ad, bd, idesc, (ks > 0 || prod > 0) ? 1u : 0u);
+                            umma_bf16_at(d_tmem, at + (uint32_t)(ac * 4), bd, idesc, (ks > 0 || prod > 0) ? 1u : 0u);
                         }
                     }
                 }
                 umma_commit(empty + s);      // N stage reusable once these MMAs finish
                 umma_commit(t_full + acc);   // accumulator ready for the epilogue
             }
-            umma_commit(a_empty);            // particle tile reusable
         }
         umma_commit(mma_done);
         for (long long i = 0; i < WAIT_LIMIT && !mbar_try(mma_done, 0); ++i) __nanosleep(64);
     } else if (warp >= 2) {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                       // TMEM lane quadrant of this warp
+        const int c = (warp - 2) >> 2;                // its half of the tile: complex rs 16c .. 16c + 15
         unsigned char *stg_w = stg + (size_t)(warp - 2) * 2 * STAGE_TILE;   // boxes of Z(mA), Z(mB)
         long long tacc = 0;
         bool ok = true;
@@ -320,17 +360,13 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                 tc_fence_after();
                 // both planes' 64 columns in flight at once, one wait; the accumulator is handed
                 // back to the MMA issuer before Z is formed and stored
-                uint32_t r4[4][32];     // [plane * 2 + chunk][32 columns = 16 complex]
-#pragma unroll
-                for (int c = 0; c < 4; ++c)
-                    tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * 2 * U_BN + 32 * c), r4[c]);
+                uint32_t ra[32], rb[32];     // this half's 32 columns (16 complex) of each plane
+                tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * 2 * U_BN + 32 * c), ra);
+                tmem_ld32(tmem_base + ((uint32_t)(32 * q) << 16) + (uint32_t)(acc * 2 * U_BN + U_BN + 32 * c), rb);
                 tmem_wait_ld();
                 tc_fence_before();
                 mbar_arrive(t_empty + acc);
-#pragma unroll
-                for (int c = 0; c < 2; ++c) {
-                    const uint32_t (&ra)[32] = r4[c];
-                    const uint32_t (&rb)[32] = r4[2 + c];
+                {
                     // the staging boxes of the previous chunk must have been read out
                     if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
                     __syncwarp();
@@ -372,7 +408,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(256));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
 }
 
@@ -543,19 +579,21 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
     up.n_rtiles = n_rtiles; up.rtile0 = rtile0; up.rtiles_m = us.rtiles;
     const size_t a_bytes = (size_t)U_BM * KC * 16, b_bytes = (size_t)U_BN * KC * 16;
-    // 1 KiB alignment slack, the particle tile, the N ring, 512 B of barriers and the
-    // epilogue's staging tiles
+    // 1 KiB alignment slack, one particle tile on its way to TMEM, the N ring (per stage both
+    // planes' row tiles), 512 B of barriers and the epilogue's staging tiles; both planes'
+    // particle tiles sit in TMEM beside the accumulators
     const size_t tail = 512 + STAGE_BYTES;
-    // both planes' particle tiles, and per ring stage both planes' row tiles
+    if (ACC_COLS + 2 * 4 * KC > TMEM_COLS)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: particle tiles too large for tensor memory");
     int stages = 4;
-    while (stages > 1 && 1024 + 2 * a_bytes + stages * 2 * b_bytes + tail > 227 * 1024) --stages;
-    if (1024 + 2 * a_bytes + stages * 2 * b_bytes + tail > 227 * 1024)
+    while (stages > 1 && 1024 + a_bytes + stages * 2 * b_bytes + tail > 227 * 1024) --stages;
+    if (1024 + a_bytes + stages * 2 * b_bytes + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
     up.stages = stages;
     up.P16 = ws.B16; up.R16 = ws.A16;
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
-    const size_t smem = 1024 + 2 * a_bytes + stages * 2 * b_bytes + tail;
+    const size_t smem = 1024 + a_bytes + stages * 2 * b_bytes + tail;
     if ((e = smem_limit((const void *)k_umma_stage1, smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
     const int nitems = ((M - 1) / 2 + 1) * n_ptiles;   // plane pairs x particle tiles
