@@ -555,7 +555,8 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
     }
     __syncthreads();
     const int cl = blockIdx.x;
-    const size_t plane = (size_t)sp.xcols * sp.xrows;
+    // Z offsets in float2 units fit 32 bits (the launcher checks P xcols xrows < 2^32)
+    const uint32_t plane = (uint32_t)sp.xcols * (uint32_t)sp.xrows;
     const float2 *Xc = X + (size_t)cl * sp.xrows;
     float kc[8];
     int ki[8];
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
             float2 v;
             asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];"
                          : "=f"(v.x), "=f"(v.y)
-                         : "l"(xr + (size_t)j * plane));
+                         : "l"(xr + (uint32_t)j * plane));
             return v;
         };
     };
@@ -671,8 +672,8 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
 //   B  D(c, rho) from Y by the length-P/2 FP64 transform of the packed half spectrum (the
 //      normaliser's k_norm_fft, split H1 x H2 = P/2), stored as 1/sqrt(D * sqsum_ptcl);
 //   C  X(c, m) in FP32, a thread per (c, m);
-//   D  the per-triple transform and argmax of each candidate (one thread each, triple_corr),
-//      then the particle's best (lowest id among equal correlations).
+//   D  the per-triple transform and argmax of each candidate (two threads each, the halves of
+//      triple_corr), then the particle's best (lowest id among equal correlations).
 template <int P> struct HalfSplit;
 template <> struct HalfSplit<64> { static constexpr int H1 = 8, H2 = 4; };
 template <> struct HalfSplit<180> { static constexpr int H1 = 10, H2 = 9; };
@@ -804,18 +805,40 @@ __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, 
         Xs[c * M + m] = make_float2(4.f * xr, 4.f * xi);
     }
     __syncthreads();
-    // D: transform and argmax per candidate
-    if (t < nc) {
+    // D: transform and argmax per candidate, two lanes of warp 0 per candidate (lanes 2c, 2c + 1):
+    // pass A by classes (class 0 and the first half of the mirror pairs; the rest and the
+    // middle class), pass B by blocks [0, LB) and [LB, P2); the halves' maxima are combined
+    // with the lowest rotation among equal maxima
+    if (t < 32) {
+        constexpr int NPAIR = (P1 + 1) / 2, PM = 1 + (NPAIR - 1) / 2, LB = (P2 + 1) / 2;
+        const int c = t >> 1, half = t & 1;
+        const bool act = c < nc;
+        const int rs = act ? rs_s[c] : -1;
         float best = -INFINITY;
         int brot = 0;
-        const int rs = rs_s[t];
+        float2 *sl = slab + (act ? c : 0);
+        auto getx = [&](int j) { return Xs[c * M + j]; };
+        auto dinv = [&](int rho) { return Ds[c * P + rho]; };
         if (rs >= 0) {
-            auto getx = [&](int j) { return Xs[t * M + j]; };
-            auto dinv = [&](int rho) { return Ds[t * P + rho]; };
-            triple_corr<P1, P2>(getx, dinv, slab + t, RS_MAX, tw, 1.0f / (2.0f * (float)N), nullptr, best, brot);
+            if (half == 0) {
+                passA_class0<P1, P2>(getx, sl, RS_MAX, tw);
+                passA_pairs<P1, P2>(1, PM, getx, sl, RS_MAX, tw);
+            } else {
+                passA_pairs<P1, P2>(PM, NPAIR, getx, sl, RS_MAX, tw);
+                passA_mid<P1, P2>(getx, sl, RS_MAX, tw);
+            }
         }
-        bc_s[t] = best;
-        bi_s[t] = rs < 0 ? 0x7fffffff : rs * N + brot;
+        __syncwarp();
+        if (rs >= 0)
+            passB<P1, P2>(half ? LB : 0, half ? P2 : LB, sl, RS_MAX, tw, dinv, 1.0f / (2.0f * (float)N), nullptr, best,
+                          brot);
+        const float ob = __shfl_xor_sync(0xffffffffu, best, 1);
+        const int orot = __shfl_xor_sync(0xffffffffu, brot, 1);
+        if (ob > best || (ob == best && orot < brot)) { best = ob; brot = orot; }
+        if (act && half == 0) {
+            bc_s[c] = best;
+            bi_s[c] = rs < 0 ? 0x7fffffff : rs * N + brot;
+        }
     }
     __syncthreads();
     if (t == 0) {
@@ -872,6 +895,7 @@ template <int P1, int P2>
 static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
                              float2 *cand, float *ccall, const int *perm)
 {
+    if ((unsigned long long)P1 * P2 * sp.xcols * sp.xrows >= (1ull << 32)) return cudaErrorInvalidValue;
     TwTables tw;
     fill_tw(tw, P1 * P2);
     // row slabs of P complex (the two-lane layout): 128 rows in flight up to P = 200, 64
