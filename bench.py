@@ -53,12 +53,13 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
-    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching"],
+    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
                          "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
                          "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
                          "prints a report line instead of the bench line); batching: a queue of chunks of the "
-                         "three batching geometries, U[50,300] references x U[500,5000] particles each")
+                         "three batching geometries, U[50,300] references x U[500,5000] particles each; project: "
+                         "the polar projector on the config-1 geometry")
     ap.add_argument("--grid-ptcls", type=int, default=200, help="particles whose problems also run the exhaustive grid")
     ap.add_argument("--report-ptcls", type=int, default=256, help="particles in the precision sample")
     return ap.parse_args()
@@ -562,6 +563,54 @@ def run_batching_report(args):
     print(json.dumps(out), flush=True)
 
 
+def run_project_report(args):
+    """The polar projector (pftcc_set_volume_ft = expand_cmat, pftcc_fproject_polar =
+    fproject_polar) on the config-1 geometry: a seeded box-128 volume FT, 500 orientations
+    (K = 39 shells x 180 rotations each); GPU wall time per call (synchronous, the host's
+    rotation matrices and uploads included), parity of three references against the
+    oracle, and the oracle's single-thread time per reference beside it."""
+    pkg = entry.load_package()
+    O = entry.load_oracle()
+    w = pkg.synth.config1()
+    box = w.box
+    rng = np.random.default_rng(5)
+    shape = (box, box, box // 2 + 1)
+    vol = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    n = w.nrefs
+    euls = np.stack([rng.uniform(0, 360, n), rng.uniform(0, 180, n), rng.uniform(0, 360, n)], 1).astype(np.float32)
+    pc = pkg.polarft_corrcalc()
+    pc.new(n, (1, 1), box=box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=False)
+    pc.set_volume_ft(vol)
+    t0 = time.perf_counter()
+    reps = 5
+    for _ in range(reps):
+        pc.set_volume_ft(vol)
+    t_expand = (time.perf_counter() - t0) / reps
+    for _ in range(3):
+        pc.fproject_polar(1, euls)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        pc.fproject_polar(1, euls)
+    t_proj = (time.perf_counter() - t0) / reps
+    g = O.geom(w.nrots, w.kfrom, w.kto, box)
+    t = O.tables(g)
+    ex = O.expand_cmat3d(vol, box)
+    worst = 0.0
+    t0 = time.perf_counter()
+    for r in range(3):
+        want = O.fproject_polar(g, t, ex, box, euls[r].astype(np.float64))
+        got = pc.get_ref_pft(r + 1, True)
+        worst = max(worst, float(np.max(np.abs(got - want)) / np.max(np.abs(want))))
+    t_cpu = (time.perf_counter() - t0) / 3
+    pc.kill()
+    samples = n * (w.kto - w.kfrom + 1) * w.pftsz
+    print(json.dumps({"report": "project", "box": box, "refs": n, "samples_per_call": samples,
+                      "gpu_seconds_per_call": t_proj, "refs_per_s": n / t_proj, "samples_per_s": samples / t_proj,
+                      "expand_cmat_seconds": t_expand, "parity_max_rel_err_vs_oracle": worst,
+                      "oracle_seconds_per_ref_1_thread": t_cpu}), flush=True)
+
+
 def main():
     args = parse()
     if args.report == "batching":
@@ -572,6 +621,9 @@ def main():
         return
     if args.report == "refine":
         run_refine_report(args)
+        return
+    if args.report == "project":
+        run_project_report(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -116,6 +116,21 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
 int pftcc_polarize_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *cmats_dev, int griddev);
 int pftcc_polarize_refs(pftcc_handle *h, int first_iref, int n, const float *cmats, int iseven, int griddev);
 
+/* ---- polar projection of a volume -------------------------------------------------- */
+/* projector%expand_cmat (simple_projector.f90:66-132): the volume's half FT
+ * image%cmat(box/2+1, box, box) (Fortran order, complex interleaved; even box with
+ * kfromto(2) <= box/2) expanded on the device by cyclic addressing and Friedel symmetry,
+ * times factor (1 unless norm4proj) */
+int pftcc_set_volume_ft(pftcc_handle *h, const float *cmat_half, int box, float factor);
+/* projector%fproject_polar (simple_projector.f90:218-239) for n orientations at once:
+ * references first_iref..first_iref+n-1 of the even (iseven != 0) or odd set from Spider
+ * Euler triplets euls[3 n] in degrees (ori%get_mat = euler2m, simple_ori.f90:1275), the
+ * 3x3x3 Kaiser-Bessel interpolation of interp_fcomp (:269-307; griddev != 0 skips the
+ * normalisation by the weights' sum); mask: K ints for shells kfrom..kto (0 = set to zero)
+ * or NULL for all */
+int pftcc_fproject_polar(pftcc_handle *h, int first_iref, int n, const float *euls, const int *mask, int iseven,
+                         int griddev);
+
 /* ---- memoisers ------------------------------------------------------------------ */
 /* memoize_ffts :848-861: prepares the particle-side angular spectra of the
  * m-domain search (no-op for the exact path, which needs none) */

@@ -78,6 +78,9 @@ def lib():
         L.orc_snhc_uniform.argtypes = [C.c_ulonglong, C.c_int, C.c_int]
         L.orc_snhc_uniform.restype = C.c_double
         L.orc_polarize.argtypes = [G, fp, fp, C.c_int, dp]
+        L.orc_euler2m.argtypes = [dp, dp]
+        L.orc_expand_cmat3d.argtypes = [C.c_int, fp, C.c_double, fp]
+        L.orc_fproject_polar.argtypes = [G, fp, C.c_int, fp, dp, ip, C.c_int, dp]
         L.orc_kb_apod.argtypes = [C.c_double]
         L.orc_kb_apod.restype = C.c_double
         L.orc_fftpath_new.argtypes = [G]
@@ -220,6 +223,35 @@ def polarize(g: Geom, t: Tables, cmat, griddev=False) -> np.ndarray:
     out = _c128_out((g.K, g.pftsz))
     lib().orc_polarize(C.byref(g), _P(t.polar, C.c_float), _P(_c64(cmat), C.c_float), int(bool(griddev)),
                        out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def euler2m(eul) -> np.ndarray:
+    """rotation matrix of a Spider Euler triplet in degrees (euler2m, simple_ori.f90:1275)"""
+    e = np.ascontiguousarray(eul, np.float64)
+    R = np.zeros(9, np.float64)
+    lib().orc_euler2m(_P(e, C.c_double), _P(R, C.c_double))
+    return R.reshape(3, 3)
+
+
+def expand_cmat3d(cmat_half, box: int, factor: float = 1.0) -> np.ndarray:
+    """cmat_half: complex64 (box, box, box//2+1) = image%cmat(h, k, m) in [m][k][h] order;
+    returns the expanded cube complex64 (S, S, S), S = box + 5, index [m + E][k + E][h + E]"""
+    S = box + 5
+    out = np.zeros((S, S, S), np.complex64)
+    lib().orc_expand_cmat3d(int(box), _P(_c64(cmat_half), C.c_float), C.c_double(factor),
+                            out.view(np.float32).ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def fproject_polar(g: Geom, t: Tables, cmat_exp, box: int, eul, mask=None, griddev=False) -> np.ndarray:
+    """polar FT (K, P) of the central section at Euler angles eul (degrees) from the expanded cube"""
+    out = _c128_out((g.K, g.pftsz))
+    e = np.ascontiguousarray(eul, np.float64)
+    m = None if mask is None else np.ascontiguousarray(mask, np.int32)
+    lib().orc_fproject_polar(C.byref(g), _P(t.polar, C.c_float), int(box), _P(_c64(cmat_exp), C.c_float),
+                             _P(e, C.c_double), _P(m, C.c_int), int(bool(griddev)),
+                             out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
     return out
 
 

@@ -500,6 +500,119 @@ void orc_polarize(const orc_geom *g, const float *polar, const float *cmat, int 
 }
 
 /* ------------------------------------------------------------------------- */
+/* Polar projection of a volume's Fourier transform (the references of refine3D). */
+
+/* rotmat :1350-1390 (angle in degrees; the z rotation is the negative one) and
+ * euler2m :1275-1284 of simple_ori.f90: R = R3(e3) R2(e2) R1(e1), z-y-z (Spider).
+ * R row-major, R[3 i + j] = r(i+1, j+1). */
+static void rotmat3(double ang_deg, int choice, double r[9])
+{
+    const double a = ang_deg * 3.14159265358979323846 / 180.0, c = cos(a), s = sin(a);
+    for (int i = 0; i < 9; ++i) r[i] = 0.0;
+    if (choice == 1) { r[0] = 1.0; r[4] = c; r[5] = -s; r[7] = s; r[8] = c; }
+    else if (choice == 2) { r[0] = c; r[2] = -s; r[4] = 1.0; r[6] = s; r[8] = c; }
+    else { r[0] = c; r[1] = s; r[3] = -s; r[4] = c; r[8] = 1.0; }
+}
+
+static void matmul3(const double a[9], const double b[9], double c[9])
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double t = 0.0;
+            for (int l = 0; l < 3; ++l) t += a[3 * i + l] * b[3 * l + j];
+            c[3 * i + j] = t;
+        }
+}
+
+void orc_euler2m(const double eul[3], double R[9])
+{
+    double r1[9], r2[9], r3[9], t[9];
+    rotmat3(eul[0], 3, r1);
+    rotmat3(eul[1], 2, r2);
+    rotmat3(eul[2], 3, r3);
+    matmul3(r3, r2, t);
+    matmul3(t, r1, R);
+}
+
+/* comp_addr_phys / get_fcomp (simple_ftiter.f90:241-265, simple_image.f90) for a
+ * volume: the half volume image%cmat(h, k, m), h = 0..B/2, stored here as
+ * [m][k][h] complex; negative h read as the conjugate of (-h, -k, -m) */
+static void get_fcomp3d(const float *cmat, int box, int h, int k, int m, double *re, double *im)
+{
+    const int ld = box / 2 + 1;
+    double sgn = 1.0;
+    if (h < 0) { h = -h; k = -k; m = -m; sgn = -1.0; }
+    const int p2 = k + (k < 0 ? box : 0), p3 = m + (m < 0 ? box : 0);
+    const size_t e = ((size_t)p3 * box + p2) * ld + h;
+    *re = cmat[2 * e];
+    *im = sgn * cmat[2 * e + 1];
+}
+
+/* expand_cmat (simple_projector.f90:66-132) of a volume of even box B: the cube
+ * cmat_exp(h, k, m), h, k, m in [-E, E] with E = B/2 + 2 (maxval(|lims|) + ceiling(KBWINSZ)),
+ * each logical address wrapped cyclically into the mode-3 limits [-B/2, B/2] x
+ * [-B/2, B/2 - 1] x [-B/2, B/2 - 1] (cyci_1d) and read with Friedel symmetry, times
+ * factor. Output [m][k][h] complex, side S = 2E + 1. */
+void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cmat_exp)
+{
+    const int E = box / 2 + 2, S = 2 * E + 1;
+    for (int m = -E; m <= E; ++m)
+        for (int k = -E; k <= E; ++k)
+            for (int h = -E; h <= E; ++h) {
+                const int hh = cyci_1d(-box / 2, box / 2, h);
+                const int kk = cyci_1d(-box / 2, box / 2 - 1, k);
+                const int mm = cyci_1d(-box / 2, box / 2 - 1, m);
+                double re, im;
+                get_fcomp3d(cmat_half, box, hh, kk, mm, &re, &im);
+                const size_t e = ((size_t)(m + E) * S + (k + E)) * S + (h + E);
+                cmat_exp[2 * e] = (float)(factor * re);
+                cmat_exp[2 * e + 1] = (float)(factor * im);
+            }
+}
+
+/* fproject_polar (simple_projector.f90:218-239) with interp_fcomp_norm / _grid
+ * (:269-307): for rotations irot < P and shells kfrom..kto, loc = vec R with
+ * vec = (polar(irot, k), polar(irot + nrots, k), 0) (get_coord), the 3x3x3 window
+ * around nint(loc), weights the product of apod(win - loc) per axis, normalised by
+ * their sum unless griddev; shells with mask[k - kfrom] == 0 are zero. */
+void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
+                        const double eul[3], const int *mask, int griddev, double *pft)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g);
+    const int E = box / 2 + 2, S = 2 * E + 1;
+    double R[9];
+    orc_euler2m(eul, R);
+    for (int ik = 0; ik < K; ++ik)
+        for (int i = 0; i < P; ++i) {
+            double accr = 0.0, acci = 0.0;
+            if (!mask || mask[ik]) {
+                const double vx = polar[ik * 2 * N + i], vy = polar[ik * 2 * N + N + i];
+                double loc[3];
+                for (int j = 0; j < 3; ++j) loc[j] = vx * R[j] + vy * R[3 + j];
+                int w0[3];
+                double wa[3][3];
+                for (int d = 0; d < 3; ++d) {
+                    w0[d] = f_nint(loc[d]) - 1;
+                    for (int l = 0; l < 3; ++l) wa[d][l] = orc_kb_apod((double)(w0[d] + l) - loc[d]);
+                }
+                double wsum = 0.0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        for (int c = 0; c < 3; ++c) {
+                            const double w = wa[0][a] * wa[1][b] * wa[2][c];
+                            const size_t e = ((size_t)(w0[2] + c + E) * S + (w0[1] + b + E)) * S + (w0[0] + a + E);
+                            accr += w * cmat_exp[2 * e];
+                            acci += w * cmat_exp[2 * e + 1];
+                            wsum += w;
+                        }
+                if (!griddev) { accr /= wsum; acci /= wsum; }
+            }
+            pft[2 * (ik * P + i)] = accr;
+            pft[2 * (ik * P + i) + 1] = acci;
+        }
+}
+
+/* ------------------------------------------------------------------------- */
 /* Project-written mixed-radix FFT (recursive decimation in time, radices 4, 2,
  * 3, 5 and a plain DFT for any other prime factor).  Stands in for FFTW. */
 typedef struct { int n; int nf; int f[32]; double *tw; float *twf; } fftplan;

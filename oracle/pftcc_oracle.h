@@ -123,6 +123,13 @@ void orc_dctfmat_ddf(const orc_geom *g, const float *polar, const orc_ctf *c, do
 void orc_polarize(const orc_geom *g, const float *polar, const float *cmat, int griddev, double *pft);
 double orc_kb_apod(double x);   /* simple_kbinterpol.f90:130-141 with Whalf=1.5, alpha=sqrt(2) */
 
+/* polar projection of a volume FT (simple_projector.f90: expand_cmat :66-132,
+ * fproject_polar :218-239, interp_fcomp :269-307; simple_ori.f90 euler2m :1275) */
+void orc_euler2m(const double eul[3], double R[9]);
+void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cmat_exp);
+void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
+                        const double eul[3], const int *mask, int griddev, double *pft);
+
 /* ---------------------------------------------------------------------------
  * FP32 FFT path, the reference's loop structure (memoize_fft :864-877 and
  * calc_corrs_over_k :1132-1162) on a project-written mixed-radix FFT that stands

@@ -73,6 +73,8 @@ SIGNATURES = {
     "pftcc_polarize_ptcls": [_h, C.c_int, C.c_int, _fp, C.c_int],
     "pftcc_polarize_ptcls_dev": [_h, C.c_int, C.c_int, _vp, C.c_int],
     "pftcc_polarize_refs": [_h, C.c_int, C.c_int, _fp, C.c_int, C.c_int],
+    "pftcc_set_volume_ft": [_h, _fp, C.c_int, C.c_float],
+    "pftcc_fproject_polar": [_h, C.c_int, C.c_int, _fp, C.POINTER(C.c_int), C.c_int, C.c_int],
     "pftcc_memoize_ffts": [_h],
     "pftcc_gencorrs": [_h, C.c_int, C.c_int, _fp, _fp],
     "pftcc_gencorr_for_rot": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp],

@@ -271,7 +271,7 @@ static void free_all(pftcc_handle *h)
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
                     h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
-                    h->ws.cand_ref};
+                    h->ws.cand_ref, h->vol_cube};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
     for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -632,6 +632,89 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
         ST(polarize_dev(h, first_slot + c0, m, (const float2 *)h->pol_stage, griddev));
     }
     CK(cudaStreamSynchronize(h->stream), "polarize");
+    return PFTCC_OK;
+}
+
+// ---- polar projection of a volume (simple_projector.f90) --------------------------------
+int pftcc_set_volume_ft(pftcc_handle *h, const float *cmat_half, int box, float factor)
+{
+    if (!h || !cmat_half || box < 2 || (box & 1)) return set_err(h, PFTCC_ERR_ARG, "set_volume_ft: bad arguments");
+    if (h->g.kto > box / 2) return set_err(h, PFTCC_ERR_ARG, "set_volume_ft: kfromto(2) beyond the volume's Nyquist");
+    if (!std::isfinite(factor)) return set_err(h, PFTCC_ERR_ARG, "set_volume_ft: factor not finite");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    const size_t half = (size_t)box * box * (box / 2 + 1), S = (size_t)box + 5;
+    if (h->vol_box != box) {
+        dev_free(h, h->vol_cube);
+        h->vol_cube = nullptr;
+        h->vol_box = 0;
+        ST(dev_alloc(h, (void **)&h->vol_cube, S * S * S * sizeof(float2), "expanded volume FT"));
+    }
+    float2 *stage = nullptr;
+    ST(dev_alloc(h, (void **)&stage, half * sizeof(float2), "volume FT upload"));
+    cudaError_t e = cudaMemcpyAsync(stage, cmat_half, half * sizeof(float2), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_expand_cmat(h, box, stage, factor, h->vol_cube);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    dev_free(h, stage);
+    if (e != cudaSuccess) return cuda_err(h, e, "set_volume_ft");
+    h->vol_box = box;
+    return PFTCC_OK;
+}
+
+int pftcc_fproject_polar(pftcc_handle *h, int first_iref, int n, const float *euls, const int *mask, int iseven,
+                         int griddev)
+{
+    if (!h || !euls || n < 0) return set_err(h, PFTCC_ERR_ARG, "fproject_polar: bad arguments");
+    if (first_iref < 1 || first_iref + n - 1 > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "fproject_polar: range");
+    if (!h->vol_cube) return set_err(h, PFTCC_ERR_STATE, "fproject_polar: no volume (set_volume_ft first)");
+    if (n == 0) return PFTCC_OK;
+    // euler2m (simple_ori.f90:1275-1284, rotmat :1350-1390): R = R3(e3) R2(e2) R1(e1), degrees
+    std::vector<double> R((size_t)n * 9);
+    for (int r = 0; r < n; ++r) {
+        double m[3][9];
+        for (int a = 0; a < 3; ++a) {
+            const double ang = (double)euls[3 * r + a];
+            if (!std::isfinite(ang)) return set_err(h, PFTCC_ERR_ARG, "fproject_polar: Euler angle not finite");
+            const double t = ang * 3.14159265358979323846 / 180.0, c = std::cos(t), sn = std::sin(t);
+            double *x = m[a];
+            for (int i = 0; i < 9; ++i) x[i] = 0.0;
+            if (a == 1) { x[0] = c; x[2] = -sn; x[4] = 1.0; x[6] = sn; x[8] = c; }    // about y (tilt)
+            else { x[0] = c; x[1] = sn; x[3] = -sn; x[4] = c; x[8] = 1.0; }          // about z
+        }
+        double t32[9], out[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int l = 0; l < 3; ++l) v += m[2][3 * i + l] * m[1][3 * l + j];
+                t32[3 * i + j] = v;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int l = 0; l < 3; ++l) v += t32[3 * i + l] * m[0][3 * l + j];
+                out[3 * i + j] = v;
+            }
+        for (int i = 0; i < 9; ++i) R[(size_t)r * 9 + i] = out[i];
+    }
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    double *dR = nullptr;
+    int *dmask = nullptr;
+    ST(dev_alloc(h, (void **)&dR, R.size() * sizeof(double), "rotation matrices"));
+    if (mask) {
+        int st = dev_alloc(h, (void **)&dmask, (size_t)h->g.K * sizeof(int), "projection shell mask");
+        if (st) { dev_free(h, dR); return st; }
+    }
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    float2 *dst = (iseven ? h->refs_even : h->refs_odd) + (size_t)(first_iref - 1) * KP;
+    cudaError_t e = cudaMemcpyAsync(dR, R.data(), R.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && mask)
+        e = cudaMemcpyAsync(dmask, mask, (size_t)h->g.K * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_fproject_polar(h, h->vol_box, h->vol_cube, dR, dmask, n, griddev ? 1 : 0, dst);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    dev_free(h, dR);
+    dev_free(h, dmask);
+    if (e != cudaSuccess) return cuda_err(h, e, "fproject_polar");
     return PFTCC_OK;
 }
 

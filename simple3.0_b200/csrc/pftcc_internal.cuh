@@ -117,6 +117,9 @@ struct pftcc_handle {
     int pol_griddev = -1;
     void *pol_stage = nullptr;           // device staging of host images
     size_t pol_stage_bytes = 0;
+    // the volume's expanded FT for polar projection (expand_cmat), side box + 5
+    float2 *vol_cube = nullptr;
+    int vol_box = 0;
     // small per-call device buffers
     pftcc::Work *d_work = nullptr;
     pftcc::Group *d_groups = nullptr;
@@ -171,6 +174,9 @@ int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *wha
 
 // ---- kernels (launch wrappers return cudaError_t of the launch) ---------------------
 cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int first_slot);
+cudaError_t launch_expand_cmat(pftcc_handle *h, int box, const float2 *half, float factor, float2 *cube);
+cudaError_t launch_fproject_polar(pftcc_handle *h, int box, const float2 *cube, const double *R, const int *mask, int n,
+                                  int griddev, float2 *out);
 cudaError_t launch_ctfmat(pftcc_handle *h, const pftcc_ctfparams *params, int n, float *out, float ddf,
                           int derivative);
 cudaError_t launch_sqsums(pftcc_handle *h, int first_slot, int n);

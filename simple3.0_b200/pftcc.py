@@ -204,6 +204,29 @@ class polarft_corrcalc:
         self._check(self._L.pftcc_polarize_refs(self._h, int(first_iref), a.shape[0], _f32p(a.view(np.float32)),
                                                 int(bool(iseven)), int(bool(griddev))))
 
+    # ---- PROJECTOR (simple_projector.f90) ---------------------------------------------------
+    def set_volume_ft(self, cmat_half, factor: float = 1.0):
+        """expand_cmat: cmat_half complex64 (box, box, box//2+1) = image%cmat(h, k, m) in [m][k][h]
+        order (the Fortran array's memory order)"""
+        a = np.ascontiguousarray(cmat_half, np.complex64)
+        box = a.shape[0]
+        if a.shape != (box, box, box // 2 + 1):
+            raise ValueError("set_volume_ft: expected (box, box, box//2+1)")
+        self._check(self._L.pftcc_set_volume_ft(self._h, _f32p(a.view(np.float32)), int(box), float(factor)))
+
+    def fproject_polar(self, first_iref: int, euls, iseven: bool = True, mask=None, griddev: bool = False):
+        """fproject_polar for len(euls) orientations (Spider Euler triplets, degrees) into
+        references first_iref.. (1-based); mask: K booleans for shells kfrom..kto or None"""
+        e = np.ascontiguousarray(euls, np.float32).reshape(-1, 3)
+        m = None
+        if mask is not None:
+            m = np.ascontiguousarray(np.asarray(mask, bool).astype(np.int32))
+            if m.shape != (self.cfg.kfromto[1] - self.cfg.kfromto[0] + 1,):
+                raise ValueError("fproject_polar: mask needs one entry per shell kfrom..kto")
+        self._check(self._L.pftcc_fproject_polar(self._h, int(first_iref), e.shape[0], _f32p(e.reshape(-1)),
+                                                 None if m is None else m.ctypes.data_as(C.POINTER(C.c_int)),
+                                                 int(bool(iseven)), int(bool(griddev))))
+
     # ---- CALCULATORS -----------------------------------------------------------------------
     def gencorrs(self, iref: int, iptcl: int, shvec=None) -> np.ndarray:
         cc = np.zeros(self.cfg.nrots, np.float32)
