@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
-    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project"],
+    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project", "euclid"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
                          "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
                          "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
@@ -611,8 +611,73 @@ def run_project_report(args):
                       "oracle_seconds_per_ref_1_thread": t_cpu}), flush=True)
 
 
+def run_euclid_report(args):
+    """The Euclidean objective (cc_objfun = OBJFUN_EUCLID) on the config-1 geometry: the exact
+    batched search (search_best, PFTCC_PREC_EXACT) of 1,000 particles over 100 references x 9
+    shifts x 360 rotations under OBJFUN_CC and under OBJFUN_EUCLID (GPU wall time per call,
+    synchronous), 1,000 batched sigma_contrib requests, parity of gencorrs_euclid for three
+    pairs against the oracle and the oracle's single-thread time per pair."""
+    pkg = entry.load_package()
+    O = entry.load_oracle()
+    w = pkg.synth.config1(nrefs=100, nptcls=1000)
+    refs, R = pkg.synth.make_refs(w)
+    parts = pkg.synth.make_particles(w, R)
+    refs = refs.numpy()
+    pc = pkg.polarft_corrcalc()
+    pc.new(w.nrefs, (1, w.nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True, ctf_frame="ref")
+    pc.set_refs(1, refs, True)
+    pc.set_refs(1, refs, False)
+    pc.polarize_ptcls(0, parts.cmat.numpy())
+    pc.create_polar_absctfmats(pkg.ctfparams_array(w.nptcls, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                   dfx=parts.dfx, dfy=parts.dfy, angast=parts.angast))
+    K = w.kto - w.kfrom + 1
+    sig = (np.random.default_rng(6).uniform(0.5, 2.0, (w.nptcls, K)) * np.linspace(4.0, 0.5, K)).astype(np.float32)
+    pc.assign_sigma2_noise(sig)
+    shifts = np.array([[x, y] for x in (-1.0, 0.0, 1.0) for y in (-1.0, 0.0, 1.0)], np.float32)
+    out = {"report": "euclid", "box": w.box, "nrefs": w.nrefs, "nptcls": w.nptcls, "nshifts": len(shifts),
+           "nrots": w.nrots, "shells": w.kto - w.kfrom + 1}
+    evals = w.nptcls * w.nrefs * len(shifts) * w.nrots
+    for name, obj in (("cc", pkg._lib.OBJFUN_CC), ("euclid", pkg._lib.OBJFUN_EUCLID)):
+        pc.set_objfun(obj)
+        pc.search_best(shifts, "exact")
+        t0 = time.perf_counter()
+        reps = 3
+        for _ in range(reps):
+            pc.search_best(shifts, "exact")
+        dt = (time.perf_counter() - t0) / reps
+        out[f"exact_search_{name}_seconds"] = dt
+        out[f"exact_search_{name}_evals_per_s"] = evals / dt
+    n = 1000
+    rng = np.random.default_rng(7)
+    ir = rng.integers(1, w.nrefs + 1, n)
+    ip = rng.integers(1, w.nptcls + 1, n)
+    ro = rng.integers(1, w.nrots + 1, n)
+    sh = rng.uniform(-2, 2, (n, 2)).astype(np.float32)
+    pc.sigma_contrib_batch(ir, ip, ro, sh)
+    t0 = time.perf_counter()
+    pc.sigma_contrib_batch(ir, ip, ro, sh)
+    out["sigma_contrib_batch_1000_seconds"] = time.perf_counter() - t0
+    g = O.geom(w.nrots, w.kfrom, w.kto, w.box)
+    t = O.tables(g)
+    worst = 0.0
+    t0 = time.perf_counter()
+    for i in range(3):
+        c = O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]), float(parts.dfy[i]),
+                                      float(parts.angast[i])))
+        want = O.gencorrs_euclid(g, t, refs[i], pc.get_ptcl_pft(i + 1), sig[i].astype(np.float64), c, [0.5, -0.5])
+        got = pc.gencorrs_euclid(i + 1, i + 1, [0.5, -0.5])
+        worst = max(worst, float(np.max(np.abs(got - want)) / np.max(np.abs(want))))
+    out["oracle_seconds_per_pair_1_thread"] = (time.perf_counter() - t0) / 3
+    out["parity_max_scaled_err_vs_oracle"] = worst
+    pc.kill()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.report == "euclid":
+        run_euclid_report(args)
+        return
     if args.report == "batching":
         run_batching_report(args)
         return

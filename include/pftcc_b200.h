@@ -41,6 +41,9 @@ enum { PFTCC_FRAME_REF = 0,     /* |CTF| applied to the reference at the referen
        PFTCC_FRAME_PTCL = 1 };  /* |CTF| at the particle's polar index n+rot with the
                                    rotation-dependent normaliser sum |ref|^2 CTF^2(n+rot);
                                    equal to FRAME_REF for an isotropic CTF               */
+/* params_glob%cc_objfun (simple_defs.f90:61): the objective gencorrs / gencorr_for_rot(_8) /
+ * gencorr_grad_for_rot_8 / the batched searches evaluate */
+enum { PFTCC_OBJFUN_CC = 0, PFTCC_OBJFUN_EUCLID = 1 };
 
 enum { PFTCC_PREC_EXACT = 0,    /* FP32 direct sums per (ref, ptcl, shift), FRAME_REF/PTCL  */
        PFTCC_PREC_FP32 = 1,     /* m-domain contraction on CUDA cores (FP32), FRAME_PTCL    */
@@ -147,6 +150,35 @@ int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const dou
                                  double *f, double *grad);
 int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
                                       double *grad);
+
+/* ---- the Euclidean objective (reference frame only) -------------------------------- */
+/* params_glob%cc_objfun: PFTCC_OBJFUN_EUCLID makes pftcc_gencorrs, pftcc_gencorr_for_rot(_8),
+ * pftcc_gencorr_grad(_only)_for_rot_8 and the PFTCC_PREC_EXACT batched searches evaluate the
+ * Euclidean objective, as gencorrs_1/_2 (:1594-1617), gencorr_for_rot(_8) (:1619-1643) and
+ * gencorr_grad(_only)_for_rot_8 (:1849-1939) dispatch on it */
+int pftcc_set_objfun(pftcc_handle *h, int objfun);
+/* assign_sigma2_noise (:581-585): sigma2_noise(kfrom:kto, fromp:top), column-major, i.e.
+ * [top - fromp + 1][kto - kfrom + 1].  The values are copied: assign again after changing them.
+ * Every held particle needs a column before a Euclidean evaluation. */
+int pftcc_assign_sigma2_noise(pftcc_handle *h, int fromp, int top, const float *sigma2);
+/* gencorrs_euclid_1 (:1536-1557, shvec NULL) / gencorrs_euclid_2 (:1559-1592), euclids[nrots] */
+int pftcc_gencorrs_euclid(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *euclids);
+/* gencorr_euclid_for_rot (:2002-2024) / _8 (:2026-2048) */
+int pftcc_gencorr_euclid_for_rot(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot, float *f);
+int pftcc_gencorr_euclid_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot, double *f);
+/* gencorr_euclid_grad_for_rot_8 (:2071-2109) / gencorr_euclid_grad_only_for_rot_8 (:2111-2148) */
+int pftcc_gencorr_euclid_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                        double *f, double *grad);
+int pftcc_gencorr_euclid_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                             double *grad);
+/* gencorr_sigma_contrib (:2150-2188): sigma_contrib[K] (and, when not NULL, ptcl_sumsq[K],
+ * ref_sumsq[K]) over every shell kfrom..kto; needs no sigma2 */
+int pftcc_gencorr_sigma_contrib(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot,
+                                float *sigma_contrib, float *ptcl_sumsq, float *ref_sumsq);
+/* gencorr_sigma_contrib for n requests in one launch: sigma_contrib [n][K] (ptcl_sumsq,
+ * ref_sumsq likewise, or NULL), shifts [n][2] (the loop of euclid_sigma2%calc_sigma2 :107-120) */
+int pftcc_sigma_contrib_batch(pftcc_handle *h, int n, const int *iref, const int *iptcl, const int *irot,
+                              const float *shifts, float *sigma_contrib, float *ptcl_sumsq, float *ref_sumsq);
 
 /* ---- batched entry points (no single reference counterpart) ---------------------- */
 /* genfrc (:1417-1441) / calc_frc (:1443-1484): the per-shell correlation at irot,

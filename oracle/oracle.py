@@ -81,6 +81,10 @@ def lib():
         L.orc_euler2m.argtypes = [dp, dp]
         L.orc_expand_cmat3d.argtypes = [C.c_int, fp, C.c_double, fp]
         L.orc_fproject_polar.argtypes = [G, fp, C.c_int, fp, dp, ip, C.c_int, dp]
+        L.orc_pxls_p_shell.argtypes = [C.c_int, C.c_int, dp]
+        L.orc_gencorrs_euclid.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
+        L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
+        L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
         L.orc_kb_apod.argtypes = [C.c_double]
         L.orc_kb_apod.restype = C.c_double
         L.orc_fftpath_new.argtypes = [G]
@@ -184,6 +188,48 @@ def gencorr_grad3(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, dctf=None,
                             int(irot), int(bool(match_filt)), _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
                             _P(f, C.c_double), _P(g3, C.c_double))
     return float(f[0]), g3
+
+
+def pxls_p_shell(g: Geom) -> np.ndarray:
+    """pixels per shell k = kfrom..kto (setup_pxls_p_shell)"""
+    out = np.zeros(g.K, np.float64)
+    lib().orc_pxls_p_shell(g.kfrom, g.kto, _P(out, C.c_double))
+    return out
+
+
+def gencorrs_euclid(g: Geom, t: Tables, ref, ptcl, sigma2, ctf=None, shvec=None) -> np.ndarray:
+    """gencorrs_euclid_1 (shvec None) / gencorrs_euclid_2; sigma2[K] is the particle's
+    sigma2_noise(kfrom:kto, iptcl)"""
+    out = np.zeros(g.nrots, np.float64)
+    sig = np.ascontiguousarray(sigma2, np.float64)
+    lib().orc_gencorrs_euclid(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                              _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double),
+                              _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double), _P(sig, C.c_double),
+                              _P(pxls_p_shell(g), C.c_double), _P(out, C.c_double))
+    return out
+
+
+def gencorr_euclid_grad_for_rot(g: Geom, t: Tables, ref, ptcl, irot: int, sigma2, ctf=None, shvec=(0.0, 0.0)):
+    """(f, grad[2]) of gencorr_euclid_grad_for_rot_8; f alone is gencorr_euclid_for_rot_8"""
+    f = np.zeros(1, np.float64)
+    gr = np.zeros(2, np.float64)
+    sig = np.ascontiguousarray(sigma2, np.float64)
+    lib().orc_gencorr_euclid_grad_for_rot(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                                          _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double), int(irot),
+                                          _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
+                                          _P(sig, C.c_double), _P(pxls_p_shell(g), C.c_double),
+                                          _P(f, C.c_double), _P(gr, C.c_double))
+    return float(f[0]), gr
+
+
+def sigma_contrib(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=(0.0, 0.0)):
+    """(sigma_contrib, ptcl_sumsq, ref_sumsq), each [K] over kfrom..kto (gencorr_sigma_contrib)"""
+    sc, ps, rs = (np.zeros(g.K, np.float64) for _ in range(3))
+    lib().orc_sigma_contrib(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                            _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double), int(irot),
+                            _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double), _P(sc, C.c_double),
+                            _P(ps, C.c_double), _P(rs, C.c_double))
+    return sc, ps, rs
 
 
 def genfrc(g: Geom, t: Tables, ref, ptcl, irot: int, ctf=None, shvec=None) -> np.ndarray:

@@ -837,3 +837,114 @@ int orc_cpu_search(const orc_geom *g, int nrefs, const float *refs, int nptcls, 
     free(polar); free(at); free(at1);
     return used;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Euclidean objective (cc_objfun = OBJFUN_EUCLID), reference frame.
+ * setup_pxls_p_shell (:879-893): pixels of the positive quadrant h, k = 1..kto whose
+ * rounded radius nint(sqrt(h^2 + k^2)) is a shell in kfrom..kto. */
+void orc_pxls_p_shell(int kfrom, int kto, double *pxls)
+{
+    for (int i = 0; i < kto - kfrom + 1; ++i) pxls[i] = 0.0;
+    for (int h = 1; h <= kto; ++h)
+        for (int k = 1; k <= kto; ++k) {
+            const int sh = (int)lround(sqrt((double)(h * h + k * k)));
+            if (sh >= kfrom && sh <= kto) pxls[sh - kfrom] += 1.0;
+        }
+}
+
+/* calc_euclidk_for_rot (:1392-1415): sum_n |ref(n) - ptcl~(n + irot - 1)|^2 with the
+ * same cyclic extension as corrk_for_rot (the reference's four-way split on irot) */
+static double euclidk_for_rot(int P, const double *ref_k, const float *ptcl_k, int irot)
+{
+    const int N = 2 * P, s = irot - 1;
+    double acc = 0.0;
+    for (int n = 0; n < P; ++n) {
+        const int j = (n + s) % N;
+        double qr, qi;
+        if (j < P) { qr = ptcl_k[2 * j]; qi = ptcl_k[2 * j + 1]; }
+        else { qr = ptcl_k[2 * (j - P)]; qi = -ptcl_k[2 * (j - P) + 1]; }
+        const double dr = ref_k[2 * n] - qr, di = ref_k[2 * n + 1] - qi;
+        acc += dr * dr + di * di;
+    }
+    return acc;
+}
+
+/* gencorrs_euclid_1/_2: for every rotation
+ *   sum_{k = kfrom..kstop} pxls(k) / P * (2 kcorrs_k(irot) - S_ptcl(k) - S_ref(k)) / (2 sigma2(k))
+ * with kcorrs_k the per-shell correlation of calc_k_corrs (:1164-1188, the same cyclic
+ * correlation as corrk_for_rot) and S the shell's square sums (:1550-1551, :1587-1588).
+ * Both variants prepare the reference as ref * ctf (* shmat); gencorrs_euclid_1 goes
+ * through prep_ref4corr, whose shell normalisation applies only with match_filt, which
+ * the Euclidean objective does not use. */
+void orc_gencorrs_euclid(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                         const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                         const double *sigma2, const double *pxls, double *euclids)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    for (int irot = 1; irot <= N; ++irot) euclids[irot - 1] = 0.0;
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double sp = sqsum_kf(P, ptcl + 2 * ik * P), sr = sqsum_k(P, pr + 2 * ik * P);
+        const double w = pxls[ik] / (double)P / (2.0 * sigma2[ik]);
+        for (int irot = 1; irot <= N; ++irot)
+            euclids[irot - 1] += w * (2.0 * corrk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot) - sp - sr);
+    }
+    free(pr);
+}
+
+/* f = -sum_{k<=kstop} k * euclidk(irot) / (2 sigma2(k)) * pxls(k) / P (calc_euclid_for_rot_8
+ * :1308-1334); grad(d) = sum_{k<=kstop} k * (corrk(T_d, irot) - Re sum_n T_d(n) conj(ref(n)))
+ * / sigma2(k) * pxls(k) / P with T_d = i * argtransf_d * ref, argtransf_x the first P rows of
+ * argtransf and argtransf_y the last P (:2090-2108) */
+void orc_gencorr_euclid_grad_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                                     const double *shvec, int irot, const double *argtransf,
+                                     const double *argtransf_shellone, const double *sigma2, const double *pxls,
+                                     double *f, double *grad)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    double *t = (double *)malloc(sizeof(double) * 2 * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    double fs = 0.0, gx = 0.0, gy = 0.0;
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double k = (double)(g->kfrom + ik);
+        const double *a = pr + 2 * ik * P;
+        const float *q = ptcl + 2 * ik * P;
+        fs -= k * euclidk_for_rot(P, a, q, irot) / (2.0 * sigma2[ik]) * pxls[ik] / (double)P;
+        for (int d = 0; d < 2; ++d) {
+            double self = 0.0;
+            for (int n = 0; n < P; ++n) {
+                const double at = argtransf[ik * N + d * P + n];
+                t[2 * n] = -at * a[2 * n + 1];   /* i * at * (ar + i ai) */
+                t[2 * n + 1] = at * a[2 * n];
+                self += t[2 * n] * a[2 * n] + t[2 * n + 1] * a[2 * n + 1];
+            }
+            const double diffsq = corrk_for_rot(P, t, q, irot) - self;
+            const double contrib = k * diffsq / sigma2[ik] * pxls[ik] / (double)P;
+            if (d == 0) gx += contrib; else gy += contrib;
+        }
+    }
+    *f = fs;
+    grad[0] = gx;
+    grad[1] = gy;
+    free(t);
+    free(pr);
+}
+
+/* sigma_contrib(k) = 0.5 * euclidk(irot) / P, ptcl_sumsq(k) = sum_n |ptcl(n,k)|^2,
+ * ref_sumsq(k) = sum_n |ref_prep(n,k)|^2, every shell kfrom..kto (:2177-2187) */
+void orc_sigma_contrib(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                       const double *shvec, int irot, const double *argtransf, const double *argtransf_shellone,
+                       double *sigma_contrib, double *ptcl_sumsq, double *ref_sumsq)
+{
+    const int P = g->pftsz, K = K_OF(g);
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    for (int ik = 0; ik < K; ++ik) {
+        sigma_contrib[ik] = 0.5 * euclidk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot) / (double)P;
+        if (ptcl_sumsq) ptcl_sumsq[ik] = sqsum_kf(P, ptcl + 2 * ik * P);
+        if (ref_sumsq) ref_sumsq[ik] = sqsum_k(P, pr + 2 * ik * P);
+    }
+    free(pr);
+}

@@ -130,6 +130,25 @@ void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cm
 void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
                         const double eul[3], const int *mask, int griddev, double *pft);
 
+/* Euclidean objective (cc_objfun = OBJFUN_EUCLID).  sigma2[K] is the particle's column
+ * sigma2_noise(kfrom:kto, iptcl); pxls[K] the pixel counts per shell of setup_pxls_p_shell
+ * (:879-893); the reference is prepared in the reference frame as ref * ctf (* shmat). */
+void orc_pxls_p_shell(int kfrom, int kto, double *pxls);
+/* gencorrs_euclid_1 (:1536-1557, shvec == NULL) / gencorrs_euclid_2 (:1559-1592) */
+void orc_gencorrs_euclid(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                         const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                         const double *sigma2, const double *pxls, double *euclids);
+/* gencorr_euclid_grad_for_rot_8 (:2071-2109): f = calc_euclid_for_rot_8 (:1308-1334),
+ * grad[2] = d f / d(sx, sy); gencorr_euclid_for_rot_8 (:2026-2048) is f alone */
+void orc_gencorr_euclid_grad_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                                     const double *shvec, int irot, const double *argtransf,
+                                     const double *argtransf_shellone, const double *sigma2, const double *pxls,
+                                     double *f, double *grad);
+/* gencorr_sigma_contrib (:2150-2188) over all shells kfrom..kto: sigma_contrib[K],
+ * ptcl_sumsq[K], ref_sumsq[K] */
+void orc_sigma_contrib(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                       const double *shvec, int irot, const double *argtransf, const double *argtransf_shellone,
+                       double *sigma_contrib, double *ptcl_sumsq, double *ref_sumsq);
 /* ---------------------------------------------------------------------------
  * FP32 FFT path, the reference's loop structure (memoize_fft :864-877 and
  * calc_corrs_over_k :1132-1162) on a project-written mixed-radix FFT that stands

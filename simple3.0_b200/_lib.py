@@ -13,6 +13,7 @@ from . import build as _build
 OK, ERR_ARG, ERR_INDEX, ERR_STATE, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NODEV, ERR_UNSUPPORTED = range(9)
 FRAME_REF, FRAME_PTCL = 0, 1
 PREC_EXACT, PREC_FP32, PREC_BF16X3 = 0, 1, 2
+OBJFUN_CC, OBJFUN_EUCLID = 0, 1
 
 
 class Config(C.Structure):
@@ -84,6 +85,15 @@ SIGNATURES = {
     "pftcc_genfrc": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp],
+    "pftcc_set_objfun": [_h, C.c_int],
+    "pftcc_assign_sigma2_noise": [_h, C.c_int, C.c_int, _fp],
+    "pftcc_gencorrs_euclid": [_h, C.c_int, C.c_int, _fp, _fp],
+    "pftcc_gencorr_euclid_for_rot": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp],
+    "pftcc_gencorr_euclid_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp],
+    "pftcc_gencorr_euclid_grad_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
+    "pftcc_gencorr_euclid_grad_only_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp],
+    "pftcc_gencorr_sigma_contrib": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp, _fp, _fp],
+    "pftcc_sigma_contrib_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp, _fp],
     "pftcc_corr_all": [_h, C.c_int, _fp, _fp],
     "pftcc_corr_all_prec": [_h, C.c_int, _fp, C.c_int, _fp],
     "pftcc_search_best": [_h, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],

@@ -191,6 +191,9 @@ cudaError_t launch_zero_beyond_kstop(pftcc_handle *h)
 //             over all shells for cc_2, exactly as the reference)
 // FRAME_PTCL: A = ref * shmat(n), Qt = ctf~(j) ptcl~(j),
 //             cc = corr / sqrt(sum_n |ref(n)|^2 ctf~(n+s)^2 * sqsum_ptcl)
+// FRAME_EUCLID: A and Qt as FRAME_REF, shell weights W(k) = pxls(k) / (P sigma2(k)),
+//             euclid = sum_{k<=kstop} W(k) (corr_k - (sum_n |A|^2 + sum_n |ptcl|^2) / 2)
+//             (gencorrs_euclid_1/_2 :1536-1592: pxls/P (2 kcorrs - sumsqptcl - sumsqref) / (2 sigma2))
 constexpr int EX_THREADS = 256;
 __host__ __device__ constexpr size_t al16(size_t b) { return (b + 15) & ~size_t(15); }
 constexpr int EX_RPT = 3;      // rotations per thread: N <= 768
@@ -201,13 +204,15 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const uint8_t *__restrict__ iseven,
     const float *__restrict__ sqsums, const double *__restrict__ argtransf, const double *__restrict__ argtransf1,
     const Group *__restrict__ groups, const Work *__restrict__ work, const float *__restrict__ shifts, int mode,
-    int cc1_kstop, float *__restrict__ out, pftcc_best *__restrict__ best)
+    int cc1_kstop, const float *__restrict__ sig2, const float *__restrict__ pxls, float *__restrict__ out,
+    pftcc_best *__restrict__ best)
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P;
     // shared layout (16-byte aligned sections, see exact_smem): sh [P] double2 running
     // shmat, sv [P] double2 shell-one phase vector, Qt [KC][N] float2, A [KC][P] float2,
-    // then for the particle frame C2t [KC][N] float and R2 [KC][P] float
+    // then for the particle frame C2t [KC][N] float and R2 [KC][P] float, for the Euclidean
+    // objective the shell weights W [K] double in their place
     char *base = reinterpret_cast<char *>(smem4);
     double2 *sh = reinterpret_cast<double2 *>(base);
     double2 *sv = sh + P;
@@ -215,6 +220,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     float2 *A = reinterpret_cast<float2 *>(reinterpret_cast<char *>(Qt) + al16(KC * N * sizeof(float2)));
     float *C2t = reinterpret_cast<float *>(reinterpret_cast<char *>(A) + al16(KC * P * sizeof(float2)));
     float *R2 = reinterpret_cast<float *>(reinterpret_cast<char *>(C2t) + al16(KC * N * sizeof(float)));
+    double *W = reinterpret_cast<double *>(C2t);
     __shared__ double red[EX_THREADS / 32];
     __shared__ float bcc[EX_THREADS / 32];
     __shared__ int brot[EX_THREADS / 32];
@@ -225,6 +231,9 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     const float *ctf = ctfmats ? ctfmats + (long long)slot * g.K * P : nullptr;
     const float2 *refs = iseven[slot] ? refs_even : refs_odd;
     const float sqp = sqsums[slot];
+    if (FRAME == FRAME_EUCLID)   // read after the __syncthreads() that opens the first shell chunk
+        for (int ik = threadIdx.x; ik < g.K; ik += blockDim.x)
+            W[ik] = (double)pxls[ik] / ((double)P * (double)sig2[(long long)slot * g.K + ik]);
     float run_best = -INFINITY;
     int run_rot = 0, run_item = -1;
 
@@ -260,7 +269,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                     const int ik = k0 + kk;
                     const float2 rv = r[(long long)ik * P + n];
                     float ar = rv.x, ai = rv.y;
-                    if (FRAME == PFTCC_FRAME_REF && ctf) {
+                    if (FRAME != PFTCC_FRAME_PTCL && ctf) {
                         const float c = ctf[ik * P + n];
                         ar *= c; ai *= c;
                     }
@@ -274,7 +283,11 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                         st = make_double2(nr, ni);
                     }
                     A[kk * P + n] = make_float2(ar, ai);
-                    if (ik < ksq) sqr += (double)ar * ar + (double)ai * ai;
+                    if (FRAME == FRAME_EUCLID) {
+                        if (ik < g.Ks) sqr += W[ik] * ((double)ar * ar + (double)ai * ai);
+                    } else if (ik < ksq) {
+                        sqr += (double)ar * ar + (double)ai * ai;
+                    }
                 }
                 if (has_shift) sh[n] = st;
             }
@@ -290,6 +303,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                     v.x *= c; v.y *= c;
                     C2t[kk * N + j] = c * c;
                 }
+                if (FRAME == FRAME_EUCLID && j < P) sqr += W[ik] * ((double)v.x * v.x + (double)v.y * v.y);
                 Qt[kk * N + j] = v;
             }
             __syncthreads();
@@ -306,14 +320,18 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                     const float2 *Ak = A + kk * P;
                     const float2 *Qk = Qt + kk * N;
                     int j = s;
+                    // the Euclidean objective weights each shell's correlation
+                    double a_k = FRAME == FRAME_EUCLID ? 0.0 : a_tot;
                     for (int n = 0; n < P; ++n) {
                         const float2 av = Ak[n];
                         const float2 qv = Qk[j];
-                        a_tot = fma((double)av.x, (double)qv.x, a_tot);
-                        a_tot = fma((double)av.y, (double)qv.y, a_tot);
+                        a_k = fma((double)av.x, (double)qv.x, a_k);
+                        a_k = fma((double)av.y, (double)qv.y, a_k);
                         if (FRAME == PFTCC_FRAME_PTCL) d_tot = fma((double)R2[kk * P + n], (double)C2t[kk * N + j], d_tot);
                         if (++j == N) j = 0;
                     }
+                    if (FRAME == FRAME_EUCLID) a_tot = fma(W[k0 + kk], a_k, a_tot);
+                    else a_tot = a_k;
                 }
                 acc[u] += a_tot;
                 dacc[u] += d_tot;
@@ -332,8 +350,13 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
         for (int u = 0; u < EX_RPT; ++u) {
             const int s = threadIdx.x + u * EX_THREADS;
             if (s >= N) break;
-            const double den = FRAME == PFTCC_FRAME_REF ? sqrt(sqr_tot * sqp) : sqrt(dacc[u] * sqp);
-            const float cc = (float)(acc[u] / den);
+            float cc;
+            if (FRAME == FRAME_EUCLID) {
+                cc = (float)(acc[u] - 0.5 * sqr_tot);
+            } else {
+                const double den = FRAME == PFTCC_FRAME_REF ? sqrt(sqr_tot * sqp) : sqrt(dacc[u] * sqp);
+                cc = (float)(acc[u] / den);
+            }
             if (mode == MODE_FULL) out[w.out + s] = cc;
             if (cc > my_best) { my_best = cc; my_rot = s; }
         }
@@ -374,6 +397,7 @@ static size_t exact_smem(const Geom &g, int frame, int kc)
     size_t b = al16(2 * g.P * sizeof(double2)) + al16((size_t)kc * g.N * sizeof(float2)) +
                al16((size_t)kc * g.P * sizeof(float2));
     if (frame == PFTCC_FRAME_PTCL) b += al16((size_t)kc * g.N * sizeof(float)) + al16((size_t)kc * g.P * sizeof(float));
+    if (frame == FRAME_EUCLID) b += al16((size_t)g.K * sizeof(double));
     return b;
 }
 
@@ -385,31 +409,33 @@ static int exact_kc(const Geom &g, int frame, size_t *smem)
     return kc;
 }
 
+template <int FRAME>
+static cudaError_t launch_exact_t(pftcc_handle *h, int kc, size_t smem, const Group *groups, int ngroups,
+                                  const Work *work, const float *shifts, int mode, int cc1_kstop, float *out,
+                                  pftcc_best *best)
+{
+    cudaError_t e = smem_limit((const void *)k_exact<FRAME>, smem);
+    if (e != cudaSuccess) return e;
+    const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_EXACT);
+    k_exact<FRAME><<<ngroups, EX_THREADS, smem, h->stream>>>(
+        h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf, h->argtransf1,
+        groups, work, shifts, mode, cc1_kstop, h->d_sig2, h->d_pxls, out, best);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, const Work *work, const float *shifts,
                          int mode, int frame, int cc1_kstop, float *out, pftcc_best *best)
 {
+    if (frame == FRAME_EUCLID && (!h->d_sig2 || !h->d_pxls)) return cudaErrorInvalidValue;
     size_t smem;
     const int kc = exact_kc(h->g, frame, &smem);
-    cudaError_t e;
-    const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
-    if (frame == PFTCC_FRAME_PTCL) {
-        e = smem_limit((const void *)k_exact<PFTCC_FRAME_PTCL>, smem);
-        if (e != cudaSuccess) return e;
-        PFTCC_LAUNCH(h);
-        KTimer kt(h, PFTCC_K_EXACT);
-        k_exact<PFTCC_FRAME_PTCL><<<ngroups, EX_THREADS, smem, h->stream>>>(
-            h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
-            h->argtransf1, groups, work, shifts, mode, cc1_kstop, out, best);
-    } else {
-        e = smem_limit((const void *)k_exact<PFTCC_FRAME_REF>, smem);
-        if (e != cudaSuccess) return e;
-        PFTCC_LAUNCH(h);
-        KTimer kt(h, PFTCC_K_EXACT);
-        k_exact<PFTCC_FRAME_REF><<<ngroups, EX_THREADS, smem, h->stream>>>(
-            h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
-            h->argtransf1, groups, work, shifts, mode, cc1_kstop, out, best);
-    }
-    return cudaGetLastError();
+    if (frame == PFTCC_FRAME_PTCL)
+        return launch_exact_t<PFTCC_FRAME_PTCL>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
+    if (frame == FRAME_EUCLID)
+        return launch_exact_t<FRAME_EUCLID>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
+    return launch_exact_t<PFTCC_FRAME_REF>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
 }
 
 // ---------------------------------------------------------------------------

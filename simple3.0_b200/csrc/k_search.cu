@@ -1071,6 +1071,8 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
 {
     const Geom &g = h->g;
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
+    if (h->objfun == PFTCC_OBJFUN_EUCLID)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the Euclidean objective is served by PFTCC_PREC_EXACT");
     if (Ks > 64) return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search supports at most 64 shells");
     const FFTPlan plan = make_plan(P);
     for (int i = 0; i < plan.nf; ++i)
@@ -1235,7 +1237,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     k_finish<<<(np + 127) / 128, 128, 0, h->stream>>>(ws.cand, d_perm, np, N, ns, nshifts_in > 0, ntop, out_dev,
                                                       h->d_work, h->d_groups);
     CKE(cudaGetLastError(), "finish");
-    CKE(launch_exact(h, h->d_groups, np, h->d_work, ws.shifts, MODE_BEST, h->cfg.ctf_frame, 1, nullptr, out_dev),
+    CKE(launch_exact(h, h->d_groups, np, h->d_work, ws.shifts, MODE_BEST, exact_frame(h), 1, nullptr, out_dev),
         "rescore");
 #undef CKE
     return PFTCC_OK;

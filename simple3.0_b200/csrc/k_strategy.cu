@@ -129,7 +129,7 @@ static int corr_all_device(pftcc_handle *h, int precision, float *dst)
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(h->d_groups, groups.data(), m * sizeof(Group), cudaMemcpyHostToDevice, h->stream);
         if (e == cudaSuccess)
-            e = launch_exact(h, h->d_groups, m, h->d_work, nullptr, MODE_FULL, h->cfg.ctf_frame, 1,
+            e = launch_exact(h, h->d_groups, m, h->d_work, nullptr, MODE_FULL, exact_frame(h), 1,
                              dst + (size_t)c0 * per_ptcl * h->g.N, nullptr);
         if (e != cudaSuccess) return cuda_err(h, e, "snhc correlations");
     }
@@ -161,6 +161,10 @@ extern "C" int pftcc_search_snhc(pftcc_handle *h, const int *order, const float 
     if (cudaSetDevice(h->dev) != cudaSuccess) return set_err(h, PFTCC_ERR_CUDA, "search_snhc: cudaSetDevice");
     if (h->cfg.with_ctf && !h->ctf_ready)
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    if (h->objfun == PFTCC_OBJFUN_EUCLID) {
+        const int est = euclid_ready(h, 1);
+        if (est != PFTCC_OK) return est;
+    }
     // global particle index of each slot (the random draws are keyed by it)
     std::vector<int> gidx(np, 0);
     for (int p = h->pfrom; p <= h->pto; ++p) {

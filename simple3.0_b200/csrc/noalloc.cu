@@ -63,6 +63,7 @@ extern "C" int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *ir
     if (cudaSetDevice(h->dev) != cudaSuccess) return set_err(h, PFTCC_ERR_CUDA, "gencorrs_noalloc: cudaSetDevice");
     if (h->cfg.with_ctf && !h->ctf_ready)
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    if (h->objfun == PFTCC_OBJFUN_EUCLID && euclid_ready(h, 0) != PFTCC_OK) return PFTCC_ERR_STATE;
     // host-side descriptors (validated) in a fixed host buffer guarded by the global lock,
     // then one copy into the fixed device scratch
     std::lock_guard<std::mutex> lk2(g_noalloc_host_mtx);
@@ -90,7 +91,7 @@ extern "C" int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *ir
     const Work *dw = reinterpret_cast<const Work *>(b);
     const Group *dg = reinterpret_cast<const Group *>(b + (size_t)npairs * sizeof(Work));
     const float *ds = reinterpret_cast<const float *>(b + (size_t)npairs * (sizeof(Work) + sizeof(Group)));
-    e = launch_exact(h, dg, npairs, dw, ds, MODE_FULL, h->cfg.ctf_frame, 1, cc_dev, nullptr);
+    e = launch_exact(h, dg, npairs, dw, ds, MODE_FULL, exact_frame(h), 1, cc_dev, nullptr);
     if (e != cudaSuccess) return cuda_err(h, e, "gencorrs_noalloc kernel");
     // the host descriptors must outlive the copy
     e = cudaStreamSynchronize(h->stream);

@@ -271,7 +271,7 @@ static void free_all(pftcc_handle *h)
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
                     h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
-                    h->ws.cand_ref, h->vol_cube};
+                    h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
     for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -422,6 +422,93 @@ int pftcc_kill(pftcc_handle *h)
     return PFTCC_OK;
 }
 
+}  // extern "C"
+
+// ---- the Euclidean objective's per-particle noise ---------------------------------------
+namespace pftcc {
+// sigma2_noise columns in slot order on the device -- NaN for a held particle outside the
+// assigned fromp:top range, counted in sig_uncovered -- and the pixels per shell
+// (setup_pxls_p_shell :879-893: the pixels h, k = 1..kto of the positive quadrant whose
+// rounded radius nint(sqrt(h^2 + k^2)) is a shell kfrom..kto)
+static int sigma2_build(pftcc_handle *h)
+{
+    const int K = h->g.K;
+    std::vector<float> px(K, 0.f);
+    const int kfrom = h->cfg.kfromto[0], kto = h->cfg.kfromto[1];
+    for (int a = 1; a <= kto; ++a)
+        for (int b = 1; b <= kto; ++b) {
+            const int sh = (int)std::lround(std::sqrt((double)(a * a + b * b)));
+            if (sh >= kfrom && sh <= kto) px[sh - kfrom] += 1.f;
+        }
+    const int slots = std::max(1, h->nptcls);
+    std::vector<float> col((size_t)slots * K, NAN);
+    int uncovered = 0;
+    for (size_t gi = 0; gi < h->pinds.size(); ++gi) {
+        const int slot = h->pinds[gi] - 1;
+        if (slot < 0) continue;
+        const int iptcl = h->pfrom + (int)gi;
+        if (iptcl < h->sig_from || iptcl > h->sig_to) {
+            ++uncovered;
+            continue;
+        }
+        std::memcpy(&col[(size_t)slot * K], &h->h_sig2[(size_t)(iptcl - h->sig_from) * K], K * sizeof(float));
+    }
+    dev_free(h, h->d_sig2);
+    h->d_sig2 = nullptr;
+    ST(dev_alloc(h, (void **)&h->d_sig2, col.size() * sizeof(float), "sigma2_noise"));
+    if (!h->d_pxls) ST(dev_alloc(h, (void **)&h->d_pxls, K * sizeof(float), "pixels per shell"));
+    CK(cudaMemcpyAsync(h->d_sig2, col.data(), col.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream), "sigma2");
+    CK(cudaMemcpyAsync(h->d_pxls, px.data(), K * sizeof(float), cudaMemcpyHostToDevice, h->stream), "pxls_p_shell");
+    CK(cudaStreamSynchronize(h->stream), "sigma2");
+    h->sig_uncovered = uncovered;
+    h->sig_dirty = 0;
+    return PFTCC_OK;
+}
+
+int euclid_ready(pftcc_handle *h, int may_alloc)
+{
+    if (h->h_sig2.empty())
+        return set_err(h, PFTCC_ERR_STATE, "the Euclidean objective needs sigma2_noise: call pftcc_assign_sigma2_noise");
+    if (h->sig_dirty || !h->d_sig2) {
+        if (!may_alloc)
+            return set_err(h, PFTCC_ERR_STATE, "sigma2_noise is not on the device for the current particles: assign it "
+                                               "again (pftcc_assign_sigma2_noise) before this call");
+        ST(sigma2_build(h));
+    }
+    if (h->sig_uncovered)
+        return set_err(h, PFTCC_ERR_STATE, std::to_string(h->sig_uncovered) +
+                                               " held particles lie outside the assigned sigma2_noise range");
+    return PFTCC_OK;
+}
+}  // namespace pftcc
+
+extern "C" {
+
+int pftcc_set_objfun(pftcc_handle *h, int objfun)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    if (objfun != PFTCC_OBJFUN_CC && objfun != PFTCC_OBJFUN_EUCLID)
+        return set_err(h, PFTCC_ERR_ARG, "objfun must be PFTCC_OBJFUN_CC or PFTCC_OBJFUN_EUCLID");
+    if (objfun == PFTCC_OBJFUN_EUCLID && h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the Euclidean objective is defined in the reference frame "
+                                                 "(ctf_frame = PFTCC_FRAME_REF)");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    h->objfun = objfun;
+    return PFTCC_OK;
+}
+
+int pftcc_assign_sigma2_noise(pftcc_handle *h, int fromp, int top, const float *sigma2)
+{
+    if (!h || !sigma2 || top < fromp) return set_err(h, PFTCC_ERR_ARG, "assign_sigma2_noise: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    h->h_sig2.assign(sigma2, sigma2 + (size_t)(top - fromp + 1) * h->g.K);
+    h->sig_from = fromp;
+    h->sig_to = top;
+    h->sig_dirty = 1;
+    return sigma2_build(h);
+}
+
 int pftcc_reallocate_ptcls(pftcc_handle *h, int nptcls, const int *pinds)
 {
     if (!h || nptcls < 1 || !pinds) return set_err(h, PFTCC_ERR_ARG, "reallocate_ptcls: bad arguments");
@@ -448,6 +535,8 @@ int pftcc_reallocate_ptcls(pftcc_handle *h, int nptcls, const int *pinds)
     }
     h->ctf_ready = 0;
     h->ws.ptcl_spectra_valid = 0;
+    h->sig_dirty = 1;
+    if (!h->h_sig2.empty()) ST(sigma2_build(h));
     return push_iseven(h);
 }
 
@@ -767,32 +856,177 @@ static int ensure_small(pftcc_handle *h, size_t nwork, size_t ngroups, size_t no
     return PFTCC_OK;
 }
 
-static int check_ctf_state(pftcc_handle *h)
+static int check_ctf_only(pftcc_handle *h)
 {
     if (h->cfg.with_ctf && !h->ctf_ready)
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
     return PFTCC_OK;
 }
 
-int pftcc_gencorrs(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *cc)
+// the state an evaluation of the current objective needs
+static int check_ctf_state(pftcc_handle *h)
 {
-    if (!h || !cc) return PFTCC_ERR_ARG;
+    ST(check_ctf_only(h));
+    if (h->objfun == PFTCC_OBJFUN_EUCLID) return euclid_ready(h, 1);
+    return PFTCC_OK;
+}
+
+static int gencorrs_frame(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *cc, int frame)
+{
     REF_OR_FAIL(iref);
     SLOT_OR_FAIL(slot, iptcl);
-    std::lock_guard<std::mutex> lk(h->mtx);
-    cudaSetDevice(h->dev);
-    ST(check_ctf_state(h));
     ST(ensure_small(h, 1, 1, h->g.N, 1));
     Work w{iref - 1, shvec ? 0 : -1, 0};
     Group gr{slot, 0, 1, 0};
     CK(cudaMemcpyAsync(h->d_work, &w, sizeof(w), cudaMemcpyHostToDevice, h->stream), "gencorrs");
     CK(cudaMemcpyAsync(h->d_groups, &gr, sizeof(gr), cudaMemcpyHostToDevice, h->stream), "gencorrs");
     if (shvec) CK(cudaMemcpyAsync(h->d_shifts, shvec, 2 * sizeof(float), cudaMemcpyHostToDevice, h->stream), "gencorrs");
-    CK(launch_exact(h, h->d_groups, 1, h->d_work, h->d_shifts, MODE_FULL, h->cfg.ctf_frame, 1, h->d_out, nullptr),
+    CK(launch_exact(h, h->d_groups, 1, h->d_work, h->d_shifts, MODE_FULL, frame, 1, h->d_out, nullptr),
        "gencorrs kernel");
     CK(cudaMemcpyAsync(cc, h->d_out, h->g.N * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "gencorrs");
     CK(cudaStreamSynchronize(h->stream), "gencorrs");
     return PFTCC_OK;
+}
+
+int pftcc_gencorrs(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *cc)
+{
+    if (!h || !cc) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    return gencorrs_frame(h, iref, iptcl, shvec, cc, exact_frame(h));
+}
+
+static int euclid_explicit_state(pftcc_handle *h)
+{
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the Euclidean objective is defined in the reference frame");
+    ST(check_ctf_only(h));
+    return euclid_ready(h, 1);
+}
+
+int pftcc_gencorrs_euclid(pftcc_handle *h, int iref, int iptcl, const float *shvec, float *euclids)
+{
+    if (!h || !euclids) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(euclid_explicit_state(h));
+    return gencorrs_frame(h, iref, iptcl, shvec, euclids, FRAME_EUCLID);
+}
+
+// n single-rotation Euclidean requests: out3 [n][3] (with_f), shells [n][3][K] (want_shells)
+static int euclid_rot_host(pftcc_handle *h, int n, const EuclidReq *rq, int with_f, int want_shells, double *out3,
+                           double *shells)
+{
+    const int K = h->g.K;
+    ST(ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)n * sizeof(EuclidReq), 4096),
+              "euclid requests"));
+    const size_t per = (with_f ? 3 : 0) + (want_shells ? 3 * (size_t)K : 0);
+    ST(ensure(h, (void **)&h->d_dout, &h->dout_cap, (size_t)n * per * sizeof(double), "euclid results"));
+    double *o3 = with_f ? h->d_dout : nullptr;
+    double *sh = want_shells ? h->d_dout + (with_f ? 3 * (size_t)n : 0) : nullptr;
+    CK(cudaMemcpyAsync(h->d_work, rq, (size_t)n * sizeof(EuclidReq), cudaMemcpyHostToDevice, h->stream), "euclid");
+    CK(launch_euclid_rot(h, reinterpret_cast<const EuclidReq *>(h->d_work), n, with_f, want_shells, o3, sh),
+       "euclid kernel");
+    if (with_f) CK(cudaMemcpyAsync(out3, o3, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "euclid");
+    if (want_shells)
+        CK(cudaMemcpyAsync(shells, sh, 3 * (size_t)n * K * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "euclid");
+    CK(cudaStreamSynchronize(h->stream), "euclid");
+    return PFTCC_OK;
+}
+
+// one rotation of the Euclidean objective: f3 = f, df/dsx, df/dsy (caller holds the lock and
+// has checked the state)
+static int euclid_single(pftcc_handle *h, int iref, int iptcl, double sx, double sy, int irot, double *f3)
+{
+    REF_OR_FAIL(iref);
+    SLOT_OR_FAIL(slot, iptcl);
+    if (irot < 1 || irot > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "irot out of range");
+    const EuclidReq rq{iref - 1, slot, irot, 0, sx, sy};
+    return euclid_rot_host(h, 1, &rq, 1, 0, f3, nullptr);
+}
+
+int pftcc_gencorr_euclid_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot, double *f)
+{
+    if (!h || !f || !shvec) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(euclid_explicit_state(h));
+    double o[3];
+    ST(euclid_single(h, iref, iptcl, shvec[0], shvec[1], irot, o));
+    *f = o[0];
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_euclid_for_rot(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot, float *f)
+{
+    if (!h || !f || !shvec) return PFTCC_ERR_ARG;
+    const double sh[2] = {(double)shvec[0], (double)shvec[1]};
+    double v;
+    ST(pftcc_gencorr_euclid_for_rot_8(h, iref, iptcl, sh, irot, &v));
+    *f = (float)v;
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_euclid_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                        double *f, double *grad)
+{
+    if (!h || !f || !grad || !shvec) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(euclid_explicit_state(h));
+    double o[3];
+    ST(euclid_single(h, iref, iptcl, shvec[0], shvec[1], irot, o));
+    *f = o[0];
+    grad[0] = o[1];
+    grad[1] = o[2];
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_euclid_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                             double *grad)
+{
+    double f;
+    return pftcc_gencorr_euclid_grad_for_rot_8(h, iref, iptcl, shvec, irot, &f, grad);
+}
+
+int pftcc_sigma_contrib_batch(pftcc_handle *h, int n, const int *iref, const int *iptcl, const int *irot,
+                              const float *shifts, float *sigma_contrib, float *ptcl_sumsq, float *ref_sumsq)
+{
+    if (!h || n < 0 || (n > 0 && (!iref || !iptcl || !irot || !shifts || !sigma_contrib)))
+        return set_err(h, PFTCC_ERR_ARG, "sigma_contrib: bad arguments");
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "sigma_contrib is defined in the reference frame");
+    ST(check_ctf_only(h));
+    std::vector<EuclidReq> rq(n);
+    for (int i = 0; i < n; ++i) {
+        if (iref[i] < 1 || iref[i] > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "sigma_contrib: iref out of range");
+        if (irot[i] < 1 || irot[i] > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "sigma_contrib: irot out of range");
+        const int sl = slot_of(h, iptcl[i]);
+        if (sl < 0) return set_err(h, PFTCC_ERR_INDEX, "sigma_contrib: particle not held");
+        rq[i] = EuclidReq{iref[i] - 1, sl, irot[i], 0, (double)shifts[2 * i], (double)shifts[2 * i + 1]};
+    }
+    const int K = h->g.K;
+    std::vector<double> sh((size_t)n * 3 * K);
+    ST(euclid_rot_host(h, n, rq.data(), 0, 1, nullptr, sh.data()));
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < K; ++k) {
+            const double *b = &sh[(size_t)i * 3 * K];
+            sigma_contrib[(size_t)i * K + k] = (float)b[k];
+            if (ptcl_sumsq) ptcl_sumsq[(size_t)i * K + k] = (float)b[K + k];
+            if (ref_sumsq) ref_sumsq[(size_t)i * K + k] = (float)b[2 * K + k];
+        }
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_sigma_contrib(pftcc_handle *h, int iref, int iptcl, const float *shvec, int irot,
+                                float *sigma_contrib, float *ptcl_sumsq, float *ref_sumsq)
+{
+    if (!h || !shvec || !sigma_contrib) return set_err(h, PFTCC_ERR_ARG, "sigma_contrib: bad arguments");
+    return pftcc_sigma_contrib_batch(h, 1, &iref, &iptcl, &irot, shvec, sigma_contrib, ptcl_sumsq, ref_sumsq);
 }
 
 static int for_rot_common(pftcc_handle *h, int iref, int iptcl, double sx, double sy, int irot, double *out5)
@@ -803,6 +1037,10 @@ static int for_rot_common(pftcc_handle *h, int iref, int iptcl, double sx, doubl
     if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "single-rotation correlations are served in the reference frame");
     ST(check_ctf_state(h));
+    if (h->objfun == PFTCC_OBJFUN_EUCLID) {   // gencorr_for_rot_8 / gencorr_grad_for_rot_8 dispatch (:1632-1643, :1849-1861)
+        out5[3] = out5[4] = 0.0;
+        return euclid_single(h, iref, iptcl, sx, sy, irot, out5);
+    }
     ST(ensure_small(h, 1, 1, h->g.N, 1));
     CK(launch_for_rot(h, iref - 1, slot, sx, sy, irot, h->cfg.match_filt, 1, 0.0, h->d_dout), "for_rot kernel");
     CK(cudaMemcpyAsync(out5, h->d_dout, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "for_rot");
@@ -929,7 +1167,7 @@ int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
         }
         CK(cudaMemcpyAsync(h->d_work, work.data(), wi * sizeof(Work), cudaMemcpyHostToDevice, h->stream), "work");
         CK(cudaMemcpyAsync(h->d_groups, groups.data(), m * sizeof(Group), cudaMemcpyHostToDevice, h->stream), "groups");
-        CK(launch_exact(h, h->d_groups, m, h->d_work, h->d_shifts, MODE_FULL, h->cfg.ctf_frame, 1, h->d_out, nullptr),
+        CK(launch_exact(h, h->d_groups, m, h->d_work, h->d_shifts, MODE_FULL, exact_frame(h), 1, h->d_out, nullptr),
            "corr_all kernel");
         CK(cudaMemcpyAsync(cc + (size_t)c0 * out_per_ptcl, h->d_out, (size_t)m * out_per_ptcl * sizeof(float),
                            cudaMemcpyDeviceToHost, h->stream), "corr_all download");
@@ -973,7 +1211,7 @@ static int search_exact(pftcc_handle *h, int nshifts, const float *shifts, pftcc
     CK(cudaMemcpyAsync(h->d_work, work.data(), wi * sizeof(Work), cudaMemcpyHostToDevice, h->stream), "work");
     CK(cudaMemcpyAsync(h->d_groups, groups.data(), groups.size() * sizeof(Group), cudaMemcpyHostToDevice, h->stream),
        "groups");
-    CK(launch_exact(h, h->d_groups, h->nptcls, h->d_work, h->d_shifts, MODE_BEST, h->cfg.ctf_frame, 1, nullptr, out_dev),
+    CK(launch_exact(h, h->d_groups, h->nptcls, h->d_work, h->d_shifts, MODE_BEST, exact_frame(h), 1, nullptr, out_dev),
        "search exact");
     return PFTCC_OK;
 }

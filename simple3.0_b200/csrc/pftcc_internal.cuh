@@ -120,6 +120,15 @@ struct pftcc_handle {
     // the volume's expanded FT for polar projection (expand_cmat), side box + 5
     float2 *vol_cube = nullptr;
     int vol_box = 0;
+    // Euclidean objective: cc_objfun, sigma2_noise(kfrom:kto, sig_from:sig_to) as assigned
+    // (host copy), its columns in slot order on the device, pixels per shell
+    int objfun = PFTCC_OBJFUN_CC;
+    std::vector<float> h_sig2;
+    int sig_from = 0, sig_to = -1;
+    int sig_dirty = 1;
+    int sig_uncovered = 0;               // held particles outside sig_from:sig_to
+    float *d_sig2 = nullptr;             // [slots][K]
+    float *d_pxls = nullptr;             // [K]
     // small per-call device buffers
     pftcc::Work *d_work = nullptr;
     pftcc::Group *d_groups = nullptr;
@@ -188,6 +197,23 @@ cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, doubl
 cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, const int *slots_dev, int nreq,
                               double *out4);
 cudaError_t launch_zero_beyond_kstop(pftcc_handle *h);
+
+// k_exact frame of the Euclidean objective: reference frame with shell weights
+// pxls(k) / (P sigma2(k)) and the distance's constant terms (gencorrs_euclid_1/_2)
+constexpr int FRAME_EUCLID = 2;
+inline int exact_frame(const pftcc_handle *h)
+{
+    return h->objfun == PFTCC_OBJFUN_EUCLID ? FRAME_EUCLID : h->cfg.ctf_frame;
+}
+// sigma2_noise on the device and covering every held particle (rebuilt first when stale
+// and may_alloc); PFTCC_OK or the error code, with the message set
+int euclid_ready(pftcc_handle *h, int may_alloc);
+// one single-rotation Euclidean request (k_euclid.cu); iref 0-based, slot = particle slot
+struct EuclidReq { int iref, slot, irot, pad; double sx, sy; };
+// out3[nreq][3] = f, df/dsx, df/dsy (with_f); shells[nreq][3][K] = sigma_contrib,
+// ptcl_sumsq, ref_sumsq over every shell (want_shells)
+cudaError_t launch_euclid_rot(pftcc_handle *h, const EuclidReq *reqs_dev, int nreq, int with_f, int want_shells,
+                              double *out3, double *shells);
 
 // adjoint requests served in one launch (pftcc_capi.cu; caller holds the handle lock)
 int grad_batch_host(pftcc_handle *h, int nreq, const pftcc_grad_req *req, double *f, double *grad3);

@@ -274,6 +274,82 @@ class polarft_corrcalc:
                                                   None if frcs is None else _f32p(frcs)))
         return (scores, frcs) if want_frc else scores
 
+    # ---- the Euclidean objective (params_glob%cc_objfun = OBJFUN_EUCLID) ---------------------
+    def set_objfun(self, objfun: int):
+        """cc_objfun: _lib.OBJFUN_CC or _lib.OBJFUN_EUCLID; gencorrs, gencorr_for_rot(_8),
+        gencorr_grad(_only)_for_rot_8 and the exact batched searches follow it"""
+        self._check(self._L.pftcc_set_objfun(self._h, int(objfun)))
+
+    def assign_sigma2_noise(self, sigma2, fromp: int | None = None):
+        """sigma2_noise(kfrom:kto, fromp:top) as an array (top - fromp + 1, K); fromp defaults
+        to pfromto(1).  The values are copied."""
+        a = np.ascontiguousarray(sigma2, np.float32)
+        K = self.cfg.kfromto[1] - self.cfg.kfromto[0] + 1
+        if a.ndim != 2 or a.shape[1] != K:
+            raise PftccError(_lib.ERR_ARG, f"sigma2 must be (nptcls, {K}), got {a.shape}")
+        lo = self.cfg.pfromto[0] if fromp is None else int(fromp)
+        self._check(self._L.pftcc_assign_sigma2_noise(self._h, lo, lo + a.shape[0] - 1, _f32p(a)))
+
+    def gencorrs_euclid(self, iref: int, iptcl: int, shvec=None) -> np.ndarray:
+        out = np.zeros(self.cfg.nrots, np.float32)
+        sh = None if shvec is None else np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_gencorrs_euclid(self._h, int(iref), int(iptcl), None if sh is None else _f32p(sh),
+                                                  _f32p(out)))
+        return out
+
+    def gencorr_euclid_for_rot(self, iref: int, iptcl: int, shvec, irot: int) -> float:
+        out = C.c_float()
+        sh = np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_gencorr_euclid_for_rot(self._h, int(iref), int(iptcl), _f32p(sh), int(irot),
+                                                         C.byref(out)))
+        return out.value
+
+    def gencorr_euclid_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int) -> float:
+        out = C.c_double()
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_euclid_for_rot_8(self._h, int(iref), int(iptcl),
+                                                           sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot),
+                                                           C.byref(out)))
+        return out.value
+
+    def gencorr_euclid_grad_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        f = C.c_double()
+        g = np.zeros(2, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_euclid_grad_for_rot_8(self._h, int(iref), int(iptcl),
+                                                                sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot),
+                                                                C.byref(f), g.ctypes.data_as(C.POINTER(C.c_double))))
+        return f.value, g
+
+    def gencorr_euclid_grad_only_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        g = np.zeros(2, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_euclid_grad_only_for_rot_8(self._h, int(iref), int(iptcl),
+                                                                     sh.ctypes.data_as(C.POINTER(C.c_double)),
+                                                                     int(irot), g.ctypes.data_as(C.POINTER(C.c_double))))
+        return g
+
+    def gencorr_sigma_contrib(self, iref: int, iptcl: int, shvec, irot: int):
+        """(sigma_contrib, ptcl_sumsq, ref_sumsq), each over the shells kfrom..kto"""
+        K = self.cfg.kfromto[1] - self.cfg.kfromto[0] + 1
+        sc, ps, rs = (np.zeros(K, np.float32) for _ in range(3))
+        sh = np.ascontiguousarray(shvec, np.float32)
+        self._check(self._L.pftcc_gencorr_sigma_contrib(self._h, int(iref), int(iptcl), _f32p(sh), int(irot),
+                                                        _f32p(sc), _f32p(ps), _f32p(rs)))
+        return sc, ps, rs
+
+    def sigma_contrib_batch(self, iref, iptcl, irot, shifts):
+        """sigma_contrib for many requests: (n, K) arrays (sigma_contrib, ptcl_sumsq, ref_sumsq)"""
+        ir, ip, ro = (np.ascontiguousarray(np.atleast_1d(v), np.int32) for v in (iref, iptcl, irot))
+        n = ir.size
+        K = self.cfg.kfromto[1] - self.cfg.kfromto[0] + 1
+        sh = np.ascontiguousarray(shifts, np.float32).reshape(n, 2)
+        sc, ps, rs = (np.zeros((n, K), np.float32) for _ in range(3))
+        ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self._L.pftcc_sigma_contrib_batch(self._h, n, ptr(ir), ptr(ip), ptr(ro), _f32p(sh), _f32p(sc),
+                                                      _f32p(ps), _f32p(rs)))
+        return sc, ps, rs
+
     def gencorr_for_rot(self, iref: int, iptcl: int, shvec, irot: int) -> float:
         out = C.c_float()
         sh = np.ascontiguousarray(shvec, np.float32)
