@@ -603,12 +603,28 @@ def run_project_report(args):
         got = pc.get_ref_pft(r + 1, True)
         worst = max(worst, float(np.max(np.abs(got - want)) / np.max(np.abs(want))))
     t_cpu = (time.perf_counter() - t0) / 3
+    # the orientation-gradient inputs: sections and their three angle derivatives
+    e64 = euls.astype(np.float64)
+    pc.fdf_project_polar(1, e64)
+    reps = 10
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        pc.fdf_project_polar(1, e64)
+    t_fdf = (time.perf_counter() - t0) / reps
+    want, dwant = O.fdf_project_polar(g, t, ex, box, e64[0])
+    fdf_err = max(float(np.max(np.abs(pc.get_ref_pft(1, True) - want)) / np.max(np.abs(want))),
+                  float(np.max(np.abs(pc.get_dref_pft(1, True) - dwant)) / np.max(np.abs(dwant))))
+    t0 = time.perf_counter()
+    O.fdf_project_polar(g, t, ex, box, e64[1])
+    t_fdf_cpu = time.perf_counter() - t0
     pc.kill()
     samples = n * (w.kto - w.kfrom + 1) * w.pftsz
     print(json.dumps({"report": "project", "box": box, "refs": n, "samples_per_call": samples,
                       "gpu_seconds_per_call": t_proj, "refs_per_s": n / t_proj, "samples_per_s": samples / t_proj,
                       "expand_cmat_seconds": t_expand, "parity_max_rel_err_vs_oracle": worst,
-                      "oracle_seconds_per_ref_1_thread": t_cpu}), flush=True)
+                      "oracle_seconds_per_ref_1_thread": t_cpu, "fdf_gpu_seconds_per_call": t_fdf,
+                      "fdf_refs_per_s": n / t_fdf, "fdf_parity_max_rel_err_vs_oracle": fdf_err,
+                      "fdf_oracle_seconds_per_ref_1_thread": t_fdf_cpu}), flush=True)
 
 
 def run_euclid_report(args):

@@ -133,6 +133,14 @@ int pftcc_set_volume_ft(pftcc_handle *h, const float *cmat_half, int box, float 
  * or NULL for all */
 int pftcc_fproject_polar(pftcc_handle *h, int first_iref, int n, const float *euls, const int *mask, int iseven,
                          int griddev);
+/* projector%fdf_project_polar (simple_projector.f90:245-267, fdf_interp_fcomp :338-400) for n
+ * orientations: the normalised sections into references first_iref.. of set iseven
+ * (set_ref_fcomp :447-457) and their derivatives with respect to the Euler angles e1, e2, e3
+ * (per radian; euler2dm, simple_ori_light.f90:87-147) into the derivative references
+ * (set_dref_fcomp :459-469); euls[3 n] in degrees, double as the reference's real(dp) */
+int pftcc_fdf_project_polar(pftcc_handle *h, int first_iref, int n, const double *euls, int iseven);
+/* the derivative references of iref: dpft [3][K][P] complex (d/de1, d/de2, d/de3) */
+int pftcc_get_dref_pft(pftcc_handle *h, int iref, int iseven, float *dpft);
 
 /* ---- memoisers ------------------------------------------------------------------ */
 /* memoize_ffts :848-861: prepares the particle-side angular spectra of the
@@ -150,6 +158,18 @@ int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const dou
                                  double *f, double *grad);
 int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
                                       double *grad);
+
+/* ---- the orientation gradient (reference frame only) -------------------------------- */
+/* gencorr_cont_shift_grad_cc_for_rot_8 (:1788-1847): f and grad[5] = d f / d(e1, e2, e3, sx, sy)
+ * at rotation irot from the references and derivative references of fdf_project_polar; the
+ * orientation part correlates the derivative references with particle iptcl */
+int pftcc_gencorr_cont_shift_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                               double *f, double *grad);
+/* gencorr_cont_grad_cc_for_rot_8 (:1735-1786): cc and dcc[3] = d cc / d(e1, e2, e3) */
+int pftcc_gencorr_cont_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                         double *cc, double *dcc);
+/* n requests in one launch (req[i].ddf unused): f[n], grad5[n][5] */
+int pftcc_cont_shift_grad_batch(pftcc_handle *h, int n, const pftcc_grad_req *req, double *f, double *grad5);
 
 /* ---- the Euclidean objective (reference frame only) -------------------------------- */
 /* params_glob%cc_objfun: PFTCC_OBJFUN_EUCLID makes pftcc_gencorrs, pftcc_gencorr_for_rot(_8),

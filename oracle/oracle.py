@@ -85,6 +85,11 @@ def lib():
         L.orc_gencorrs_euclid.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
         L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
         L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_euler2dm.argtypes = [dp, dp]
+        L.orc_kb_dapod.argtypes = [C.c_double]
+        L.orc_kb_dapod.restype = C.c_double
+        L.orc_fdf_project_polar.argtypes = [G, fp, C.c_int, fp, dp, dp, dp]
+        L.orc_gencorr_cont_shift_grad.argtypes = [G, fp, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp]
         L.orc_kb_apod.argtypes = [C.c_double]
         L.orc_kb_apod.restype = C.c_double
         L.orc_fftpath_new.argtypes = [G]
@@ -299,6 +304,39 @@ def fproject_polar(g: Geom, t: Tables, cmat_exp, box: int, eul, mask=None, gridd
                              _P(e, C.c_double), _P(m, C.c_int), int(bool(griddev)),
                              out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
     return out
+
+
+def euler2dm(eul) -> np.ndarray:
+    """(3, 3, 3): dR/de_j (per radian) of euler2m for j = 1..3"""
+    out = np.zeros(27, np.float64)
+    lib().orc_euler2dm(_P(np.asarray(eul, np.float64), C.c_double), _P(out, C.c_double))
+    return out.reshape(3, 3, 3)
+
+
+def kb_dapod(x: float) -> float:
+    return lib().orc_kb_dapod(float(x))
+
+
+def fdf_project_polar(g: Geom, t: Tables, cmat_exp, box: int, eul):
+    """(pft [K, P], dpft [3, K, P]) of fdf_project_polar"""
+    pft = _c128_out((g.K, g.pftsz))
+    dpft = _c128_out((3, g.K, g.pftsz))
+    lib().orc_fdf_project_polar(C.byref(g), _P(t.polar, C.c_float), int(box), _P(_c64(cmat_exp), C.c_float),
+                                _P(np.asarray(eul, np.float64), C.c_double),
+                                pft.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                dpft.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return pft, dpft
+
+
+def gencorr_cont_shift_grad(g: Geom, t: Tables, ref, dref, ptcl, irot: int, ctf=None, shvec=(0.0, 0.0)):
+    """(f, grad[5]) of gencorr_cont_shift_grad_cc_for_rot_8; dref (3, K, P)"""
+    f = np.zeros(1, np.float64)
+    gr = np.zeros(5, np.float64)
+    lib().orc_gencorr_cont_shift_grad(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(dref), C.c_float),
+                                      _P(_c64(ptcl), C.c_float), _P(_ctf_arg(ctf), C.c_double),
+                                      _P(_shv(shvec), C.c_double), int(irot), _P(t.argtransf, C.c_double),
+                                      _P(t.argtransf1, C.c_double), _P(f, C.c_double), _P(gr, C.c_double))
+    return float(f[0]), gr
 
 
 def kb_apod(x: float) -> float:

@@ -948,3 +948,160 @@ void orc_sigma_contrib(const orc_geom *g, const float *ref, const float *ptcl, c
     }
     free(pr);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Orientation derivatives.  drotmat (simple_ori_light.f90:107-146): d rotmat / d angle with
+ * the angle in radians. */
+static void drotmat3(double ang_deg, int choice, double r[9])
+{
+    const double a = ang_deg * 3.14159265358979323846 / 180.0, c = cos(a), s = sin(a);
+    for (int i = 0; i < 9; ++i) r[i] = 0.0;
+    if (choice == 1) { r[4] = -s; r[5] = -c; r[7] = c; r[8] = -s; }
+    else if (choice == 2) { r[0] = -s; r[2] = -c; r[6] = c; r[8] = -s; }
+    else { r[0] = -s; r[1] = c; r[3] = -c; r[4] = -s; }
+}
+
+/* euler2dm: with R = r3 r2 r1, dR/de1 = r3 r2 dr1, dR/de2 = r3 dr2 r1, dR/de3 = dr3 r2 r1 */
+void orc_euler2dm(const double eul[3], double dR[27])
+{
+    double r1[9], r2[9], r3[9], d1[9], d2[9], d3[9], t[9];
+    rotmat3(eul[0], 3, r1);
+    rotmat3(eul[1], 2, r2);
+    rotmat3(eul[2], 3, r3);
+    drotmat3(eul[0], 3, d1);
+    drotmat3(eul[1], 2, d2);
+    drotmat3(eul[2], 3, d3);
+    matmul3(r3, r2, t);
+    matmul3(t, d1, dR);
+    matmul3(r3, d2, t);
+    matmul3(t, r1, dR + 9);
+    matmul3(d3, r2, t);
+    matmul3(t, r1, dR + 18);
+}
+
+/* I1 by the Abramowitz & Stegun 9.8.3 / 9.8.4 polynomial approximations (bessi1,
+ * simple_kbinterpol.f90:282-308); x >= 0 */
+static double bessi1(double x)
+{
+    if (x < 3.75) {
+        double y = x / 3.75;
+        y *= y;
+        return x * (0.5 + y * (0.87890594 + y * (0.51498869 + y * (0.15084934 + y * (0.2658733e-1 +
+                    y * (0.301532e-2 + y * 0.32411e-3))))));
+    }
+    const double y = 3.75 / x;
+    return (0.39894228 + y * (-0.3988024e-1 + y * (-0.362018e-2 + y * (0.163801e-2 + y * (-0.1031555e-1 +
+            y * (0.2282967e-1 + y * (-0.2895312e-1 + y * (0.1787654e-1 + y * (-0.420059e-2))))))))) *
+           exp(x) / sqrt(x);
+}
+
+/* d apod / dx = -4 beta x I1(beta s) / (s W^3), s = sqrt(1 - (2x/W)^2); 0 where s^2 <= 0 */
+double orc_kb_dapod(double x)
+{
+    const double W = 3.0, beta = 7.4;
+    double arg = (2.0 / W) * x;
+    arg = 1.0 - arg * arg;
+    if (arg <= 0.0) return 0.0;
+    const double s = sqrt(arg);
+    return -4.0 * beta * x * bessi1(beta * s) / s / (W * W * W);
+}
+
+/* fdf_interp_fcomp for every sample of the reference: the window and weights of
+ * interp_fcomp_norm, N = sum w c, D = sum w, and for each angle e_j the weight derivative
+ * wd_j = sum over the axes d of (-dapod(win_d - loc_d) * dloc_d/de_j) times the other two
+ * axes' apod, dloc/de_j = vec dR_j; fcomp = N / D, dfcomp_j = (sum wd_j c * D - N sum wd_j) / D^2.
+ * Every shell kfrom..kto, no mask (fdf_project_polar :257-266). */
+void orc_fdf_project_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
+                           const double eul[3], double *pft, double *dpft)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g);
+    const int E = box / 2 + 2, S = 2 * E + 1;
+    double R[9], dR[27];
+    orc_euler2m(eul, R);
+    orc_euler2dm(eul, dR);
+    for (int ik = 0; ik < K; ++ik)
+        for (int i = 0; i < P; ++i) {
+            const double vx = polar[ik * 2 * N + i], vy = polar[ik * 2 * N + N + i];
+            double loc[3], dl[3][3];
+            for (int d = 0; d < 3; ++d) {
+                loc[d] = vx * R[d] + vy * R[3 + d];
+                for (int j = 0; j < 3; ++j) dl[j][d] = vx * dR[9 * j + d] + vy * dR[9 * j + 3 + d];
+            }
+            int w0[3];
+            double wa[3][3], da[3][3];
+            for (int d = 0; d < 3; ++d) {
+                w0[d] = f_nint(loc[d]) - 1;
+                for (int l = 0; l < 3; ++l) {
+                    wa[d][l] = orc_kb_apod((double)(w0[d] + l) - loc[d]);
+                    da[d][l] = orc_kb_dapod((double)(w0[d] + l) - loc[d]);
+                }
+            }
+            double nr = 0.0, ni = 0.0, D = 0.0, njr[3] = {0, 0, 0}, nji[3] = {0, 0, 0}, dj[3] = {0, 0, 0};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c) {
+                        const size_t e = ((size_t)(w0[2] + c + E) * S + (w0[1] + b + E)) * S + (w0[0] + a + E);
+                        const double cr = cmat_exp[2 * e], ci = cmat_exp[2 * e + 1];
+                        const double w = wa[0][a] * wa[1][b] * wa[2][c];
+                        nr += w * cr; ni += w * ci; D += w;
+                        for (int j = 0; j < 3; ++j) {
+                            const double wd = -da[0][a] * dl[j][0] * wa[1][b] * wa[2][c]
+                                              - wa[0][a] * da[1][b] * dl[j][1] * wa[2][c]
+                                              - wa[0][a] * wa[1][b] * da[2][c] * dl[j][2];
+                            njr[j] += wd * cr; nji[j] += wd * ci; dj[j] += wd;
+                        }
+                    }
+            pft[2 * (ik * P + i)] = nr / D;
+            pft[2 * (ik * P + i) + 1] = ni / D;
+            for (int j = 0; j < 3; ++j) {
+                const size_t o = 2 * ((size_t)j * K * P + ik * P + i);
+                dpft[o] = (njr[j] * D - nr * dj[j]) / (D * D);
+                dpft[o + 1] = (nji[j] * D - ni * dj[j]) / (D * D);
+            }
+        }
+}
+
+void orc_gencorr_cont_shift_grad(const orc_geom *g, const float *ref, const float *dref, const float *ptcl,
+                                 const double *ctfmat, const double *shvec, int irot, const double *argtransf,
+                                 const double *argtransf_shellone, double *f, double *grad5)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    double *pd = (double *)malloc(sizeof(double) * 2 * K * P);
+    double *t = (double *)malloc(sizeof(double) * 2 * P);
+    prep_ref(g, ref, ctfmat, shvec, argtransf, argtransf_shellone, pr);
+    double y = 0.0, sqr = 0.0, sqp = 0.0, T1[3] = {0, 0, 0}, T2[3] = {0, 0, 0};
+    for (int ik = 0; ik < Ks; ++ik) {
+        y += corrk_for_rot(P, pr + 2 * ik * P, ptcl + 2 * ik * P, irot);
+        sqr += sqsum_k(P, pr + 2 * ik * P);
+        sqp += sqsum_kf(P, ptcl + 2 * ik * P);
+    }
+    for (int j = 0; j < 3; ++j) {
+        /* pft_dref(:,:,j) * ctf * shmat, the prepared reference's own operations */
+        prep_ref(g, dref + (size_t)j * 2 * K * P, ctfmat, shvec, argtransf, argtransf_shellone, pd);
+        for (int ik = 0; ik < Ks; ++ik) {
+            const double *a = pd + 2 * ik * P, *b = pr + 2 * ik * P;
+            T1[j] += corrk_for_rot(P, a, ptcl + 2 * ik * P, irot);
+            for (int n = 0; n < P; ++n) T2[j] += a[2 * n] * b[2 * n] + a[2 * n + 1] * b[2 * n + 1];
+        }
+    }
+    const double den = sqrt(sqr * sqp);
+    *f = y / den;
+    for (int j = 0; j < 3; ++j) grad5[j] = (T1[j] - y * T2[j] / sqr) / den;
+    for (int d = 0; d < 2; ++d) {
+        double c = 0.0;
+        for (int ik = 0; ik < Ks; ++ik) {
+            const double *a = pr + 2 * ik * P;
+            for (int n = 0; n < P; ++n) {
+                const double at = argtransf[ik * N + d * P + n];
+                t[2 * n] = -at * a[2 * n + 1];
+                t[2 * n + 1] = at * a[2 * n];
+            }
+            c += corrk_for_rot(P, t, ptcl + 2 * ik * P, irot);
+        }
+        grad5[3 + d] = c / den;
+    }
+    free(t);
+    free(pd);
+    free(pr);
+}

@@ -130,6 +130,20 @@ void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cm
 void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
                         const double eul[3], const int *mask, int griddev, double *pft);
 
+/* orientation derivatives: euler2dm (simple_ori_light.f90:87-147), dR[j] = dR/de_j per radian,
+ * three row-major 3x3 matrices; dapod (simple_kbinterpol.f90:179-192); fdf_project_polar
+ * (simple_projector.f90:245-267 with fdf_interp_fcomp :338-400): pft [K][P] and its three
+ * angle derivatives dpft [3][K][P], complex */
+void orc_euler2dm(const double eul[3], double dR[27]);
+double orc_kb_dapod(double x);
+void orc_fdf_project_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
+                           const double eul[3], double *pft, double *dpft);
+/* gencorr_cont_shift_grad_cc_for_rot_8 (:1788-1847): f and grad[5] = d f / d(e1, e2, e3, sx, sy);
+ * dref [3][K][P] complex FP32 as pfts_drefs holds it.  gencorr_cont_grad_cc_for_rot_8
+ * (:1735-1786) is f and grad[0..2]. */
+void orc_gencorr_cont_shift_grad(const orc_geom *g, const float *ref, const float *dref, const float *ptcl,
+                                 const double *ctfmat, const double *shvec, int irot, const double *argtransf,
+                                 const double *argtransf_shellone, double *f, double *grad5);
 /* Euclidean objective (cc_objfun = OBJFUN_EUCLID).  sigma2[K] is the particle's column
  * sigma2_noise(kfrom:kto, iptcl); pxls[K] the pixel counts per shell of setup_pxls_p_shell
  * (:879-893); the reference is prepared in the reference frame as ref * ctf (* shmat). */

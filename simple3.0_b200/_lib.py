@@ -85,6 +85,11 @@ SIGNATURES = {
     "pftcc_genfrc": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp],
+    "pftcc_fdf_project_polar": [_h, C.c_int, C.c_int, _dp, C.c_int],
+    "pftcc_get_dref_pft": [_h, C.c_int, C.c_int, _fp],
+    "pftcc_gencorr_cont_shift_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
+    "pftcc_gencorr_cont_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
+    "pftcc_cont_shift_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
     "pftcc_set_objfun": [_h, C.c_int],
     "pftcc_assign_sigma2_noise": [_h, C.c_int, C.c_int, _fp],
     "pftcc_gencorrs_euclid": [_h, C.c_int, C.c_int, _fp, _fp],

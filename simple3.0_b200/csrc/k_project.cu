@@ -117,6 +117,117 @@ __global__ void __launch_bounds__(256) k_fproject_polar(Geom g, int box, const f
     }
 }
 
+// I1 by the Abramowitz & Stegun 9.8.3 / 9.8.4 polynomial approximations (the reference's
+// bessi1, simple_kbinterpol.f90:282-308), x >= 0, in FP64
+__device__ double kb_i1(double x)
+{
+    if (x < 3.75) {
+        double y = x / 3.75;
+        y = y * y;
+        return x * (0.5 + y * (0.87890594 + y * (0.51498869 + y * (0.15084934 + y * (0.2658733e-1 +
+                    y * (0.301532e-2 + y * 0.32411e-3))))));
+    }
+    const double y = 3.75 / x;
+    return (0.39894228 + y * (-0.3988024e-1 + y * (-0.362018e-2 + y * (0.163801e-2 + y * (-0.1031555e-1 +
+            y * (0.2282967e-1 + y * (-0.2895312e-1 + y * (0.1787654e-1 + y * (-0.420059e-2))))))))) *
+           exp(x) / sqrt(x);
+}
+
+// dapod (simple_kbinterpol.f90:179-192): d apod / dx = -4 beta x I1(beta s) / (s W^3),
+// s = sqrt(1 - (2x/W)^2), 0 where s^2 <= 0
+__device__ double kb_dapod(double x)
+{
+    const double W = 3.0, beta = 7.4;
+    double a = (2.0 / W) * x;
+    a = 1.0 - a * a;
+    if (a <= 0.0) return 0.0;
+    const double s = sqrt(a);
+    return -4.0 * beta * x * kb_i1(beta * s) / s / (W * W * W);
+}
+
+// fdf_project_polar (simple_projector.f90:245-267) with fdf_interp_fcomp (:338-400), one
+// thread per (reference, shell, rotation) sample: the normalised interpolation N / D of
+// interp_fcomp_norm and its derivatives with respect to the three Euler angles (per radian).
+// d loc / d e_j = vec dR_j (euler2dm); each tap's weight derivative is the sum over the axes of
+// -dapod(win - loc) d loc / d e_j times the other two axes' apod, and
+// dfcomp_j = (sum wd_j c * D - N sum wd_j) / D^2.  FP64 throughout, FP32 out as set_ref_fcomp /
+// set_dref_fcomp store it.  RD: 36 doubles per reference, R then dR/de1..3, row-major.
+__global__ void __launch_bounds__(256) k_fdf_project_polar(Geom g, int box, const float2 *__restrict__ cube,
+                                                           const float *__restrict__ polar,
+                                                           const double *__restrict__ RD, int n,
+                                                           float2 *__restrict__ out, float2 *__restrict__ dout)
+{
+    const int E = box / 2 + 2, S = 2 * E + 1;
+    const int N = g.N, P = g.P, K = g.K;
+    const long long total = (long long)n * K * P;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e % P), ik = (int)((e / P) % K), r = (int)(e / ((long long)K * P));
+        const double *rm = RD + (size_t)r * 36, *dm = rm + 9;
+        const double vx = polar[(size_t)ik * 2 * N + i], vy = polar[(size_t)ik * 2 * N + N + i];
+        double loc[3], dl[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            loc[d] = vx * rm[d] + vy * rm[3 + d];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) dl[j][d] = vx * dm[9 * j + d] + vy * dm[9 * j + 3 + d];
+        }
+        int w0[3];
+        double wa[3][3], da[3][3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            w0[d] = (int)round(loc[d]) - 1;
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                wa[d][l] = kb_apod((double)(w0[d] + l) - loc[d]);
+                da[d][l] = kb_dapod((double)(w0[d] + l) - loc[d]);
+            }
+        }
+        double nr = 0.0, ni = 0.0, D = 0.0, njr[3] = {0.0, 0.0, 0.0}, nji[3] = {0.0, 0.0, 0.0},
+               dj[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const float2 *row = cube + ((size_t)(w0[2] + c + E) * S + (w0[1] + b + E)) * S + (w0[0] + E);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float2 v = __ldg(row + a);
+                    const double w = wa[0][a] * wa[1][b] * wa[2][c];
+                    nr += w * v.x;
+                    ni += w * v.y;
+                    D += w;
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        const double wd = -da[0][a] * dl[j][0] * wa[1][b] * wa[2][c] -
+                                          wa[0][a] * da[1][b] * dl[j][1] * wa[2][c] -
+                                          wa[0][a] * wa[1][b] * da[2][c] * dl[j][2];
+                        njr[j] += wd * v.x;
+                        nji[j] += wd * v.y;
+                        dj[j] += wd;
+                    }
+                }
+            }
+        out[e] = make_float2((float)(nr / D), (float)(ni / D));
+        const double d2 = D * D;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            dout[((size_t)r * 3 + j) * K * P + (size_t)ik * P + i] =
+                make_float2((float)((njr[j] * D - nr * dj[j]) / d2), (float)((nji[j] * D - ni * dj[j]) / d2));
+    }
+}
+
+cudaError_t launch_fdf_project_polar(pftcc_handle *h, int box, const float2 *cube, const double *RD, int n,
+                                     float2 *out, float2 *dout)
+{
+    const long long total = (long long)n * h->g.K * h->g.P;
+    PFTCC_LAUNCH(h);
+    KTimer kt(h, PFTCC_K_POLARIZE);
+    k_fdf_project_polar<<<(int)std::min<long long>((total + 255) / 256, 8192), 256, 0, h->stream>>>(
+        h->g, box, cube, h->polar, RD, n, out, dout);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_expand_cmat(pftcc_handle *h, int box, const float2 *half, float factor, float2 *cube)
 {
     const long long S = box + 5, n = S * S * S;

@@ -271,7 +271,7 @@ static void free_all(pftcc_handle *h)
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
                     h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
-                    h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls};
+                    h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls, h->drefs_even, h->drefs_odd};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
     for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -725,6 +725,51 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
 }
 
 // ---- polar projection of a volume (simple_projector.f90) --------------------------------
+}  // extern "C"
+
+// euler2m (simple_ori.f90:1275-1284, rotmat :1350-1390): R = R3(e3) R2(e2) R1(e1), angles in
+// degrees, row-major; with dR, euler2dm (simple_ori_light.f90:87-147): dR/de1 = R3 R2 dR1,
+// dR/de2 = R3 dR2 R1, dR/de3 = dR3 R2 R1, the derivatives per radian (drotmat :107-146)
+static void host_euler2m(const double e[3], double *R, double *dR)
+{
+    double m[3][9], d[3][9];
+    for (int a = 0; a < 3; ++a) {
+        const double t = e[a] * 3.14159265358979323846 / 180.0, c = std::cos(t), sn = std::sin(t);
+        double *x = m[a], *y = d[a];
+        for (int i = 0; i < 9; ++i) x[i] = y[i] = 0.0;
+        if (a == 1) {   // about y (tilt)
+            x[0] = c; x[2] = -sn; x[4] = 1.0; x[6] = sn; x[8] = c;
+            y[0] = -sn; y[2] = -c; y[6] = c; y[8] = -sn;
+        } else {        // about z
+            x[0] = c; x[1] = sn; x[3] = -sn; x[4] = c; x[8] = 1.0;
+            y[0] = -sn; y[1] = c; y[3] = -c; y[4] = -sn;
+        }
+    }
+    auto mul3 = [](const double *a, const double *b, const double *c, double *out) {
+        double t[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int l = 0; l < 3; ++l) v += a[3 * i + l] * b[3 * l + j];
+                t[3 * i + j] = v;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int l = 0; l < 3; ++l) v += t[3 * i + l] * c[3 * l + j];
+                out[3 * i + j] = v;
+            }
+    };
+    mul3(m[2], m[1], m[0], R);
+    if (dR) {
+        mul3(m[2], m[1], d[0], dR);
+        mul3(m[2], d[1], m[0], dR + 9);
+        mul3(d[2], m[1], m[0], dR + 18);
+    }
+}
+
+extern "C" {
+
 int pftcc_set_volume_ft(pftcc_handle *h, const float *cmat_half, int box, float factor)
 {
     if (!h || !cmat_half || box < 2 || (box & 1)) return set_err(h, PFTCC_ERR_ARG, "set_volume_ft: bad arguments");
@@ -757,33 +802,12 @@ int pftcc_fproject_polar(pftcc_handle *h, int first_iref, int n, const float *eu
     if (first_iref < 1 || first_iref + n - 1 > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "fproject_polar: range");
     if (!h->vol_cube) return set_err(h, PFTCC_ERR_STATE, "fproject_polar: no volume (set_volume_ft first)");
     if (n == 0) return PFTCC_OK;
-    // euler2m (simple_ori.f90:1275-1284, rotmat :1350-1390): R = R3(e3) R2(e2) R1(e1), degrees
     std::vector<double> R((size_t)n * 9);
     for (int r = 0; r < n; ++r) {
-        double m[3][9];
-        for (int a = 0; a < 3; ++a) {
-            const double ang = (double)euls[3 * r + a];
-            if (!std::isfinite(ang)) return set_err(h, PFTCC_ERR_ARG, "fproject_polar: Euler angle not finite");
-            const double t = ang * 3.14159265358979323846 / 180.0, c = std::cos(t), sn = std::sin(t);
-            double *x = m[a];
-            for (int i = 0; i < 9; ++i) x[i] = 0.0;
-            if (a == 1) { x[0] = c; x[2] = -sn; x[4] = 1.0; x[6] = sn; x[8] = c; }    // about y (tilt)
-            else { x[0] = c; x[1] = sn; x[3] = -sn; x[4] = c; x[8] = 1.0; }          // about z
-        }
-        double t32[9], out[9];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) {
-                double v = 0.0;
-                for (int l = 0; l < 3; ++l) v += m[2][3 * i + l] * m[1][3 * l + j];
-                t32[3 * i + j] = v;
-            }
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) {
-                double v = 0.0;
-                for (int l = 0; l < 3; ++l) v += t32[3 * i + l] * m[0][3 * l + j];
-                out[3 * i + j] = v;
-            }
-        for (int i = 0; i < 9; ++i) R[(size_t)r * 9 + i] = out[i];
+        const double e[3] = {(double)euls[3 * r], (double)euls[3 * r + 1], (double)euls[3 * r + 2]};
+        if (!std::isfinite(e[0]) || !std::isfinite(e[1]) || !std::isfinite(e[2]))
+            return set_err(h, PFTCC_ERR_ARG, "fproject_polar: Euler angle not finite");
+        host_euler2m(e, &R[(size_t)r * 9], nullptr);
     }
     std::lock_guard<std::mutex> lk(h->mtx);
     cudaSetDevice(h->dev);
@@ -804,6 +828,112 @@ int pftcc_fproject_polar(pftcc_handle *h, int first_iref, int n, const float *eu
     dev_free(h, dR);
     dev_free(h, dmask);
     if (e != cudaSuccess) return cuda_err(h, e, "fproject_polar");
+    return PFTCC_OK;
+}
+
+static int ensure_drefs(pftcc_handle *h)
+{
+    if (h->drefs_even && h->drefs_odd) return PFTCC_OK;
+    const size_t bytes = (size_t)h->nrefs * 3 * h->g.K * h->g.P * sizeof(float2);
+    ST(dev_alloc(h, (void **)&h->drefs_even, bytes, "derivative references (even)"));
+    ST(dev_alloc(h, (void **)&h->drefs_odd, bytes, "derivative references (odd)"));
+    CK(cudaMemsetAsync(h->drefs_even, 0, bytes, h->stream), "zero drefs");
+    CK(cudaMemsetAsync(h->drefs_odd, 0, bytes, h->stream), "zero drefs");
+    return PFTCC_OK;
+}
+
+int pftcc_fdf_project_polar(pftcc_handle *h, int first_iref, int n, const double *euls, int iseven)
+{
+    if (!h || !euls || n < 0) return set_err(h, PFTCC_ERR_ARG, "fdf_project_polar: bad arguments");
+    if (first_iref < 1 || first_iref + n - 1 > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "fdf_project_polar: range");
+    if (!h->vol_cube) return set_err(h, PFTCC_ERR_STATE, "fdf_project_polar: no volume (set_volume_ft first)");
+    if (n == 0) return PFTCC_OK;
+    std::vector<double> RD((size_t)n * 36);
+    for (int r = 0; r < n; ++r) {
+        const double *e = euls + 3 * r;
+        if (!std::isfinite(e[0]) || !std::isfinite(e[1]) || !std::isfinite(e[2]))
+            return set_err(h, PFTCC_ERR_ARG, "fdf_project_polar: Euler angle not finite");
+        host_euler2m(e, &RD[(size_t)r * 36], &RD[(size_t)r * 36 + 9]);
+    }
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(ensure_drefs(h));
+    double *dRD = nullptr;
+    ST(dev_alloc(h, (void **)&dRD, RD.size() * sizeof(double), "rotation matrices and derivatives"));
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    float2 *dst = (iseven ? h->refs_even : h->refs_odd) + (size_t)(first_iref - 1) * KP;
+    float2 *ddst = (iseven ? h->drefs_even : h->drefs_odd) + (size_t)(first_iref - 1) * 3 * KP;
+    cudaError_t e = cudaMemcpyAsync(dRD, RD.data(), RD.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_fdf_project_polar(h, h->vol_box, h->vol_cube, dRD, n, dst, ddst);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    dev_free(h, dRD);
+    if (e != cudaSuccess) return cuda_err(h, e, "fdf_project_polar");
+    return PFTCC_OK;
+}
+
+int pftcc_get_dref_pft(pftcc_handle *h, int iref, int iseven, float *dpft)
+{
+    if (!h || !dpft) return PFTCC_ERR_ARG;
+    REF_OR_FAIL(iref);
+    if (!h->drefs_even) return set_err(h, PFTCC_ERR_STATE, "no derivative references (fdf_project_polar first)");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    const size_t n3 = (size_t)3 * h->g.K * h->g.P;
+    const float2 *src = (iseven ? h->drefs_even : h->drefs_odd) + (size_t)(iref - 1) * n3;
+    CK(cudaMemcpyAsync(dpft, src, n3 * sizeof(float2), cudaMemcpyDeviceToHost, h->stream), "get_dref_pft");
+    CK(cudaStreamSynchronize(h->stream), "get_dref_pft");
+    return PFTCC_OK;
+}
+
+int pftcc_cont_shift_grad_batch(pftcc_handle *h, int n, const pftcc_grad_req *req, double *f, double *grad5)
+{
+    if (!h || n < 0 || (n > 0 && (!req || !f || !grad5)))
+        return set_err(h, PFTCC_ERR_ARG, "cont_shift_grad: bad arguments");
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the orientation gradient is served in the reference frame");
+    if (h->cfg.with_ctf && !h->ctf_ready)
+        return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    if (!h->drefs_even) return set_err(h, PFTCC_ERR_STATE, "no derivative references (fdf_project_polar first)");
+    std::vector<EuclidReq> rq(n);
+    for (int i = 0; i < n; ++i) {
+        if (req[i].iref < 1 || req[i].iref > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "cont_shift_grad: iref out of range");
+        if (req[i].irot < 1 || req[i].irot > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "cont_shift_grad: irot out of range");
+        const int sl = slot_of(h, req[i].iptcl);
+        if (sl < 0) return set_err(h, PFTCC_ERR_INDEX, "cont_shift_grad: particle not held");
+        rq[i] = EuclidReq{req[i].iref - 1, sl, req[i].irot, 0, req[i].sx, req[i].sy};
+    }
+    ST(ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)n * sizeof(EuclidReq), 4096), "requests"));
+    ST(ensure(h, (void **)&h->d_dout, &h->dout_cap, (size_t)n * 6 * sizeof(double), "results"));
+    CK(cudaMemcpyAsync(h->d_work, rq.data(), (size_t)n * sizeof(EuclidReq), cudaMemcpyHostToDevice, h->stream), "requests");
+    CK(launch_cont_shift_grad(h, reinterpret_cast<const EuclidReq *>(h->d_work), n, h->d_dout), "cont_shift_grad kernel");
+    std::vector<double> o((size_t)n * 6);
+    CK(cudaMemcpyAsync(o.data(), h->d_dout, o.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "results");
+    CK(cudaStreamSynchronize(h->stream), "cont_shift_grad");
+    for (int i = 0; i < n; ++i) {
+        f[i] = o[6 * (size_t)i];
+        for (int d = 0; d < 5; ++d) grad5[5 * (size_t)i + d] = o[6 * (size_t)i + 1 + d];
+    }
+    return PFTCC_OK;
+}
+
+int pftcc_gencorr_cont_shift_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                               double *f, double *grad)
+{
+    if (!h || !shvec || !f || !grad) return set_err(h, PFTCC_ERR_ARG, "cont_shift_grad: bad arguments");
+    pftcc_grad_req r{iref, iptcl, irot, 0, shvec[0], shvec[1], 0.0};
+    return pftcc_cont_shift_grad_batch(h, 1, &r, f, grad);
+}
+
+int pftcc_gencorr_cont_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
+                                         double *cc, double *dcc)
+{
+    if (!h || !shvec || !cc || !dcc) return set_err(h, PFTCC_ERR_ARG, "cont_grad: bad arguments");
+    double g5[5];
+    ST(pftcc_gencorr_cont_shift_grad_cc_for_rot_8(h, iref, iptcl, shvec, irot, cc, g5));
+    for (int d = 0; d < 3; ++d) dcc[d] = g5[d];
     return PFTCC_OK;
 }
 

@@ -120,6 +120,8 @@ struct pftcc_handle {
     // the volume's expanded FT for polar projection (expand_cmat), side box + 5
     float2 *vol_cube = nullptr;
     int vol_box = 0;
+    // the orientation derivatives of the references (fdf_project_polar), [nrefs][3][K][P]
+    float2 *drefs_even = nullptr, *drefs_odd = nullptr;
     // Euclidean objective: cc_objfun, sigma2_noise(kfrom:kto, sig_from:sig_to) as assigned
     // (host copy), its columns in slot order on the device, pixels per shell
     int objfun = PFTCC_OBJFUN_CC;
@@ -186,6 +188,10 @@ cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int fir
 cudaError_t launch_expand_cmat(pftcc_handle *h, int box, const float2 *half, float factor, float2 *cube);
 cudaError_t launch_fproject_polar(pftcc_handle *h, int box, const float2 *cube, const double *R, const int *mask, int n,
                                   int griddev, float2 *out);
+// fdf_project_polar: RD = 36 doubles per reference (R, then dR/de1..3); out [n][K][P],
+// dout [n][3][K][P]
+cudaError_t launch_fdf_project_polar(pftcc_handle *h, int box, const float2 *cube, const double *RD, int n,
+                                     float2 *out, float2 *dout);
 cudaError_t launch_ctfmat(pftcc_handle *h, const pftcc_ctfparams *params, int n, float *out, float ddf,
                           int derivative);
 cudaError_t launch_sqsums(pftcc_handle *h, int first_slot, int n);
@@ -205,6 +211,10 @@ inline int exact_frame(const pftcc_handle *h)
 {
     return h->objfun == PFTCC_OBJFUN_EUCLID ? FRAME_EUCLID : h->cfg.ctf_frame;
 }
+// gencorr_cont_shift_grad_cc_for_rot_8 for nreq requests (k_orisrch.cu; the request layout of
+// EuclidReq): out6[nreq][6] = f, d/de1..3, d/dsx, d/dsy
+struct EuclidReq;
+cudaError_t launch_cont_shift_grad(pftcc_handle *h, const EuclidReq *reqs_dev, int nreq, double *out6);
 // sigma2_noise on the device and covering every held particle (rebuilt first when stale
 // and may_alloc); PFTCC_OK or the error code, with the message set
 int euclid_ready(pftcc_handle *h, int may_alloc);

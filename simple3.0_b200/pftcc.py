@@ -227,6 +227,20 @@ class polarft_corrcalc:
                                                  None if m is None else m.ctypes.data_as(C.POINTER(C.c_int)),
                                                  int(bool(iseven)), int(bool(griddev))))
 
+    def fdf_project_polar(self, first_iref: int, euls, iseven: bool = True):
+        """projector%fdf_project_polar for n orientations (n, 3) in degrees: the sections into
+        references first_iref.. and their Euler-angle derivatives into the derivative references"""
+        e = np.ascontiguousarray(np.atleast_2d(euls), np.float64)
+        self._check(self._L.pftcc_fdf_project_polar(self._h, int(first_iref), e.shape[0],
+                                                    e.ctypes.data_as(C.POINTER(C.c_double)), int(bool(iseven))))
+
+    def get_dref_pft(self, iref: int, iseven: bool = True) -> np.ndarray:
+        """(3, K, P) derivatives of reference iref with respect to e1, e2, e3 (per radian)"""
+        K = self.cfg.kfromto[1] - self.cfg.kfromto[0] + 1
+        out = np.zeros((3, K, self.cfg.nrots // 2), np.complex64)
+        self._check(self._L.pftcc_get_dref_pft(self._h, int(iref), int(bool(iseven)), _f32p(out.view(np.float32))))
+        return out
+
     # ---- CALCULATORS -----------------------------------------------------------------------
     def gencorrs(self, iref: int, iptcl: int, shvec=None) -> np.ndarray:
         cc = np.zeros(self.cfg.nrots, np.float32)
@@ -447,6 +461,39 @@ class polarft_corrcalc:
                                              f.ctypes.data_as(C.POINTER(C.c_double)),
                                              g.ctypes.data_as(C.POINTER(C.c_double))))
         return f, g
+
+    def cont_shift_grad_batch(self, iref, iptcl, irot, sx, sy):
+        """f and grad5 = d f / d(e1, e2, e3, shift_x, shift_y) (gencorr_cont_shift_grad_cc_for_rot_8)
+        for arrays of requests, from the references and derivative references of fdf_project_polar"""
+        iref, iptcl, irot, sx, sy = np.broadcast_arrays(*(np.asarray(v) for v in (iref, iptcl, irot, sx, sy)))
+        n = iref.size
+        req = np.zeros(n, dtype=_GRAD_REQ)
+        req["iref"], req["iptcl"], req["irot"] = iref.ravel(), iptcl.ravel(), irot.ravel()
+        req["sx"], req["sy"] = sx.ravel(), sy.ravel()
+        f = np.zeros(n, np.float64)
+        g = np.zeros((n, 5), np.float64)
+        self._check(self._L.pftcc_cont_shift_grad_batch(self._h, n, req.ctypes.data_as(C.POINTER(_lib.GradReq)),
+                                                        f.ctypes.data_as(C.POINTER(C.c_double)),
+                                                        g.ctypes.data_as(C.POINTER(C.c_double))))
+        return f, g
+
+    def gencorr_cont_shift_grad_cc_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        f = C.c_double()
+        g = np.zeros(5, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_cont_shift_grad_cc_for_rot_8(
+            self._h, int(iref), int(iptcl), sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot), C.byref(f),
+            g.ctypes.data_as(C.POINTER(C.c_double))))
+        return f.value, g
+
+    def gencorr_cont_grad_cc_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
+        cc = C.c_double()
+        g = np.zeros(3, np.float64)
+        sh = np.ascontiguousarray(shvec, np.float64)
+        self._check(self._L.pftcc_gencorr_cont_grad_cc_for_rot_8(
+            self._h, int(iref), int(iptcl), sh.ctypes.data_as(C.POINTER(C.c_double)), int(irot), C.byref(cc),
+            g.ctypes.data_as(C.POINTER(C.c_double))))
+        return cc.value, g
 
     def refine_batch(self, iref, iptcl, irot, x0, lb, ub, maxits: int = 100, pgtol: float = 1e-5,
                      factr: float = 1e7):
