@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
-    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project", "euclid"],
+    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project", "euclid", "ingest"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
                          "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
                          "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
@@ -689,8 +689,55 @@ def run_euclid_report(args):
     print(json.dumps(out), flush=True)
 
 
+def run_ingest_report(args):
+    """Particle ingestion (pftcc_prep_ptcls: prepimg4align + polarize) on the config-1 geometry:
+    4,096 seeded box-128 particle images (shifted Gaussian blobs in noise, random shifts within
+    +-5 px, CTFFLAG_YES with astigmatic defocus), GPU wall time per call with the images copied
+    from host memory inside it, parity of three particles against the oracle's prepimg4align +
+    polarize, and the oracle's single-thread time per particle."""
+    pkg = entry.load_package()
+    O = entry.load_oracle()
+    w = pkg.synth.config1()
+    B, n, msk = w.box, 4096, w.box / 2 - 10.0
+    rng = np.random.default_rng(8)
+    yy, xx = np.mgrid[0:B, 0:B]
+    base = np.exp(-((xx - B / 2) ** 2 + (yy - B / 2) ** 2) / (2 * 12.0 ** 2)).astype(np.float32)
+    imgs = (2.0 + 4.0 * base[None] + 0.8 * rng.standard_normal((n, B, B))).astype(np.float32)
+    xy = rng.uniform(-5, 5, (n, 2)).astype(np.float32)
+    flags = np.ones(n, np.int32)
+    dfx = rng.uniform(1.0, 3.0, n)
+    ctfp = pkg.ctfparams_array(n, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca, dfx=dfx, dfy=dfx - 0.2,
+                               angast=rng.uniform(0, 180, n))
+    pc = pkg.polarft_corrcalc()
+    pc.new(1, (1, n), box=B, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=False)
+    pc.prep_ptcls(0, imgs, xy, flags, ctfp, msk)
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        pc.prep_ptcls(0, imgs, xy, flags, ctfp, msk)
+    dt = (time.perf_counter() - t0) / reps
+    g = O.geom(w.nrots, w.kfrom, w.kto, B)
+    t = O.tables(g)
+    worst = 0.0
+    t0 = time.perf_counter()
+    for i in range(3):
+        c = O.make_ctf(smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca, dfx=float(np.float32(dfx[i])),
+                       dfy=float(np.float32(dfx[i] - 0.2)), angast=float(ctfp[i].angast))
+        want = O.polarize(g, t, O.prepimg4align(imgs[i], B, msk, float(xy[i, 0]), float(xy[i, 1]), c))
+        worst = max(worst, float(np.max(np.abs(pc.get_ptcl_pft(i + 1) - want)) / np.max(np.abs(want))))
+    t_cpu = (time.perf_counter() - t0) / 3
+    pc.kill()
+    print(json.dumps({"report": "ingest", "box": B, "particles": n, "gpu_seconds_per_call": dt,
+                      "particles_per_s": n / dt, "h2d_bytes_per_call": int(imgs.nbytes),
+                      "parity_max_rel_err_vs_oracle": worst, "oracle_seconds_per_particle_1_thread": t_cpu}),
+          flush=True)
+
+
 def main():
     args = parse()
+    if args.report == "ingest":
+        run_ingest_report(args)
+        return
     if args.report == "euclid":
         run_euclid_report(args)
         return

@@ -119,6 +119,22 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
 int pftcc_polarize_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *cmats_dev, int griddev);
 int pftcc_polarize_refs(pftcc_handle *h, int first_iref, int n, const float *cmats, int iseven, int griddev);
 
+/* ---- particle ingestion --------------------------------------------------------------- */
+/* spproj%get_ctfparams(...)%ctfflag (simple_defs.f90:55) */
+enum { PFTCC_CTFFLAG_NO = 0, PFTCC_CTFFLAG_YES = 1, PFTCC_CTFFLAG_FLIP = 2 };
+/* prepimg4align (simple_strategy2D3D_common.f90:316-366) followed by polarize
+ * (build_pftcc_batch_particles :353-376) for n particle images of side box_in (even,
+ * >= boxmatch = cfg.box), imgs [n][box_in][box_in] real, rmat(x, y) order: noise normalisation
+ * against the background outside the disc of radius msk, FFT, shift by -(x, y) = -xy[2 i..],
+ * the CTF phase flip for ctfflag[i] == PFTCC_CTFFLAG_YES (ctf[i]; ctf may be NULL when no flag
+ * is YES), inverse FFT, clip to boxmatch, soft mask of radius msk (no inner or focus mask),
+ * FFT and the factor boxmatch^2 / box_in^2, then the polar gridding into slots
+ * first_slot..first_slot+n-1 (griddev 'no'); the _dev form takes the images in device memory */
+int pftcc_prep_ptcls(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
+                     const int *ctfflag, const pftcc_ctfparams *ctf, float msk);
+int pftcc_prep_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
+                         const int *ctfflag, const pftcc_ctfparams *ctf, float msk);
+
 /* ---- polar projection of a volume -------------------------------------------------- */
 /* projector%expand_cmat (simple_projector.f90:66-132): the volume's half FT
  * image%cmat(box/2+1, box, box) (Fortran order, complex interleaved; even box with

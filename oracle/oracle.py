@@ -85,6 +85,7 @@ def lib():
         L.orc_gencorrs_euclid.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
         L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
         L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_prepimg4align.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.POINTER(Ctf), dp]
         L.orc_euler2dm.argtypes = [dp, dp]
         L.orc_kb_dapod.argtypes = [C.c_double]
         L.orc_kb_dapod.restype = C.c_double
@@ -303,6 +304,18 @@ def fproject_polar(g: Geom, t: Tables, cmat_exp, box: int, eul, mask=None, gridd
     lib().orc_fproject_polar(C.byref(g), _P(t.polar, C.c_float), int(box), _P(_c64(cmat_exp), C.c_float),
                              _P(e, C.c_double), _P(m, C.c_int), int(bool(griddev)),
                              out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def prepimg4align(img, boxmatch: int, msk: float, x: float = 0.0, y: float = 0.0, ctf: "Ctf | None" = None):
+    """prepimg4align of one particle image img (box, box) [y][x]: its FT (boxmatch, boxmatch/2+1)
+    [k][h] as polarize takes it; ctf None for ctfflag no / flip, a Ctf for the phase flip"""
+    a = np.ascontiguousarray(img, np.float32)
+    box = a.shape[0]
+    out = _c128_out((boxmatch, boxmatch // 2 + 1))
+    lib().orc_prepimg4align(int(box), int(boxmatch), _P(a, C.c_float), float(msk), float(x), float(y),
+                            None if ctf is None else C.byref(ctf),
+                            out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
     return out
 
 

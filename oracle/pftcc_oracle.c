@@ -1105,3 +1105,193 @@ void orc_gencorr_cont_shift_grad(const orc_geom *g, const float *ref, const floa
     free(pd);
     free(pr);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Particle ingestion, prepimg4align (simple_strategy2D3D_common.f90:316-366), stated step by
+ * step as the reference's image methods run:
+ *  noise_norm (simple_image.f90:6623-6640) against the background, the pixels outside the disc
+ *    of radius msk (disc_2 :506-523; cendist :2719-2748 measures from B/2 + 1, 1-based);
+ *  fft (fwd_ft :5773-5782): shift_phorig (quadrant swap), r2c, / B^2;
+ *  shift2Dserial([-x, -y]) (:6149-6174) when |x| or |y| > SHTHRESH = 0.001 (:31): cmat(h, k) times
+ *    exp(i (h sh1 + k sh2)), sh = shvec * shconst in single precision, shconst = PI / (B/2)
+ *    (:445), the phase in double and rounded to single;
+ *  phase flip (simple_ctf.f90 apply_serial 'flip' :312-403): sign(1, tval), tval = sin(evalPhSh
+ *    (+ phshift) + amp_contr_const) at spaFreqSq = (h/B)^2 + (k/B)^2, ang = atan2(k, h);
+ *  ifft (bwd_ft :5784-5791): c2r, shift_phorig;
+ *  clip (:6471-6516): the centred boxmatch window from (B - Bm)/2 + 1;
+ *  mask 'soft' (:6208-6300): zero_background (:5176-5203) -- the mean of the k-th smallest values,
+ *    k = Bm/2 (selec, simple_math.f90:2204), of the four border lines, subtracted when its
+ *    magnitude exceeds TINY = 1e-10 -- then cosedge (simple_math.f90:1089-1103) with box
+ *    minlen = min(nint(2 (msk + COSMSKHALFWIDTH)), Bm), COSMSKHALFWIDTH = 6 (simple_defs.f90:130),
+ *    evaluated at (cis(i), cjs(j)) = (-Bm/2 + i - 1, -Bm/2 + j - 1) for i, j <= Bm/2 and applied to
+ *    the four mirrored pixels, skipped where e > 0.9999;
+ *  fft and the factor Bm^2 / B^2 (:364-365). */
+static void fft2d(int B, double *z, int sign)
+{
+    double *a = (double *)malloc(sizeof(double) * 2 * B), *b = (double *)malloc(sizeof(double) * 2 * B);
+    for (int r = 0; r < B; ++r) {   /* along x */
+        orc_cfft(B, z + 2 * (size_t)r * B, b, sign);
+        memcpy(z + 2 * (size_t)r * B, b, sizeof(double) * 2 * B);
+    }
+    for (int c = 0; c < B; ++c) {   /* along y */
+        for (int r = 0; r < B; ++r) { a[2 * r] = z[2 * ((size_t)r * B + c)]; a[2 * r + 1] = z[2 * ((size_t)r * B + c) + 1]; }
+        orc_cfft(B, a, b, sign);
+        for (int r = 0; r < B; ++r) { z[2 * ((size_t)r * B + c)] = b[2 * r]; z[2 * ((size_t)r * B + c) + 1] = b[2 * r + 1]; }
+    }
+    free(a);
+    free(b);
+}
+
+/* shift_phorig (:6016-6114) of an even square image: swap quadrant (i, j) with (i + B/2, j + B/2) */
+static void phorig(int B, double *r)
+{
+    const int H = B / 2;
+    for (int j = 0; j < H; ++j)
+        for (int i = 0; i < B; ++i) {
+            const int i2 = (i + H) % B, j2 = j + H;
+            const double t = r[(size_t)j * B + i];
+            r[(size_t)j * B + i] = r[(size_t)j2 * B + i2];
+            r[(size_t)j2 * B + i2] = t;
+        }
+}
+
+static int cmp_dbl(const void *a, const void *b)
+{
+    const double x = *(const double *)a, y = *(const double *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, double x, double y, const orc_ctf *ctf,
+                       double *cmat_out)
+{
+    const int B = box, Bm = boxmatch, hB = B / 2 + 1, hBm = Bm / 2 + 1;
+    double *r = (double *)malloc(sizeof(double) * B * B);
+    double *z = (double *)malloc(sizeof(double) * 2 * B * B);
+    for (int e = 0; e < B * B; ++e) r[e] = img[e];
+    /* noise_norm */
+    {
+        const double c = B / 2 + 1;
+        long npix = 0;
+        double s = 0.0;
+        unsigned char *bg = (unsigned char *)malloc((size_t)B * B);
+        for (int j = 0; j < B; ++j)
+            for (int i = 0; i < B; ++i) {
+                const double di = (i + 1) - c, dj = (j + 1) - c;
+                bg[(size_t)j * B + i] = !(sqrt(di * di + dj * dj) <= msk);
+                if (bg[(size_t)j * B + i]) { ++npix; s += r[(size_t)j * B + i]; }
+            }
+        const double ave = s / (double)npix;
+        if (fabs(ave) > 1e-10)
+            for (int e = 0; e < B * B; ++e) r[e] -= ave;
+        double ep = 0.0, var = 0.0;
+        for (int e = 0; e < B * B; ++e)
+            if (bg[e]) { ep += r[e]; var += r[e] * r[e]; }
+        var = (var - ep * ep / (double)npix) / ((double)npix - 1.0);
+        if (var == var && var > 0.0) {
+            const double sd = sqrt(var);
+            for (int e = 0; e < B * B; ++e) r[e] /= sd;
+        }
+        free(bg);
+    }
+    /* fft */
+    phorig(B, r);
+    for (int e = 0; e < B * B; ++e) { z[2 * e] = r[e] / ((double)B * B); z[2 * e + 1] = 0.0; }
+    fft2d(B, z, -1);
+    /* shift and phase flip on the half plane h = 0..B/2, k = -B/2..B/2-1, mirrored onto the
+     * Friedel mates so that the inverse transform stays real */
+    const int do_shift = fabs(x) > 0.001 || fabs(y) > 0.001;
+    const float shconst = (float)3.14159265358979323846 / (float)(B / 2);
+    const double sh1 = (double)((float)(-x) * shconst), sh2 = (double)((float)(-y) * shconst);
+    ctf_consts kc;
+    if (ctf) { kc = ctf_setup(ctf); kc.phshift = ctf->phshift; }
+    for (int kphys = 0; kphys < B; ++kphys) {
+        const int k = kphys < B / 2 ? kphys : kphys - B;
+        for (int h = 0; h <= B / 2; ++h) {
+            double fr = 1.0, fi = 0.0;
+            if (do_shift) {
+                const double a = h * sh1 + k * sh2;
+                fr = (double)(float)cos(a);
+                fi = (double)(float)sin(a);
+            }
+            if (ctf) {
+                const double hinv = (double)h / B, kinv = (double)k / B;
+                const double t = sin(ctf_chi(&kc, hinv * hinv + kinv * kinv, atan2((double)k, (double)h)));
+                const double sg = t >= 0.0 ? 1.0 : -1.0;
+                fr *= sg; fi *= sg;
+            }
+            double *v = z + 2 * ((size_t)kphys * B + h);
+            const double vr = v[0] * fr - v[1] * fi, vi = v[0] * fi + v[1] * fr;
+            v[0] = vr; v[1] = vi;
+            if (h > 0 && h < B / 2) {   /* Friedel mate (-h, -k) */
+                double *w = z + 2 * ((size_t)((B - kphys) % B) * B + (B - h));
+                w[0] = vr; w[1] = -vi;
+            }
+        }
+    }
+    /* ifft: c2r of the half plane (the full spectrum is Hermitian), then shift_phorig */
+    fft2d(B, z, +1);
+    for (int e = 0; e < B * B; ++e) r[e] = z[2 * e];
+    phorig(B, r);
+    /* clip */
+    double *m = (double *)malloc(sizeof(double) * Bm * Bm);
+    const int st = (B - Bm) / 2;
+    for (int j = 0; j < Bm; ++j)
+        for (int i = 0; i < Bm; ++i) m[(size_t)j * Bm + i] = r[(size_t)(j + st) * B + (i + st)];
+    /* zero_background */
+    {
+        double *line = (double *)malloc(sizeof(double) * Bm);
+        double med = 0.0;
+        for (int which = 0; which < 4; ++which) {
+            for (int t = 0; t < Bm; ++t) {
+                switch (which) {
+                case 0: line[t] = m[(size_t)t * Bm + 0]; break;              /* rmat(1, :)  */
+                case 1: line[t] = m[(size_t)t * Bm + (Bm - 1)]; break;       /* rmat(Bm, :) */
+                case 2: line[t] = m[t]; break;                                /* rmat(:, 1)  */
+                default: line[t] = m[(size_t)(Bm - 1) * Bm + t]; break;      /* rmat(:, Bm) */
+                }
+            }
+            qsort(line, Bm, sizeof(double), cmp_dbl);
+            med += line[Bm / 2 - 1];
+        }
+        med /= 4.0;
+        if (fabs(med) > 1e-10)
+            for (int e = 0; e < Bm * Bm; ++e) m[e] -= med;
+        free(line);
+    }
+    /* cosine edge */
+    {
+        int minlen = (int)f_nint(2.0 * (msk + 6.0));
+        if (minlen > Bm) minlen = Bm;
+        const double maxrad = (double)(minlen / 2), width = 2.0 * (maxrad - msk);
+        for (int i = 1; i <= Bm / 2; ++i)
+            for (int j = 1; j <= Bm / 2; ++j) {
+                const double cx = -Bm / 2.0 + (i - 1), cy = -Bm / 2.0 + (j - 1);
+                const double rad = sqrt(cx * cx + cy * cy);
+                double e = 1.0;
+                if (rad >= maxrad) e = 0.0;
+                else if (rad >= maxrad - width) e = (cos(((rad - (maxrad - width)) / width) * 3.14159265358979323846) + 1.0) / 2.0;
+                if (e > 0.9999) continue;
+                const int ir = Bm + 1 - i, jr = Bm + 1 - j;
+                m[(size_t)(j - 1) * Bm + (i - 1)] *= e;
+                m[(size_t)(jr - 1) * Bm + (i - 1)] *= e;
+                m[(size_t)(j - 1) * Bm + (ir - 1)] *= e;
+                m[(size_t)(jr - 1) * Bm + (ir - 1)] *= e;
+            }
+    }
+    /* fft and the box factor */
+    phorig(Bm, m);
+    double *zm = (double *)malloc(sizeof(double) * 2 * Bm * Bm);
+    const double f = 1.0 / ((double)Bm * Bm) * ((double)Bm * Bm) / ((double)B * B);
+    for (int e = 0; e < Bm * Bm; ++e) { zm[2 * e] = m[e] * f; zm[2 * e + 1] = 0.0; }
+    fft2d(Bm, zm, -1);
+    for (int kphys = 0; kphys < Bm; ++kphys)
+        for (int h = 0; h < hBm; ++h) {
+            cmat_out[2 * ((size_t)kphys * hBm + h)] = zm[2 * ((size_t)kphys * Bm + h)];
+            cmat_out[2 * ((size_t)kphys * hBm + h) + 1] = zm[2 * ((size_t)kphys * Bm + h) + 1];
+        }
+    (void)hB;
+    free(zm);
+    free(m);
+    free(z);
+    free(r);
+}

@@ -130,6 +130,13 @@ void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cm
 void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
                         const double eul[3], const int *mask, int griddev, double *pft);
 
+/* particle ingestion: prepimg4align (simple_strategy2D3D_common.f90:316-366) for one particle
+ * with the soft mask of radius msk (no inner or focus mask) and griddev 'no'; img [box][box]
+ * real in C order [y][x] (rmat(x, y)); (x, y) the particle's shift; ctf NULL for ctfflag
+ * no / flip, else the phase flip of ctfflag yes; out [boxmatch][boxmatch/2+1] complex, i.e.
+ * cmat(h, k) with k at its physical index */
+void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, double x, double y, const orc_ctf *ctf,
+                       double *cmat_out);
 /* orientation derivatives: euler2dm (simple_ori_light.f90:87-147), dR[j] = dR/de_j per radian,
  * three row-major 3x3 matrices; dapod (simple_kbinterpol.f90:179-192); fdf_project_polar
  * (simple_projector.f90:245-267 with fdf_interp_fcomp :338-400): pft [K][P] and its three

@@ -14,6 +14,7 @@ OK, ERR_ARG, ERR_INDEX, ERR_STATE, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NODEV, ER
 FRAME_REF, FRAME_PTCL = 0, 1
 PREC_EXACT, PREC_FP32, PREC_BF16X3 = 0, 1, 2
 OBJFUN_CC, OBJFUN_EUCLID = 0, 1
+CTFFLAG_NO, CTFFLAG_YES, CTFFLAG_FLIP = 0, 1, 2
 
 
 class Config(C.Structure):
@@ -85,6 +86,8 @@ SIGNATURES = {
     "pftcc_genfrc": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore": [_h, C.c_int, C.c_int, C.c_int, _fp, _fp],
     "pftcc_specscore_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp],
+    "pftcc_prep_ptcls": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp, _ip, C.POINTER(CtfParams), C.c_float],
+    "pftcc_prep_ptcls_dev": [_h, C.c_int, C.c_int, C.c_void_p, C.c_int, _fp, _ip, C.POINTER(CtfParams), C.c_float],
     "pftcc_fdf_project_polar": [_h, C.c_int, C.c_int, _dp, C.c_int],
     "pftcc_get_dref_pft": [_h, C.c_int, C.c_int, _fp],
     "pftcc_gencorr_cont_shift_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],

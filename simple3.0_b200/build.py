@@ -44,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH, *FLAGS, "-o", tmp, *sources()]
+    cmd = [nvcc(), *ARCH, *FLAGS, "-o", tmp, *sources(), "-lcufft"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

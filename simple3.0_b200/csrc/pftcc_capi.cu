@@ -274,6 +274,7 @@ static void free_all(pftcc_handle *h)
                     h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls, h->drefs_even, h->drefs_odd};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
+    ingest_free(h);
     for (auto &p : h->prof_pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
     cudaStream_t own = h->own_stream ? h->own_stream : h->stream;
@@ -722,6 +723,72 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
     }
     CK(cudaStreamSynchronize(h->stream), "polarize");
     return PFTCC_OK;
+}
+
+// ---- particle ingestion (prepimg4align) ------------------------------------------------
+static int prep_ptcls_common(pftcc_handle *h, int first_slot, int n, const float *imgs, int imgs_on_device,
+                             int box_in, const float *xy, const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
+{
+    if (!h || !imgs || !xy || !ctfflag || n < 0) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: bad arguments");
+    if (first_slot < 0 || first_slot + n > h->nptcls) return set_err(h, PFTCC_ERR_INDEX, "prep_ptcls: slot range");
+    const int Bm = h->g.box;
+    if (box_in < Bm || (box_in & 1)) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: box must be even and >= boxmatch");
+    if (!(msk > 0.f) || !(msk < 0.5f * Bm)) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: msk must lie in (0, boxmatch/2)");
+    for (int i = 0; i < n; ++i) {
+        if (ctfflag[i] < 0 || ctfflag[i] > 2) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: unsupported CTF flag");
+        if (ctfflag[i] == 1 && !ctf) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: CTFFLAG_YES needs CTF parameters");
+        if (!std::isfinite(xy[2 * i]) || !std::isfinite(xy[2 * i + 1]))
+            return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: shift not finite");
+    }
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    const int cap = std::min(n, ingest_batch_max(box_in));
+    const size_t img_in = (size_t)box_in * box_in * sizeof(float);
+    const size_t img_out = (size_t)Bm * (Bm / 2 + 1) * sizeof(float2);
+    // staging: input images (host path), the cap half-plane outputs, per-image descriptors
+    const size_t in_bytes = imgs_on_device ? 0 : (size_t)cap * img_in;
+    const size_t desc_bytes = (size_t)cap * (2 * sizeof(float) + sizeof(int) + sizeof(pftcc_ctfparams));
+    ST(ensure(h, &h->pol_stage, &h->pol_stage_bytes, in_bytes + (size_t)cap * img_out + desc_bytes + 256, "ingest staging"));
+    char *base = static_cast<char *>(h->pol_stage);
+    float2 *cm = reinterpret_cast<float2 *>(base);
+    float *in = reinterpret_cast<float *>(base + (size_t)cap * img_out);
+    char *desc = base + (size_t)cap * img_out + in_bytes;
+    float *dxy = reinterpret_cast<float *>(desc);
+    int *dflag = reinterpret_cast<int *>(desc + (size_t)cap * 2 * sizeof(float));
+    pftcc_ctfparams *dctf = reinterpret_cast<pftcc_ctfparams *>(
+        (reinterpret_cast<uintptr_t>(dflag + cap) + 15) & ~uintptr_t(15));
+    for (int c0 = 0; c0 < n; c0 += cap) {
+        const int m = std::min(cap, n - c0);
+        const float *src = imgs_on_device ? imgs + (size_t)c0 * box_in * box_in : in;
+        if (!imgs_on_device)
+            CK(cudaMemcpyAsync(in, imgs + (size_t)c0 * box_in * box_in, (size_t)m * img_in, cudaMemcpyHostToDevice,
+                               h->stream), "prep_ptcls upload");
+        CK(cudaMemcpyAsync(dxy, xy + 2 * (size_t)c0, (size_t)m * 2 * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+           "prep_ptcls shifts");
+        CK(cudaMemcpyAsync(dflag, ctfflag + c0, (size_t)m * sizeof(int), cudaMemcpyHostToDevice, h->stream),
+           "prep_ptcls flags");
+        if (ctf)
+            CK(cudaMemcpyAsync(dctf, ctf + c0, (size_t)m * sizeof(pftcc_ctfparams), cudaMemcpyHostToDevice, h->stream),
+               "prep_ptcls ctf");
+        ST(ingest_images(h, src, m, cap, box_in, dxy, dflag, dctf, msk, cm));
+        ST(polarize_dev(h, first_slot + c0, m, cm, 0));
+        // the staging is reused by the next chunk's uploads
+        CK(cudaStreamSynchronize(h->stream), "prep_ptcls");
+    }
+    return PFTCC_OK;
+}
+
+int pftcc_prep_ptcls(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
+                     const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
+{
+    return prep_ptcls_common(h, first_slot, n, imgs, 0, box_in, xy, ctfflag, ctf, msk);
+}
+
+int pftcc_prep_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
+                         const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
+{
+    return prep_ptcls_common(h, first_slot, n, static_cast<const float *>(imgs_dev), 1, box_in, xy, ctfflag, ctf, msk);
 }
 
 // ---- polar projection of a volume (simple_projector.f90) --------------------------------

@@ -120,6 +120,8 @@ struct pftcc_handle {
     // the volume's expanded FT for polar projection (expand_cmat), side box + 5
     float2 *vol_cube = nullptr;
     int vol_box = 0;
+    // particle ingestion state (k_ingest.cu: cuFFT plans and scratch)
+    void *ingest = nullptr;
     // the orientation derivatives of the references (fdf_project_polar), [nrefs][3][K][P]
     float2 *drefs_even = nullptr, *drefs_odd = nullptr;
     // Euclidean objective: cc_objfun, sigma2_noise(kfrom:kto, sig_from:sig_to) as assigned
@@ -215,6 +217,12 @@ inline int exact_frame(const pftcc_handle *h)
 // EuclidReq): out6[nreq][6] = f, d/de1..3, d/dsx, d/dsy
 struct EuclidReq;
 cudaError_t launch_cont_shift_grad(pftcc_handle *h, const EuclidReq *reqs_dev, int nreq, double *out6);
+// particle ingestion (k_ingest.cu): prepimg4align of n <= cap images [n][B][B] into cap half-plane
+// FTs [cap][box][box/2+1] (box = boxmatch); xy [n][2], flag [n], ctf [n] on the device
+int ingest_images(pftcc_handle *h, const float *imgs_dev, int n, int cap, int B, const float *xy_dev,
+                  const int *flag_dev, const pftcc_ctfparams *ctf_dev, float msk, float2 *cm_out);
+int ingest_batch_max(int B);
+void ingest_free(pftcc_handle *h);
 // sigma2_noise on the device and covering every held particle (rebuilt first when stale
 // and may_alloc); PFTCC_OK or the error code, with the message set
 int euclid_ready(pftcc_handle *h, int may_alloc);

@@ -227,6 +227,18 @@ class polarft_corrcalc:
                                                  None if m is None else m.ctypes.data_as(C.POINTER(C.c_int)),
                                                  int(bool(iseven)), int(bool(griddev))))
 
+    def prep_ptcls(self, first_slot: int, imgs, xy=None, ctfflag=None, ctfparams=None, msk: float | None = None):
+        """prepimg4align + polarize for images (n, box_in, box_in) [y][x] into slots first_slot..:
+        xy (n, 2) the particles' shifts, ctfflag (n,) of _lib.CTFFLAG_*, ctfparams a ctypes array
+        (ctfparams_array) needed where a flag is CTFFLAG_YES, msk the mask radius (pixels)"""
+        a = np.ascontiguousarray(imgs, np.float32)
+        n, box_in = a.shape[0], a.shape[1]
+        v = np.zeros((n, 2), np.float32) if xy is None else np.ascontiguousarray(xy, np.float32).reshape(n, 2)
+        f = np.zeros(n, np.int32) if ctfflag is None else np.ascontiguousarray(ctfflag, np.int32).reshape(n)
+        m = float(self.cfg.box / 2 - 4 if msk is None else msk)
+        self._check(self._L.pftcc_prep_ptcls(self._h, int(first_slot), n, _f32p(a), int(box_in), _f32p(v),
+                                             f.ctypes.data_as(C.POINTER(C.c_int)), ctfparams, m))
+
     def fdf_project_polar(self, first_iref: int, euls, iseven: bool = True):
         """projector%fdf_project_polar for n orientations (n, 3) in degrees: the sections into
         references first_iref.. and their Euler-angle derivatives into the derivative references"""
