@@ -186,6 +186,19 @@ int pftcc_gencorr_cont_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, c
                                          double *cc, double *dcc);
 /* n requests in one launch (req[i].ddf unused): f[n], grad5[n][5] */
 int pftcc_cont_shift_grad_batch(pftcc_handle *h, int n, const pftcc_grad_req *req, double *f, double *grad5);
+/* pftcc_orisrch_grad%minimize (simple_pftcc_orisrch_grad.f90:60-122) for n particles at once on the
+ * volume of pftcc_set_volume_ft: variables (e1, e2, e3) in degrees within e +- angerr_deg and a
+ * shift within +- maxhwshift, started at (e, 0, 0); cost -corr of
+ * gencorr_cont_shift_grad_cc_for_rot_8 at irot = 1 on the sections of fdf_project_polar at the
+ * trial angles, its gradient as that routine gives it (angle components per radian);
+ * bound-constrained L-BFGS (pgtol, factr as pftcc_refine_batch).  out: the angles and the shift
+ * rotated by rotmat2d(e3) when the cost fell below its start (found_better), else the input
+ * angles and a zero shift; corr and the starting corr_init.  One volume per call: odd and even
+ * particles whose volumes differ are searched in two calls. */
+typedef struct { int iptcl, pad; double e[3]; double angerr_deg, maxhwshift; } pftcc_orisrch_req;
+typedef struct { double e[3], shift[2], corr, corr_init; int found_better, nevals, niter, converged, pad; } pftcc_orisrch_out;
+int pftcc_orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
+                        pftcc_orisrch_out *out);
 
 /* ---- the Euclidean objective (reference frame only) -------------------------------- */
 /* params_glob%cc_objfun: PFTCC_OBJFUN_EUCLID makes pftcc_gencorrs, pftcc_gencorr_for_rot(_8),

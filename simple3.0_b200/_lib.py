@@ -38,6 +38,17 @@ class GradReq(C.Structure):
                 ("sx", C.c_double), ("sy", C.c_double), ("ddf", C.c_double)]
 
 
+class OrisrchReq(C.Structure):
+    _fields_ = [("iptcl", C.c_int), ("pad", C.c_int), ("e", C.c_double * 3), ("angerr_deg", C.c_double),
+                ("maxhwshift", C.c_double)]
+
+
+class OrisrchOut(C.Structure):
+    _fields_ = [("e", C.c_double * 3), ("shift", C.c_double * 2), ("corr", C.c_double), ("corr_init", C.c_double),
+                ("found_better", C.c_int), ("nevals", C.c_int), ("niter", C.c_int), ("converged", C.c_int),
+                ("pad", C.c_int)]
+
+
 class RefineReq(C.Structure):
     _fields_ = [("iref", C.c_int), ("iptcl", C.c_int), ("irot", C.c_int), ("pad", C.c_int),
                 ("x0", C.c_double * 3)]
@@ -93,6 +104,8 @@ SIGNATURES = {
     "pftcc_gencorr_cont_shift_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
     "pftcc_gencorr_cont_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],
     "pftcc_cont_shift_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
+    "pftcc_orisrch_batch": [_h, C.c_int, C.POINTER(OrisrchReq), C.c_int, C.c_double, C.c_double,
+                            C.POINTER(OrisrchOut)],
     "pftcc_set_objfun": [_h, C.c_int],
     "pftcc_assign_sigma2_noise": [_h, C.c_int, C.c_int, _fp],
     "pftcc_gencorrs_euclid": [_h, C.c_int, C.c_int, _fp, _fp],

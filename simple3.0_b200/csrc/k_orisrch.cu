@@ -10,9 +10,13 @@
 //   f = y / den,  grad_j = (T1_j - y T2_j / S) / den,
 //   grad_{4,5} = Re sum_n (i argtransf_{x,y} A)(n) conj(ptcl~(n + irot - 1)) / den.
 // T1 correlates with the particle being scored (the reference passes iref to
-// calc_T1_T2_for_rot_8 as the particle slot, :1776 / :1831, which names that particle only
+// calc_T1_T2_for_rot_8 as the particle slot, :1781 / :1836, which names that particle only
 // when the two indices coincide).  One block per request, threads over the polar angles.
 #include "pftcc_internal.cuh"
+#include "lbfgsb.h"
+
+#include <cmath>
+#include <vector>
 
 namespace pftcc {
 
@@ -35,15 +39,18 @@ __global__ void __launch_bounds__(OG_THREADS) k_cont_shift_grad(
     const float2 *__restrict__ refs_odd, const float2 *__restrict__ drefs_even, const float2 *__restrict__ drefs_odd,
     const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const uint8_t *__restrict__ iseven,
     const float *__restrict__ sqsums, const double *__restrict__ argtransf, const double *__restrict__ argtransf1,
-    double *__restrict__ out6 /* [nreq][6]: f, d/de1, d/de2, d/de3, d/dsx, d/dsy */)
+    int scratch, double *__restrict__ out6 /* [nreq][6]: f, d/de1, d/de2, d/de3, d/dsx, d/dsy */)
 {
     __shared__ double red[OG_THREADS / 32];
     const EuclidReq rq = reqs[blockIdx.x];
     const int N = g.N, P = g.P, K = g.K;
     const bool ev = iseven[rq.slot] != 0;
     const float2 *q = ptcls + (long long)rq.slot * K * P;
-    const float2 *r = (ev ? refs_even : refs_odd) + (long long)rq.iref * K * P;
-    const float2 *dr = (ev ? drefs_even : drefs_odd) + (long long)rq.iref * 3 * K * P;
+    // scratch: request b's own section and derivatives at refs_even / drefs_even + b
+    const float2 *r = scratch ? refs_even + (long long)blockIdx.x * K * P
+                              : (ev ? refs_even : refs_odd) + (long long)rq.iref * K * P;
+    const float2 *dr = scratch ? drefs_even + (long long)blockIdx.x * 3 * K * P
+                               : (ev ? drefs_even : drefs_odd) + (long long)rq.iref * 3 * K * P;
     const float *ctf = ctfmats ? ctfmats + (long long)rq.slot * K * P : nullptr;
     const int s = rq.irot - 1;
     double y = 0.0, sqr = 0.0, gx = 0.0, gy = 0.0, t1[3] = {0.0, 0.0, 0.0}, t2[3] = {0.0, 0.0, 0.0};
@@ -109,8 +116,129 @@ cudaError_t launch_cont_shift_grad(pftcc_handle *h, const EuclidReq *reqs_dev, i
     KTimer kt(h, PFTCC_K_EXACT);
     k_cont_shift_grad<<<nreq, OG_THREADS, 0, h->stream>>>(h->g, reqs_dev, h->refs_even, h->refs_odd, h->drefs_even,
                                                           h->drefs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums,
-                                                          h->argtransf, h->argtransf1, out6);
+                                                          h->argtransf, h->argtransf1, 0, out6);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// pftcc_orisrch_grad%minimize (simple_pftcc_orisrch_grad.f90:60-122) for n particles at once:
+// variables (e1, e2, e3 in degrees, sx, sy), box e +- angerr_deg and |s| <= maxHWshift, start
+// (e_in, 0, 0), cost -corr and gradient -grad of gencorr_cont_shift_grad_cc_for_rot_8 at
+// irot = 1 on the sections fdf_project_polar makes at the trial angles (fdfcostfun :178-207).
+// The gradient's angle components are per radian while the variables are degrees, as the
+// reference pairs them.  Every round, the pending trial points of all unfinished problems are
+// projected by ONE k_fdf_project_polar launch into per-request scratch sections and scored by
+// ONE k_cont_shift_grad launch.  A problem whose final cost is not below its starting cost keeps
+// its angles and returns a zero shift (:101-117); the shift found is rotated into the reference
+// frame by rotmat2d(e3) (:106-109).
+static int orisrch_eval(pftcc_handle *h, int nb, const int *slots, const double *xt, double *f, double *g5,
+                        float2 *scr_ref, float2 *scr_dref, double *dRD, EuclidReq *dreq, double *dout,
+                        std::vector<double> &RD, std::vector<EuclidReq> &rq, std::vector<double> &o)
+{
+    RD.resize((size_t)nb * 36);
+    rq.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        host_euler2m(&xt[5 * b], &RD[(size_t)b * 36], &RD[(size_t)b * 36 + 9]);
+        rq[b] = EuclidReq{0, slots[b], 1, 0, xt[5 * b + 3], xt[5 * b + 4]};
+    }
+    cudaError_t e = cudaMemcpyAsync(dRD, RD.data(), RD.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dreq, rq.data(), (size_t)nb * sizeof(EuclidReq), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = launch_fdf_project_polar(h, h->vol_box, h->vol_cube, dRD, nb, scr_ref, scr_dref);
+    if (e == cudaSuccess) {
+        const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
+        PFTCC_LAUNCH(h);
+        KTimer kt(h, PFTCC_K_EXACT);
+        k_cont_shift_grad<<<nb, OG_THREADS, 0, h->stream>>>(h->g, dreq, scr_ref, scr_ref, scr_dref, scr_dref,
+                                                             h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
+                                                             h->argtransf1, 1, dout);
+        e = cudaGetLastError();
+    }
+    o.resize((size_t)nb * 6);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(o.data(), dout, o.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_err(h, e, "orisrch evaluation");
+    for (int b = 0; b < nb; ++b) {
+        f[b] = -o[6 * (size_t)b];
+        for (int v = 0; v < 5; ++v) g5[5 * (size_t)b + v] = -o[6 * (size_t)b + 1 + v];
+    }
+    return PFTCC_OK;
+}
+
+int orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
+                  pftcc_orisrch_out *out)
+{
+    constexpr int NV = 5;
+    std::vector<int> slot(n);
+    std::vector<double> x0((size_t)n * NV), lb((size_t)n * NV), ub((size_t)n * NV);
+    for (int i = 0; i < n; ++i) {
+        slot[i] = -1;
+        if (req[i].iptcl >= h->pfrom && req[i].iptcl <= h->pto) slot[i] = h->pinds[req[i].iptcl - h->pfrom] - 1;
+        if (slot[i] < 0) return set_err(h, PFTCC_ERR_INDEX, "orisrch: particle not held");
+        for (int v = 0; v < 3; ++v) {
+            x0[(size_t)i * NV + v] = req[i].e[v];
+            lb[(size_t)i * NV + v] = req[i].e[v] - req[i].angerr_deg;
+            ub[(size_t)i * NV + v] = req[i].e[v] + req[i].angerr_deg;
+        }
+        for (int v = 3; v < 5; ++v) {
+            x0[(size_t)i * NV + v] = 0.0;
+            lb[(size_t)i * NV + v] = -req[i].maxhwshift;
+            ub[(size_t)i * NV + v] = req[i].maxhwshift;
+        }
+    }
+    // scratch for the largest round: n sections, their derivatives, matrices, requests, results
+    const size_t KP = (size_t)h->g.K * h->g.P;
+    float2 *scr = nullptr;
+    double *dRD = nullptr, *dout = nullptr;
+    EuclidReq *dreq = nullptr;
+    int st = dev_alloc(h, (void **)&scr, (size_t)n * 4 * KP * sizeof(float2), "orisrch sections");
+    if (st == PFTCC_OK) st = dev_alloc(h, (void **)&dRD, (size_t)n * 36 * sizeof(double), "orisrch matrices");
+    if (st == PFTCC_OK) st = dev_alloc(h, (void **)&dreq, (size_t)n * sizeof(EuclidReq), "orisrch requests");
+    if (st == PFTCC_OK) st = dev_alloc(h, (void **)&dout, (size_t)n * 6 * sizeof(double), "orisrch results");
+    std::vector<double> f0(n, 0.0);
+    std::vector<char> have_f0(n, 0);
+    if (st == PFTCC_OK) {
+        std::vector<int> sl;
+        std::vector<double> RD, o;
+        std::vector<EuclidReq> rq;
+        auto eval = [&](int nb, const int *idx, const double *xt, double *f, double *g) -> int {
+            sl.resize(nb);
+            for (int b = 0; b < nb; ++b) sl[b] = slot[idx[b]];
+            const int s2 = orisrch_eval(h, nb, sl.data(), xt, f, g, scr, scr + (size_t)n * KP, dRD, dreq, dout, RD,
+                                        rq, o);
+            if (s2 != PFTCC_OK) return s2;
+            for (int b = 0; b < nb; ++b)
+                if (!have_f0[idx[b]]) { have_f0[idx[b]] = 1; f0[idx[b]] = f[b]; }
+            return 0;
+        };
+        std::vector<lbfgsb::Result<NV>> res(n);
+        st = lbfgsb::minimize_batch(n, x0.data(), lb.data(), ub.data(), maxits, pgtol, factr, eval, res.data());
+        if (st == PFTCC_OK) {
+            for (int i = 0; i < n; ++i) {
+                pftcc_orisrch_out &q = out[i];
+                const bool better = res[i].f < f0[i];
+                q.found_better = better ? 1 : 0;
+                q.corr = better ? -res[i].f : -f0[i];
+                q.corr_init = -f0[i];
+                for (int v = 0; v < 3; ++v) q.e[v] = better ? res[i].x[v] : req[i].e[v];
+                q.shift[0] = q.shift[1] = 0.0;
+                if (better) {   // cxy(2:) = matmul(x(4:5), rotmat2d(x(3))), rotmat2d = [c s; -s c]
+                    const double a = res[i].x[2] * 3.14159265358979323846 / 180.0, c = std::cos(a), sn = std::sin(a);
+                    q.shift[0] = res[i].x[3] * c - res[i].x[4] * sn;
+                    q.shift[1] = res[i].x[3] * sn + res[i].x[4] * c;
+                }
+                q.nevals = res[i].nevals;
+                q.niter = res[i].niter;
+                q.converged = res[i].converged;
+                q.pad = 0;
+            }
+        }
+    }
+    dev_free(h, scr);
+    dev_free(h, dRD);
+    dev_free(h, dreq);
+    dev_free(h, dout);
+    return st;
 }
 
 }  // namespace pftcc

@@ -1,5 +1,5 @@
 // lbfgsb.h -- batched bound-constrained limited-memory BFGS for small problems
-// (three variables), host C++ with no CUDA dependency, in reverse communication: every
+// (a few variables), host C++ with no CUDA dependency, in reverse communication: every
 // round collects the pending cost+gradient requests of all unfinished problems and
 // hands them to ONE caller-supplied evaluation (the GPU adjoint launch for the
 // refinement; analytic functions or the oracle in the host tests).
@@ -26,13 +26,13 @@
 namespace pftcc {
 namespace lbfgsb {
 
-constexpr int NV = 3;
-
+template <int NV>
 struct Result {
     double x[NV], f;
     int nevals, niter, converged;
 };
 
+template <int NV>
 struct Prob {
     double x[NV], f = 0, g[NV];
     double lb[NV], ub[NV];
@@ -45,7 +45,8 @@ struct Prob {
     int converged = 0;
 };
 
-inline double proj_grad_norm(const Prob &p)
+template <int NV>
+inline double proj_grad_norm(const Prob<NV> &p)
 {
     double m = 0;
     for (int i = 0; i < NV; ++i) {
@@ -57,7 +58,8 @@ inline double proj_grad_norm(const Prob &p)
 }
 
 // dense B = BFGS updates of theta*I with the stored pairs (oldest first)
-inline void form_B(const Prob &p, double B[NV][NV])
+template <int NV>
+inline void form_B(const Prob<NV> &p, double B[NV][NV])
 {
     for (int i = 0; i < NV; ++i)
         for (int j = 0; j < NV; ++j) B[i][j] = i == j ? p.theta : 0.0;
@@ -77,7 +79,8 @@ inline void form_B(const Prob &p, double B[NV][NV])
 }
 
 // generalised Cauchy point, then the subspace minimiser backtracked into the box
-inline void direction(const Prob &p, double d[NV])
+template <int NV>
+inline void direction(const Prob<NV> &p, double d[NV])
 {
     double B[NV][NV];
     form_B(p, B);
@@ -89,7 +92,8 @@ inline void direction(const Prob &p, double d[NV])
         else tb[i] = DBL_MAX;
         if (tb[i] < 0) tb[i] = 0;
     }
-    int order[NV] = {0, 1, 2};
+    int order[NV];
+    for (int i = 0; i < NV; ++i) order[i] = i;
     std::sort(order, order + NV, [&](int a, int b) { return tb[a] < tb[b]; });
     double xc[NV], dir[NV];
     bool fixed[NV];
@@ -136,7 +140,7 @@ inline void direction(const Prob &p, double d[NV])
             r[i] = p.g[i];
             for (int j = 0; j < NV; ++j) r[i] += B[i][j] * (xc[j] - p.x[j]);
         }
-        // solve B_FF du = -r_F (Gaussian elimination with partial pivoting, nf <= 3)
+        // solve B_FF du = -r_F (Gaussian elimination with partial pivoting, nf <= NV)
         double A[NV][NV + 1];
         for (int a = 0; a < nf; ++a) {
             for (int b = 0; b < nf; ++b) A[a][b] = B[fr[a]][fr[b]];
@@ -175,13 +179,13 @@ inline void direction(const Prob &p, double d[NV])
 // evaluates the cost and its gradient of problems idx[0..nb) at the points xt[nb][NV]
 // into f[nb] and g[nb][NV] and returns 0, or a non-zero status that aborts the run.
 // The result of a problem does not depend on which other problems share the batch.
-template <class Eval>
+template <int NV, class Eval>
 int minimize_batch(int n, const double *x0, const double *lb, const double *ub, int maxits, double pgtol,
-                   double factr, Eval &&eval, Result *out)
+                   double factr, Eval &&eval, Result<NV> *out)
 {
     const double eps = DBL_EPSILON, ftol = 1e-3;
     const int mem = 15;
-    std::vector<Prob> P(n);
+    std::vector<Prob<NV>> P(n);
     for (int i = 0; i < n; ++i) {
         for (int v = 0; v < NV; ++v) {
             P[i].lb[v] = lb[i * NV + v];
@@ -206,7 +210,7 @@ int minimize_batch(int n, const double *x0, const double *lb, const double *ub, 
         const int st = eval((int)who.size(), who.data(), xt.data(), f.data(), g.data());
         if (st != 0) return st;
         for (size_t b = 0; b < who.size(); ++b) {
-            Prob &p = P[who[b]];
+            Prob<NV> &p = P[who[b]];
             const double ft = f[b];
             const double *gt = &g[NV * b];
             ++p.nevals;
@@ -275,7 +279,7 @@ int minimize_batch(int n, const double *x0, const double *lb, const double *ub, 
         }
     }
     for (int i = 0; i < n; ++i) {
-        Result &o = out[i];
+        Result<NV> &o = out[i];
         for (int v = 0; v < NV; ++v) o.x[v] = P[i].x[v];
         o.f = P[i].f;
         o.nevals = P[i].nevals;

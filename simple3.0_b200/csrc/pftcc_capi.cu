@@ -797,7 +797,7 @@ int pftcc_prep_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *img
 // euler2m (simple_ori.f90:1275-1284, rotmat :1350-1390): R = R3(e3) R2(e2) R1(e1), angles in
 // degrees, row-major; with dR, euler2dm (simple_ori_light.f90:87-147): dR/de1 = R3 R2 dR1,
 // dR/de2 = R3 dR2 R1, dR/de3 = dR3 R2 R1, the derivatives per radian (drotmat :107-146)
-static void host_euler2m(const double e[3], double *R, double *dR)
+void pftcc::host_euler2m(const double e[3], double *R, double *dR)
 {
     double m[3][9], d[3][9];
     for (int a = 0; a < 3; ++a) {
@@ -992,6 +992,28 @@ int pftcc_gencorr_cont_shift_grad_cc_for_rot_8(pftcc_handle *h, int iref, int ip
     if (!h || !shvec || !f || !grad) return set_err(h, PFTCC_ERR_ARG, "cont_shift_grad: bad arguments");
     pftcc_grad_req r{iref, iptcl, irot, 0, shvec[0], shvec[1], 0.0};
     return pftcc_cont_shift_grad_batch(h, 1, &r, f, grad);
+}
+
+int pftcc_orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
+                        pftcc_orisrch_out *out)
+{
+    if (!h || n < 0 || (n > 0 && (!req || !out)) || maxits < 1 || !(pgtol >= 0) || !(factr >= 0))
+        return set_err(h, PFTCC_ERR_ARG, "orisrch_batch: bad arguments");
+    for (int i = 0; i < n; ++i) {
+        bool ok = std::isfinite(req[i].angerr_deg) && req[i].angerr_deg >= 0 && std::isfinite(req[i].maxhwshift) &&
+                  req[i].maxhwshift >= 0;
+        for (int v = 0; v < 3; ++v) ok = ok && std::isfinite(req[i].e[v]);
+        if (!ok) return set_err(h, PFTCC_ERR_ARG, "orisrch_batch: angles and bounds must be finite and non-negative");
+    }
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the orientation gradient is served in the reference frame");
+    if (!h->vol_cube) return set_err(h, PFTCC_ERR_STATE, "orisrch_batch: no volume (set_volume_ft first)");
+    if (h->cfg.with_ctf && !h->ctf_ready)
+        return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    return orisrch_batch(h, n, req, maxits, pgtol, factr, out);
 }
 
 int pftcc_gencorr_cont_grad_cc_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,

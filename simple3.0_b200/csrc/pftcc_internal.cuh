@@ -223,6 +223,11 @@ int ingest_images(pftcc_handle *h, const float *imgs_dev, int n, int cap, int B,
                   const int *flag_dev, const pftcc_ctfparams *ctf_dev, float msk, float2 *cm_out);
 int ingest_batch_max(int B);
 void ingest_free(pftcc_handle *h);
+// euler2m (and with dR, euler2dm per radian) of Spider angles in degrees, row-major, FP64
+void host_euler2m(const double e[3], double *R, double *dR);
+// batched pftcc_orisrch_grad%minimize (k_orisrch.cu); the caller holds the lock
+int orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
+                  pftcc_orisrch_out *out);
 // sigma2_noise on the device and covering every held particle (rebuilt first when stale
 // and may_alloc); PFTCC_OK or the error code, with the message set
 int euclid_ready(pftcc_handle *h, int may_alloc);

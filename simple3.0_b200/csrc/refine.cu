@@ -14,7 +14,7 @@ namespace pftcc {
 int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub, int maxits,
                  double pgtol, double factr, pftcc_refine_out *out)
 {
-    using lbfgsb::NV;
+    constexpr int NV = 3;
     std::vector<double> x0((size_t)n * NV);
     for (int i = 0; i < n; ++i)
         for (int v = 0; v < NV; ++v) x0[(size_t)i * NV + v] = req[i].x0[v];
@@ -36,7 +36,7 @@ int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const doub
         }
         return 0;
     };
-    std::vector<lbfgsb::Result> res(n);
+    std::vector<lbfgsb::Result<NV>> res(n);
     const int st = lbfgsb::minimize_batch(n, x0.data(), lb, ub, maxits, pgtol, factr, eval, res.data());
     if (st != 0) return st;
     for (int i = 0; i < n; ++i) {

@@ -489,6 +489,28 @@ class polarft_corrcalc:
                                                         g.ctypes.data_as(C.POINTER(C.c_double))))
         return f, g
 
+    def orisrch_batch(self, iptcl, e, angerr_deg, maxhwshift, maxits: int = 100, pgtol: float = 1e-5,
+                      factr: float = 1e7):
+        """pftcc_orisrch_grad%minimize for arrays of particles (n,) from Euler angles e (n, 3) in
+        degrees: list of dicts with e, shift (rotated into the reference frame), corr, corr_init,
+        found_better, nevals, niter, converged"""
+        ip = np.atleast_1d(np.asarray(iptcl, np.int64))
+        ee = np.asarray(e, np.float64).reshape(-1, 3)
+        n = ip.size
+        ang = np.broadcast_to(np.asarray(angerr_deg, np.float64), (n,))
+        msh = np.broadcast_to(np.asarray(maxhwshift, np.float64), (n,))
+        req = (_lib.OrisrchReq * n)()
+        for i in range(n):
+            req[i].iptcl = int(ip[i])
+            for v in range(3):
+                req[i].e[v] = float(ee[i, v])
+            req[i].angerr_deg, req[i].maxhwshift = float(ang[i]), float(msh[i])
+        out = (_lib.OrisrchOut * n)()
+        self._check(self._L.pftcc_orisrch_batch(self._h, n, req, int(maxits), float(pgtol), float(factr), out))
+        return [dict(e=np.array(o.e[:]), shift=np.array(o.shift[:]), corr=o.corr, corr_init=o.corr_init,
+                     found_better=bool(o.found_better), nevals=o.nevals, niter=o.niter, converged=bool(o.converged))
+                for o in out]
+
     def gencorr_cont_shift_grad_cc_for_rot_8(self, iref: int, iptcl: int, shvec, irot: int):
         f = C.c_double()
         g = np.zeros(5, np.float64)

@@ -11,7 +11,7 @@ typedef int (*lbfgsb_eval_fn)(int nb, const int *idx, const double *xt, double *
 int lbfgsb_run(int n, const double *x0, const double *lb, const double *ub, int maxits, double pgtol, double factr,
                lbfgsb_eval_fn cb, double *x_out, double *f_out, int *nevals, int *niter, int *converged)
 {
-    std::vector<pftcc::lbfgsb::Result> res(n);
+    std::vector<pftcc::lbfgsb::Result<3>> res(n);
     auto eval = [&](int nb, const int *idx, const double *xt, double *f, double *g) { return cb(nb, idx, xt, f, g); };
     const int st = pftcc::lbfgsb::minimize_batch(n, x0, lb, ub, maxits, pgtol, factr, eval, res.data());
     for (int i = 0; i < n; ++i) {

@@ -118,3 +118,47 @@ def test_orisrch_state_errors(pkg):
         assert e.value.status == pkg._lib.ERR_INDEX
     finally:
         pc.kill()
+
+
+def _smooth_vol(box, seed, sigma=5.0):
+    """a random volume FT under a Gaussian low-pass: broad correlation peaks in angle"""
+    v = _vol(box, seed)
+    f = np.fft.fftfreq(box) * box
+    h = np.arange(box // 2 + 1)
+    r2 = f[:, None, None] ** 2 + f[None, :, None] ** 2 + h[None, None, :] ** 2
+    return (v * np.exp(-r2 / (2 * sigma ** 2))).astype(np.complex64)
+
+
+def test_orisrch_batch_recovers_orientation(pkg):
+    """particles made as sections of the volume at known angles (zero shifts), searched from
+    perturbed starts: the search improves the correlation, moves the angles towards the truth,
+    and its reported correlation is the correlator's value at the reported point"""
+    box, nrots, kto, n = 64, 128, 14, 5
+    vol = _smooth_vol(box, 21)
+    rng = np.random.default_rng(4)
+    truth = np.stack([rng.uniform(20, 340, n), rng.uniform(30, 150, n), rng.uniform(20, 340, n)], 1)
+    pc = pkg.polarft_corrcalc()
+    pc.new(n + 1, (1, n), box=box, nrots=nrots, kfromto=(2, kto), ctf=False, ctf_frame="ref")
+    try:
+        pc.set_volume_ft(vol)
+        pc.fproject_polar(1, truth.astype(np.float32), iseven=True)
+        for i in range(n):
+            pc.set_ptcl_pft(i + 1, pc.get_ref_pft(i + 1, True))
+        start = truth + rng.uniform(-2.0, 2.0, (n, 3))
+        res = pc.orisrch_batch(np.arange(1, n + 1), start, angerr_deg=6.0, maxhwshift=2.0, maxits=60)
+        for i, r in enumerate(res):
+            assert r["found_better"] and r["corr"] > r["corr_init"]
+            assert np.max(np.abs(r["e"] - truth[i])) < np.max(np.abs(start[i] - truth[i]))
+            assert r["corr"] > 0.99
+            # the reported value is the correlator's at the reported point: undo rotmat2d(e3)
+            a = np.radians(r["e"][2])
+            M = np.array([[np.cos(a), np.sin(a)], [-np.sin(a), np.cos(a)]])
+            x45 = r["shift"] @ M.T
+            pc.fdf_project_polar(n + 1, r["e"][None], iseven=True)
+            f, _ = pc.gencorr_cont_shift_grad_cc_for_rot_8(n + 1, i + 1, x45, 1)
+            assert abs(f - r["corr"]) < 1e-9
+        # a search started at the truth cannot improve beyond rounding
+        res0 = pc.orisrch_batch([1], truth[:1], angerr_deg=6.0, maxhwshift=2.0)
+        assert res0[0]["corr"] - res0[0]["corr_init"] < 1e-6
+    finally:
+        pc.kill()
