@@ -686,6 +686,30 @@ def run_euclid_report(args):
     out["oracle_seconds_per_pair_1_thread"] = (time.perf_counter() - t0) / 3
     out["parity_max_scaled_err_vs_oracle"] = worst
     pc.kill()
+    # the m-domain search (particle CTF frame, BF16 hi+lo products, FP32 re-score of the top 8)
+    # over a 9 x 9 shift grid under both objectives
+    pc = pkg.polarft_corrcalc()
+    pc.new(w.nrefs, (1, w.nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True, ctf_frame="ptcl")
+    pc.set_refs(1, refs, True)
+    pc.set_refs(1, refs, False)
+    pc.polarize_ptcls(0, parts.cmat.numpy())
+    pc.create_polar_absctfmats(pkg.ctfparams_array(w.nptcls, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                   dfx=parts.dfx, dfy=parts.dfy, angast=parts.angast))
+    pc.assign_sigma2_noise(sig)
+    grid = np.array(w.shift_grid, np.float32).reshape(-1, 2)
+    evals_md = w.nptcls * w.nrefs * len(grid) * w.nrots
+    out["mdomain_nshifts"] = len(grid)
+    for name, obj in (("cc", pkg._lib.OBJFUN_CC), ("euclid", pkg._lib.OBJFUN_EUCLID)):
+        pc.set_objfun(obj)
+        pc.search_best(grid, "bf16x3", ntop=8)
+        t0 = time.perf_counter()
+        reps = 5
+        for _ in range(reps):
+            pc.search_best(grid, "bf16x3", ntop=8)
+        dt = (time.perf_counter() - t0) / reps
+        out[f"mdomain_search_{name}_seconds"] = dt
+        out[f"mdomain_search_{name}_evals_per_s"] = evals_md / dt
+    pc.kill()
     print(json.dumps(out), flush=True)
 
 

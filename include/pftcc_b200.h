@@ -204,7 +204,10 @@ int pftcc_orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, in
 /* params_glob%cc_objfun: PFTCC_OBJFUN_EUCLID makes pftcc_gencorrs, pftcc_gencorr_for_rot(_8),
  * pftcc_gencorr_grad(_only)_for_rot_8 and the PFTCC_PREC_EXACT batched searches evaluate the
  * Euclidean objective, as gencorrs_1/_2 (:1594-1617), gencorr_for_rot(_8) (:1619-1643) and
- * gencorr_grad(_only)_for_rot_8 (:1849-1939) dispatch on it */
+ * gencorr_grad(_only)_for_rot_8 (:1849-1939) dispatch on it (reference frame).  On a
+ * particle-frame handle the FP32 / BF16X3 batched searches evaluate it instead, with the CTF at
+ * the particle's polar index: -1/2 sum_k w_k sum_n |ref shmat ctf~(n+rot) - ptcl~(n+rot)|^2,
+ * w_k = pxls(k) / (P sigma2(k)) (the exact and per-pair calls refuse it there) */
 int pftcc_set_objfun(pftcc_handle *h, int objfun);
 /* assign_sigma2_noise (:581-585): sigma2_noise(kfrom:kto, fromp:top), column-major, i.e.
  * [top - fromp + 1][kto - kfrom + 1].  The values are copied: assign again after changing them.

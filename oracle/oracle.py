@@ -83,6 +83,7 @@ def lib():
         L.orc_fproject_polar.argtypes = [G, fp, C.c_int, fp, dp, ip, C.c_int, dp]
         L.orc_pxls_p_shell.argtypes = [C.c_int, C.c_int, dp]
         L.orc_gencorrs_euclid.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
+        L.orc_gencorrs_euclid_ptclframe.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
         L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
         L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
         L.orc_prepimg4align.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.POINTER(Ctf), dp]
@@ -212,6 +213,17 @@ def gencorrs_euclid(g: Geom, t: Tables, ref, ptcl, sigma2, ctf=None, shvec=None)
                               _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double),
                               _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double), _P(sig, C.c_double),
                               _P(pxls_p_shell(g), C.c_double), _P(out, C.c_double))
+    return out
+
+
+def gencorrs_euclid_ptclframe(g: Geom, t: Tables, ref, ptcl, sigma2, ctf=None, shvec=None) -> np.ndarray:
+    """the Euclidean objective in the particle CTF frame (the m-domain search's), every rotation"""
+    out = np.zeros(g.nrots, np.float64)
+    sig = np.ascontiguousarray(sigma2, np.float64)
+    lib().orc_gencorrs_euclid_ptclframe(C.byref(g), _P(_c64(ref), C.c_float), _P(_c64(ptcl), C.c_float),
+                                        _P(_ctf_arg(ctf), C.c_double), _P(_shv(shvec), C.c_double),
+                                        _P(t.argtransf, C.c_double), _P(t.argtransf1, C.c_double),
+                                        _P(sig, C.c_double), _P(pxls_p_shell(g), C.c_double), _P(out, C.c_double))
     return out
 
 

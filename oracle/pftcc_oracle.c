@@ -1295,3 +1295,31 @@ void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, doub
     free(z);
     free(r);
 }
+
+void orc_gencorrs_euclid_ptclframe(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                                   const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                                   const double *sigma2, const double *pxls, double *euclids)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    double *pr = (double *)malloc(sizeof(double) * 2 * K * P);
+    prep_ref(g, ref, NULL, shvec, argtransf, argtransf_shellone, pr);   /* A = ref * shmat */
+    for (int s = 0; s < N; ++s) {
+        double acc = 0.0;
+        for (int ik = 0; ik < Ks; ++ik) {
+            const double w = pxls[ik] / (double)P / sigma2[ik];
+            const double *a = pr + 2 * ik * P;
+            const float *q = ptcl + 2 * ik * P;
+            double e = 0.0;
+            for (int n = 0; n < P; ++n) {
+                const int j = (n + s) % N, jp = j % P;
+                const double c = ctfmat ? ctfmat[ik * P + jp] : 1.0;
+                const double qr = q[2 * jp], qi = j < P ? q[2 * jp + 1] : -q[2 * jp + 1];
+                const double dr = a[2 * n] * c - qr, di = a[2 * n + 1] * c - qi;
+                e += dr * dr + di * di;
+            }
+            acc += w * e;
+        }
+        euclids[s] = -0.5 * acc;
+    }
+    free(pr);
+}

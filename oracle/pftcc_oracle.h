@@ -159,6 +159,12 @@ void orc_pxls_p_shell(int kfrom, int kto, double *pxls);
 void orc_gencorrs_euclid(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
                          const double *shvec, const double *argtransf, const double *argtransf_shellone,
                          const double *sigma2, const double *pxls, double *euclids);
+/* the Euclidean objective in the particle CTF frame (the m-domain search's frame): the CTF at the
+ * particle's polar index, euclid(s) = -1/2 sum_{k<=kstop} w_k sum_n |A(n) ctf~(n+s) - ptcl~(n+s)|^2,
+ * A = ref * shmat, w_k = pxls(k) / (P sigma2(k)); equal to gencorrs_euclid_2 for an isotropic CTF */
+void orc_gencorrs_euclid_ptclframe(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,
+                                   const double *shvec, const double *argtransf, const double *argtransf_shellone,
+                                   const double *sigma2, const double *pxls, double *euclids);
 /* gencorr_euclid_grad_for_rot_8 (:2071-2109): f = calc_euclid_for_rot_8 (:1308-1334),
  * grad[2] = d f / d(sx, sy); gencorr_euclid_for_rot_8 (:2026-2048) is f alone */
 void orc_gencorr_euclid_grad_for_rot(const orc_geom *g, const float *ref, const float *ptcl, const double *ctfmat,

@@ -45,11 +45,11 @@ int stage2_fast_p2(int P);
 int stage2_fast_dlen(int P);
 cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
                                int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
-                               float2 *cand, float *ccall, const int *perm);
+                               float2 *cand, float *ccall, const int *perm, int eu);
 cudaError_t launch_rescore_md(pftcc_handle *h, int P, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
                               const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
                               const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
-                              pftcc_best *out);
+                              pftcc_best *out, int eu);
 
 static constexpr int MAXF = 12;
 struct FFTPlan {
@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
 template <int N1, int N2>
 __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg, int nr, int c0, int ncols, int dcols,
                                                   const float *__restrict__ sqp, float *__restrict__ D, int p2,
-                                                  double dscale)
+                                                  double dscale, int eu)
 {
     constexpr int H = N1 * N2, P = 2 * H, J = H + 1;
     constexpr int NB = 256 / (N1 > N2 ? N1 : N2);
@@ -809,7 +809,9 @@ __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg
                     if (p2 == 0) {
                         dst[rho] = y;
                     } else {
-                        const float v = (float)dscale * y;
+                        // the Euclidean objective: the additive term -(D + sum_k w_k |ptcl_k|^2) / 2,
+                        // sq holding the weighted particle term
+                        const float v = eu ? (float)(-0.5 * (d + sq)) : (float)dscale * y;
 #pragma unroll
                         for (int hh = 0; hh < 2; ++hh) {   // rot = rho and rho + P
                             const int rot = rho + hh * P, lr = rot >> 1, l2 = lr % p2;
@@ -826,19 +828,19 @@ __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg
 
 template <int N1, int N2>
 static cudaError_t launch_norm_fft(pftcc_handle *h, const double2 *Y, int nr, int c0, int ncols, int dcols,
-                                   const float *sqp, float *D, int p2, double dscale)
+                                   const float *sqp, float *D, int p2, double dscale, int eu)
 {
     constexpr int H = N1 * N2, NB = 256 / (N1 > N2 ? N1 : N2);
     const size_t smem = (size_t)(2 * H + NB * N2 * (N1 + 1)) * sizeof(double2);
     cudaError_t e = smem_limit((const void *)k_norm_fft<N1, N2>, smem);
     if (e != cudaSuccess) return e;
-    k_norm_fft<N1, N2><<<ncols, 256, smem, h->stream>>>(Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    k_norm_fft<N1, N2><<<ncols, 256, smem, h->stream>>>(Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
     return cudaGetLastError();
 }
 
 static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU, const double2 *CV, int r0, int nr,
                                int c0, int ncols, int dcols, const float *sqp, double2 *Y, float *D, int p2,
-                               double dscale)
+                               double dscale, int eu)
 {
     const int J = g.P / 2 + 1;
     cudaError_t e;
@@ -853,11 +855,12 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU
     }
     PFTCC_LAUNCH(h);
     switch (g.P) {
-    case 64: return launch_norm_fft<8, 4>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
-    case 180: return launch_norm_fft<10, 9>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
-    case 300: return launch_norm_fft<15, 10>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale);
+    case 64: return launch_norm_fft<8, 4>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
+    case 180: return launch_norm_fft<10, 9>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
+    case 300: return launch_norm_fft<15, 10>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
     default: break;
     }
+    if (eu) return cudaErrorInvalidValue;   // the Euclidean objective needs the transform lengths above
     const size_t smem = ((size_t)NORM_RB * (J | 1) + g.P) * sizeof(double2);
     if (g.P % 4 == 0) {
         if ((e = smem_limit((const void *)k_norm<4>, smem))) return e;
@@ -1066,13 +1069,60 @@ static int ensure_ws(pftcc_handle *h, void **p, size_t bytes, const char *what)
 
 struct WsSizes { size_t UA, UB, RU, CV, D, X, cand, sqp, perm; };
 
+// The Euclidean objective in the particle CTF frame (gencorrs_euclid_1/_2 with the CTF at the
+// particle's polar index, as the correlation of this search): for column c (particle slot perm[c])
+// the shell weights w_k = pxls(k) / (P sigma2(k)) scale its spectra UB (the correlation term) and
+// CV (CTF^2, the reference-energy term), and sqp[c] becomes sum_{k<=kstop} w_k sum_n |ptcl(n,k)|^2,
+// so that the search scores sum_k w_k (corr_k - (E_ref,k(rot) + E_ptcl,k) / 2).  One block per column.
+__global__ void __launch_bounds__(256) k_euclid_weigh(Geom g, int np, int cols_pad, int M, const int *__restrict__ perm,
+                                                      const float *__restrict__ sig2, const float *__restrict__ pxls,
+                                                      const float2 *__restrict__ ptcls, float2 *__restrict__ UB,
+                                                      double2 *__restrict__ CV, float *__restrict__ sqp)
+{
+    __shared__ double w[64];
+    __shared__ double red[8];
+    const int c = blockIdx.x;
+    if (c >= np) return;
+    const int slot = perm[c], Ks = g.Ks, P = g.P, J = P / 2 + 1;
+    for (int k = threadIdx.x; k < Ks; k += blockDim.x)
+        w[k] = (double)pxls[k] / ((double)P * (double)sig2[(size_t)slot * g.K + k]);
+    __syncthreads();
+    for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
+        const int m = e / Ks, k = e - m * Ks;
+        float2 *u = UB + ((size_t)m * cols_pad + c) * Ks + k;
+        const float wk = (float)w[k];
+        *u = make_float2(u->x * wk, u->y * wk);
+    }
+    for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) {
+        const int k = e % Ks;
+        double2 *v = CV + (size_t)c * J * Ks + e;
+        *v = make_double2(v->x * w[k], v->y * w[k]);
+    }
+    double s = 0.0;
+    const float2 *q = ptcls + (size_t)slot * g.K * P;
+    for (int e = threadIdx.x; e < Ks * P; e += blockDim.x) {
+        const float2 v = q[e];
+        s += w[e / P] * ((double)v.x * v.x + (double)v.y * v.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < 8; ++i) t += red[i];
+        sqp[c] = (float)t;
+    }
+}
+
 int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, int precision, int ntop, pftcc_best *out_dev,
                    float *ccall_dev)
 {
     const Geom &g = h->g;
     const int N = g.N, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
-    if (h->objfun == PFTCC_OBJFUN_EUCLID)
-        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the Euclidean objective is served by PFTCC_PREC_EXACT");
+    const int eu = h->objfun == PFTCC_OBJFUN_EUCLID;
+    if (eu && (h->cfg.ctf_frame != PFTCC_FRAME_PTCL || !stage2_fast_supported(P)))
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the m-domain Euclidean objective is served in the particle CTF frame "
+                                                 "for nrots/2 in {64, 180, 300}; use PFTCC_PREC_EXACT in the reference frame");
     if (Ks > 64) return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search supports at most 64 shells");
     const FFTPlan plan = make_plan(P);
     for (int i = 0; i < plan.nf; ++i)
@@ -1139,6 +1189,12 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     {
         KTimer kt(h, PFTCC_K_SPEC_PTCL);
         CKE(launch_spec_ptcl(h, g, ctf, d_perm, np, cols_pad, ws.UB, ws.CV, ws.sqp), "spec_ptcl");
+        if (eu) {   // shell weights into the particle side, the weighted particle term into sqp
+            PFTCC_LAUNCH(h);
+            k_euclid_weigh<<<np, 256, 0, h->stream>>>(g, np, cols_pad, M, d_perm, h->d_sig2, h->d_pxls, h->ptcls,
+                                                      ws.UB, ws.CV, ws.sqp);
+            CKE(cudaGetLastError(), "euclid weights");
+        }
         PFTCC_LAUNCH(h);
         k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
         CKE(cudaGetLastError(), "cand_init");
@@ -1192,10 +1248,10 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                 }
                 // the split-radix stage 2 reads the factor in its visiting order, times 1/(2N)
                 CKE(launch_norm(h, g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t, ws.sqp, ws.Yn, ws.D,
-                                fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N)), "norm");
+                                fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N), eu), "norm");
                 if (fast_s2) {
                     e = launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,
-                                           ws.cand, ccall_dev, d_perm);
+                                           ws.cand, ccall_dev, d_perm, eu);
                     if (e != cudaSuccess)
                         return set_err(h, e == cudaErrorMemoryAllocation ? PFTCC_ERR_OOM : PFTCC_ERR_CUDA,
                                        "stage2 (P " + std::to_string(P) + ", rows " + std::to_string(rows) + ", columns " +
@@ -1214,7 +1270,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         // overwrites them)
         if (md_rescore && out_dev)
             CKE(launch_rescore_md(h, P, gc1 - gc0, ntop, Ks, ns, nshifts_in > 0, ws.UA, rows_pad, ws.UB, cols_pad,
-                                  ws.RU, ws.CV, ws.sqp, ws.cand, d_perm, gc0, out_dev), "rescore");
+                                  ws.RU, ws.CV, ws.sqp, ws.cand, d_perm, gc0, out_dev, eu), "rescore");
     }
     if (precision == PFTCC_PREC_BF16X3) {
         int st = umma_check(h);
@@ -1229,6 +1285,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         CKE(cudaGetLastError(), "finish");
         return PFTCC_OK;
     }
+    if (eu) return set_err(h, PFTCC_ERR_UNSUPPORTED, "the m-domain Euclidean objective re-scores in the m-domain");
     int st = ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)np * ntop * sizeof(Work), 4096), "work");
     if (st) return st;
     st = ensure(h, (void **)&h->d_groups, &h->group_cap, std::max<size_t>((size_t)np * sizeof(Group), 256), "groups");

@@ -367,8 +367,9 @@ __device__ __forceinline__ void passA_mid(const GetX &getx, float2 *slab, int T,
     }
 }
 
-// pass B for l2 in [L0, L1): length-P1 DFTs, correlations, argmax (lowest rotation on ties)
-template <int P1, int P2, class Dinv>
+// pass B for l2 in [L0, L1): length-P1 DFTs, correlations, argmax (lowest rotation on ties).
+// EU (the Euclidean objective): dinv(rho) is the additive term, the value scale * v + dinv(rho)
+template <int P1, int P2, class Dinv, bool EU = false>
 __device__ __forceinline__ void passB(int L0, int L1, const float2 *slab, int T, const TwTables &tw, const Dinv &dinv,
                                       float scale, float *cc_out, float &best, int &brot)
 {
@@ -383,8 +384,10 @@ __device__ __forceinline__ void passB(int L0, int L1, const float2 *slab, int T,
         for (int l1 = 0; l1 < P1; ++l1) {
             const int l = l2 + P2 * l1;
             const int r0 = 2 * l, r1 = 2 * l + 1;
-            const float c0 = scale * v[l1].x * dinv(r0 < P ? r0 : r0 - P);
-            const float c1 = scale * v[l1].y * dinv(r1 < P ? r1 : r1 - P);
+            const float c0 = EU ? fmaf(scale, v[l1].x, dinv(r0 < P ? r0 : r0 - P))
+                                : scale * v[l1].x * dinv(r0 < P ? r0 : r0 - P);
+            const float c1 = EU ? fmaf(scale, v[l1].y, dinv(r1 < P ? r1 : r1 - P))
+                                : scale * v[l1].y * dinv(r1 < P ? r1 : r1 - P);
             if (cc_out) { cc_out[r0] = c0; cc_out[r1] = c1; }
             if (c0 > best || (c0 == best && r0 < brot)) { best = c0; brot = r0; }
             if (c1 > best || (c1 == best && r1 < brot)) { best = c1; brot = r1; }
@@ -395,10 +398,11 @@ __device__ __forceinline__ void passB(int L0, int L1, const float2 *slab, int T,
 // pass B on the block pair (l, l + 1), l even: two length-P1 DFTs (one per lane) of the
 // slab blocks, times the normalising factors -- stored in pair order, four per l1:
 // (l, re), (l + 1, re), (l, im), (l + 1, im), already carrying the 1/(2N) scale -- leaving
-// the correlation of rot = 2 (l + lane + P2 l1) + part in lane `lane` of v[l1].r / v[l1].i
-template <int P1, int P2>
+// the correlation of rot = 2 (l + lane + P2 l1) + part in lane `lane` of v[l1].r / v[l1].i.
+// EU: the factors are the Euclidean objective's additive terms, the value escale * v + d
+template <int P1, int P2, bool EU>
 __device__ __forceinline__ void passB_pair(int l, const float2 *slab, int T, const TwTables &tw, const float4 *Dp,
-                                           C2 (&v)[P1])
+                                           float escale, C2 (&v)[P1])
 {
     const float4 *dq = Dp + (size_t)(l >> 1) * P1;
     float4 d[P1];
@@ -408,10 +412,19 @@ __device__ __forceinline__ void passB_pair(int l, const float2 *slab, int T, con
 #pragma unroll
     for (int j1 = 0; j1 < P1; ++j1) v[j1] = {sq[(2 * j1) * T], sq[(2 * j1 + 1) * T]};
     PFFT<P1, P2>::run(v, tw);
+    if constexpr (EU) {
+        const float2 sc = f2_s(escale);
 #pragma unroll
-    for (int l1 = 0; l1 < P1; ++l1) {
-        v[l1].r = f2_mul(v[l1].r, make_float2(d[l1].x, d[l1].y));
-        v[l1].i = f2_mul(v[l1].i, make_float2(d[l1].z, d[l1].w));
+        for (int l1 = 0; l1 < P1; ++l1) {
+            v[l1].r = f2_fma(v[l1].r, sc, make_float2(d[l1].x, d[l1].y));
+            v[l1].i = f2_fma(v[l1].i, sc, make_float2(d[l1].z, d[l1].w));
+        }
+    } else {
+#pragma unroll
+        for (int l1 = 0; l1 < P1; ++l1) {
+            v[l1].r = f2_mul(v[l1].r, make_float2(d[l1].x, d[l1].y));
+            v[l1].i = f2_mul(v[l1].i, make_float2(d[l1].z, d[l1].w));
+        }
     }
 }
 
@@ -421,9 +434,9 @@ __device__ __forceinline__ void passB_pair(int l, const float2 *slab, int T, con
 // with max; afterwards the winning pair -- every pair when another one reached the same
 // maximum -- is evaluated again by the same code (identical values) and scanned for the
 // lowest rotation holding the maximum.
-template <int P1, int P2>
+template <int P1, int P2, bool EU>
 __device__ __forceinline__ void passB_search(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
-                                             const float4 *Dp, float &best, int &brot)
+                                             const float4 *Dp, float escale, float &best, int &brot)
 {
     float bv = -INFINITY;
     int bl = -1, l = L0, lend = L1, stage = 0, rmin = 0x7fffffff;
@@ -431,7 +444,7 @@ __device__ __forceinline__ void passB_search(int L0, int L1, const float2 *slab,
 #pragma unroll 1
     while (true) {
         C2 v[P1];
-        passB_pair<P1, P2>(l, slab, T, tw, Dp, v);
+        passB_pair<P1, P2, EU>(l, slab, T, tw, Dp, escale, v);
         if (stage == 0) {
             float m = fmaxf(v[0].r.x, v[0].r.y);
             m = max3f(m, v[0].i.x, v[0].i.y);
@@ -467,14 +480,14 @@ __device__ __forceinline__ void passB_search(int L0, int L1, const float2 *slab,
 }
 
 // pass B writing every correlation (corr_all), with the per-rotation argmax
-template <int P1, int P2>
+template <int P1, int P2, bool EU>
 __device__ __forceinline__ void passB_all(int L0, int L1, const float2 *slab, int T, const TwTables &tw,
-                                          const float4 *Dp, float *cc_out, float &best, int &brot)
+                                          const float4 *Dp, float escale, float *cc_out, float &best, int &brot)
 {
 #pragma unroll 1
     for (int l = L0; l < L1; l += 2) {
         C2 v[P1];
-        passB_pair<P1, P2>(l, slab, T, tw, Dp, v);
+        passB_pair<P1, P2, EU>(l, slab, T, tw, Dp, escale, v);
         const bool two = l + 1 < P2;
 #pragma unroll
         for (int l1 = 0; l1 < P1; ++l1) {
@@ -511,6 +524,7 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
 // ---------------------------------------------------------------------------------------
 struct S2Fast {
     int rows, xrows, xcols, row0, nshifts, r0, dcols, col0, N, nrs_total;
+    float escale;   // the Euclidean objective: the transform's scale 1/(2N) (the factors are additive)
 };
 
 // the normalising factors per (reference, particle) in the order the search's pass B
@@ -529,7 +543,7 @@ __device__ __forceinline__ bool ranks_above(float c, int id, float c2, int id2) 
 // roles 1.. hand their argmax over).  Role 0 keeps its rows' running top-8 in registers; at
 // the end the block merges those lists with the particle's running top-8.
 // X here is the packed spectrum Z, P planes of [col][row].
-template <int P1, int P2, int ROWS, int NT, bool WRITE>
+template <int P1, int P2, int ROWS, int NT, bool WRITE, bool EU>
 __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
                                                             const float *__restrict__ Dinv, float2 *__restrict__ cand,
                                                             float *__restrict__ ccall, const int *__restrict__ perm)
@@ -592,9 +606,9 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
         if (active) {
             if constexpr (WRITE) {
                 float *cc_out = ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N;
-                passB_all<P1, P2>(lb0, lb1, slab, ROWS, tw, Dr, cc_out, best, brot);
+                passB_all<P1, P2, EU>(lb0, lb1, slab, ROWS, tw, Dr, sp.escale, cc_out, best, brot);
             } else {
-                passB_search<P1, P2>(lb0, lb1, slab, ROWS, tw, Dr, best, brot);
+                passB_search<P1, P2, EU>(lb0, lb1, slab, ROWS, tw, Dr, sp.escale, best, brot);
             }
             if (role > 0) { xfer_c[(role - 1) * ROWS + lr] = best; xfer_r[(role - 1) * ROWS + lr] = brot; }
         }
@@ -689,7 +703,7 @@ template <int P1, int P2> __host__ __device__ constexpr size_t rescore_smem_byte
            sizeof(float2) * ((size_t)RS_MAX * (P + 1) + (size_t)P * RS_MAX) + sizeof(float) * (size_t)RS_MAX * P;
 }
 
-template <int P1, int P2>
+template <int P1, int P2, bool EU>
 __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, int Ks, int N, int nshifts,
                                                            int has_shifts, const TwTables tw,
                                                            const float2 *__restrict__ UA, int rows_pad,
@@ -784,8 +798,13 @@ __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, 
 #pragma unroll
         for (int k1 = 0; k1 < H1; ++k1) {
             const int l = k2 + H2 * k1;
-            Ds[c * P + 2 * l] = (float)(1.0 / sqrt(x[k1].x * sq));
-            Ds[c * P + 2 * l + 1] = (float)(1.0 / sqrt(-x[k1].y * sq));
+            if constexpr (EU) {   // -(D + sum_k w_k |ptcl_k|^2) / 2
+                Ds[c * P + 2 * l] = (float)(-0.5 * (x[k1].x + sq));
+                Ds[c * P + 2 * l + 1] = (float)(-0.5 * (-x[k1].y + sq));
+            } else {
+                Ds[c * P + 2 * l] = (float)(1.0 / sqrt(x[k1].x * sq));
+                Ds[c * P + 2 * l + 1] = (float)(1.0 / sqrt(-x[k1].y * sq));
+            }
         }
     }
     // C: X
@@ -830,8 +849,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, 
         }
         __syncwarp();
         if (rs >= 0)
-            passB<P1, P2>(half ? LB : 0, half ? P2 : LB, sl, RS_MAX, tw, dinv, 1.0f / (2.0f * (float)N), nullptr, best,
-                          brot);
+            passB<P1, P2, decltype(dinv), EU>(half ? LB : 0, half ? P2 : LB, sl, RS_MAX, tw, dinv,
+                                              1.0f / (2.0f * (float)N), nullptr, best, brot);
         const float ob = __shfl_xor_sync(0xffffffffu, best, 1);
         const int orot = __shfl_xor_sync(0xffffffffu, brot, 1);
         if (ob > best || (ob == best && orot < brot)) { best = ob; brot = orot; }
@@ -893,7 +912,7 @@ int stage2_fast_dlen(int P)
 
 template <int P1, int P2>
 static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
-                             float2 *cand, float *ccall, const int *perm)
+                             float2 *cand, float *ccall, const int *perm, bool eu)
 {
     if ((unsigned long long)P1 * P2 * sp.xcols * sp.xrows >= (1ull << 32)) return cudaErrorInvalidValue;
     TwTables tw;
@@ -905,7 +924,8 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
     const size_t smem = (size_t)((P2 + 1) / 2) * P1 * 2 * ROWS * sizeof(float2) +
                         (size_t)P1 * P2 * (sizeof(float4) + sizeof(float2)) +
                         (size_t)(NT - 1) * ROWS * (sizeof(float) + sizeof(int));
-    auto kern = ccall ? k_stage2_fast<P1, P2, ROWS, NT, true> : k_stage2_fast<P1, P2, ROWS, NT, false>;
+    auto kern = ccall ? (eu ? k_stage2_fast<P1, P2, ROWS, NT, true, true> : k_stage2_fast<P1, P2, ROWS, NT, true, false>)
+                      : (eu ? k_stage2_fast<P1, P2, ROWS, NT, false, true> : k_stage2_fast<P1, P2, ROWS, NT, false, false>);
     cudaError_t e = smem_limit((const void *)kern, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
@@ -916,18 +936,18 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
 
 cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
                                int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
-                               float2 *cand, float *ccall, const int *perm)
+                               float2 *cand, float *ccall, const int *perm, int eu)
 {
-    S2Fast sp{rows, xrows, xcols, row0, nshifts, r0, dcols, col0, 2 * P, nrs_total};
+    S2Fast sp{rows, xrows, xcols, row0, nshifts, r0, dcols, col0, 2 * P, nrs_total, 1.0f / (2.0f * (float)(2 * P))};
     switch (P) {
-    case 64: return launch_s2<8, 8>(h, sp, cols, X, Dinv, cand, ccall, perm);
-    case 180: return launch_s2<12, 15>(h, sp, cols, X, Dinv, cand, ccall, perm);
-    case 300: return launch_s2<15, 20>(h, sp, cols, X, Dinv, cand, ccall, perm);
+    case 64: return launch_s2<8, 8>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
+    case 180: return launch_s2<12, 15>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
+    case 300: return launch_s2<15, 20>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
     default: return cudaErrorInvalidValue;
     }
 }
 
-template <int P1, int P2>
+template <int P1, int P2, bool EU>
 static cudaError_t launch_rs(pftcc_handle *h, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
                              const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
                              const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
@@ -938,24 +958,37 @@ static cudaError_t launch_rs(pftcc_handle *h, int ncols, int ntop, int Ks, int n
     fill_tw(tw, P);
     if (ntop < 1 || ntop > RS_MAX) return cudaErrorInvalidValue;
     const size_t smem = rescore_smem_bytes<P1, P2>();
-    cudaError_t e = smem_limit((const void *)k_rescore_md<P1, P2>, smem);
+    cudaError_t e = smem_limit((const void *)k_rescore_md<P1, P2, EU>, smem);
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_EXACT);
-    k_rescore_md<P1, P2><<<ncols, RS_THREADS, smem, h->stream>>>(
+    k_rescore_md<P1, P2, EU><<<ncols, RS_THREADS, smem, h->stream>>>(
         ncols, ntop, Ks, 2 * P, nshifts, has_shifts, tw, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
     return cudaGetLastError();
+}
+
+template <int P1, int P2>
+static cudaError_t launch_rs_eu(pftcc_handle *h, int eu, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
+                                const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
+                                const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
+                                pftcc_best *out)
+{
+    if (eu)
+        return launch_rs<P1, P2, true>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV,
+                                       sqp, cand, perm, c0, out);
+    return launch_rs<P1, P2, false>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp,
+                                    cand, perm, c0, out);
 }
 
 cudaError_t launch_rescore_md(pftcc_handle *h, int P, int ncols, int ntop, int Ks, int nshifts, int has_shifts,
                               const float2 *UA, int rows_pad, const float2 *UB, int cols_pad, const double2 *RU,
                               const double2 *CV, const float *sqp, const float2 *cand, const int *perm, int c0,
-                              pftcc_best *out)
+                              pftcc_best *out, int eu)
 {
     switch (P) {
-    case 64: return launch_rs<8, 8>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
-    case 180: return launch_rs<12, 15>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
-    case 300: return launch_rs<15, 20>(h, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    case 64: return launch_rs_eu<8, 8>(h, eu, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    case 180: return launch_rs_eu<12, 15>(h, eu, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
+    case 300: return launch_rs_eu<15, 20>(h, eu, ncols, ntop, Ks, nshifts, has_shifts, UA, rows_pad, UB, cols_pad, RU, CV, sqp, cand, perm, c0, out);
     default: return cudaErrorInvalidValue;
     }
 }

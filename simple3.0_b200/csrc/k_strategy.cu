@@ -109,6 +109,8 @@ static int corr_all_device(pftcc_handle *h, int precision, float *dst)
 {
     if (precision == PFTCC_PREC_FP32 || precision == PFTCC_PREC_BF16X3)
         return search_mdomain(h, 0, nullptr, precision, 0, nullptr, dst);
+    const int ok = exact_objfun_ok(h);
+    if (ok != PFTCC_OK) return ok;
     const size_t per_ptcl = (size_t)h->nrefs;
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>(h->nptcls, 65536 / std::max<size_t>(1, per_ptcl) + 1));
     int st = ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>((size_t)chunk * per_ptcl * sizeof(Work), 4096),

@@ -466,6 +466,14 @@ static int sigma2_build(pftcc_handle *h)
     return PFTCC_OK;
 }
 
+int exact_objfun_ok(pftcc_handle *h)
+{
+    if (h->objfun == PFTCC_OBJFUN_EUCLID && h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "in the particle CTF frame the Euclidean objective is served by the "
+                                                 "m-domain search (PFTCC_PREC_FP32 / PFTCC_PREC_BF16X3)");
+    return PFTCC_OK;
+}
+
 int euclid_ready(pftcc_handle *h, int may_alloc)
 {
     if (h->h_sig2.empty())
@@ -490,9 +498,6 @@ int pftcc_set_objfun(pftcc_handle *h, int objfun)
     if (!h) return PFTCC_ERR_ARG;
     if (objfun != PFTCC_OBJFUN_CC && objfun != PFTCC_OBJFUN_EUCLID)
         return set_err(h, PFTCC_ERR_ARG, "objfun must be PFTCC_OBJFUN_CC or PFTCC_OBJFUN_EUCLID");
-    if (objfun == PFTCC_OBJFUN_EUCLID && h->cfg.ctf_frame != PFTCC_FRAME_REF)
-        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the Euclidean objective is defined in the reference frame "
-                                                 "(ctf_frame = PFTCC_FRAME_REF)");
     std::lock_guard<std::mutex> lk(h->mtx);
     h->objfun = objfun;
     return PFTCC_OK;
@@ -1113,6 +1118,7 @@ int pftcc_gencorrs(pftcc_handle *h, int iref, int iptcl, const float *shvec, flo
     std::lock_guard<std::mutex> lk(h->mtx);
     cudaSetDevice(h->dev);
     ST(check_ctf_state(h));
+    ST(exact_objfun_ok(h));
     return gencorrs_frame(h, iref, iptcl, shvec, cc, exact_frame(h));
 }
 
@@ -1363,6 +1369,7 @@ int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
     std::lock_guard<std::mutex> lk(h->mtx);
     cudaSetDevice(h->dev);
     ST(check_ctf_state(h));
+    ST(exact_objfun_ok(h));
     const int ns = std::max(1, nshifts);
     const size_t per_ptcl = (size_t)h->nrefs * ns;
     // bounded output chunks of particles
@@ -1414,6 +1421,7 @@ int pftcc_corr_all_prec(pftcc_handle *h, int nshifts, const float *shifts, int p
 
 static int search_exact(pftcc_handle *h, int nshifts, const float *shifts, pftcc_best *out_dev)
 {
+    ST(exact_objfun_ok(h));
     const int ns = std::max(1, nshifts);
     const size_t per_ptcl = (size_t)h->nrefs * ns;
     ST(ensure_small(h, (size_t)h->nptcls * per_ptcl, h->nptcls, 1, ns));

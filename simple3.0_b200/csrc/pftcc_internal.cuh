@@ -213,6 +213,9 @@ inline int exact_frame(const pftcc_handle *h)
 {
     return h->objfun == PFTCC_OBJFUN_EUCLID ? FRAME_EUCLID : h->cfg.ctf_frame;
 }
+// the exact kernel's Euclidean objective is the reference's (reference frame); in the particle
+// frame the Euclidean objective is served by the m-domain search alone
+int exact_objfun_ok(pftcc_handle *h);
 // gencorr_cont_shift_grad_cc_for_rot_8 for nreq requests (k_orisrch.cu; the request layout of
 // EuclidReq): out6[nreq][6] = f, d/de1..3, d/dsx, d/dsy
 struct EuclidReq;

@@ -126,3 +126,36 @@ def test_euclid_recovers_rotation_and_shift(O, j):
     eu = O.gencorrs_euclid(g, t, ref, ptcl, sigma2, None, sh)
     assert eu.argmax() == j % N
     assert eu.max() <= 0.0
+
+
+@pytest.mark.parametrize("geom", GEOMS)
+def test_particle_frame_euclid(O, geom):
+    """the particle-frame objective equals gencorrs_euclid_2 for an isotropic CTF and without
+    CTF, equals its expanded form sum_k w_k (corr_k - (E_ref,k(rot) + E_ptcl,k) / 2) with the
+    reference energy taken at the particle's CTF, and differs from the reference frame for an
+    astigmatic CTF"""
+    g, t, ref, ptcl, ctf, sigma2 = setup(O, geom, seed=4)
+    sh = (0.6, -0.4)
+    iso = O.ctfmat(g, t, O.make_ctf(dfx=2.0, dfy=2.0))
+    # an isotropic CTF on the polar grid varies with the angle only through the FP32 grid
+    # coordinates (k^2 = x^2 + y^2 to rounding): agreement to that level
+    for c, tol in ((None, 1e-10), (iso, 1e-6)):
+        a = O.gencorrs_euclid_ptclframe(g, t, ref, ptcl, sigma2, c, sh)
+        b = O.gencorrs_euclid(g, t, ref, ptcl, sigma2, c, sh)
+        assert np.max(np.abs(a - b)) < tol * np.max(np.abs(b))
+    got = O.gencorrs_euclid_ptclframe(g, t, ref, ptcl, sigma2, ctf, sh)
+    P, N = g.pftsz, g.nrots
+    A = ref.astype(np.complex128) * O.shmat(g, t, *sh)
+    full = np.concatenate([ptcl, np.conj(ptcl)], axis=1).astype(np.complex128)
+    cfull = np.concatenate([ctf, ctf], axis=1)
+    w = O.pxls_p_shell(g) / P / sigma2
+    for s in (0, 5, P, N - 1):
+        q = np.roll(full, -s, axis=1)[:, :P]
+        c = np.roll(cfull, -s, axis=1)[:, :P]
+        corr = np.sum((A * c * np.conj(q)).real, axis=1)
+        eref = np.sum(np.abs(ref.astype(np.complex128)) ** 2 * c ** 2, axis=1)
+        eptcl = np.sum(np.abs(ptcl.astype(np.complex128)) ** 2, axis=1)
+        want = np.sum((w * (corr - 0.5 * (eref + eptcl)))[:g.Ks])
+        assert abs(got[s] - want) < 1e-10 * abs(want)
+    ref_frame = O.gencorrs_euclid(g, t, ref, ptcl, sigma2, ctf, sh)
+    assert np.max(np.abs(got - ref_frame)) > 1e-6 * np.max(np.abs(ref_frame))

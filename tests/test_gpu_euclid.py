@@ -117,7 +117,7 @@ def test_sigma_contrib(pkg, O):
 
 def test_euclid_batched_exact_search(pkg, O):
     """corr_all / search_best (exact) under OBJFUN_EUCLID equal the per-pair gencorrs_euclid
-    and their maxloc; the FP32 / BF16 m-domain paths refuse the Euclidean objective"""
+    and their maxloc; in the reference frame the FP32 / BF16 m-domain paths refuse it"""
     w = pkg.synth.config0(nrefs=4, nptcls=5)
     pc, refs, parts, sig, g, t = setup(pkg, O, w, seed=3)
     pc.set_objfun(pkg._lib.OBJFUN_EUCLID)
@@ -167,9 +167,64 @@ def test_euclid_state_errors(pkg, O):
     assert np.all(np.isfinite(a)) and a.max() <= 0.0
     # sigma_contrib needs no sigma2, the Euclidean objective needs the reference frame
     pc.kill()
+    # in the particle frame the Euclidean objective is the m-domain search's: the exact calls refuse
     pc = pkg.polarft_corrcalc()
     pc.new(1, (1, 3), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=False, ctf_frame="ptcl")
-    with pytest.raises(pkg.PftccError) as e:
-        pc.set_objfun(pkg._lib.OBJFUN_EUCLID)
-    assert e.value.status == pkg._lib.ERR_UNSUPPORTED
+    pc.set_refs(1, refs.numpy(), True)
+    pc.polarize_ptcls(0, parts.cmat.numpy())
+    pc.set_objfun(pkg._lib.OBJFUN_EUCLID)
+    pc.assign_sigma2_noise(np.ones((3, K), np.float32))
+    for call in (lambda: pc.gencorrs(1, 1), lambda: pc.search_best(None, "exact"), lambda: pc.corr_all(None)):
+        with pytest.raises(pkg.PftccError) as e:
+            call()
+        assert e.value.status == pkg._lib.ERR_UNSUPPORTED
     pc.kill()
+
+
+def test_mdomain_euclid_matches_oracle(pkg, O):
+    """the m-domain search under OBJFUN_EUCLID (particle CTF frame: shell weights on the particle
+    spectra and the CTF^2 spectra, the additive normaliser): every value of corr_all_prec against
+    the oracle's particle-frame objective (2e-5 of the row's largest magnitude in FP32, 2e-4 with
+    the BF16 hi+lo products), and search_best with the FP32 re-score of the top 8 at the argmax"""
+    w = pkg.synth.config0(nrefs=4, nptcls=6)
+    refs, R = pkg.synth.make_refs(w)
+    parts = pkg.synth.make_particles(w, R)
+    refs = refs.numpy()
+    pc = pkg.polarft_corrcalc()
+    pc.new(w.nrefs, (1, w.nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True, ctf_frame="ptcl")
+    try:
+        pc.set_refs(1, refs, True)
+        pc.set_refs(1, refs, False)
+        pc.polarize_ptcls(0, parts.cmat.numpy())
+        pc.create_polar_absctfmats(pkg.ctfparams_array(w.nptcls, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                       dfx=parts.dfx, dfy=parts.dfy, angast=parts.angast))
+        K = w.kto - w.kfrom + 1
+        rng = np.random.default_rng(5)
+        sig = (rng.uniform(0.5, 2.0, (w.nptcls, K)) * np.linspace(4.0, 0.5, K)).astype(np.float32)
+        pc.assign_sigma2_noise(sig)
+        pc.set_objfun(pkg._lib.OBJFUN_EUCLID)
+        shifts = np.array([[0, 0], [0.5, -1.0], [-1.5, 1.0]], np.float32)
+        g = O.geom(w.nrots, w.kfrom, w.kto, w.box)
+        t = O.tables(g)
+        want = np.zeros((w.nptcls, w.nrefs, len(shifts), w.nrots))
+        for i in range(w.nptcls):
+            c = O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]), float(parts.dfy[i]),
+                                          float(parts.angast[i])))
+            pft = pc.get_ptcl_pft(i + 1)
+            for r in range(w.nrefs):
+                for s in range(len(shifts)):
+                    want[i, r, s] = O.gencorrs_euclid_ptclframe(g, t, refs[r], pft, sig[i].astype(np.float64), c,
+                                                                shifts[s].astype(np.float64))
+        for prec, tol in (("fp32", 2e-5), ("bf16x3", 2e-4)):
+            got = pc.corr_all_prec(shifts, prec)
+            err = np.max(np.abs(got - want), axis=-1) / np.max(np.abs(want), axis=-1)
+            print(f"m-domain Euclid {prec}: max error {err.max():.2e} of the row's scale")
+            assert err.max() < tol
+            best = pc.search_best(shifts, prec, ntop=8)
+            for i in range(w.nptcls):
+                flat = want[i].ravel()
+                got_v = want[i, best["iref"][i] - 1, best["ishift"][i], best["irot"][i] - 1]
+                assert got_v >= flat.max() - 1e-5 * np.abs(flat).max()
+                assert abs(best["corr"][i] - got_v) < 2e-5 * np.abs(flat).max()
+    finally:
+        pc.kill()
