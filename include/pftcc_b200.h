@@ -175,6 +175,20 @@ int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const dou
 int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
                                       double *grad);
 
+/* ---- the matched-filter mode (pftcc_config.match_filt = params_glob%l_match_filt) ---------- */
+/* With match_filt the correlators apply shellnorm_and_filter_ref(_8) (:756-807) to the reference:
+ * shell k <= kstop scaled by ref_optlp(k, iref) / sqrt(mean power of the raw shell) (gencorrs_cc_1/_2,
+ * gencorrs_euclid_1, gencorr_cc_for_rot(_8), gencorr_cc_grad_for_rot_8, the continuous-gradient
+ * correlators' reference, genfrc / calc_frc, the batched searches).  set_ref_optlp (:587-592):
+ * ref_optlp(kfrom:kstop, iref) = optlp[kstop - kfrom + 1] (1 until set). */
+int pftcc_set_ref_optlp(pftcc_handle *h, int iref, const float *optlp);
+/* prep_matchfilt (:987-1095), l_match_filt branch: particle iptcl re-weighted in place against
+ * reference iref (its eo set, times |CTF|) at rotation irot by the shell-normalised, Savitzky-Golay
+ * smoothed Wiener-like filter; iref 0 or match_filt off: nothing to do.  The batch holds each
+ * particle at most once. */
+int pftcc_prep_matchfilt(pftcc_handle *h, int iptcl, int iref, int irot);
+int pftcc_prep_matchfilt_batch(pftcc_handle *h, int n, const int *iptcl, const int *iref, const int *irot);
+
 /* ---- the orientation gradient (reference frame only) -------------------------------- */
 /* gencorr_cont_shift_grad_cc_for_rot_8 (:1788-1847): f and grad[5] = d f / d(e1, e2, e3, sx, sy)
  * at rotation irot from the references and derivative references of fdf_project_polar; the

@@ -86,6 +86,9 @@ def lib():
         L.orc_gencorrs_euclid_ptclframe.argtypes = [G, fp, fp, dp, dp, dp, dp, dp, dp, dp]
         L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
         L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
+        L.orc_shellnorm_factors.argtypes = [G, fp, fp, dp]
+        L.orc_savgol7.argtypes = [C.c_int, dp]
+        L.orc_prep_matchfilt.argtypes = [G, fp, dp, fp, C.c_int, fp]
         L.orc_prepimg4align.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.POINTER(Ctf), dp]
         L.orc_euler2dm.argtypes = [dp, dp]
         L.orc_kb_dapod.argtypes = [C.c_double]
@@ -316,6 +319,29 @@ def fproject_polar(g: Geom, t: Tables, cmat_exp, box: int, eul, mask=None, gridd
     lib().orc_fproject_polar(C.byref(g), _P(t.polar, C.c_float), int(box), _P(_c64(cmat_exp), C.c_float),
                              _P(e, C.c_double), _P(m, C.c_int), int(bool(griddev)),
                              out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def shellnorm_factors(g: Geom, ref, optlp=None) -> np.ndarray:
+    """per-shell factors k <= kstop of shellnorm_and_filter_ref (l_match_filt)"""
+    out = np.zeros(g.Ks, np.float64)
+    o = None if optlp is None else np.ascontiguousarray(optlp, np.float32)
+    lib().orc_shellnorm_factors(C.byref(g), _P(_c64(ref), C.c_float), _P(o, C.c_float), _P(out, C.c_double))
+    return out
+
+
+def savgol7(y) -> np.ndarray:
+    a = np.array(y, np.float64)
+    lib().orc_savgol7(a.size, _P(a, C.c_double))
+    return a
+
+
+def prep_matchfilt(g: Geom, ref, ptcl, irot: int, ctf=None, optlp=None) -> np.ndarray:
+    """the particle after prep_matchfilt against ref at irot (l_match_filt branch)"""
+    out = np.ascontiguousarray(ptcl, np.complex64).copy()
+    o = None if optlp is None else np.ascontiguousarray(optlp, np.float32)
+    lib().orc_prep_matchfilt(C.byref(g), _P(_c64(ref), C.c_float), _P(_ctf_arg(ctf), C.c_double), _P(o, C.c_float),
+                             int(irot), out.view(np.float32).ctypes.data_as(C.POINTER(C.c_float)))
     return out
 
 

@@ -1323,3 +1323,94 @@ void orc_gencorrs_euclid_ptclframe(const orc_geom *g, const float *ref, const fl
     }
     free(pr);
 }
+
+/* ------------------------------------------------------------------------- */
+/* The matched-filter mode.  shellnorm_and_filter_ref_8 (:783-807), l_match_filt branch. */
+void orc_shellnorm_factors(const orc_geom *g, const float *ref, const float *optlp, double *scale)
+{
+    const int P = g->pftsz, Ks = g->kstop - g->kfrom + 1;
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double pw = sqsum_kf(P, ref + 2 * ik * P) / (double)P;
+        const double o = optlp ? (double)optlp[ik] : 1.0;
+        scale[ik] = pw > 1e-12 ? o / sqrt(pw) : o;
+    }
+}
+
+/* The Savitzky & Golay (1964) least-squares smoothing coefficients for a 7-point window and a
+ * quartic, c_{-3..3} = (5, -30, 75, 131, 75, -30, 5) / 231 (the values savgol's normal equations
+ * give for nl = nr = 3, m = 4, ld = 0); y(i) = sum_k c_k y(i + k) for i <= n - 3 with the points
+ * left of the first skipped, as SavitzkyGolay_filter applies them. */
+void orc_savgol7(int n, double *y)
+{
+    static const double c[7] = {5.0 / 231.0, -30.0 / 231.0, 75.0 / 231.0, 131.0 / 231.0,
+                                75.0 / 231.0, -30.0 / 231.0, 5.0 / 231.0};
+    double *ys = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+    for (int i = 0; i < n; ++i) ys[i] = y[i];
+    for (int i = 0; i < n - 3; ++i) {
+        double v = 0.0;
+        for (int k = -3; k <= 3; ++k)
+            if (i + k >= 0) v += c[k + 3] * ys[i + k];
+        y[i] = v;
+    }
+    free(ys);
+}
+
+void orc_prep_matchfilt(const orc_geom *g, const float *ref, const double *ctfmat, const float *optlp, int irot,
+                        float *ptcl)
+{
+    const int P = g->pftsz, Ks = g->kstop - g->kfrom + 1, N = g->nrots;
+    double *pr = (double *)malloc(sizeof(double) * 2 * Ks * P);
+    double *pp = (double *)malloc(sizeof(double) * 2 * Ks * P);
+    double *diff = (double *)malloc(sizeof(double) * Ks), *fit = (double *)malloc(sizeof(double) * Ks);
+    /* reference times |CTF|, particle as held; both shell-normalised by optlp / sqrt(power) */
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double o = optlp ? (double)optlp[ik] : 1.0;
+        double pwr = 0.0, pwp = 0.0;
+        for (int n = 0; n < P; ++n) {
+            const double c = ctfmat ? ctfmat[ik * P + n] : 1.0;
+            const double rr = ref[2 * (ik * P + n)] * c, ri = ref[2 * (ik * P + n) + 1] * c;
+            pr[2 * (ik * P + n)] = rr; pr[2 * (ik * P + n) + 1] = ri;
+            pwr += rr * rr + ri * ri;
+            const double qr = ptcl[2 * (ik * P + n)], qi = ptcl[2 * (ik * P + n) + 1];
+            pp[2 * (ik * P + n)] = qr; pp[2 * (ik * P + n) + 1] = qi;
+            pwp += qr * qr + qi * qi;
+        }
+        pwr /= P;
+        pwp /= P;
+        const double wp = pwp > 1e-12 ? o / sqrt(pwp) : o, wr = pwr > 1e-12 ? o / sqrt(pwr) : o;
+        for (int n = 0; n < 2 * P; ++n) { pp[2 * ik * P + n] *= wp; pr[2 * ik * P + n] *= wr; }
+    }
+    /* power of the difference at irot: ref(n) - ptcl~(n + irot - 1) (the reference's case split) */
+    for (int ik = 0; ik < Ks; ++ik) {
+        double d = 0.0;
+        for (int n = 0; n < P; ++n) {
+            const int j = (n + irot - 1) % N, jp = j % P;
+            const double qr = pp[2 * (ik * P + jp)], qi = j < P ? pp[2 * (ik * P + jp) + 1] : -pp[2 * (ik * P + jp) + 1];
+            const double dr = pr[2 * (ik * P + n)] - qr, di = pr[2 * (ik * P + n) + 1] - qi;
+            d += dr * dr + di * di;
+        }
+        diff[ik] = d / P;
+        fit[ik] = diff[ik];
+    }
+    orc_savgol7(Ks, fit);
+    for (int ik = 0; ik < Ks; ++ik)
+        if (fit[ik] <= 0.0) fit[ik] = diff[ik];
+    for (int ik = 0; ik < 3 && ik < Ks; ++ik) fit[ik] = diff[ik];
+    /* filter: the normalised particle times 1/sqrt(its power) and sqrt(ssnr / (ssnr + 1)) */
+    for (int ik = 0; ik < Ks; ++ik) {
+        double pwp = 0.0, pwr = 0.0;
+        for (int n = 0; n < P; ++n) {
+            pwp += pp[2 * (ik * P + n)] * pp[2 * (ik * P + n)] + pp[2 * (ik * P + n) + 1] * pp[2 * (ik * P + n) + 1];
+            pwr += pr[2 * (ik * P + n)] * pr[2 * (ik * P + n)] + pr[2 * (ik * P + n) + 1] * pr[2 * (ik * P + n) + 1];
+        }
+        pwp /= P;
+        pwr /= P;
+        double w = pwp > 1e-12 ? 1.0 / sqrt(pwp) : 1.0;
+        if (fit[ik] > 1e-12) {
+            const double ssnr = pwr / fit[ik];
+            w *= sqrt(ssnr / (ssnr + 1.0));
+        }
+        for (int n = 0; n < 2 * P; ++n) ptcl[2 * ik * P + n] = (float)(w * pp[2 * ik * P + n]);
+    }
+    free(fit); free(diff); free(pp); free(pr);
+}

@@ -130,6 +130,18 @@ void orc_expand_cmat3d(int box, const float *cmat_half, double factor, float *cm
 void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const float *cmat_exp,
                         const double eul[3], const int *mask, int griddev, double *pft);
 
+/* the matched-filter mode (params_glob%l_match_filt): shellnorm_and_filter_ref(_8) (:756-807) scales
+ * shell k <= kstop of the raw reference by optlp(k) / sqrt(pw), pw = sum_n |ref(n,k)|^2 / P, or by
+ * optlp(k) where pw <= 1e-12; scale[Ks] (optlp = ref_optlp(:, iref), 1 unless set_ref_optlp) */
+void orc_shellnorm_factors(const orc_geom *g, const float *ref, const float *optlp, double *scale);
+/* SavitzkyGolay_filter (simple_math.f90:3511-3588): 7-point quartic smoothing (nl = nr = 3, m = 4)
+ * of y[n] in place, points left of the first omitted, the last 3 points unchanged */
+void orc_savgol7(int n, double *y);
+/* prep_matchfilt (:987-1095), the l_match_filt branch (l_pssnr off): the particle ptcl[K][P] is
+ * rescaled per shell k <= kstop against reference ref (raw, its set chosen by the caller) times
+ * ctfmat (NULL without CTF) at rotation irot (1-based), optlp the reference's ref_optlp column */
+void orc_prep_matchfilt(const orc_geom *g, const float *ref, const double *ctfmat, const float *optlp, int irot,
+                        float *ptcl);
 /* particle ingestion: prepimg4align (simple_strategy2D3D_common.f90:316-366) for one particle
  * with the soft mask of radius msk (no inner or focus mask) and griddev 'no'; img [box][box]
  * real in C order [y][x] (rmat(x, y)); (x, y) the particle's shift; ctf NULL for ctfflag

@@ -106,6 +106,9 @@ SIGNATURES = {
     "pftcc_cont_shift_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
     "pftcc_orisrch_batch": [_h, C.c_int, C.POINTER(OrisrchReq), C.c_int, C.c_double, C.c_double,
                             C.POINTER(OrisrchOut)],
+    "pftcc_set_ref_optlp": [_h, C.c_int, _fp],
+    "pftcc_prep_matchfilt": [_h, C.c_int, C.c_int, C.c_int],
+    "pftcc_prep_matchfilt_batch": [_h, C.c_int, _ip, _ip, _ip],
     "pftcc_set_objfun": [_h, C.c_int],
     "pftcc_assign_sigma2_noise": [_h, C.c_int, C.c_int, _fp],
     "pftcc_gencorrs_euclid": [_h, C.c_int, C.c_int, _fp, _fp],

@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const uint8_t *__restrict__ iseven,
     const float *__restrict__ sqsums, const double *__restrict__ argtransf, const double *__restrict__ argtransf1,
     const Group *__restrict__ groups, const Work *__restrict__ work, const float *__restrict__ shifts, int mode,
-    int cc1_kstop, const float *__restrict__ sig2, const float *__restrict__ pxls, float *__restrict__ out,
-    pftcc_best *__restrict__ best)
+    int cc1_kstop, const float *__restrict__ sig2, const float *__restrict__ pxls, const float *__restrict__ snorm,
+    int nrefs, float *__restrict__ out, pftcc_best *__restrict__ best)
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P;
@@ -241,6 +241,11 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
         const Work w = work[grp.first + it];
         const float2 *r = refs + (long long)w.iref * g.K * P;
         const bool has_shift = w.ishift >= 0;
+        // matched-filter mode: the reference's shell factors (shellnorm_and_filter_ref), which
+        // gencorrs_cc_1/_2 apply and, of the Euclidean pair, gencorrs_euclid_1 alone
+        const float *sn = (snorm && (FRAME != FRAME_EUCLID || !has_shift))
+                              ? snorm + ((size_t)(iseven[slot] ? 0 : 1) * nrefs + w.iref) * g.Ks
+                              : nullptr;
         if (has_shift) {
             const double sx = (double)shifts[2 * w.ishift], sy = (double)shifts[2 * w.ishift + 1];
             for (int n = threadIdx.x; n < P; n += blockDim.x) {
@@ -267,7 +272,8 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                 const double2 v = has_shift ? sv[n] : make_double2(1.0, 0.0);
                 for (int kk = 0; kk < kc; ++kk) {
                     const int ik = k0 + kk;
-                    const float2 rv = r[(long long)ik * P + n];
+                    float2 rv = r[(long long)ik * P + n];
+                    if (sn && ik < g.Ks) { rv.x *= sn[ik]; rv.y *= sn[ik]; }
                     float ar = rv.x, ai = rv.y;
                     if (FRAME != PFTCC_FRAME_PTCL && ctf) {
                         const float c = ctf[ik * P + n];
@@ -421,7 +427,7 @@ static cudaError_t launch_exact_t(pftcc_handle *h, int kc, size_t smem, const Gr
     KTimer kt(h, PFTCC_K_EXACT);
     k_exact<FRAME><<<ngroups, EX_THREADS, smem, h->stream>>>(
         h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf, h->argtransf1,
-        groups, work, shifts, mode, cc1_kstop, h->d_sig2, h->d_pxls, out, best);
+        groups, work, shifts, mode, cc1_kstop, h->d_sig2, h->d_pxls, snorm_ptr(h), h->nrefs, out, best);
     return cudaGetLastError();
 }
 
@@ -488,13 +494,15 @@ __global__ void __launch_bounds__(FR_THREADS) k_for_rot(
     const float2 *__restrict__ refs_odd, const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats,
     const pftcc_ctfparams *__restrict__ ctfp, const uint8_t *__restrict__ iseven, const float *__restrict__ polar,
     const double *__restrict__ argtransf, const double *__restrict__ argtransf1, int with_ctf, int match_filt,
-    double *__restrict__ out /* [nreq][5]: f, d/dsx, d/dsy, d/ddf, unused */)
+    const float *__restrict__ snorm, int nrefs, double *__restrict__ out /* [nreq][5]: f, d/dsx, d/dsy, d/ddf, unused */)
 {
     __shared__ double red[FR_THREADS / 32];
     const RotReq rq = reqs[blockIdx.x];
     const int N = g.N, P = g.P;
     const float2 *q = ptcls + (long long)rq.slot * g.K * P;
     const float2 *r = (iseven[rq.slot] ? refs_even : refs_odd) + (long long)rq.iref * g.K * P;
+    // matched-filter mode: shellnorm_and_filter_ref_8's factors
+    const float *sn = snorm ? snorm + ((size_t)(iseven[rq.slot] ? 0 : 1) * nrefs + rq.iref) * g.Ks : nullptr;
     const int s = rq.irot - 1;
     double corr = 0, sqr = 0, sqp = 0, gx = 0, gy = 0, gd = 0, dsq = 0;
     // thread per n; the shift phase of every shell follows the de Moivre recurrence
@@ -521,7 +529,8 @@ __global__ void __launch_bounds__(FR_THREADS) k_for_rot(
                 }
             }
             const float2 rv = r[(long long)ik * P + n];
-            const double rr = (double)rv.x * c, ri = (double)rv.y * c;
+            const double f = sn ? (double)sn[ik] : 1.0;
+            const double rr = (double)rv.x * f * c, ri = (double)rv.y * f * c;
             const double ar = rr * st_r - ri * st_i, ai = rr * st_i + ri * st_r;   // prepared reference
             const float2 qv = q[(long long)ik * P + jp];
             const double qr = qv.x, qi = qs * qv.y;                                // ptcl~(j)
@@ -533,7 +542,7 @@ __global__ void __launch_bounds__(FR_THREADS) k_for_rot(
             gx += wgt * ax * (-ai * qr + ar * qi);
             gy += wgt * ay * (-ai * qr + ar * qi);
             if (with_ctf && rq.ctf_mode == 1) {
-                const double dr = (double)rv.x * dc, di = (double)rv.y * dc;
+                const double dr = (double)rv.x * f * dc, di = (double)rv.y * f * dc;
                 const double br = dr * st_r - di * st_i, bi = dr * st_i + di * st_r;
                 gd += wgt * (br * qr + bi * qi);
                 dsq += wgt * 2.0 * (ar * br + ai * bi);
@@ -573,7 +582,7 @@ cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, doubl
     k_for_rot<<<1, FR_THREADS, 0, h->stream>>>(h->g, reinterpret_cast<const RotReq *>(h->d_work), h->refs_even,
                                                 h->refs_odd, h->ptcls, h->ctfmats, h->d_ctfp, h->d_iseven, h->polar,
                                                 h->argtransf, h->argtransf1, h->cfg.with_ctf && h->ctf_ready,
-                                                match_filt, out5);
+                                                match_filt, snorm_ptr(h), h->nrefs, out5);
     return cudaGetLastError();
 }
 
@@ -689,7 +698,8 @@ cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, co
     PFTCC_LAUNCH(h);
     k_for_rot<<<nreq, FR_THREADS, 0, h->stream>>>(h->g, rq, h->refs_even, h->refs_odd, h->ptcls, h->ctfmats,
                                                    h->d_ctfp, h->d_iseven, h->polar, h->argtransf, h->argtransf1,
-                                                   h->cfg.with_ctf && h->ctf_ready, h->cfg.match_filt, out5);
+                                                   h->cfg.with_ctf && h->ctf_ready, h->cfg.match_filt, snorm_ptr(h),
+                                                   h->nrefs, out5);
     return cudaGetLastError();
 }
 

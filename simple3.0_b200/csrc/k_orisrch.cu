@@ -39,7 +39,8 @@ __global__ void __launch_bounds__(OG_THREADS) k_cont_shift_grad(
     const float2 *__restrict__ refs_odd, const float2 *__restrict__ drefs_even, const float2 *__restrict__ drefs_odd,
     const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const uint8_t *__restrict__ iseven,
     const float *__restrict__ sqsums, const double *__restrict__ argtransf, const double *__restrict__ argtransf1,
-    int scratch, double *__restrict__ out6 /* [nreq][6]: f, d/de1, d/de2, d/de3, d/dsx, d/dsy */)
+    int scratch, const float *__restrict__ snorm, int nrefs,
+    double *__restrict__ out6 /* [nreq][6]: f, d/de1, d/de2, d/de3, d/dsx, d/dsy */)
 {
     __shared__ double red[OG_THREADS / 32];
     const EuclidReq rq = reqs[blockIdx.x];
@@ -52,6 +53,9 @@ __global__ void __launch_bounds__(OG_THREADS) k_cont_shift_grad(
     const float2 *dr = scratch ? drefs_even + (long long)blockIdx.x * 3 * K * P
                                : (ev ? drefs_even : drefs_odd) + (long long)rq.iref * 3 * K * P;
     const float *ctf = ctfmats ? ctfmats + (long long)rq.slot * K * P : nullptr;
+    // matched-filter mode: the reference (not its derivatives) shell-normalised, as
+    // gencorr_cont_shift_grad_cc_for_rot_8 applies shellnorm_and_filter_ref_8 to pft_ref alone
+    const float *sn = (snorm && !scratch) ? snorm + ((size_t)(ev ? 0 : 1) * nrefs + rq.iref) * g.Ks : nullptr;
     const int s = rq.irot - 1;
     double y = 0.0, sqr = 0.0, gx = 0.0, gy = 0.0, t1[3] = {0.0, 0.0, 0.0}, t2[3] = {0.0, 0.0, 0.0};
     for (int n = threadIdx.x; n < P; n += blockDim.x) {
@@ -65,7 +69,8 @@ __global__ void __launch_bounds__(OG_THREADS) k_cont_shift_grad(
         for (int ik = 0; ik < g.Ks; ++ik) {
             const double c = ctf ? (double)ctf[ik * P + n] : 1.0;
             const float2 rv = r[(long long)ik * P + n];
-            const double rr = (double)rv.x * c, ri = (double)rv.y * c;
+            const double f = sn ? (double)sn[ik] : 1.0;
+            const double rr = (double)rv.x * f * c, ri = (double)rv.y * f * c;
             const double ar = rr * st_r - ri * st_i, ai = rr * st_i + ri * st_r;
             const float2 qv = q[(long long)ik * P + jp];
             const double qr = qv.x, qi = qs * qv.y;
@@ -116,7 +121,7 @@ cudaError_t launch_cont_shift_grad(pftcc_handle *h, const EuclidReq *reqs_dev, i
     KTimer kt(h, PFTCC_K_EXACT);
     k_cont_shift_grad<<<nreq, OG_THREADS, 0, h->stream>>>(h->g, reqs_dev, h->refs_even, h->refs_odd, h->drefs_even,
                                                           h->drefs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums,
-                                                          h->argtransf, h->argtransf1, 0, out6);
+                                                          h->argtransf, h->argtransf1, 0, snorm_ptr(h), h->nrefs, out6);
     return cudaGetLastError();
 }
 
@@ -151,7 +156,7 @@ static int orisrch_eval(pftcc_handle *h, int nb, const int *slots, const double 
         KTimer kt(h, PFTCC_K_EXACT);
         k_cont_shift_grad<<<nb, OG_THREADS, 0, h->stream>>>(h->g, dreq, scr_ref, scr_ref, scr_dref, scr_dref,
                                                              h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf,
-                                                             h->argtransf1, 1, dout);
+                                                             h->argtransf1, 1, nullptr, 0, dout);
         e = cudaGetLastError();
     }
     o.resize((size_t)nb * 6);

@@ -1223,7 +1223,9 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         { KTimer kt(h, PFTCC_K_SPEC_REF);
         k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
         CKE(cudaGetLastError(), "spec_r2");
-        CKE(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref"); }
+        CKE(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref");
+        if (h->cfg.match_filt)   // the references' shell factors (shellnorm_and_filter_ref) on their spectra
+            CKE(launch_shellnorm_apply(h, M, nrs, rows_pad, ns, grp, ws.UA, ws.RU), "shell factors"); }
         if (precision == PFTCC_PREC_BF16X3) {
             int st = umma_stage1(h, M, Ks, ws.UA, 0, nrs, rows_pad, ws.UB, gc0, gc1 - gc0, cols_pad, nullptr, 1, grp);
             if (st != PFTCC_OK) return st;

@@ -167,6 +167,10 @@ extern "C" int pftcc_search_snhc(pftcc_handle *h, const int *order, const float 
         const int est = euclid_ready(h, 1);
         if (est != PFTCC_OK) return est;
     }
+    {
+        const int sst = snorm_ready(h, 0, h->nrefs);
+        if (sst != PFTCC_OK) return sst;
+    }
     // global particle index of each slot (the random draws are keyed by it)
     std::vector<int> gidx(np, 0);
     for (int p = h->pfrom; p <= h->pto; ++p) {

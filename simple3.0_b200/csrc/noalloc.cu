@@ -65,6 +65,7 @@ extern "C" int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *ir
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
     if (h->objfun == PFTCC_OBJFUN_EUCLID && euclid_ready(h, 0) != PFTCC_OK) return PFTCC_ERR_STATE;
     if (exact_objfun_ok(h) != PFTCC_OK) return PFTCC_ERR_UNSUPPORTED;
+    if (snorm_ready(h, 0, h->nrefs) != PFTCC_OK) return PFTCC_ERR_CUDA;   // matched-filter factors (no allocation)
     // host-side descriptors (validated) in a fixed host buffer guarded by the global lock,
     // then one copy into the fixed device scratch
     std::lock_guard<std::mutex> lk2(g_noalloc_host_mtx);

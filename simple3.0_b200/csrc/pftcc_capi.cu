@@ -271,7 +271,8 @@ static void free_all(pftcc_handle *h)
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
                     h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
-                    h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls, h->drefs_even, h->drefs_odd};
+                    h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls, h->drefs_even, h->drefs_odd, h->d_optlp,
+                    h->d_snorm};
     for (void *p : ptrs) dev_free(h, p);
     umma_free(h);
     ingest_free(h);
@@ -409,6 +410,17 @@ int pftcc_new(const pftcc_config *cfg, const int *ptcl_mask, const int *eoarr, p
                 if (h->pinds[i] > 0) h->iseven[h->pinds[i] - 1] = eoarr[i] == 0;
     }
     if (push_iseven(h) != PFTCC_OK) return fail(PFTCC_ERR_CUDA, h->last_err);
+    if (h->cfg.match_filt) {
+        // matched-filter mode: ref_optlp = 1 (allocated with source = 1., :255) and the shell factors
+        const size_t nf = (size_t)std::max(1, h->nrefs) * h->g.Ks;
+        std::vector<float> ones(nf, 1.f);
+        if ((st = dev_alloc(h, (void **)&h->d_optlp, nf * sizeof(float), "ref_optlp")) ||
+            (st = dev_alloc(h, (void **)&h->d_snorm, 2 * nf * sizeof(float), "shell factors")))
+            return fail(st, h->last_err);
+        if (cudaMemcpyAsync(h->d_optlp, ones.data(), nf * sizeof(float), cudaMemcpyHostToDevice, h->stream) ||
+            cudaStreamSynchronize(h->stream))
+            return fail(PFTCC_ERR_CUDA, "ref_optlp upload failed");
+    }
     *out = h;
     return PFTCC_OK;
 }
@@ -466,6 +478,14 @@ static int sigma2_build(pftcc_handle *h)
     return PFTCC_OK;
 }
 
+int snorm_ready(pftcc_handle *h, int r0, int n)
+{
+    if (!h->cfg.match_filt || n <= 0) return PFTCC_OK;
+    if (!h->d_snorm || !h->d_optlp) return set_err(h, PFTCC_ERR_STATE, "matched-filter arrays missing");
+    CK(launch_shellnorm(h, r0, n), "shell factors");
+    return PFTCC_OK;
+}
+
 int exact_objfun_ok(pftcc_handle *h)
 {
     if (h->objfun == PFTCC_OBJFUN_EUCLID && h->cfg.ctf_frame != PFTCC_FRAME_REF)
@@ -501,6 +521,56 @@ int pftcc_set_objfun(pftcc_handle *h, int objfun)
     std::lock_guard<std::mutex> lk(h->mtx);
     h->objfun = objfun;
     return PFTCC_OK;
+}
+
+int pftcc_set_ref_optlp(pftcc_handle *h, int iref, const float *optlp)
+{
+    if (!h || !optlp) return set_err(h, PFTCC_ERR_ARG, "set_ref_optlp: bad arguments");
+    REF_OR_FAIL(iref);
+    if (!h->cfg.match_filt || !h->d_optlp)
+        return set_err(h, PFTCC_ERR_STATE, "set_ref_optlp: the handle was created without match_filt");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    CK(cudaMemcpyAsync(h->d_optlp + (size_t)(iref - 1) * h->g.Ks, optlp, h->g.Ks * sizeof(float),
+                       cudaMemcpyHostToDevice, h->stream), "set_ref_optlp");
+    CK(cudaStreamSynchronize(h->stream), "set_ref_optlp");
+    return PFTCC_OK;
+}
+
+int pftcc_prep_matchfilt_batch(pftcc_handle *h, int n, const int *iptcl, const int *iref, const int *irot)
+{
+    if (!h || n < 0 || (n > 0 && (!iptcl || !iref || !irot))) return set_err(h, PFTCC_ERR_ARG, "prep_matchfilt: bad arguments");
+    if (n == 0 || !h->cfg.match_filt) return PFTCC_OK;   // memoize_fft only: nothing to hold (:997-1001)
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.with_ctf && !h->ctf_ready)
+        return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
+    struct Req { int iref, slot, irot, pad; };
+    std::vector<Req> rq;
+    rq.reserve(n);
+    std::vector<char> seen(std::max(1, h->nptcls), 0);
+    for (int i = 0; i < n; ++i) {
+        const int sl = slot_of(h, iptcl[i]);
+        if (sl < 0) return set_err(h, PFTCC_ERR_INDEX, "prep_matchfilt: particle not held");
+        if (iref[i] < 0 || iref[i] > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "prep_matchfilt: iref out of range");
+        if (irot[i] < 1 || irot[i] > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "prep_matchfilt: irot out of range");
+        if (seen[sl]) return set_err(h, PFTCC_ERR_ARG, "prep_matchfilt: a particle appears twice in one batch");
+        seen[sl] = 1;
+        if (iref[i] == 0) continue;   // iref 0: memoization only (:997)
+        rq.push_back(Req{iref[i] - 1, sl, irot[i], 0});
+    }
+    if (rq.empty()) return PFTCC_OK;
+    ST(ensure(h, (void **)&h->d_work, &h->work_cap, std::max<size_t>(rq.size() * sizeof(Req), 4096), "matchfilt requests"));
+    CK(cudaMemcpyAsync(h->d_work, rq.data(), rq.size() * sizeof(Req), cudaMemcpyHostToDevice, h->stream), "matchfilt");
+    CK(launch_prep_matchfilt(h, h->d_work, (int)rq.size()), "prep_matchfilt kernel");
+    CK(cudaStreamSynchronize(h->stream), "prep_matchfilt");
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_prep_matchfilt(pftcc_handle *h, int iptcl, int iref, int irot)
+{
+    return pftcc_prep_matchfilt_batch(h, 1, &iptcl, &iref, &irot);
 }
 
 int pftcc_assign_sigma2_noise(pftcc_handle *h, int fromp, int top, const float *sigma2)
@@ -969,6 +1039,7 @@ int pftcc_cont_shift_grad_batch(pftcc_handle *h, int n, const pftcc_grad_req *re
     if (h->cfg.with_ctf && !h->ctf_ready)
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
     if (!h->drefs_even) return set_err(h, PFTCC_ERR_STATE, "no derivative references (fdf_project_polar first)");
+    ST(snorm_ready(h, 0, h->nrefs));
     std::vector<EuclidReq> rq(n);
     for (int i = 0; i < n; ++i) {
         if (req[i].iref < 1 || req[i].iref > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "cont_shift_grad: iref out of range");
@@ -1087,10 +1158,12 @@ static int check_ctf_only(pftcc_handle *h)
     return PFTCC_OK;
 }
 
-// the state an evaluation of the current objective needs
+// the state an evaluation of the current objective needs (and, in the matched-filter mode, the
+// references' current shell factors)
 static int check_ctf_state(pftcc_handle *h)
 {
     ST(check_ctf_only(h));
+    ST(snorm_ready(h, 0, h->nrefs));
     if (h->objfun == PFTCC_OBJFUN_EUCLID) return euclid_ready(h, 1);
     return PFTCC_OK;
 }

@@ -120,6 +120,10 @@ struct pftcc_handle {
     // the volume's expanded FT for polar projection (expand_cmat), side box + 5
     float2 *vol_cube = nullptr;
     int vol_box = 0;
+    // matched-filter mode: ref_optlp(kfrom:kstop, nrefs) as [nrefs][Ks] (1 until set_ref_optlp)
+    // and the shell factors of shellnorm_and_filter_ref [2 sets][nrefs][Ks]
+    float *d_optlp = nullptr;
+    float *d_snorm = nullptr;
     // particle ingestion state (k_ingest.cu: cuFFT plans and scratch)
     void *ingest = nullptr;
     // the orientation derivatives of the references (fdf_project_polar), [nrefs][3][K][P]
@@ -231,6 +235,17 @@ void host_euler2m(const double e[3], double *R, double *dR);
 // batched pftcc_orisrch_grad%minimize (k_orisrch.cu); the caller holds the lock
 int orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
                   pftcc_orisrch_out *out);
+// matched-filter mode (k_matchfilt.cu): the shell factors of references r0..r0+n-1 (both sets);
+// the factors of reference set `set` on the m-domain spectra; prep_matchfilt requests
+// {iref (0-based), slot, irot, pad}
+cudaError_t launch_shellnorm(pftcc_handle *h, int r0, int n);
+cudaError_t launch_shellnorm_apply(pftcc_handle *h, int M, int nrs, int rows_pad, int nshifts, int set, float2 *UA,
+                                   double2 *RU);
+cudaError_t launch_prep_matchfilt(pftcc_handle *h, const void *reqs_dev, int nreq);
+// allocates ref_optlp (ones) and the factors on first use and computes the factors of references
+// r0..r0+n-1 when match_filt is on; snorm_ptr(h) is the factor array or null when it is off
+int snorm_ready(pftcc_handle *h, int r0, int n);
+inline const float *snorm_ptr(const pftcc_handle *h) { return h->cfg.match_filt ? h->d_snorm : nullptr; }
 // sigma2_noise on the device and covering every held particle (rebuilt first when stale
 // and may_alloc); PFTCC_OK or the error code, with the message set
 int euclid_ready(pftcc_handle *h, int may_alloc);

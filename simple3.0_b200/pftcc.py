@@ -300,6 +300,20 @@ class polarft_corrcalc:
                                                   None if frcs is None else _f32p(frcs)))
         return (scores, frcs) if want_frc else scores
 
+    # ---- the matched-filter mode (new(..., match_filt=True)) ----------------------------------
+    def set_ref_optlp(self, iref: int, optlp):
+        """ref_optlp(kfrom:kstop, iref) = optlp (the reference's matched filter)"""
+        a = np.ascontiguousarray(optlp, np.float32)
+        self._check(self._L.pftcc_set_ref_optlp(self._h, int(iref), _f32p(a)))
+
+    def prep_matchfilt(self, iptcl: int, iref: int, irot: int):
+        self._check(self._L.pftcc_prep_matchfilt(self._h, int(iptcl), int(iref), int(irot)))
+
+    def prep_matchfilt_batch(self, iptcl, iref, irot):
+        ip, ir, ro = (np.ascontiguousarray(np.atleast_1d(v), np.int32) for v in (iptcl, iref, irot))
+        ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self._L.pftcc_prep_matchfilt_batch(self._h, ip.size, ptr(ip), ptr(ir), ptr(ro)))
+
     # ---- the Euclidean objective (params_glob%cc_objfun = OBJFUN_EUCLID) ---------------------
     def set_objfun(self, objfun: int):
         """cc_objfun: _lib.OBJFUN_CC or _lib.OBJFUN_EUCLID; gencorrs, gencorr_for_rot(_8),

@@ -167,13 +167,18 @@ def test_for_rot_and_gradients(pkg, O):
         for i in range(3):
             g, t, c = oracle_ctx(O, w, parts, i)
             pft = pc.get_ptcl_pft(i + 1)
+            ref0 = refs[0]
+            if mf:   # match_filt: the reference shell-normalised first (shellnorm_and_filter_ref_8, ref_optlp = 1)
+                s = O.shellnorm_factors(g, refs[0])
+                ref0 = refs[0].copy()
+                ref0[:g.Ks] = (ref0[:g.Ks] * s[:, None].astype(np.float32)).astype(np.complex64)
             for irot in (1, 40, 128):
                 sh = np.array([0.7, -0.3])
-                want = O.gencorr_for_rot(g, t, refs[0], pft, irot, c, sh, mf)
+                want = O.gencorr_for_rot(g, t, ref0, pft, irot, c, sh, mf)
                 assert abs(pc.gencorr_for_rot_8(1, i + 1, sh, irot) - want) < 1e-6
                 assert abs(pc.gencorr_for_rot(1, i + 1, sh, irot) - want) < 1e-5
                 f, gr = pc.gencorr_grad_for_rot_8(1, i + 1, sh, irot)
-                fo, go = O.gencorr_grad3(g, t, refs[0], pft, irot, c, None, sh, mf)
+                fo, go = O.gencorr_grad3(g, t, ref0, pft, irot, c, None, sh, mf)
                 assert abs(f - fo) < 1e-6
                 assert np.max(np.abs(gr - go[:2])) < 1e-6 * max(1, np.max(np.abs(go)))
                 assert np.allclose(pc.gencorr_grad_only_for_rot_8(1, i + 1, sh, irot), gr)
