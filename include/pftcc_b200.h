@@ -175,6 +175,21 @@ int pftcc_gencorr_grad_for_rot_8(pftcc_handle *h, int iref, int iptcl, const dou
 int pftcc_gencorr_grad_only_for_rot_8(pftcc_handle *h, int iref, int iptcl, const double *shvec, int irot,
                                       double *grad);
 
+/* ---- remaining procedures of the object ----------------------------------------------- */
+/* cp_refs (:491-495): both reference sets copied from src (same nrefs, shells and angles) */
+int pftcc_cp_refs(pftcc_handle *h, const pftcc_handle *src);
+/* set_ptcl_fcomp (:471-476): one component pfts_ptcls(irot, k, pinds(iptcl)) = comp[2]
+ * (irot 1..nrots/2, k kfrom..kto); the square sum is not refreshed, as in the reference */
+int pftcc_set_ptcl_fcomp(pftcc_handle *h, int iptcl, int irot, int k, const float *comp);
+/* calc_ptcl_pspec (:897-904): pspec[kto - kfrom + 1], the mean power of each shell */
+int pftcc_calc_ptcl_pspec(pftcc_handle *h, int iptcl, float *pspec);
+/* assign_pinds (:706-710): pinds[pfromto(2) - pfromto(1) + 1], each index's slot (1-based, 0 = not held) */
+int pftcc_assign_pinds(const pftcc_handle *h, int *pinds);
+/* calc_roinv_corrmat (:2207-2231), particles and references the same set (nptcls == nrefs):
+ * corrmat[nptcls][nptcls], the best in-plane correlation of reference i with particle pfrom + j
+ * for i < j (gencorrs maxloc), symmetrised, 1 on the diagonal */
+int pftcc_calc_roinv_corrmat(pftcc_handle *h, float *corrmat);
+
 /* ---- the matched-filter mode (pftcc_config.match_filt = params_glob%l_match_filt) ---------- */
 /* With match_filt the correlators apply shellnorm_and_filter_ref(_8) (:756-807) to the reference:
  * shell k <= kstop scaled by ref_optlp(k, iref) / sqrt(mean power of the raw shell) (gencorrs_cc_1/_2,

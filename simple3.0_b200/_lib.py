@@ -106,6 +106,11 @@ SIGNATURES = {
     "pftcc_cont_shift_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
     "pftcc_orisrch_batch": [_h, C.c_int, C.POINTER(OrisrchReq), C.c_int, C.c_double, C.c_double,
                             C.POINTER(OrisrchOut)],
+    "pftcc_cp_refs": [_h, _h],
+    "pftcc_set_ptcl_fcomp": [_h, C.c_int, C.c_int, C.c_int, _fp],
+    "pftcc_calc_ptcl_pspec": [_h, C.c_int, _fp],
+    "pftcc_assign_pinds": [_h, _ip],
+    "pftcc_calc_roinv_corrmat": [_h, _fp],
     "pftcc_set_ref_optlp": [_h, C.c_int, _fp],
     "pftcc_prep_matchfilt": [_h, C.c_int, C.c_int, C.c_int],
     "pftcc_prep_matchfilt_batch": [_h, C.c_int, _ip, _ip, _ip],

@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
             if (mode == MODE_FULL) out[w.out + s] = cc;
             if (cc > my_best) { my_best = cc; my_rot = s; }
         }
-        if (mode == MODE_BEST) {
+        if (mode == MODE_BEST || mode == MODE_ITEMMAX) {
             // block argmax, lowest rotation on ties (maxloc)
             for (int o = 16; o > 0; o >>= 1) {
                 const float ob = __shfl_xor_sync(0xffffffffu, my_best, o);
@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
             for (int wi = 1; wi < EX_THREADS / 32; ++wi)
                 if (bcc[wi] > bb || (bcc[wi] == bb && brot[wi] < br)) { bb = bcc[wi]; br = brot[wi]; }
             if (bb > run_best) { run_best = bb; run_rot = br; run_item = it; }
+            if (mode == MODE_ITEMMAX && threadIdx.x == 0) out[w.out] = bb;
         }
         __syncthreads();
     }

@@ -185,6 +185,30 @@ __global__ void __launch_bounds__(MF_THREADS) k_prep_matchfilt(Geom g, const Mat
     if (threadIdx.x == 0) sqsums[rq.slot] = (float)s;
 }
 
+// calc_ptcl_pspec (:897-904): sum_n |ptcl(n,k)|^2 / P for every shell kfrom..kto, a warp per shell
+__global__ void __launch_bounds__(MF_THREADS) k_ptcl_pspec(Geom g, const float2 *__restrict__ ptcls, int slot,
+                                                           float *__restrict__ pspec)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float2 *q = ptcls + (size_t)slot * g.K * g.P;
+    for (int k = warp; k < g.K; k += MF_THREADS / 32) {
+        double s = 0.0;
+        for (int n = lane; n < g.P; n += 32) {
+            const float2 v = q[(size_t)k * g.P + n];
+            s += (double)v.x * v.x + (double)v.y * v.y;
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) pspec[k] = (float)(s / g.P);
+    }
+}
+
+cudaError_t launch_ptcl_pspec(pftcc_handle *h, int slot, float *pspec_dev)
+{
+    PFTCC_LAUNCH(h);
+    k_ptcl_pspec<<<1, MF_THREADS, 0, h->stream>>>(h->g, h->ptcls, slot, pspec_dev);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_shellnorm(pftcc_handle *h, int r0, int n)
 {
     if (n <= 0) return cudaSuccess;

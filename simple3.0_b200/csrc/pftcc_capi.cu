@@ -1436,6 +1436,109 @@ int pftcc_genfrc(pftcc_handle *h, int iref, int iptcl, int irot, const float *sh
     return pftcc_specscore_batch(h, 1, &iref, &iptcl, &irot, shvec, &score, frc);
 }
 
+int pftcc_cp_refs(pftcc_handle *h, const pftcc_handle *src)
+{
+    if (!h || !src) return set_err(h, PFTCC_ERR_ARG, "cp_refs: bad arguments");
+    if (src->nrefs != h->nrefs || src->g.K != h->g.K || src->g.P != h->g.P)
+        return set_err(h, PFTCC_ERR_ARG, "cp_refs: the two objects' reference sets differ in shape");
+    if (src->dev != h->dev) return set_err(h, PFTCC_ERR_ARG, "cp_refs: the two objects live on different devices");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    const size_t bytes = (size_t)h->nrefs * h->g.K * h->g.P * sizeof(float2);
+    // self%pfts_refs_odd = self2%pfts_refs_odd; self%pfts_refs_even = self2%pfts_refs_even (:491-495)
+    CK(cudaStreamSynchronize(src->stream), "cp_refs");
+    CK(cudaMemcpyAsync(h->refs_odd, src->refs_odd, bytes, cudaMemcpyDeviceToDevice, h->stream), "cp_refs");
+    CK(cudaMemcpyAsync(h->refs_even, src->refs_even, bytes, cudaMemcpyDeviceToDevice, h->stream), "cp_refs");
+    CK(cudaStreamSynchronize(h->stream), "cp_refs");
+    return PFTCC_OK;
+}
+
+int pftcc_set_ptcl_fcomp(pftcc_handle *h, int iptcl, int irot, int k, const float *comp)
+{
+    if (!h || !comp) return set_err(h, PFTCC_ERR_ARG, "set_ptcl_fcomp: bad arguments");
+    SLOT_OR_FAIL(slot, iptcl);
+    if (irot < 1 || irot > h->g.P || k < h->g.kfrom || k > h->g.kto)
+        return set_err(h, PFTCC_ERR_INDEX, "set_ptcl_fcomp: irot or k out of range");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    // pfts_ptcls(irot, k, pinds(iptcl)) = comp (:471-476); the square sum is left as it is, as there
+    float2 *dst = h->ptcls + ((size_t)slot * h->g.K + (k - h->g.kfrom)) * h->g.P + (irot - 1);
+    CK(cudaMemcpyAsync(dst, comp, sizeof(float2), cudaMemcpyHostToDevice, h->stream), "set_ptcl_fcomp");
+    CK(cudaStreamSynchronize(h->stream), "set_ptcl_fcomp");
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_calc_ptcl_pspec(pftcc_handle *h, int iptcl, float *pspec)
+{
+    if (!h || !pspec) return set_err(h, PFTCC_ERR_ARG, "calc_ptcl_pspec: bad arguments");
+    SLOT_OR_FAIL(slot, iptcl);
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(ensure(h, (void **)&h->d_out, &h->out_cap, std::max<size_t>((size_t)h->g.K * sizeof(float), 256), "pspec"));
+    CK(launch_ptcl_pspec(h, slot, h->d_out), "calc_ptcl_pspec kernel");
+    CK(cudaMemcpyAsync(pspec, h->d_out, h->g.K * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "calc_ptcl_pspec");
+    CK(cudaStreamSynchronize(h->stream), "calc_ptcl_pspec");
+    return PFTCC_OK;
+}
+
+int pftcc_assign_pinds(const pftcc_handle *h, int *pinds)
+{
+    if (!h || !pinds) return PFTCC_ERR_ARG;
+    // self%pinds(pfromto(1):pfromto(2)): each index's particle slot, 1-based, 0 where not held
+    for (size_t i = 0; i < h->pinds.size(); ++i) pinds[i] = h->pinds[i];
+    return PFTCC_OK;
+}
+
+int pftcc_calc_roinv_corrmat(pftcc_handle *h, float *corrmat)
+{
+    if (!h || !corrmat) return set_err(h, PFTCC_ERR_ARG, "calc_roinv_corrmat: bad arguments");
+    if (h->nptcls != h->nrefs)
+        return set_err(h, PFTCC_ERR_ARG, "nptcls == nrefs in pftcc required; calc_roinv_corrmat");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    ST(exact_objfun_ok(h));
+    const int n = h->nptcls;
+    // particle iptcl = pfrom + g (g = 0..n-1) is correlated with references 1..g (iref < iptcl),
+    // the best rotation's value kept and the matrix symmetrised with 1 on the diagonal (:2207-2231)
+    std::vector<int> slot_of_g(n, -1);
+    for (int gq = 0; gq < n; ++gq) {
+        const int gi = h->pfrom + gq;
+        slot_of_g[gq] = gi <= h->pto ? h->pinds[gi - h->pfrom] - 1 : -1;
+        if (slot_of_g[gq] < 0)
+            return set_err(h, PFTCC_ERR_INDEX, "calc_roinv_corrmat: particles pfrom..pfrom+nptcls-1 must be held");
+    }
+    const size_t npairs = (size_t)n * (n - 1) / 2;
+    std::vector<float> mat((size_t)n * n, 1.f);
+    if (npairs > 0) {
+        ST(ensure_small(h, npairs, n, npairs, 1));
+        std::vector<Work> work(npairs);
+        std::vector<Group> groups;
+        size_t wi = 0;
+        for (int ip = 1; ip < n; ++ip) {
+            groups.push_back(Group{slot_of_g[ip], (int)wi, ip, (int)groups.size()});
+            for (int ir = 0; ir < ip; ++ir, ++wi) work[wi] = Work{ir, -1, (long long)wi};
+        }
+        CK(cudaMemcpyAsync(h->d_work, work.data(), wi * sizeof(Work), cudaMemcpyHostToDevice, h->stream), "corrmat");
+        CK(cudaMemcpyAsync(h->d_groups, groups.data(), groups.size() * sizeof(Group), cudaMemcpyHostToDevice, h->stream),
+           "corrmat");
+        CK(launch_exact(h, h->d_groups, (int)groups.size(), h->d_work, nullptr, MODE_ITEMMAX, exact_frame(h), 1,
+                        h->d_out, nullptr), "corrmat kernel");
+        std::vector<float> mx(npairs);
+        CK(cudaMemcpyAsync(mx.data(), h->d_out, npairs * sizeof(float), cudaMemcpyDeviceToHost, h->stream), "corrmat");
+        CK(cudaStreamSynchronize(h->stream), "corrmat");
+        wi = 0;
+        for (int ip = 1; ip < n; ++ip)
+            for (int ir = 0; ir < ip; ++ir, ++wi) {
+                mat[(size_t)ir * n + ip] = mx[wi];
+                mat[(size_t)ip * n + ir] = mx[wi];
+            }
+    }
+    std::copy(mat.begin(), mat.end(), corrmat);
+    return PFTCC_OK;
+}
+
 int pftcc_corr_all(pftcc_handle *h, int nshifts, const float *shifts, float *cc)
 {
     if (!h || !cc || nshifts < 0 || (nshifts > 0 && !shifts)) return set_err(h, PFTCC_ERR_ARG, "corr_all: bad arguments");

@@ -57,7 +57,7 @@ struct Group {          // all work items of one particle slot
     int out_best;       // index of the pftcc_best written in MODE_BEST
 };
 
-enum { MODE_FULL = 0, MODE_BEST = 1 };
+enum { MODE_FULL = 0, MODE_BEST = 1, MODE_ITEMMAX = 2 };   // ITEMMAX: out[w.out] = max over rotations
 
 // state of the tcgen05 stage 1 (packed operand geometry, device error word)
 struct UmmaState {
@@ -235,6 +235,8 @@ void host_euler2m(const double e[3], double *R, double *dR);
 // batched pftcc_orisrch_grad%minimize (k_orisrch.cu); the caller holds the lock
 int orisrch_batch(pftcc_handle *h, int n, const pftcc_orisrch_req *req, int maxits, double pgtol, double factr,
                   pftcc_orisrch_out *out);
+// calc_ptcl_pspec: mean power per shell of slot's particle, all K shells, into pspec_dev[K]
+cudaError_t launch_ptcl_pspec(pftcc_handle *h, int slot, float *pspec_dev);
 // matched-filter mode (k_matchfilt.cu): the shell factors of references r0..r0+n-1 (both sets);
 // the factors of reference set `set` on the m-domain spectra; prep_matchfilt requests
 // {iref (0-based), slot, irot, pad}

@@ -300,6 +300,31 @@ class polarft_corrcalc:
                                                   None if frcs is None else _f32p(frcs)))
         return (scores, frcs) if want_frc else scores
 
+    # ---- remaining procedures ------------------------------------------------------------------
+    def cp_refs(self, other: "polarft_corrcalc"):
+        """both reference sets copied from another object of the same shape"""
+        self._check(self._L.pftcc_cp_refs(self._h, other._h))
+
+    def set_ptcl_fcomp(self, iptcl: int, irot: int, k: int, comp: complex):
+        a = np.asarray([comp], np.complex64)
+        self._check(self._L.pftcc_set_ptcl_fcomp(self._h, int(iptcl), int(irot), int(k), _f32p(a.view(np.float32))))
+
+    def calc_ptcl_pspec(self, iptcl: int) -> np.ndarray:
+        out = np.zeros(self.K, np.float32)
+        self._check(self._L.pftcc_calc_ptcl_pspec(self._h, int(iptcl), _f32p(out)))
+        return out
+
+    def assign_pinds(self) -> np.ndarray:
+        out = np.zeros(self.cfg.pfromto[1] - self.cfg.pfromto[0] + 1, np.int32)
+        self._check(self._L.pftcc_assign_pinds(self._h, out.ctypes.data_as(C.POINTER(C.c_int))))
+        return out
+
+    def calc_roinv_corrmat(self) -> np.ndarray:
+        n = self.get_nptcls()
+        out = np.zeros((n, n), np.float32)
+        self._check(self._L.pftcc_calc_roinv_corrmat(self._h, _f32p(out)))
+        return out
+
     # ---- the matched-filter mode (new(..., match_filt=True)) ----------------------------------
     def set_ref_optlp(self, iref: int, optlp):
         """ref_optlp(kfrom:kstop, iref) = optlp (the reference's matched filter)"""
