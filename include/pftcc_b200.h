@@ -54,7 +54,10 @@ typedef struct pftcc_handle pftcc_handle;
 
 /* new() arguments plus the params_glob fields polarft_corrcalc reads implicitly
  * (boxmatch :235, ring2 -> nrots :251-252, kfromto/kstop :256-258, ctf :355-356,
- * l_match_filt :254). */
+ * l_match_filt :254).  Not served: params_glob%l_pssnr (the per-shell SSNR weighting of
+ * shellnorm_and_filter_ref :763-770 and prep_matchfilt :1006-1018) and clsfrcs = 'yes'
+ * (l_clsfrcs :415, the particle's own class filter ref_optlp(:, iptcl) at :976-980);
+ * the matched filter is always ref_optlp(:, iref). */
 typedef struct {
     int nrefs;            /* new(nrefs, ...)                                    */
     int pfromto[2];       /* new(..., pfromto, ...), global particle index range */
@@ -329,17 +332,18 @@ typedef struct { int iref, irot, found_better, nrefs_eval; float corr; int pad[3
 int pftcc_search_snhc(pftcc_handle *h, const int *order, const float *prev_corr, const int *cls_pops, int nrefs_bound,
                       unsigned long long seed, int precision, pftcc_snhc_out *out);
 
-/* gencorrs for npairs (reference, particle, shift) pairs that allocates no memory, for
- * callers that cannot let a library call cudaMalloc (work being captured into a CUDA
- * graph, applications that budget all device memory in their own pool, services
- * that must not grow after start-up).  No counterpart in the reference.  The work
- * descriptors live in a fixed 256 KiB device array that every GPU loading the library
- * holds until exit, so npairs is limited to 6553 (larger batches are rejected with
- * PFTCC_ERR_ARG -- split them).  iref/iptcl are 1-based as in pftcc_gencorrs, shifts is
- * [npairs][2] or NULL (gencorrs_cc_1), cc_dev a device buffer of npairs*nrots floats
- * written as cc_dev[pair*nrots + irot-1].  The first call on a device resolves the
- * array's device address (make it before any stream capture); calls that overlap on
- * the GPU race on the shared array -- order them on one stream. */
+/* gencorrs for npairs (reference, particle, shift) pairs that allocates no memory.  It
+ * is for callers that cannot let a library call cudaMalloc: applications that hand all
+ * device memory to their own pool at start-up (an allocation behind the pool's back can
+ * fail or fragment it) and services that must keep a fixed device footprint.  No
+ * counterpart in the reference.  The work descriptors live in a fixed 256 KiB device
+ * array that every GPU loading the library holds until exit, so npairs is limited to
+ * 6553 (larger batches are rejected with PFTCC_ERR_ARG -- split them).  iref/iptcl are
+ * 1-based as in pftcc_gencorrs, shifts is [npairs][2] or NULL (gencorrs_cc_1), cc_dev a
+ * device buffer of npairs*nrots floats written as cc_dev[pair*nrots + irot-1].  The
+ * first call on a device looks up the array's device address, so make that first call
+ * before any stream capture; calls that overlap on the GPU race on the shared array --
+ * order them on one stream. */
 int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *iref, const int *iptcl, const float *shifts,
                            float *cc_dev);
 

@@ -105,6 +105,8 @@ def lib():
         L.orc_fftpath_memoize.argtypes = [C.c_void_p, fp, fp]
         L.orc_fftpath_gencorrs.argtypes = [C.c_void_p, fp, fp, C.c_float, fp, fp, dp, dp, fp]
         L.orc_cpu_search.argtypes = [G, C.c_int, fp, C.c_int, fp, fp, C.c_int, fp, ip, ip, ip, fp, C.c_int]
+        L.orc_fftpath_allcorrs.argtypes = [G, C.c_int, fp, fp, fp, C.c_int, fp, fp, C.c_int]
+        L.orc_fftpath_allcorrs.restype = C.c_int
         L.orc_cpu_search.restype = C.c_int
         L.orc_cfft.argtypes = [C.c_int, dp, dp, C.c_int]
         _lib = L
@@ -450,3 +452,96 @@ def cpu_search(g: Geom, refs, ptcls, ctfmats, shifts, nthreads: int = 0):
                                 _P(sh, C.c_float), _P(br, C.c_int), _P(bro, C.c_int), _P(bs, C.c_int),
                                 _P(bcc, C.c_float), int(nthreads))
     return br, bro, bs, bcc, used
+
+
+def fftpath_allcorrs(g: Geom, refs, ptcl, ctf, shifts, nthreads: int = 0):
+    """Every correlation of one particle (K, P) against refs (nrefs, K, P) x shifts (ns, 2)
+    through the reference's FP32 FFT loop (gencorrs_cc_2 per pair, calc_corrs_over_k
+    :1132-1162), OpenMP over the pairs: float32 (nrefs, ns, nrots) and the threads used."""
+    refs = np.ascontiguousarray(refs, np.complex64)
+    sh = np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+    out = np.zeros((refs.shape[0], sh.shape[0], g.nrots), np.float32)
+    ctf32 = None if ctf is None else np.ascontiguousarray(ctf, np.float32)
+    used = lib().orc_fftpath_allcorrs(C.byref(g), refs.shape[0], _P(refs.view(np.float32), C.c_float),
+                                      _P(_c64(ptcl), C.c_float), _P(ctf32, C.c_float), sh.shape[0],
+                                      _P(sh, C.c_float), _P(out, C.c_float), int(nthreads))
+    return out, used
+
+
+def _ext(x):
+    """a half-circle polar FT x(..., P) extended over the full circle: x(n + P) = conj x(n)"""
+    return np.concatenate([x, np.conj(x)], axis=-1)
+
+
+def iter_allcorrs64(g: Geom, t: Tables, refs, ptcls, ctfs, shifts, frame: str = "ref", ref_chunk: int = 8):
+    """Every correlation of particles (np, K, P) against refs (nrefs, K, P) x shifts (ns, 2)
+    in FP64, yielded per block of references as (r0, r1, cc[np, r1 - r0, ns, nrots]).
+
+    The same sums as the direct oracle (gencorrs_cc_2 :1502-1534 with calc_corr_for_rot_8
+    :1218-1243 in the reference frame; gencorrs_ptclframe for the particle frame), each
+    circular correlation over the full circle evaluated through length-nrots FP64 FFTs:
+    with x~ the conjugate-symmetric extension (x~(n + P) = conj x(n)),
+        sum_{n<P} Re A(n) conj Q~(n + rot) = 1/(2N) Re sum_m F[A~](m) conj F[Q~](m) w^{-m rot}.
+    Reference frame: A = ref * ctf_p * shmat_s (gen_shmat_8 de Moivre phases, FP64), the
+    reference square sum over all K shells (:1531) or kfrom..kstop without shifts (:984).
+    Particle frame: A = ref * shmat_s against ctf_p~ Q~, normaliser
+    sum_k sum_n |ref(n)|^2 ctf_p~(n + rot)^2 times the particle square sum."""
+    import scipy.fft as sf
+    N, P, K, Ks = g.nrots, g.pftsz, g.K, g.Ks
+    refs = np.asarray(refs, np.complex64).astype(np.complex128)
+    Q = np.asarray(ptcls, np.complex64).astype(np.complex128)[:, :Ks]
+    npt, nr = Q.shape[0], refs.shape[0]
+    ctf = None if ctfs is None else np.asarray(ctfs, np.float64)
+    has_shift = shifts is not None
+    sh = np.stack([shmat(g, t, float(x), float(y)) for x, y in np.asarray(shifts, np.float64).reshape(-1, 2)]) \
+        if has_shift else np.ones((1, K, P), np.complex128)
+    ns = sh.shape[0]
+    sqp = np.sum(Q.real ** 2 + Q.imag ** 2, axis=(1, 2))
+    if frame == "ref":
+        FQc = np.conj(sf.fft(_ext(Q), axis=-1, workers=-1))                         # (np, Ks, N)
+        ksq = K if has_shift else Ks
+        for r0 in range(0, nr, ref_chunk):
+            r1 = min(nr, r0 + ref_chunk)
+            R = refs[r0:r1]
+            A = R[None, :, None] * sh[None, None]                                   # (1, rc, ns, K, P)
+            if ctf is not None:
+                A = A * ctf[:, None, None]                                          # (np, rc, ns, K, P)
+            A = np.broadcast_to(A, (npt,) + A.shape[1:])
+            sqr = np.sum(A[..., :ksq, :].real ** 2 + A[..., :ksq, :].imag ** 2, axis=(-2, -1))
+            FA = sf.fft(_ext(A[..., :Ks, :]), axis=-1, workers=-1)                  # (np, rc, ns, Ks, N)
+            X = np.einsum("prskm,pkm->prsm", FA, FQc, optimize=True)
+            num = sf.fft(X, axis=-1, workers=-1).real / (2.0 * N)
+            yield r0, r1, num / np.sqrt(sqr * sqp[:, None, None])[..., None]
+    elif frame == "ptcl":
+        Qc = Q if ctf is None else Q * ctf[:, :Ks]
+        FQc = np.conj(sf.fft(_ext(Qc), axis=-1, workers=-1))                        # (np, Ks, N)
+        R2 = refs[:, :Ks].real ** 2 + refs[:, :Ks].imag ** 2                        # (nr, Ks, P)
+        C2 = np.ones((npt, Ks, P)) if ctf is None else ctf[:, :Ks] ** 2
+        FR2 = sf.fft(np.concatenate([R2, R2], axis=-1), axis=-1, workers=-1)        # (nr, Ks, N)
+        FC2c = np.conj(sf.fft(np.concatenate([C2, C2], axis=-1), axis=-1, workers=-1))
+        Bm = np.ascontiguousarray(FQc.transpose(2, 1, 0))                           # (N, Ks, np)
+        for r0 in range(0, nr, ref_chunk):
+            r1 = min(nr, r0 + ref_chunk)
+            rc = r1 - r0
+            A = refs[r0:r1, None, :Ks] * sh[None, :, :Ks]                           # (rc, ns, Ks, P)
+            FA = sf.fft(_ext(A), axis=-1, workers=-1)                               # (rc, ns, Ks, N)
+            Am = np.ascontiguousarray(FA.reshape(rc * ns, Ks, N).transpose(2, 0, 1))  # (N, rc*ns, Ks)
+            X = np.matmul(Am, Bm)                                                   # (N, rc*ns, np)
+            X = X.transpose(2, 1, 0).reshape(npt, rc, ns, N)
+            num = sf.fft(X, axis=-1, workers=-1).real / (2.0 * N)
+            Y = np.einsum("rkm,pkm->prm", FR2[r0:r1], FC2c, optimize=True)          # (np, rc, N)
+            den = sf.fft(Y, axis=-1, workers=-1).real / (2.0 * N)
+            yield r0, r1, num / np.sqrt(den[:, :, None, :] * sqp[:, None, None, None])
+    else:
+        raise ValueError("frame must be 'ref' or 'ptcl'")
+
+
+def allcorrs64(g: Geom, t: Tables, refs, ptcls, ctfs, shifts, frame: str = "ref", ref_chunk: int = 8) -> np.ndarray:
+    """all of iter_allcorrs64 in one array (np, nrefs, ns, nrots), for small cases"""
+    nr = np.asarray(refs).shape[0]
+    out = None
+    for r0, r1, cc in iter_allcorrs64(g, t, refs, ptcls, ctfs, shifts, frame, ref_chunk):
+        if out is None:
+            out = np.zeros((cc.shape[0], nr) + cc.shape[2:], np.float64)
+        out[:, r0:r1] = cc
+    return out

@@ -787,6 +787,48 @@ void orc_fftpath_gencorrs(orc_fftpath *p, const float *ref, const float *ptcl_me
     free(pr); free(work); free(acc); free(sh8);
 }
 
+/* every correlation of one particle against nrefs references x nshifts shifts through the
+ * FP32 FFT path (gencorrs_cc_2 :1502-1534 per (reference, shift) pair, the particle's
+ * transforms memoized once as memoize_fft :864-877 does), OpenMP over the pairs.
+ * out[(r * nshifts + s) * nrots + irot - 1]; the error of the reference's own FP32 loop
+ * is measured on this output. */
+int orc_fftpath_allcorrs(const orc_geom *g, int nrefs, const float *refs, const float *ptcl, const float *ctfmat,
+                         int nshifts, const float *shifts, float *out, int nthreads)
+{
+    const int N = g->nrots, P = g->pftsz, K = K_OF(g), Ks = g->kstop - g->kfrom + 1;
+    float *polar = (float *)malloc(sizeof(float) * 2 * N * K);
+    double *at = (double *)malloc(sizeof(double) * N * K);
+    double *at1 = (double *)malloc(sizeof(double) * N);
+    orc_tables(g, polar, at, at1);
+    orc_fftpath *fp0 = orc_fftpath_new(g);
+    float *memo = (float *)malloc(sizeof(float) * orc_fftpath_memo_size(g));
+    orc_fftpath_memoize(fp0, ptcl, memo);
+    float sqp = 0.0f;
+    for (int j = 0; j < 2 * Ks * P; ++j) sqp += ptcl[j] * ptcl[j];
+    int used = 1;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    #pragma omp parallel
+    {
+#ifdef _OPENMP
+        #pragma omp single
+        used = omp_get_num_threads();
+#endif
+        orc_fftpath *fp = orc_fftpath_new(g);
+        #pragma omp for schedule(dynamic, 4)
+        for (int rs = 0; rs < nrefs * nshifts; ++rs) {
+            const int r = rs / nshifts, s = rs % nshifts;
+            orc_fftpath_gencorrs(fp, refs + (size_t)r * 2 * K * P, memo, sqp, ctfmat, shifts + 2 * s, at, at1,
+                                 out + (size_t)rs * N);
+        }
+        orc_fftpath_free(fp);
+    }
+    orc_fftpath_free(fp0);
+    free(memo); free(polar); free(at); free(at1);
+    return used;
+}
+
 /* exhaustive search: the greedy strategy's loop over all references
  * (simple_strategy2D_greedy.f90:33-58) with the shift grid of the exhaustive
  * in-plane search (simple_pftcc_shsrch_grad.f90:182-199), each call a

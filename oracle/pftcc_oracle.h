@@ -203,6 +203,12 @@ void orc_fftpath_gencorrs(orc_fftpath *p, const float *ref, const float *ptcl_me
                           const float *ctfmat, const float *shvec, const double *argtransf,
                           const double *argtransf_shellone, float *cc);
 
+/* all correlations of one particle ptcl [K][P] (ctfmat [K][P] float, nullable) against
+ * refs [nrefs][K][P] x shifts [nshifts][2] through the FP32 FFT path, OpenMP over the
+ * (reference, shift) pairs: out [nrefs][nshifts][nrots].  Returns the threads used. */
+int orc_fftpath_allcorrs(const orc_geom *g, int nrefs, const float *refs, const float *ptcl, const float *ctfmat,
+                         int nshifts, const float *shifts, float *out, int nthreads);
+
 /* exhaustive CPU search (greedy strategy over all refs x shift grid, OpenMP over particles).
  * refs [nrefs][K][P], ptcls [nptcls][K][P], ctfmats [nptcls][K][P] (float, nullable),
  * shifts [nshifts][2].  Output per particle: best ref (0-based), best irot (1-based),

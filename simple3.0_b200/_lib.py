@@ -2,7 +2,7 @@
 
 There is no fallback: if the shared library is missing or no sm_100 device is
 present the calls raise.  This mirrors what a Fortran ISO_C_BINDING interface
-module would bind (see INTEGRATION.md)."""
+module would bind."""
 from __future__ import annotations
 
 import ctypes as C

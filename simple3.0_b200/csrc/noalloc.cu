@@ -1,18 +1,18 @@
 // noalloc.cu -- gencorrs for a batch of (reference, particle, shift) pairs without any
-// device allocation, for callers that cannot let a library call cudaMalloc: code
-// running while a CUDA stream is being captured into a graph (cudaMalloc is not a
-// capturable operation), applications that hand all device memory to their own
-// pool and budget it up front, and long-running services that must not grow their
-// footprint after start-up.
+// device allocation.  It serves callers that cannot let a library call cudaMalloc:
+// applications that hand all device memory to their own pool at start-up and budget
+// it there (an allocation made behind the pool's back can fail or fragment it), and
+// long-running services that must keep a fixed device footprint after start-up.
 //
 // The per-call work descriptors live in one file-scope device array of a fixed size
-// (noalloc_scratch, 256 KiB); every GPU that loads this library holds that array
-// until the process exits.  Host code cannot use the symbol itself as a device
-// address, so the first call on each device resolves it with cudaGetSymbolAddress
-// (with that device current) and caches the pointer; make that first call before
-// any stream capture begins.  All calls share the array and each call rewrites the
-// part it uses (nothing in it has to start at zero); calls whose work overlaps on the
-// GPU race on it, so order them on one stream.
+// (noalloc_scratch, 256 KiB, so at most 6553 pairs per call); every GPU that loads this
+// library holds that array until the process exits.  In host code the array's name
+// stands for a host-side shadow, not a device address, so the first call on each
+// device resolves the address with cudaGetSymbolAddress (with that device current)
+// and caches it; make that first call before any stream capture begins.  All calls
+// share the array and each call rewrites the part it uses (nothing in it has to start
+// at zero); calls whose work overlaps on the GPU race on it, so order them on one
+// stream.
 #include "pftcc_internal.cuh"
 
 #include <mutex>
@@ -65,7 +65,10 @@ extern "C" int pftcc_gencorrs_noalloc(pftcc_handle *h, int npairs, const int *ir
         return set_err(h, PFTCC_ERR_STATE, "CTF is on but create_polar_absctfmats has not been called");
     if (h->objfun == PFTCC_OBJFUN_EUCLID && euclid_ready(h, 0) != PFTCC_OK) return PFTCC_ERR_STATE;
     if (exact_objfun_ok(h) != PFTCC_OK) return PFTCC_ERR_UNSUPPORTED;
-    if (snorm_ready(h, 0, h->nrefs) != PFTCC_OK) return PFTCC_ERR_CUDA;   // matched-filter factors (no allocation)
+    {   // matched-filter factors: computed into arrays that pftcc_new allocated
+        const int st = snorm_ready(h, 0, h->nrefs);
+        if (st != PFTCC_OK) return st;
+    }
     // host-side descriptors (validated) in a fixed host buffer guarded by the global lock,
     // then one copy into the fixed device scratch
     std::lock_guard<std::mutex> lk2(g_noalloc_host_mtx);

@@ -1442,7 +1442,17 @@ int pftcc_cp_refs(pftcc_handle *h, const pftcc_handle *src)
     if (src->nrefs != h->nrefs || src->g.K != h->g.K || src->g.P != h->g.P)
         return set_err(h, PFTCC_ERR_ARG, "cp_refs: the two objects' reference sets differ in shape");
     if (src->dev != h->dev) return set_err(h, PFTCC_ERR_ARG, "cp_refs: the two objects live on different devices");
-    std::lock_guard<std::mutex> lk(h->mtx);
+    // both objects locked (std::scoped_lock orders the two locks, so two threads copying in
+    // opposite directions cannot deadlock); src's references cannot change under the copy
+    std::mutex &src_mtx = const_cast<pftcc_handle *>(src)->mtx;
+    std::unique_lock<std::mutex> lk1, lk2;
+    if (src == h) {
+        lk1 = std::unique_lock<std::mutex>(h->mtx);
+    } else {
+        std::lock(h->mtx, src_mtx);
+        lk1 = std::unique_lock<std::mutex>(h->mtx, std::adopt_lock);
+        lk2 = std::unique_lock<std::mutex>(src_mtx, std::adopt_lock);
+    }
     cudaSetDevice(h->dev);
     const size_t bytes = (size_t)h->nrefs * h->g.K * h->g.P * sizeof(float2);
     // self%pfts_refs_odd = self2%pfts_refs_odd; self%pfts_refs_even = self2%pfts_refs_even (:491-495)

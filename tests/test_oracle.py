@@ -297,3 +297,50 @@ def test_snhc_pick_is_uniform_over_improving_rotations(O):
         counts[irot - 1] += 1
     assert set(np.flatnonzero(counts)) == set(good)
     assert np.all(np.abs(counts[good] - 1000) < 120)
+
+
+@pytest.mark.parametrize("geom", GEOMS)
+@pytest.mark.parametrize("frame", ["ref", "ptcl"])
+def test_batched_fp64_correlations_equal_direct_sums(O, geom, frame):
+    """the FFT-evaluated FP64 batch (iter_allcorrs64) equals the direct FP64 sums of
+    gencorrs_cc_2 / the particle frame for every (particle, reference, shift, rotation)"""
+    g = O.geom(*geom)
+    t = O.tables(g)
+    rng = np.random.default_rng(7)
+    refs = np.stack([rand_pft(rng, g.K, g.pftsz) for _ in range(3)])
+    ptcls = np.stack([(0.3 * refs[i % 3] + rand_pft(rng, g.K, g.pftsz)).astype(np.complex64) for i in range(2)])
+    ctfs = np.stack([O.ctfmat(g, t, O.make_ctf(dfx=1.6 + 0.4 * i, dfy=1.5 + 0.4 * i, angast=25.0 + 40 * i))
+                     for i in range(2)])
+    shifts = np.array([[0.0, 0.0], [0.7, -1.2], [-2.0, 1.5]])
+    got = O.allcorrs64(g, t, refs, ptcls, ctfs, shifts, frame=frame, ref_chunk=2)
+    fn = O.gencorrs if frame == "ref" else O.gencorrs_ptclframe
+    for p in range(2):
+        for r in range(3):
+            for s in range(3):
+                want = fn(g, t, refs[r], ptcls[p], ctfs[p], shifts[s])
+                assert np.max(np.abs(got[p, r, s] - want)) < 1e-12
+    # without shifts: gencorrs_cc_1 (reference square sum over kfrom..kstop)
+    g2 = O.geom(geom[0], geom[1], geom[2], geom[3], kstop=geom[2] - 3)
+    t2 = O.tables(g2)
+    got1 = O.allcorrs64(g2, t2, refs, ptcls, ctfs, None, frame=frame)
+    fn(g2, t2, refs[1], ptcls[0], ctfs[0], None)
+    assert np.max(np.abs(got1[0, 1, 0] - fn(g2, t2, refs[1], ptcls[0], ctfs[0], None))) < 1e-12
+
+
+def test_batched_fft_loop_equals_single_calls(O):
+    """fftpath_allcorrs (OpenMP over pairs) gives each pair's FFT-loop result (the particle
+    square sum is accumulated in a different order, hence the FP32 tolerance)"""
+    g = O.geom(128, 2, 20, 64)
+    t = O.tables(g)
+    rng = np.random.default_rng(8)
+    refs = np.stack([rand_pft(rng, g.K, g.pftsz) for _ in range(3)])
+    ptcl = (0.5 * refs[0] + rand_pft(rng, g.K, g.pftsz)).astype(np.complex64)
+    ctf = O.ctfmat(g, t, O.make_ctf(dfx=2.1, dfy=1.9, angast=10.0))
+    shifts = np.array([[0.0, 0.0], [0.5, -1.0]], np.float32)
+    got, used = O.fftpath_allcorrs(g, refs, ptcl, ctf, shifts, nthreads=2)
+    assert used >= 1
+    fp = O.FFTPath(g)
+    for r in range(3):
+        for s in range(2):
+            want = fp.gencorrs(refs[r], ptcl, ctf, shifts[s])
+            assert np.max(np.abs(got[r, s] - want)) < 1e-6 * np.abs(want).max()

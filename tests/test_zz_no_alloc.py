@@ -1,9 +1,10 @@
-"""GPU test of pftcc_gencorrs_noalloc, the gencorrs batch that allocates no memory
-(for callers that cannot let a library call cudaMalloc, e.g. inside CUDA graph
-capture or under their own fixed memory budget).  Called through the C ABI, its
-output must equal the allocating pftcc_gencorrs within the exact path's tolerance
-on two calls in a row (the second call reuses the shared fixed scratch).  The file
-is named to be collected last."""
+"""GPU test of pftcc_gencorrs_noalloc, the gencorrs batch that allocates no device
+memory (for callers that hand all device memory to their own pool at start-up, or
+that must keep a fixed device footprint, and so cannot let a library call
+cudaMalloc).  Called through the C ABI, its output must equal the allocating
+pftcc_gencorrs within the exact path's tolerance on two calls in a row (the second
+call reuses the shared fixed scratch), and the device's free memory must not change
+across a call.  The file is named to be collected last."""
 import numpy as np
 import pytest
 
@@ -28,10 +29,15 @@ def test_gencorrs_noalloc_matches_gencorrs(pkg):
     shifts = rng.uniform(-2, 2, (n, 2)).astype(np.float32)
     want = np.stack([pc.gencorrs(int(iref[i]), int(iptcl[i]), shifts[i]) for i in range(n)])
     want1 = np.stack([pc.gencorrs(int(iref[i]), int(iptcl[i])) for i in range(n)])
+    outs = [torch.full((n, w.nrots), float("nan"), dtype=torch.float32, device="cuda:0") for _ in range(2)]
     for call in range(2):
-        out = torch.full((n, w.nrots), float("nan"), dtype=torch.float32, device="cuda:0")
+        out = outs[call]
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(0)[0]
         pc.gencorrs_noalloc(iref, iptcl, shifts, out.data_ptr())
         torch.cuda.synchronize()
+        if call == 1:   # the first call may load the library's device code; later calls allocate nothing
+            assert torch.cuda.mem_get_info(0)[0] == free0
         got = out.cpu().numpy()
         assert np.max(np.abs(got - want)) < 1e-6, call
         out1 = torch.full((n, w.nrots), float("nan"), dtype=torch.float32, device="cuda:0")
