@@ -312,6 +312,37 @@ typedef struct { double x[3]; double f; int nevals, niter, converged, pad; } pft
 int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub,
                        int maxits, double pgtol, double factr, pftcc_refine_out *out);
 
+/* pftcc_shsrch_grad (simple_pftcc_shsrch_grad.f90:44-391) for n (reference, particle)
+ * problems at once, each with its own shift box lims = [[x_lo, x_hi], [y_lo, y_hi]]
+ * (ospec%limits).  The optimiser is L-BFGS-B as the reference specifies it (:67-68: line
+ * search ftol 1e-1, gtol 1e-3; factr 1e7, pgtol 1e-5, 15 pairs) on the cost
+ * -gencorr_for_rot_8 with the gradient of gencorr_grad_for_rot_8 (:85-131, the branch
+ * cfg.match_filt selects); maxits bounds its cost+gradient evaluations per run as
+ * simple_opt_lbfgsb.f90:120-122 does.  Every round's pending evaluations of all problems
+ * go to the GPU in one launch per kind (the single-rotation adjoint; gencorrs over all
+ * rotations with maxloc, in the reference frame).
+ *   PFTCC_SHSRCH_MINIMIZE, opt_angle = 1 (grad_shsrch_minimize :262-298): the in-plane
+ *     index from gencorrs at zero shift, optionally the 5 x 5 coarse grid
+ *     (coarse_search_opt_angle :364-389), then up to max_evals cycles of L-BFGS-B (the
+ *     in-plane index re-picked by gencorrs at every new iterate, :139-144) each followed by
+ *     a re-pick that ends the cycles when it keeps the index.
+ *   PFTCC_SHSRCH_MINIMIZE, opt_angle = 0 (:299-337): the fixed in-plane index req.irot,
+ *     optionally the 5 x 5 grid of coarse_search (:340-362), one L-BFGS-B run.
+ *   PFTCC_SHSRCH_EXHAUSTIVE (minimize_exhaustive :159-251): the coarse grid of step
+ *     (hi - lo) / (2 floor((hi - lo) / 4) + 1) around zero, two 3 x 3 refinements at half and
+ *     a quarter of the step, with the rotations limited to within halfrot degrees of req.irot
+ *     when halfrot > 0 (req.irot <= 0 means get_roind(0)), then L-BFGS-B from the best.
+ * out: irot (0 when minimize found nothing better than its start, as the reference
+ * signals), found_better, corr = cxy(1), shift = cxy(2:3) rotated into the reference frame
+ * by rotmat2d(get_rot(irot)); nevals counts the optimiser's cost+gradient evaluations and
+ * ncycles the L-BFGS-B runs. */
+enum { PFTCC_SHSRCH_MINIMIZE = 0, PFTCC_SHSRCH_EXHAUSTIVE = 1 };
+typedef struct { int opt_angle, coarse_init, maxits, max_evals; float halfrot; int pad; } pftcc_shsrch_opts;
+typedef struct { int iref, iptcl, irot, pad; float lims[2][2]; } pftcc_shsrch_req;
+typedef struct { int irot, found_better, nevals, ncycles; float corr, shift[2], pad; } pftcc_shsrch_out;
+int pftcc_shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts *opts, int n, const pftcc_shsrch_req *req,
+                       pftcc_shsrch_out *out);
+
 /* stochastic neighbourhood hill climbing over the references for every held particle
  * (strategy2D_snhc srch_snhc, simple_strategy2D_snhc.f90:33-93, with shcloc,
  * simple_rnd.f90:273-295): order is [nptcls][nrefs] (slot order; each row the particle's

@@ -10,6 +10,7 @@ import os
 
 from . import build as _build
 
+SHSRCH_MINIMIZE, SHSRCH_EXHAUSTIVE = 0, 1
 OK, ERR_ARG, ERR_INDEX, ERR_STATE, ERR_CUDA, ERR_OOM, ERR_TIMEOUT, ERR_NODEV, ERR_UNSUPPORTED = range(9)
 FRAME_REF, FRAME_PTCL = 0, 1
 PREC_EXACT, PREC_FP32, PREC_BF16X3 = 0, 1, 2
@@ -57,6 +58,21 @@ class RefineReq(C.Structure):
 class RefineOut(C.Structure):
     _fields_ = [("x", C.c_double * 3), ("f", C.c_double), ("nevals", C.c_int), ("niter", C.c_int),
                 ("converged", C.c_int), ("pad", C.c_int)]
+
+
+class ShsrchOpts(C.Structure):
+    _fields_ = [("opt_angle", C.c_int), ("coarse_init", C.c_int), ("maxits", C.c_int), ("max_evals", C.c_int),
+                ("halfrot", C.c_float), ("pad", C.c_int)]
+
+
+class ShsrchReq(C.Structure):
+    _fields_ = [("iref", C.c_int), ("iptcl", C.c_int), ("irot", C.c_int), ("pad", C.c_int),
+                ("lims", (C.c_float * 2) * 2)]
+
+
+class ShsrchOut(C.Structure):
+    _fields_ = [("irot", C.c_int), ("found_better", C.c_int), ("nevals", C.c_int), ("ncycles", C.c_int),
+                ("corr", C.c_float), ("shift", C.c_float * 2), ("pad", C.c_float)]
 
 
 class SnhcOut(C.Structure):
@@ -131,6 +147,7 @@ SIGNATURES = {
     "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
                            C.POINTER(RefineOut)],
     "pftcc_gencorrs_noalloc": [_h, C.c_int, _ip, _ip, _fp, _vp],
+    "pftcc_shsrch_batch": [_h, C.c_int, C.POINTER(ShsrchOpts), C.c_int, C.POINTER(ShsrchReq), C.POINTER(ShsrchOut)],
     "pftcc_search_snhc": [_h, _ip, _fp, _ip, C.c_int, C.c_ulonglong, C.c_int, C.POINTER(SnhcOut)],
     "pftcc_get_nrots": [_h, _ip],
     "pftcc_get_pftsz": [_h, _ip],

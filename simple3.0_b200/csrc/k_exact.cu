@@ -7,6 +7,8 @@
 // rotation at once, with the reference prepared exactly as gencorrs_cc_1/_2 do
 // (prep_ref4corr :961-985, gen_shmat_8 :1098-1120, :1526-1531).
 #include "pftcc_internal.cuh"
+
+#include <cstddef>
 #include <cmath>
 
 namespace pftcc {
@@ -205,7 +207,7 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
     const float *__restrict__ sqsums, const double *__restrict__ argtransf, const double *__restrict__ argtransf1,
     const Group *__restrict__ groups, const Work *__restrict__ work, const float *__restrict__ shifts, int mode,
     int cc1_kstop, const float *__restrict__ sig2, const float *__restrict__ pxls, const float *__restrict__ snorm,
-    int nrefs, float *__restrict__ out, pftcc_best *__restrict__ best)
+    int nrefs, float *__restrict__ out, pftcc_best *__restrict__ best, const uint8_t *__restrict__ rotmask)
 {
     extern __shared__ float4 smem4[];
     const int N = g.N, P = g.P;
@@ -364,7 +366,8 @@ __global__ void __launch_bounds__(EX_THREADS) k_exact(
                 cc = (float)(acc[u] / den);
             }
             if (mode == MODE_FULL) out[w.out + s] = cc;
-            if (cc > my_best) { my_best = cc; my_rot = s; }
+            // rotmask [group][N] (optional): rotations outside the mask take no part in the maximum
+            if (cc > my_best && (!rotmask || rotmask[(size_t)blockIdx.x * N + s])) { my_best = cc; my_rot = s; }
         }
         if (mode == MODE_BEST || mode == MODE_ITEMMAX) {
             // block argmax, lowest rotation on ties (maxloc)
@@ -419,7 +422,7 @@ static int exact_kc(const Geom &g, int frame, size_t *smem)
 template <int FRAME>
 static cudaError_t launch_exact_t(pftcc_handle *h, int kc, size_t smem, const Group *groups, int ngroups,
                                   const Work *work, const float *shifts, int mode, int cc1_kstop, float *out,
-                                  pftcc_best *best)
+                                  pftcc_best *best, const uint8_t *rotmask)
 {
     cudaError_t e = smem_limit((const void *)k_exact<FRAME>, smem);
     if (e != cudaSuccess) return e;
@@ -428,21 +431,24 @@ static cudaError_t launch_exact_t(pftcc_handle *h, int kc, size_t smem, const Gr
     KTimer kt(h, PFTCC_K_EXACT);
     k_exact<FRAME><<<ngroups, EX_THREADS, smem, h->stream>>>(
         h->g, kc, h->refs_even, h->refs_odd, h->ptcls, ctf, h->d_iseven, h->sqsums, h->argtransf, h->argtransf1,
-        groups, work, shifts, mode, cc1_kstop, h->d_sig2, h->d_pxls, snorm_ptr(h), h->nrefs, out, best);
+        groups, work, shifts, mode, cc1_kstop, h->d_sig2, h->d_pxls, snorm_ptr(h), h->nrefs, out, best, rotmask);
     return cudaGetLastError();
 }
 
 cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, const Work *work, const float *shifts,
-                         int mode, int frame, int cc1_kstop, float *out, pftcc_best *best)
+                         int mode, int frame, int cc1_kstop, float *out, pftcc_best *best, const uint8_t *rotmask)
 {
     if (frame == FRAME_EUCLID && (!h->d_sig2 || !h->d_pxls)) return cudaErrorInvalidValue;
     size_t smem;
     const int kc = exact_kc(h->g, frame, &smem);
     if (frame == PFTCC_FRAME_PTCL)
-        return launch_exact_t<PFTCC_FRAME_PTCL>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
+        return launch_exact_t<PFTCC_FRAME_PTCL>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best,
+                                                rotmask);
     if (frame == FRAME_EUCLID)
-        return launch_exact_t<FRAME_EUCLID>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
-    return launch_exact_t<PFTCC_FRAME_REF>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best);
+        return launch_exact_t<FRAME_EUCLID>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best,
+                                            rotmask);
+    return launch_exact_t<PFTCC_FRAME_REF>(h, kc, smem, groups, ngroups, work, shifts, mode, cc1_kstop, out, best,
+                                           rotmask);
 }
 
 // ---------------------------------------------------------------------------
@@ -456,6 +462,8 @@ cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, cons
 // One block per request.  ctf_mode 0: stored ctfmats (the drop-in calls);
 // ctf_mode 1: |CTF| and its derivative recomputed at defocus + ddf.
 struct RotReq { int iref, slot, irot, ctf_mode; double sx, sy, ddf; };
+static_assert(sizeof(RotReq) == sizeof(RotReqH) && offsetof(RotReq, sx) == offsetof(RotReqH, sx),
+              "RotReqH mirrors RotReq");
 
 __device__ __forceinline__ double ctf_abs_d(const pftcc_ctfparams &c, double s2, double ang, double ddf, double *dctf)
 {
@@ -584,6 +592,18 @@ cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, doubl
                                                 h->refs_odd, h->ptcls, h->ctfmats, h->d_ctfp, h->d_iseven, h->polar,
                                                 h->argtransf, h->argtransf1, h->cfg.with_ctf && h->ctf_ready,
                                                 match_filt, snorm_ptr(h), h->nrefs, out5);
+    return cudaGetLastError();
+}
+
+// n single-rotation requests already on the device (reqs_dev: RotReq layout, see
+// pftcc_internal.cuh), out5 [n][5] = f, df/dsx, df/dsy, df/ddf, unused
+cudaError_t launch_rot_reqs(pftcc_handle *h, const void *reqs_dev, int n, double *out5)
+{
+    PFTCC_LAUNCH(h);
+    k_for_rot<<<n, FR_THREADS, 0, h->stream>>>(h->g, reinterpret_cast<const RotReq *>(reqs_dev), h->refs_even,
+                                                h->refs_odd, h->ptcls, h->ctfmats, h->d_ctfp, h->d_iseven, h->polar,
+                                                h->argtransf, h->argtransf1, h->cfg.with_ctf && h->ctf_ready,
+                                                h->cfg.match_filt, snorm_ptr(h), h->nrefs, out5);
     return cudaGetLastError();
 }
 

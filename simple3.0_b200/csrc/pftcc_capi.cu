@@ -1688,6 +1688,39 @@ int pftcc_refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, cons
     return refine_batch(h, n, req, lb, ub, maxits, pgtol, factr, out);
 }
 
+int pftcc_shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts *opts, int n, const pftcc_shsrch_req *req,
+                       pftcc_shsrch_out *out)
+{
+    if (!h || !opts || n < 0 || (n > 0 && (!req || !out))) return set_err(h, PFTCC_ERR_ARG, "shsrch_batch: bad arguments");
+    if (mode != PFTCC_SHSRCH_MINIMIZE && mode != PFTCC_SHSRCH_EXHAUSTIVE)
+        return set_err(h, PFTCC_ERR_ARG, "shsrch_batch: mode must be PFTCC_SHSRCH_MINIMIZE or PFTCC_SHSRCH_EXHAUSTIVE");
+    if (opts->maxits < 1 || opts->max_evals < 1) return set_err(h, PFTCC_ERR_ARG, "shsrch_batch: maxits and max_evals >= 1");
+    if (n == 0) return PFTCC_OK;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    if (h->cfg.ctf_frame != PFTCC_FRAME_REF)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "the shift search is served in the reference frame");
+    // minimize_exhaustive's rotation window (:167-170)
+    if (mode == PFTCC_SHSRCH_EXHAUSTIVE && opts->halfrot > 0.f &&
+        (opts->halfrot >= 180.f || opts->halfrot < fabsf(h->angtab[1] - h->angtab[0])))
+        return set_err(h, PFTCC_ERR_ARG, "shsrch_batch: invalid rotation boundary (halfrot)");
+    std::vector<int> slots(n);
+    for (int i = 0; i < n; ++i) {
+        if (req[i].iref < 1 || req[i].iref > h->nrefs) return set_err(h, PFTCC_ERR_INDEX, "shsrch_batch: iref");
+        const int sl = slot_of(h, req[i].iptcl);
+        if (sl < 0) return set_err(h, PFTCC_ERR_INDEX, "shsrch_batch: particle not held");
+        slots[i] = sl;
+        if (mode == PFTCC_SHSRCH_MINIMIZE && !opts->opt_angle && (req[i].irot < 1 || req[i].irot > h->g.N))
+            return set_err(h, PFTCC_ERR_INDEX, "shsrch_batch: irot");
+        if (mode == PFTCC_SHSRCH_EXHAUSTIVE && req[i].irot > h->g.N) return set_err(h, PFTCC_ERR_INDEX, "shsrch_batch: irot");
+        if (!(req[i].lims[0][0] <= req[i].lims[0][1]) || !(req[i].lims[1][0] <= req[i].lims[1][1]))
+            return set_err(h, PFTCC_ERR_ARG, "shsrch_batch: empty shift box");
+    }
+    ST(check_ctf_state(h));
+    ST(exact_objfun_ok(h));
+    return shsrch_batch(h, mode, *opts, n, req, slots.data(), out);
+}
+
 }  // extern "C"
 
 // pending requests of the adjoint, evaluated in one launch (the caller holds the lock)

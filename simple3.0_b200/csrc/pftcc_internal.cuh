@@ -201,9 +201,16 @@ cudaError_t launch_fdf_project_polar(pftcc_handle *h, int box, const float2 *cub
 cudaError_t launch_ctfmat(pftcc_handle *h, const pftcc_ctfparams *params, int n, float *out, float ddf,
                           int derivative);
 cudaError_t launch_sqsums(pftcc_handle *h, int first_slot, int n);
+// rotmask (optional) [ngroups][N]: MODE_BEST / MODE_ITEMMAX take their maxima over the
+// rotations whose mask byte is non-zero
 cudaError_t launch_exact(pftcc_handle *h, const Group *groups, int ngroups, const Work *work,
                          const float *shifts, int mode, int frame, int cc1_kstop, float *out,
-                         pftcc_best *best);
+                         pftcc_best *best, const uint8_t *rotmask = nullptr);
+// single-rotation correlation requests for k_for_rot: iref 0-based, slot, irot 1-based,
+// ctf_mode 0 = the stored |CTF| matrices (the drop-in calls), 1 = |CTF| recomputed at
+// defocus + ddf; out5 [n][5] = f, df/dsx, df/dsy, df/ddf, unused
+struct RotReqH { int iref, slot, irot, ctf_mode; double sx, sy, ddf; };
+cudaError_t launch_rot_reqs(pftcc_handle *h, const void *reqs_dev, int n, double *out5);
 cudaError_t launch_for_rot(pftcc_handle *h, int iref, int slot, double sx, double sy, int irot,
                            int match_filt, int want_grad, double ddf, double *out5);
 cudaError_t launch_grad_batch(pftcc_handle *h, const pftcc_grad_req *req_dev, const int *slots_dev, int nreq,
@@ -266,6 +273,10 @@ cudaError_t launch_specscore(pftcc_handle *h, const FrcReq *reqs_dev, int nreq, 
 // batched bound-constrained quasi-Newton refinement (refine.cu)
 int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const double *lb, const double *ub, int maxits,
                  double pgtol, double factr, pftcc_refine_out *out);
+
+// batched pftcc_shsrch_grad (shsrch.cu); slots[n] the particles' slots, the caller holds the lock
+int shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts &o, int n, const pftcc_shsrch_req *req,
+                 const int *slots, pftcc_shsrch_out *out);
 
 // tcgen05 stage 1 (k_umma.cu)
 int umma_check(pftcc_handle *h);

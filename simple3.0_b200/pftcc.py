@@ -592,6 +592,30 @@ class polarft_corrcalc:
         return (x, np.array([o.f for o in out]), np.array([o.nevals for o in out]),
                 np.array([o.niter for o in out]), np.array([o.converged for o in out], bool))
 
+    def shsrch_batch(self, iref, iptcl, lims, mode: str = "minimize", irot=0, opt_angle: bool = True,
+                     coarse_init: bool = False, maxits: int = 100, max_evals: int = 5, halfrot: float = 0.0):
+        """pftcc_shsrch_grad (minimize / minimize_exhaustive) for many (reference, particle)
+        problems; lims (2, 2) for all problems or (n, 2, 2) per problem.  Returns a structured
+        array (irot, found_better, nevals, ncycles, corr, shift[2]) per problem"""
+        iref, iptcl, irot = (np.atleast_1d(np.asarray(v)) for v in (iref, iptcl, irot))
+        n = max(iref.size, iptcl.size)
+        lims = np.broadcast_to(np.asarray(lims, np.float32), (n, 2, 2))
+        req = (_lib.ShsrchReq * n)()
+        for i in range(n):
+            req[i].iref, req[i].iptcl = int(iref.flat[i % iref.size]), int(iptcl.flat[i % iptcl.size])
+            req[i].irot = int(irot.flat[i % irot.size])
+            for a in range(2):
+                for b in range(2):
+                    req[i].lims[a][b] = float(lims[i, a, b])
+        opts = _lib.ShsrchOpts(int(bool(opt_angle)), int(bool(coarse_init)), int(maxits), int(max_evals),
+                               float(halfrot), 0)
+        out = (_lib.ShsrchOut * n)()
+        m = {"minimize": _lib.SHSRCH_MINIMIZE, "exhaustive": _lib.SHSRCH_EXHAUSTIVE}[mode]
+        self._check(self._L.pftcc_shsrch_batch(self._h, m, C.byref(opts), n, req, out))
+        dt = np.dtype([("irot", np.int32), ("found_better", np.int32), ("nevals", np.int32), ("ncycles", np.int32),
+                       ("corr", np.float32), ("shift", np.float32, 2), ("pad", np.float32)])
+        return np.frombuffer(out, dtype=dt).copy()
+
     # ---- GETTERS ----------------------------------------------------------------------------
     def get_nrots(self) -> int:
         return self._geti(self._L.pftcc_get_nrots)
