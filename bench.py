@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--nrefs", type=int, default=0, help="override the reference count (testing)")
     ap.add_argument("--ntop", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-arms", action="store_true", help="skip the FP32 / exact / reference-frame arms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
@@ -343,6 +344,26 @@ def run_ours(args):
                "h2d_bytes_per_step": int(host_cm.numel() * host_cm.element_size() + w.nptcls * 36),
                "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": ems}
 
+    # the other arms on the same workload, after the timed region: the plain FP32 m-domain
+    # search (the BF16 split's comparison), the exact drop-in kernel on a bounded sample, and the
+    # search in the reference CTF frame (the drop-in semantics: top 8 re-scored by the exact
+    # kernel).  Device time over steps with CUDA events on the launching stream.
+    arms = None
+    if not args.no_arms and args.precision == "bf16x3":
+        arms = other_arms(pkg, pc, w, shifts, parts, r_host, ctfp, cmats, best, stream, dev, args, world)
+    if arms is not None:
+        arms["bf16x3_over_fp32"] = value / arms["fp32_mdomain"]["value"]
+        # the contraction's tensor work (3 issued BF16 products per complex MAC) over the whole step
+        fl3, _ = algorithmic_costs(w, ns, "stage1")
+        st1 = prof.get("stage1", (0.0, 0))
+        roof["tensor"] = {"kernel": "k_umma_stage1", "issued_flops_per_step": fl3,
+                          "achieved_stage1": fl3 / (st1[0] / args.steps / 1e3) / 1e12 if st1[0] else None,
+                          "achieved_whole_step": fl3 / (ms / 1e3) / 1e12, "peak": tc_peak, "unit": "TFLOP/s",
+                          "peak_source": f"{peak_src} bf16 sustained"}
+        if st1[0]:
+            roof["tensor"]["frac_stage1"] = roof["tensor"]["achieved_stage1"] / tc_peak
+        roof["tensor"]["frac_whole_step"] = roof["tensor"]["achieved_whole_step"] / tc_peak
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_sample(pkg, entry.load_oracle(), w, shifts, args.cpu_seconds)
@@ -358,10 +379,72 @@ def run_ours(args):
                            "l2": "inputs larger than L2 (1.33 GB particle FTs)", "parallelism": f"dp{world}"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks}
+        if arms is not None:
+            line["value_fp32"] = arms["fp32_mdomain"]["value"]
+            line["bf16_over_fp32"] = arms["bf16x3_over_fp32"]
+            line["arms"] = arms
         print(json.dumps(line), flush=True)
     pc.kill()
     if world > 1:
         dist.destroy_process_group()
+
+
+def other_arms(pkg, pc, w, shifts, parts, r_host, ctfp, cmats, best, stream, dev, args, world):
+    """rates of the other search paths on the same workload (evals/s, device time)"""
+    import torch
+    ns = len(shifts)
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    def handle(nrefs, nptcls, frame, cp):
+        h = pkg.polarft_corrcalc()
+        h.new(nrefs, (1, nptcls), box=w.box, nrots=w.nrots, kfromto=(w.kfrom, w.kto), ctf=True, ctf_frame=frame,
+              device=dev.index)
+        h.set_stream(stream.cuda_stream)
+        h.set_refs(1, r_host[:nrefs], True)
+        h.set_refs(1, r_host[:nrefs], False)
+        h.polarize_ptcls_dev(0, nptcls, cmats.data_ptr())
+        h.create_polar_absctfmats(cp)
+        return h
+
+    out = {}
+    k = max(1, min(args.steps, 3))
+    # plain FP32: the m-domain contraction on the CUDA cores, FP32 end to end
+    ms32 = timed(lambda: pc.search_best_dev(shifts, "fp32", args.ntop, best.data_ptr()), k, 1)
+    out["fp32_mdomain"] = {"value": evals_per_step(w, ns) * world / (ms32 / 1e3), "ms_per_step": ms32, "steps": k,
+                           "what": "search_best PFTCC_PREC_FP32 (particle frame, the same top-8 re-score), "
+                                   "inputs resident"}
+    # the exact drop-in kernel (direct sums, FP32 products, FP64 accumulation) on a bounded
+    # sample: 2 particles per SM x 50 references x every shift x every rotation
+    ne, nre = min(w.nptcls, 296), min(w.nrefs, 50)
+    pe = handle(nre, ne, "ref", pkg.ctfparams_array(ne, smpd=w.smpd, kv=w.kv, cs=w.cs, fraca=w.fraca,
+                                                    dfx=parts.dfx[:ne], dfy=parts.dfy[:ne], angast=parts.angast[:ne]))
+    bdev = torch.empty((ne, 4), dtype=torch.int32, device=dev)
+    msx = timed(lambda: pe.search_best_dev(shifts, "exact", 0, bdev.data_ptr()), 1, 1)
+    out["exact_ref_frame"] = {"value": float(ne) * nre * ns * w.nrots * world / (msx / 1e3), "ms_per_step": msx,
+                              "sample": f"{ne} particles x {nre} refs x {ns} shifts x {w.nrots} rots",
+                              "what": "search_best PFTCC_PREC_EXACT (the drop-in gencorrs kernel), inputs resident"}
+    pe.kill()
+    # the m-domain search in the reference frame: particle-frame screening with BF16 products,
+    # the top 8 re-scored by the exact kernel in the reference frame
+    pr = handle(w.nrefs, w.nptcls, "ref", ctfp)
+    kr = max(1, min(args.steps, 2))
+    msr = timed(lambda: pr.search_best_dev(shifts, "bf16x3", 8, best.data_ptr()), kr, 1)
+    out["bf16x3_ref_frame"] = {"value": evals_per_step(w, ns) * world / (msr / 1e3), "ms_per_step": msr, "steps": kr,
+                               "what": "search_best PFTCC_PREC_BF16X3 on a reference-frame handle: top 8 re-scored "
+                                       "by the exact kernel in the reference frame, inputs resident"}
+    pr.kill()
+    return out
 
 
 # ------------------------------------------------------------------ precision report

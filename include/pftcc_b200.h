@@ -406,6 +406,12 @@ int pftcc_synchronize(pftcc_handle *h);
  * handle's own stream) -- lets a caller order the library with its own kernels and
  * time it with events on that stream */
 int pftcc_set_stream(pftcc_handle *h, void *stream);
+/* bounded waits of the tensor-core kernels (no counterpart in the reference): a pipeline
+ * wait inside k_umma_stage1 gives up after `polls` polls of its barrier (0 restores the
+ * default, about a second), the kernel then drains the copies and MMAs it has issued,
+ * frees its tensor memory and returns, and the call reports PFTCC_ERR_TIMEOUT.  A short
+ * limit lets a caller (or a test) exercise that path on a normal launch. */
+int pftcc_set_wait_limit(pftcc_handle *h, long long polls);
 /* per-kernel device timing with CUDA events recorded on the handle's stream around
  * each launch of a kernel class (PFTCC_K_*): enable, then read total milliseconds and
  * launch counts (reading synchronises the stream), reset clears the totals */

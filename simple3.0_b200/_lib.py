@@ -168,6 +168,7 @@ SIGNATURES = {
     "pftcc_kernel_launches": ([_h], C.c_longlong),
     "pftcc_synchronize": [_h],
     "pftcc_set_stream": [_h, _vp],
+    "pftcc_set_wait_limit": [_h, C.c_longlong],
     "pftcc_prof_enable": [_h, C.c_int],
     "pftcc_prof_read": [_h, C.c_int, _dp, C.POINTER(C.c_longlong)],
     "pftcc_prof_reset": [_h],

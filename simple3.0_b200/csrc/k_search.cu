@@ -1215,6 +1215,10 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     // the top-ntop re-score: FP32 m-domain in the particle frame, the exact kernel in
     // the reference frame
     const bool md_rescore = ntop > 0 && fast_s2 && h->cfg.ctf_frame == PFTCC_FRAME_PTCL;
+    if (precision == PFTCC_PREC_BF16X3) {
+        const int st = umma_reset(h);
+        if (st != PFTCC_OK) return st;
+    }
     for (int grp = 0; grp < 2; ++grp) {
         const int gc0 = grp == 0 ? 0 : n_even, gc1 = grp == 0 ? n_even : np;
         if (gc1 <= gc0) continue;

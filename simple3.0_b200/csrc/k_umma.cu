@@ -31,7 +31,9 @@
 //            written out with one TMA bulk store each to Z[plane][col][rs]
 // The factor 4 of X is carried by the packed particle operand (exact in BF16).
 // Every mbarrier wait is bounded; on timeout the kernel records an error code,
-// drains its own outstanding copies (bounded), frees its TMEM and returns.
+// drains its own outstanding copies (bounded), frees its TMEM and returns.  The pipeline
+// waits take their poll limit from the launch (pftcc_set_wait_limit); the drains keep the
+// full limit, so a short limit never leaves a copy or an MMA running after the exit.
 #include "pftcc_internal.cuh"
 
 #include <cuda.h>
@@ -68,6 +70,8 @@ struct UmmaParams {
     float2 *X;          // output Z: [P][xcols][xrows]
     int xrows, xcols;
     int *err;           // device error word (0 = ok)
+    long long wait_limit;   // polls of a pipeline wait before the kernel gives up (the drains of
+                            // copies and MMAs already issued always use WAIT_LIMIT)
 };
 
 // ---- PTX wrappers --------------------------------------------------------------------
@@ -101,10 +105,10 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait: false on timeout or when another role has aborted
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag)
+// bounded wait: false after `limit` polls or when another role has aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, long long limit)
 {
-    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+    for (long long i = 0; i < limit; ++i) {
         if (mbar_try(bar, parity)) return true;
         if (*abort_flag) return false;
         if (i > 64) __nanosleep(64);
@@ -258,14 +262,14 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             const int pm[2] = {mp, mp == 0 ? P : P - mp};
             // both planes' particle tiles, one at a time through sA (the MMA issuer copies each to TMEM)
             for (int h = 0; h < 2; ++h, ++na) {
-                if (na > 0 && !mbar_wait(a_empty, (uint32_t)((na - 1) & 1), abort_flag)) { fail(1); ok = false; break; }
+                if (na > 0 && !mbar_wait(a_empty, (uint32_t)((na - 1) & 1), abort_flag, up.wait_limit)) { fail(1); ok = false; break; }
                 mbar_expect_tx(a_full, a_bytes);
                 bulk_load(sA, up.P16 + (size_t)(pm[h] * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
             }
             if (!ok) break;
             for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
                 const int s = (int)(itb % up.stages);
-                if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag)) {
+                if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag, up.wait_limit)) {
                     fail(2); ok = false; break;
                 }
                 mbar_expect_tx(full + s, 2 * b_bytes);
@@ -297,10 +301,10 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             if (ii > 0) {
                 // the previous item's MMAs read the TMEM particle tiles: let them finish first
                 umma_commit(item_done);
-                if (!mbar_wait(item_done, (uint32_t)((ii - 1) & 1), abort_flag)) { fail(7); ok = false; break; }
+                if (!mbar_wait(item_done, (uint32_t)((ii - 1) & 1), abort_flag, up.wait_limit)) { fail(7); ok = false; break; }
             }
             for (int h = 0; h < 2; ++h, ++na) {
-                if (!mbar_wait(a_full, (uint32_t)(na & 1), abort_flag)) { fail(3); ok = false; break; }
+                if (!mbar_wait(a_full, (uint32_t)(na & 1), abort_flag, up.wait_limit)) { fail(3); ok = false; break; }
                 tc_fence_after();
                 const uint32_t tcol = tmem_base + ACC_COLS + (uint32_t)(h * acol);
                 for (int st = 0; st < up.KC / 2; ++st)
@@ -310,9 +314,9 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             if (!ok) break;
             for (int j = 0; j < up.n_rtiles; ++j, ++itb, ++tacc) {
                 const int s = (int)(itb % up.stages);
-                if (!mbar_wait(full + s, (uint32_t)((itb / up.stages) & 1), abort_flag)) { fail(4); ok = false; break; }
+                if (!mbar_wait(full + s, (uint32_t)((itb / up.stages) & 1), abort_flag, up.wait_limit)) { fail(4); ok = false; break; }
                 const int acc = (int)(tacc & 1);
-                if (tacc >= 2 && !mbar_wait(t_empty + acc, (uint32_t)((tacc / 2 - 1) & 1), abort_flag)) {
+                if (tacc >= 2 && !mbar_wait(t_empty + acc, (uint32_t)((tacc / 2 - 1) & 1), abort_flag, up.wait_limit)) {
                     fail(5); ok = false; break;
                 }
                 tc_fence_after();
@@ -355,7 +359,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
             for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
                 const int acc = (int)(tacc & 1);
                 // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
-                const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag));
+                const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag, up.wait_limit));
                 if (!got) { if (lane == 0) fail(6); ok = false; break; }
                 tc_fence_after();
                 // both planes' 64 columns in flight at once, one wait; the accumulator is handed
@@ -545,10 +549,6 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
         if (st) return st;
         st = ensure(h, (void **)&ws.B16, &ws.B16_elems, p16 * sizeof(__nv_bfloat16), "packed particles");
         if (st) return st;
-        if (!us.err) {
-            st = dev_alloc(h, (void **)&us.err, sizeof(int), "umma error word");
-            if (st) return st;
-        }
         us.Kp = Kp; us.KC = KC; us.rtiles = rtiles; us.ptiles = ptiles; us.group_c0 = c0;
         int dev = 0;
         cudaGetDevice(&dev);
@@ -560,7 +560,6 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
         PFTCC_LAUNCH(h);
         k_pack_cols<<<us.sms * 8, 256, 0, h->stream>>>(M, Ks, Kp, KC, ptiles, cols_pad, c0, UB, ws.B16);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "pack cols");
-        if ((e = cudaMemsetAsync(us.err, 0, sizeof(int), h->stream)) != cudaSuccess) return cuda_err(h, e, "err reset");
         return PFTCC_OK;
     }
     if (rs0 % U_RS || nrs_w % U_RS || (c0 - us.group_c0) % U_BM || ncols_w % U_BM)
@@ -593,6 +592,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     up.P16 = ws.B16; up.R16 = ws.A16;
     up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
     up.err = us.err;
+    up.wait_limit = h->wait_limit > 0 ? h->wait_limit : WAIT_LIMIT;
     const size_t smem = 1024 + a_bytes + stages * 2 * b_bytes + tail;
     if ((e = smem_limit((const void *)k_umma_stage1, smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
@@ -603,6 +603,17 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmX, up);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "umma stage 1 launch");
     return PFTCC_OK;
+}
+
+int umma_reset(pftcc_handle *h)
+{
+    UmmaState &us = ustate(h);
+    if (!us.err) {
+        const int st = dev_alloc(h, (void **)&us.err, sizeof(int), "umma error word");
+        if (st) return st;
+    }
+    const cudaError_t e = cudaMemsetAsync(us.err, 0, sizeof(int), h->stream);
+    return e == cudaSuccess ? PFTCC_OK : cuda_err(h, e, "umma error word reset");
 }
 
 int umma_check(pftcc_handle *h)

@@ -1871,6 +1871,14 @@ int pftcc_set_stream(pftcc_handle *h, void *stream)
     return PFTCC_OK;
 }
 
+int pftcc_set_wait_limit(pftcc_handle *h, long long polls)
+{
+    if (!h || polls < 0) return set_err(h, PFTCC_ERR_ARG, "set_wait_limit: polls >= 0");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    h->wait_limit = polls;
+    return PFTCC_OK;
+}
+
 static void prof_collect(pftcc_handle *h)
 {
     if (h->prof_pending.empty()) return;

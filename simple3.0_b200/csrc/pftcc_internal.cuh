@@ -153,6 +153,7 @@ struct pftcc_handle {
     std::mutex mtx;
     std::string last_err;
     long long launches = 0;
+    long long wait_limit = 0;            // pipeline-wait polls of the tcgen05 kernels (0 = default)
     cudaStream_t own_stream = nullptr;
     // per-kernel-class event timing
     int prof = 0;
@@ -279,6 +280,8 @@ int shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts &o, int n, c
                  const int *slots, pftcc_shsrch_out *out);
 
 // tcgen05 stage 1 (k_umma.cu)
+// the device error word cleared once per search (every stage-1 launch of the search may set it)
+int umma_reset(pftcc_handle *h);
 int umma_check(pftcc_handle *h);
 void umma_free(pftcc_handle *h);
 

@@ -678,6 +678,11 @@ class polarft_corrcalc:
     def synchronize(self):
         self._check(self._L.pftcc_synchronize(self._h))
 
+    def set_wait_limit(self, polls: int):
+        """polls of a tensor-core pipeline wait before the call gives up with PFTCC_ERR_TIMEOUT
+        (0 = the default)"""
+        self._check(self._L.pftcc_set_wait_limit(self._h, int(polls)))
+
     def set_stream(self, stream_handle: int | None):
         """run on a caller's cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)"""
         self._check(self._L.pftcc_set_stream(self._h, None if not stream_handle else C.c_void_p(stream_handle)))
