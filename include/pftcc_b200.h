@@ -130,13 +130,25 @@ enum { PFTCC_CTFFLAG_NO = 0, PFTCC_CTFFLAG_YES = 1, PFTCC_CTFFLAG_FLIP = 2 };
  * >= boxmatch = cfg.box), imgs [n][box_in][box_in] real, rmat(x, y) order: noise normalisation
  * against the background outside the disc of radius msk, FFT, shift by -(x, y) = -xy[2 i..],
  * the CTF phase flip for ctfflag[i] == PFTCC_CTFFLAG_YES (ctf[i]; ctf may be NULL when no flag
- * is YES), inverse FFT, clip to boxmatch, soft mask of radius msk (no inner or focus mask),
+ * is YES), inverse FFT, clip to boxmatch, soft mask of radius msk,
  * FFT and the factor boxmatch^2 / box_in^2, then the polar gridding into slots
  * first_slot..first_slot+n-1 (griddev 'no'); the _dev form takes the images in device memory */
 int pftcc_prep_ptcls(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
                      const int *ctfflag, const pftcc_ctfparams *ctf, float msk);
 int pftcc_prep_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
                          const int *ctfflag, const pftcc_ctfparams *ctf, float msk);
+/* the same with prepimg4align's other mask modes (:349-362): msk as above (the noise
+ * normalisation's disc, build_glob%lmsk); inner > 0 (params_glob%l_innermsk) masks with the
+ * inner cosine edge too, mask(msk, 'soft', inner, width), width <= 0 meaning the default 10;
+ * else focusmsk > 0 (params_glob%l_focusmsk) takes mask(focusmsk, 'soft') for the final mask;
+ * griddev = 1 (params_glob%griddev 'yes') divides the masked image by the gridding's instrument
+ * function (div_by_instrfun, simple_polarizer.f90:111-116) and grids with un-normalised
+ * weights (init_polarizer :87) */
+typedef struct { float msk, inner, width, focusmsk; int griddev; } pftcc_prep_opts;
+int pftcc_prep_ptcls_opts(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
+                          const int *ctfflag, const pftcc_ctfparams *ctf, const pftcc_prep_opts *opts);
+int pftcc_prep_ptcls_opts_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
+                              const int *ctfflag, const pftcc_ctfparams *ctf, const pftcc_prep_opts *opts);
 
 /* ---- polar projection of a volume -------------------------------------------------- */
 /* projector%expand_cmat (simple_projector.f90:66-132): the volume's half FT

@@ -90,6 +90,8 @@ def lib():
         L.orc_savgol7.argtypes = [C.c_int, dp]
         L.orc_prep_matchfilt.argtypes = [G, fp, dp, fp, C.c_int, fp]
         L.orc_prepimg4align.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.POINTER(Ctf), dp]
+        L.orc_prepimg4align_opts.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                             C.c_int, C.c_double, C.c_double, C.POINTER(Ctf), dp]
         L.orc_euler2dm.argtypes = [dp, dp]
         L.orc_kb_dapod.argtypes = [C.c_double]
         L.orc_kb_dapod.restype = C.c_double
@@ -356,6 +358,19 @@ def prepimg4align(img, boxmatch: int, msk: float, x: float = 0.0, y: float = 0.0
     lib().orc_prepimg4align(int(box), int(boxmatch), _P(a, C.c_float), float(msk), float(x), float(y),
                             None if ctf is None else C.byref(ctf),
                             out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
+    return out
+
+
+def prepimg4align_opts(img, boxmatch: int, msk: float, inner: float = 0.0, width: float = 0.0, focusmsk: float = 0.0,
+                       griddev: bool = False, x: float = 0.0, y: float = 0.0, ctf: "Ctf | None" = None):
+    """prepimg4align with the inner / focus mask and griddev modes (see pftcc_oracle.h)"""
+    a = np.ascontiguousarray(img, np.float32)
+    box = a.shape[0]
+    out = _c128_out((boxmatch, boxmatch // 2 + 1))
+    lib().orc_prepimg4align_opts(int(box), int(boxmatch), _P(a, C.c_float), float(msk), float(inner), float(width),
+                                 float(focusmsk), int(bool(griddev)), float(x), float(y),
+                                 None if ctf is None else C.byref(ctf),
+                                 out.view(np.float64).ctypes.data_as(C.POINTER(C.c_double)))
     return out
 
 

@@ -1203,8 +1203,24 @@ static int cmp_dbl(const void *a, const void *b)
     return x < y ? -1 : (x > y ? 1 : 0);
 }
 
+/* kbinterpol%instr (simple_kbinterpol.f90:211-225) for the window of half-width 1.5 (W = 3,
+ * beta = 7.4, :97-103): sinh(y) / y, y = sqrt(beta^2 - (pi W x)^2) (|x| <= 1/2 lies below the
+ * threshold beta / (pi W)); the single-precision constants and argument of the reference */
+static double kb_instr(double x)
+{
+    const double piW = (double)(3.14159265f * 3.0f), betasq = (double)(7.4f * 7.4f);
+    const double y = sqrt(betasq - (piW * x) * (piW * x));
+    return y < 1e-10 ? 1.0 : sinh(y) / y;
+}
+
 void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, double x, double y, const orc_ctf *ctf,
                        double *cmat_out)
+{
+    orc_prepimg4align_opts(box, boxmatch, img, msk, 0.0, 0.0, 0.0, 0, x, y, ctf, cmat_out);
+}
+
+void orc_prepimg4align_opts(int box, int boxmatch, const float *img, double msk, double inner, double width,
+                            double focusmsk, int griddev, double x, double y, const orc_ctf *ctf, double *cmat_out)
 {
     const int B = box, Bm = boxmatch, hB = B / 2 + 1, hBm = Bm / 2 + 1;
     double *r = (double *)malloc(sizeof(double) * B * B);
@@ -1300,24 +1316,45 @@ void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, doub
             for (int e = 0; e < Bm * Bm; ++e) m[e] -= med;
         free(line);
     }
-    /* cosine edge */
+    /* cosine edge: mask(msk, 'soft', inner, width) with l_innermsk, else mask(focusmsk, 'soft')
+     * with l_focusmsk, else mask(msk, 'soft') (prepimg4align :349-358; mask :6208-6300) */
     {
-        int minlen = (int)f_nint(2.0 * (msk + 6.0));
+        const double mrad = inner > 0.0 ? msk : (focusmsk > 0.0 ? focusmsk : msk);
+        const double iw = width > 0.0 ? width : 10.0;
+        int minlen = (int)f_nint(2.0 * (mrad + 6.0));
         if (minlen > Bm) minlen = Bm;
-        const double maxrad = (double)(minlen / 2), width = 2.0 * (maxrad - msk);
+        const double maxrad = (double)(minlen / 2), cwidth = 2.0 * (maxrad - mrad);
         for (int i = 1; i <= Bm / 2; ++i)
             for (int j = 1; j <= Bm / 2; ++j) {
                 const double cx = -Bm / 2.0 + (i - 1), cy = -Bm / 2.0 + (j - 1);
                 const double rad = sqrt(cx * cx + cy * cy);
                 double e = 1.0;
                 if (rad >= maxrad) e = 0.0;
-                else if (rad >= maxrad - width) e = (cos(((rad - (maxrad - width)) / width) * 3.14159265358979323846) + 1.0) / 2.0;
+                else if (rad >= maxrad - cwidth) e = (cos(((rad - (maxrad - cwidth)) / cwidth) * 3.14159265358979323846) + 1.0) / 2.0;
+                if (inner > 0.0) {   /* cosedge_inner (simple_math.f90:1128-1140) */
+                    double wi;
+                    if (rad < inner - iw) wi = 0.0;
+                    else if (rad > inner) wi = 1.0;
+                    else wi = (1.0 + cos(3.14159265358979323846 * (inner - rad) / iw)) / 2.0;
+                    e *= wi;
+                }
                 if (e > 0.9999) continue;
                 const int ir = Bm + 1 - i, jr = Bm + 1 - j;
                 m[(size_t)(j - 1) * Bm + (i - 1)] *= e;
                 m[(size_t)(jr - 1) * Bm + (i - 1)] *= e;
                 m[(size_t)(j - 1) * Bm + (ir - 1)] *= e;
                 m[(size_t)(jr - 1) * Bm + (ir - 1)] *= e;
+            }
+    }
+    /* griddev 'yes': div_by_instrfun (simple_polarizer.f90:111-116) with the instrument function
+     * image of gen_instrfun_img (simple_gridding.f90:18-55): w(i) w(j), w(i) = instr((i - c) / Bm),
+     * c = Bm/2 + 1, 1-based i */
+    if (griddev) {
+        for (int j = 1; j <= Bm; ++j)
+            for (int i = 1; i <= Bm; ++i) {
+                const double wi = kb_instr((double)(float)((float)(i - (Bm / 2 + 1)) / (float)Bm));
+                const double wj = kb_instr((double)(float)((float)(j - (Bm / 2 + 1)) / (float)Bm));
+                m[(size_t)(j - 1) * Bm + (i - 1)] /= wi * wj;
             }
     }
     /* fft and the box factor */

@@ -149,6 +149,11 @@ void orc_prep_matchfilt(const orc_geom *g, const float *ref, const double *ctfma
  * cmat(h, k) with k at its physical index */
 void orc_prepimg4align(int box, int boxmatch, const float *img, double msk, double x, double y, const orc_ctf *ctf,
                        double *cmat_out);
+/* the same with the other mask modes of prepimg4align (:349-362): inner > 0 the inner cosine
+ * edge of width width (<= 0: 10), else focusmsk > 0 the final mask's radius, griddev the
+ * division by the gridding's instrument function */
+void orc_prepimg4align_opts(int box, int boxmatch, const float *img, double msk, double inner, double width,
+                            double focusmsk, int griddev, double x, double y, const orc_ctf *ctf, double *cmat_out);
 /* orientation derivatives: euler2dm (simple_ori_light.f90:87-147), dR[j] = dR/de_j per radian,
  * three row-major 3x3 matrices; dapod (simple_kbinterpol.f90:179-192); fdf_project_polar
  * (simple_projector.f90:245-267 with fdf_interp_fcomp :338-400): pft [K][P] and its three

@@ -60,6 +60,11 @@ class RefineOut(C.Structure):
                 ("converged", C.c_int), ("pad", C.c_int)]
 
 
+class PrepOpts(C.Structure):
+    _fields_ = [("msk", C.c_float), ("inner", C.c_float), ("width", C.c_float), ("focusmsk", C.c_float),
+                ("griddev", C.c_int)]
+
+
 class ShsrchOpts(C.Structure):
     _fields_ = [("opt_angle", C.c_int), ("coarse_init", C.c_int), ("maxits", C.c_int), ("max_evals", C.c_int),
                 ("halfrot", C.c_float), ("pad", C.c_int)]
@@ -115,6 +120,9 @@ SIGNATURES = {
     "pftcc_specscore_batch": [_h, C.c_int, _ip, _ip, _ip, _fp, _fp, _fp],
     "pftcc_prep_ptcls": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp, _ip, C.POINTER(CtfParams), C.c_float],
     "pftcc_prep_ptcls_dev": [_h, C.c_int, C.c_int, C.c_void_p, C.c_int, _fp, _ip, C.POINTER(CtfParams), C.c_float],
+    "pftcc_prep_ptcls_opts": [_h, C.c_int, C.c_int, _fp, C.c_int, _fp, _ip, C.POINTER(CtfParams), C.POINTER(PrepOpts)],
+    "pftcc_prep_ptcls_opts_dev": [_h, C.c_int, C.c_int, C.c_void_p, C.c_int, _fp, _ip, C.POINTER(CtfParams),
+                                  C.POINTER(PrepOpts)],
     "pftcc_fdf_project_polar": [_h, C.c_int, C.c_int, _dp, C.c_int],
     "pftcc_get_dref_pft": [_h, C.c_int, C.c_int, _fp],
     "pftcc_gencorr_cont_shift_grad_cc_for_rot_8": [_h, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp],

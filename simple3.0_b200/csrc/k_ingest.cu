@@ -21,9 +21,11 @@
 //                   C2R input is a valid half spectrum;
 //   cuFFT C2R       B x B, batched, unnormalised;
 //   k_ingest_mask   one block per image: the centred boxmatch window, the lower medians of its
-//                   four border lines (rank selection in shared memory), the cosine edge, and the
-//                   quadrant swap of the final fft's phase origin folded into the store, with the
-//                   factor 1 / B^2 (= 1 / boxmatch^2 of fwd_ft times boxmatch^2 / B^2);
+//                   four border lines (rank selection in shared memory), the cosine edge (of the
+//                   inner mask, the focus mask or msk, :349-358), the division by the gridding's
+//                   instrument function for griddev 'yes' (:360-362), and the quadrant swap of the
+//                   final fft's phase origin folded into the store, with the factor 1 / B^2
+//                   (= 1 / boxmatch^2 of fwd_ft times boxmatch^2 / B^2);
 //   cuFFT R2C       boxmatch x boxmatch, batched: the half-plane cmat(h, k), k at its physical index.
 #include "pftcc_internal.cuh"
 
@@ -183,7 +185,21 @@ __global__ void __launch_bounds__(IN_THREADS) k_ingest_freq(float2 *__restrict__
 
 // the centred Bm window of the inverse transform, zero_background, cosine edge, quadrant swap and
 // 1 / B^2 into the final transform's input.  Shared memory: 4 border lines of Bm floats.
+// the gridding's instrument function (gen_instrfun_img, simple_gridding.f90:18-55, with
+// kbinterpol%instr, simple_kbinterpol.f90:211-225): w(i) = sinh(y) / y with
+// y = sqrt(beta^2 - (pi W x)^2), x = (i - (Bm/2 + 1)) / Bm for the 1-based index i, W = 3 and
+// beta = 7.4 (the window of half-width 1.5, :97-103); |x| <= 1/2 always lies below the threshold
+// beta / (pi W), so every sample takes the sinh branch
+__device__ __forceinline__ double instrfun(int i, int Bm)
+{
+    const double piW = (double)(3.14159265f * 3.0f), betasq = (double)(7.4f * 7.4f);
+    const double x = (double)(float)((float)(i - (Bm / 2 + 1)) / (float)Bm);
+    const double y = sqrt(betasq - (piW * x) * (piW * x));
+    return y < 1e-10 ? 1.0 : sinh(y) / y;
+}
+
 __global__ void __launch_bounds__(IN_THREADS) k_ingest_mask(const float *__restrict__ R, int B, int Bm, float msk,
+                                                            float inner, float iwidth, int griddev,
                                                             float *__restrict__ out)
 {
     extern __shared__ float lines[];   // [4][Bm]
@@ -227,8 +243,14 @@ __global__ void __launch_bounds__(IN_THREADS) k_ingest_mask(const float *__restr
         double w = 1.0;
         if (rad >= maxrad) w = 0.0;
         else if (rad >= maxrad - width) w = (cos(((rad - (maxrad - width)) / width) * 3.141592653589793) + 1.0) / 2.0;
+        if (inner > 0.f) {   // cosedge_inner (simple_math.f90:1128-1140): zero inside inner - width
+            const double mi = (double)inner, wi = (double)iwidth;
+            if (rad < mi - wi) w = 0.0;
+            else if (rad <= mi) w *= (1.0 + cos(3.141592653589793 * (mi - rad) / wi)) / 2.0;
+        }
         if (w > 0.9999) w = 1.0;
-        const double v = ((double)src[(size_t)(st + j - 1) * B + st + i - 1] - med) * w;
+        double v = ((double)src[(size_t)(st + j - 1) * B + st + i - 1] - med) * w;
+        if (griddev) v /= instrfun(i, Bm) * instrfun(j, Bm);   // div_by_instrfun (simple_polarizer.f90:111-116)
         const int io = (i - 1 + Bm / 2) % Bm, jo = (j - 1 + Bm / 2) % Bm;   // shift_phorig
         dst[(size_t)jo * Bm + io] = (float)(v * scale);
     }
@@ -269,8 +291,12 @@ int ingest_batch_max(int B)
 // transformed at the full count, the surplus slots holding stale data that nothing reads), so a
 // tail batch needs no new plans; cm_out holds cap half-plane images
 int ingest_images(pftcc_handle *h, const float *imgs_dev, int n, int cap, int B, const float *xy_dev,
-                  const int *flag_dev, const pftcc_ctfparams *ctf_dev, float msk, float2 *cm_out)
+                  const int *flag_dev, const pftcc_ctfparams *ctf_dev, const pftcc_prep_opts &o, float2 *cm_out)
 {
+    const float msk = o.msk;
+    // the final soft mask: inner mask, else focus mask, else msk (prepimg4align :349-358)
+    const float fmsk = o.inner > 0.f ? msk : (o.focusmsk > 0.f ? o.focusmsk : msk);
+    const float iwidth = o.width > 0.f ? o.width : 10.f;
     const int Bm = h->g.box;
     IngestState *s = static_cast<IngestState *>(h->ingest);
     if (s && (s->B != B || s->Bm != Bm || s->batch != cap)) {
@@ -318,7 +344,8 @@ int ingest_images(pftcc_handle *h, const float *imgs_dev, int n, int cap, int B,
     PFTCC_LAUNCH(h);
     {
         KTimer kt(h, PFTCC_K_POLARIZE);
-        k_ingest_mask<<<n, IN_THREADS, 4 * Bm * sizeof(float), h->stream>>>(s->R, B, Bm, msk, s->Rm);
+        k_ingest_mask<<<n, IN_THREADS, 4 * Bm * sizeof(float), h->stream>>>(s->R, B, Bm, fmsk, o.inner, iwidth,
+                                                                           o.griddev, s->Rm);
     }
     CK(cudaGetLastError(), "ingest mask");
     if (cufftExecR2C(s->fwdm, s->Rm, reinterpret_cast<cufftComplex *>(cm_out)) != CUFFT_SUCCESS)

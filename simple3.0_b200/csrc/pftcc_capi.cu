@@ -802,13 +802,19 @@ int pftcc_polarize_ptcls(pftcc_handle *h, int first_slot, int n, const float *cm
 
 // ---- particle ingestion (prepimg4align) ------------------------------------------------
 static int prep_ptcls_common(pftcc_handle *h, int first_slot, int n, const float *imgs, int imgs_on_device,
-                             int box_in, const float *xy, const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
+                             int box_in, const float *xy, const int *ctfflag, const pftcc_ctfparams *ctf,
+                             const pftcc_prep_opts &o)
 {
     if (!h || !imgs || !xy || !ctfflag || n < 0) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: bad arguments");
     if (first_slot < 0 || first_slot + n > h->nptcls) return set_err(h, PFTCC_ERR_INDEX, "prep_ptcls: slot range");
     const int Bm = h->g.box;
+    const float msk = o.msk;
     if (box_in < Bm || (box_in & 1)) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: box must be even and >= boxmatch");
     if (!(msk > 0.f) || !(msk < 0.5f * Bm)) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: msk must lie in (0, boxmatch/2)");
+    if (!std::isfinite(o.inner) || !std::isfinite(o.width) || !std::isfinite(o.focusmsk) ||
+        (o.focusmsk > 0.f && !(o.focusmsk < 0.5f * Bm)) || (o.inner > 0.f && !(o.inner < msk)) ||
+        (o.griddev != 0 && o.griddev != 1))
+        return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: inner must lie below msk, focusmsk below boxmatch/2, griddev 0 or 1");
     for (int i = 0; i < n; ++i) {
         if (ctfflag[i] < 0 || ctfflag[i] > 2) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: unsupported CTF flag");
         if (ctfflag[i] == 1 && !ctf) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: CTFFLAG_YES needs CTF parameters");
@@ -846,8 +852,8 @@ static int prep_ptcls_common(pftcc_handle *h, int first_slot, int n, const float
         if (ctf)
             CK(cudaMemcpyAsync(dctf, ctf + c0, (size_t)m * sizeof(pftcc_ctfparams), cudaMemcpyHostToDevice, h->stream),
                "prep_ptcls ctf");
-        ST(ingest_images(h, src, m, cap, box_in, dxy, dflag, dctf, msk, cm));
-        ST(polarize_dev(h, first_slot + c0, m, cm, 0));
+        ST(ingest_images(h, src, m, cap, box_in, dxy, dflag, dctf, o, cm));
+        ST(polarize_dev(h, first_slot + c0, m, cm, o.griddev));
         // the staging is reused by the next chunk's uploads
         CK(cudaStreamSynchronize(h->stream), "prep_ptcls");
     }
@@ -857,13 +863,29 @@ static int prep_ptcls_common(pftcc_handle *h, int first_slot, int n, const float
 int pftcc_prep_ptcls(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
                      const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
 {
-    return prep_ptcls_common(h, first_slot, n, imgs, 0, box_in, xy, ctfflag, ctf, msk);
+    const pftcc_prep_opts o{msk, 0.f, 0.f, 0.f, 0};
+    return prep_ptcls_common(h, first_slot, n, imgs, 0, box_in, xy, ctfflag, ctf, o);
 }
 
 int pftcc_prep_ptcls_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
                          const int *ctfflag, const pftcc_ctfparams *ctf, float msk)
 {
-    return prep_ptcls_common(h, first_slot, n, static_cast<const float *>(imgs_dev), 1, box_in, xy, ctfflag, ctf, msk);
+    const pftcc_prep_opts o{msk, 0.f, 0.f, 0.f, 0};
+    return prep_ptcls_common(h, first_slot, n, static_cast<const float *>(imgs_dev), 1, box_in, xy, ctfflag, ctf, o);
+}
+
+int pftcc_prep_ptcls_opts(pftcc_handle *h, int first_slot, int n, const float *imgs, int box_in, const float *xy,
+                          const int *ctfflag, const pftcc_ctfparams *ctf, const pftcc_prep_opts *opts)
+{
+    if (!opts) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: no options");
+    return prep_ptcls_common(h, first_slot, n, imgs, 0, box_in, xy, ctfflag, ctf, *opts);
+}
+
+int pftcc_prep_ptcls_opts_dev(pftcc_handle *h, int first_slot, int n, const void *imgs_dev, int box_in, const float *xy,
+                              const int *ctfflag, const pftcc_ctfparams *ctf, const pftcc_prep_opts *opts)
+{
+    if (!opts) return set_err(h, PFTCC_ERR_ARG, "prep_ptcls: no options");
+    return prep_ptcls_common(h, first_slot, n, static_cast<const float *>(imgs_dev), 1, box_in, xy, ctfflag, ctf, *opts);
 }
 
 // ---- polar projection of a volume (simple_projector.f90) --------------------------------

@@ -235,7 +235,7 @@ cudaError_t launch_cont_shift_grad(pftcc_handle *h, const EuclidReq *reqs_dev, i
 // particle ingestion (k_ingest.cu): prepimg4align of n <= cap images [n][B][B] into cap half-plane
 // FTs [cap][box][box/2+1] (box = boxmatch); xy [n][2], flag [n], ctf [n] on the device
 int ingest_images(pftcc_handle *h, const float *imgs_dev, int n, int cap, int B, const float *xy_dev,
-                  const int *flag_dev, const pftcc_ctfparams *ctf_dev, float msk, float2 *cm_out);
+                  const int *flag_dev, const pftcc_ctfparams *ctf_dev, const pftcc_prep_opts &opts, float2 *cm_out);
 int ingest_batch_max(int B);
 void ingest_free(pftcc_handle *h);
 // euler2m (and with dR, euler2dm per radian) of Spider angles in degrees, row-major, FP64

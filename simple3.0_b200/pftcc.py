@@ -227,15 +227,22 @@ class polarft_corrcalc:
                                                  None if m is None else m.ctypes.data_as(C.POINTER(C.c_int)),
                                                  int(bool(iseven)), int(bool(griddev))))
 
-    def prep_ptcls(self, first_slot: int, imgs, xy=None, ctfflag=None, ctfparams=None, msk: float | None = None):
+    def prep_ptcls(self, first_slot: int, imgs, xy=None, ctfflag=None, ctfparams=None, msk: float | None = None,
+                   inner: float = 0.0, width: float = 0.0, focusmsk: float = 0.0, griddev: bool = False):
         """prepimg4align + polarize for images (n, box_in, box_in) [y][x] into slots first_slot..:
         xy (n, 2) the particles' shifts, ctfflag (n,) of _lib.CTFFLAG_*, ctfparams a ctypes array
-        (ctfparams_array) needed where a flag is CTFFLAG_YES, msk the mask radius (pixels)"""
+        (ctfparams_array) needed where a flag is CTFFLAG_YES, msk the mask radius (pixels); inner
+        (with width) the inner mask, focusmsk the focus mask, griddev 'yes' (pftcc_prep_opts)"""
         a = np.ascontiguousarray(imgs, np.float32)
         n, box_in = a.shape[0], a.shape[1]
         v = np.zeros((n, 2), np.float32) if xy is None else np.ascontiguousarray(xy, np.float32).reshape(n, 2)
         f = np.zeros(n, np.int32) if ctfflag is None else np.ascontiguousarray(ctfflag, np.int32).reshape(n)
         m = float(self.cfg.box / 2 - 4 if msk is None else msk)
+        if inner or width or focusmsk or griddev:
+            o = _lib.PrepOpts(m, float(inner), float(width), float(focusmsk), int(bool(griddev)))
+            self._check(self._L.pftcc_prep_ptcls_opts(self._h, int(first_slot), n, _f32p(a), int(box_in), _f32p(v),
+                                                      f.ctypes.data_as(C.POINTER(C.c_int)), ctfparams, C.byref(o)))
+            return
         self._check(self._L.pftcc_prep_ptcls(self._h, int(first_slot), n, _f32p(a), int(box_in), _f32p(v),
                                              f.ctypes.data_as(C.POINTER(C.c_int)), ctfparams, m))
 

@@ -59,6 +59,43 @@ def test_prep_ptcls_matches_oracle(pkg, O, B, Bm, msk, nrots, kto):
         pc.kill()
 
 
+@pytest.mark.parametrize("inner,width,focusmsk,griddev", [
+    (10.0, 0.0, 0.0, False), (12.0, 4.0, 0.0, True), (0.0, 0.0, 18.0, False), (0.0, 0.0, 0.0, True)])
+def test_prep_ptcls_mask_modes_match_oracle(pkg, O, inner, width, focusmsk, griddev):
+    """the inner mask, the focus mask and griddev 'yes' (pftcc_prep_ptcls_opts) against the oracle:
+    prepimg4align in the same mode, gridded with normalised or (griddev) raw weights"""
+    n, B, Bm, msk, nrots, kto = 4, 80, 64, 26.0, 128, 24
+    imgs = particles(n, B, 77)
+    rng = np.random.default_rng(2)
+    xy = rng.uniform(-2, 2, (n, 2)).astype(np.float32)
+    flags = np.array([1, 0, 1, 2], np.int32)
+    dfx = rng.uniform(1.0, 2.5, n)
+    dfy = dfx - rng.uniform(0.0, 0.3, n)
+    ang = rng.uniform(0, 180, n)
+    ctfp = pkg.ctfparams_array(n, smpd=2.0, dfx=dfx, dfy=dfy, angast=ang)
+    pc = pkg.polarft_corrcalc()
+    pc.new(1, (1, n), box=Bm, nrots=nrots, kfromto=(2, kto), ctf=False)
+    try:
+        pc.prep_ptcls(0, imgs, xy, flags, ctfp, msk, inner=inner, width=width, focusmsk=focusmsk, griddev=griddev)
+        g = O.geom(nrots, 2, kto, Bm)
+        t = O.tables(g)
+        worst = 0.0
+        for i in range(n):
+            c = None
+            if flags[i] == 1:
+                c = O.make_ctf(smpd=2.0, dfx=float(np.float32(dfx[i])), dfy=float(np.float32(dfy[i])),
+                               angast=float(np.float32(ang[i])))
+            cm = O.prepimg4align_opts(imgs[i], Bm, msk, inner, width, focusmsk, griddev, float(xy[i, 0]),
+                                      float(xy[i, 1]), c)
+            want = O.polarize(g, t, cm, griddev=griddev)
+            got = pc.get_ptcl_pft(i + 1)
+            worst = max(worst, float(np.max(np.abs(got - want)) / np.max(np.abs(want))))
+        print(f"prep_ptcls inner {inner} width {width} focusmsk {focusmsk} griddev {griddev}: max error {worst:.2e}")
+        assert worst < 2e-5
+    finally:
+        pc.kill()
+
+
 def test_prep_ptcls_errors(pkg):
     pc = pkg.polarft_corrcalc()
     pc.new(1, (1, 2), box=64, nrots=128, kfromto=(2, 24), ctf=False)

@@ -23,7 +23,15 @@ def _ctf_chi(c, s2, ang):
     return math.pi * wl * s2 * (df - 0.5 * wl * wl * s2 * cs) + c.phshift + ampc
 
 
-def prep_numpy(img, Bm, msk, x=0.0, y=0.0, ctf=None):
+def instr_numpy(x):
+    """kbinterpol%instr for W = 3, beta = 7.4: sinh(y) / y, y = sqrt(beta^2 - (pi W x)^2)"""
+    piW = float(np.float32(np.float32(math.pi) * np.float32(3.0)))
+    betasq = float(np.float32(np.float32(7.4) * np.float32(7.4)))
+    yv = np.sqrt(betasq - (piW * x) ** 2)
+    return np.sinh(yv) / yv
+
+
+def prep_numpy(img, Bm, msk, x=0.0, y=0.0, ctf=None, inner=0.0, iwidth=0.0, focusmsk=0.0, griddev=False):
     r = np.asarray(img, np.float64).copy()
     B = r.shape[0]
     c = B // 2 + 1
@@ -58,9 +66,11 @@ def prep_numpy(img, Bm, msk, x=0.0, y=0.0, ctf=None):
     med = np.mean([np.sort(v)[Bm // 2 - 1] for v in (m[:, 0], m[:, Bm - 1], m[0, :], m[Bm - 1, :])])
     if abs(med) > 1e-10:
         m -= med
-    minlen = min(int(math.floor(2 * (msk + 6.0) + 0.5)), Bm)
+    mrad = msk if inner > 0 else (focusmsk if focusmsk > 0 else msk)
+    iw = iwidth if iwidth > 0 else 10.0
+    minlen = min(int(math.floor(2 * (mrad + 6.0) + 0.5)), Bm)
     maxrad = float(minlen // 2)
-    width = 2.0 * (maxrad - msk)
+    width = 2.0 * (maxrad - mrad)
     for i in range(1, Bm // 2 + 1):
         for j in range(1, Bm // 2 + 1):
             cx, cy = -Bm / 2 + (i - 1), -Bm / 2 + (j - 1)
@@ -70,11 +80,18 @@ def prep_numpy(img, Bm, msk, x=0.0, y=0.0, ctf=None):
                 e = 0.0
             elif rad >= maxrad - width:
                 e = (math.cos(((rad - (maxrad - width)) / width) * math.pi) + 1.0) / 2.0
+            if inner > 0:
+                e *= 0.0 if rad < inner - iw else (1.0 if rad > inner else
+                                                   (1.0 + math.cos(math.pi * (inner - rad) / iw)) / 2.0)
             if e > 0.9999:
                 continue
             for jj in (j, Bm + 1 - j):
                 for ii_ in (i, Bm + 1 - i):
                     m[jj - 1, ii_ - 1] *= e
+    if griddev:
+        xs = np.array([float(np.float32(np.float32(i - (Bm // 2 + 1)) / np.float32(Bm))) for i in range(1, Bm + 1)])
+        w = instr_numpy(xs)
+        m /= w[None, :] * w[:, None]
     return np.fft.rfft2(np.fft.fftshift(m)) / (B * B)
 
 
@@ -98,6 +115,39 @@ def test_prepimg4align_matches_numpy(O, B, Bm, msk, x, y, with_ctf):
     want = prep_numpy(img, Bm, msk, x, y, ctf)
     assert got.shape == (Bm, Bm // 2 + 1)
     assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
+
+
+@pytest.mark.parametrize("inner,iwidth,focusmsk,griddev", [
+    (10.0, 0.0, 0.0, False),      # inner mask, the default width 10
+    (12.0, 4.0, 0.0, True),       # inner mask of width 4, griddev 'yes'
+    (0.0, 0.0, 16.0, False),      # focus mask
+    (0.0, 0.0, 0.0, True),        # griddev alone
+])
+def test_prepimg4align_mask_modes(O, inner, iwidth, focusmsk, griddev):
+    """l_innermsk, l_focusmsk and griddev 'yes' (prepimg4align :349-362) against the numpy chain"""
+    img = particle(64, 9)
+    ctf = O.make_ctf(smpd=2.1, dfx=1.9, dfy=1.5, angast=35.0)
+    got = O.prepimg4align_opts(img, 56, 24.0, inner, iwidth, focusmsk, griddev, 0.7, -1.2, ctf)
+    want = prep_numpy(img, 56, 24.0, 0.7, -1.2, ctf, inner, iwidth, focusmsk, griddev)
+    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
+    plain = O.prepimg4align(img, 56, 24.0, 0.7, -1.2, ctf)
+    assert np.max(np.abs(got - plain)) > 1e-3 * np.max(np.abs(plain))     # the mode changes the output
+
+
+def test_instrument_function_values(O):
+    """the instrument function is 1 at the centre only in ratio: w(x) / w(0) falls towards the
+    edges (the window's transform), symmetric, and is the sinh form of I0's transform"""
+    x = np.linspace(-0.5, 0.5, 11)
+    w = instr_numpy(x)
+    assert np.allclose(w, w[::-1])
+    assert np.all(np.diff(w[:6]) > 0)
+    # sinh(y)/y is the continuous transform of the Kaiser-Bessel window I0(beta sqrt(1 - (2u/W)^2))
+    # over |u| <= W/2 up to a constant: check at x = 0.3 by quadrature
+    from scipy.special import i0
+    u = np.linspace(-1.5, 1.5, 200001)
+    kb = i0(7.4 * np.sqrt(np.clip(1 - (2 * u / 3.0) ** 2, 0, None)))
+    ft = lambda xx: np.trapezoid(kb * np.cos(2 * np.pi * u * xx), u)
+    assert abs(ft(0.3) / ft(0.0) - instr_numpy(0.3) / instr_numpy(0.0)) < 1e-4
 
 
 def test_noise_norm_makes_intensity_scale_irrelevant(O):
