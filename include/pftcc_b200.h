@@ -54,10 +54,9 @@ typedef struct pftcc_handle pftcc_handle;
 
 /* new() arguments plus the params_glob fields polarft_corrcalc reads implicitly
  * (boxmatch :235, ring2 -> nrots :251-252, kfromto/kstop :256-258, ctf :355-356,
- * l_match_filt :254).  Not served: params_glob%l_pssnr (the per-shell SSNR weighting of
- * shellnorm_and_filter_ref :763-770 and prep_matchfilt :1006-1018) and clsfrcs = 'yes'
- * (l_clsfrcs :415, the particle's own class filter ref_optlp(:, iptcl) at :976-980);
- * the matched filter is always ref_optlp(:, iref). */
+ * l_match_filt :254; l_pssnr through pftcc_set_pssnr).  Not served: clsfrcs = 'yes'
+ * (l_clsfrcs :415, which filters with the column ref_optlp(:, iptcl) of the particle's global
+ * index, :976-980); the matched filter is always ref_optlp(:, iref). */
 typedef struct {
     int nrefs;            /* new(nrefs, ...)                                    */
     int pfromto[2];       /* new(..., pfromto, ...), global particle index range */
@@ -206,6 +205,12 @@ int pftcc_assign_pinds(const pftcc_handle *h, int *pinds);
 int pftcc_calc_roinv_corrmat(pftcc_handle *h, float *corrmat);
 
 /* ---- the matched-filter mode (pftcc_config.match_filt = params_glob%l_match_filt) ---------- */
+/* params_glob%l_pssnr (implies l_match_filt, simple_parameters.f90:1364-1365): the shell
+ * factors of shellnorm_and_filter_ref(_8) become sqrt(ssnr k) / sqrt(power) (:763-770,
+ * :789-796) with ssnr = ref_optlp(k, iref), and prep_matchfilt rescales the particle's shells
+ * by sqrt(k) / sqrt(power) and sqrt(1 + ssnr |CTF|^2) per sample (:999-1019).
+ * PFTCC_ERR_STATE on a handle created without match_filt. */
+int pftcc_set_pssnr(pftcc_handle *h, int on);
 /* With match_filt the correlators apply shellnorm_and_filter_ref(_8) (:756-807) to the reference:
  * shell k <= kstop scaled by ref_optlp(k, iref) / sqrt(mean power of the raw shell) (gencorrs_cc_1/_2,
  * gencorrs_euclid_1, gencorr_cc_for_rot(_8), gencorr_cc_grad_for_rot_8, the continuous-gradient

@@ -87,6 +87,8 @@ def lib():
         L.orc_gencorr_euclid_grad_for_rot.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp, dp]
         L.orc_sigma_contrib.argtypes = [G, fp, fp, dp, dp, C.c_int, dp, dp, dp, dp, dp]
         L.orc_shellnorm_factors.argtypes = [G, fp, fp, dp]
+        L.orc_shellnorm_factors_mode.argtypes = [G, fp, fp, C.c_int, dp]
+        L.orc_prep_matchfilt_pssnr.argtypes = [G, dp, fp, fp]
         L.orc_savgol7.argtypes = [C.c_int, dp]
         L.orc_prep_matchfilt.argtypes = [G, fp, dp, fp, C.c_int, fp]
         L.orc_prepimg4align.argtypes = [C.c_int, C.c_int, fp, C.c_double, C.c_double, C.c_double, C.POINTER(Ctf), dp]
@@ -326,11 +328,21 @@ def fproject_polar(g: Geom, t: Tables, cmat_exp, box: int, eul, mask=None, gridd
     return out
 
 
-def shellnorm_factors(g: Geom, ref, optlp=None) -> np.ndarray:
-    """per-shell factors k <= kstop of shellnorm_and_filter_ref (l_match_filt)"""
+def shellnorm_factors(g: Geom, ref, optlp=None, pssnr: bool = False) -> np.ndarray:
+    """per-shell factors k <= kstop of shellnorm_and_filter_ref (l_match_filt; l_pssnr with pssnr)"""
     out = np.zeros(g.Ks, np.float64)
     o = None if optlp is None else np.ascontiguousarray(optlp, np.float32)
-    lib().orc_shellnorm_factors(C.byref(g), _P(_c64(ref), C.c_float), _P(o, C.c_float), _P(out, C.c_double))
+    lib().orc_shellnorm_factors_mode(C.byref(g), _P(_c64(ref), C.c_float), _P(o, C.c_float), int(bool(pssnr)),
+                                     _P(out, C.c_double))
+    return out
+
+
+def prep_matchfilt_pssnr(g: Geom, ptcl, ctf=None, optlp=None) -> np.ndarray:
+    """the particle after prep_matchfilt's l_pssnr branch"""
+    out = np.ascontiguousarray(ptcl, np.complex64).copy()
+    o = None if optlp is None else np.ascontiguousarray(optlp, np.float32)
+    lib().orc_prep_matchfilt_pssnr(C.byref(g), _P(_ctf_arg(ctf), C.c_double), _P(o, C.c_float),
+                                   out.view(np.float32).ctypes.data_as(C.POINTER(C.c_float)))
     return out
 
 

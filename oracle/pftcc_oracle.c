@@ -1407,11 +1407,40 @@ void orc_gencorrs_euclid_ptclframe(const orc_geom *g, const float *ref, const fl
 /* The matched-filter mode.  shellnorm_and_filter_ref_8 (:783-807), l_match_filt branch. */
 void orc_shellnorm_factors(const orc_geom *g, const float *ref, const float *optlp, double *scale)
 {
+    orc_shellnorm_factors_mode(g, ref, optlp, 0, scale);
+}
+
+/* pssnr = 1: the l_pssnr branch of shellnorm_and_filter_ref(_8) (:763-770, :789-796):
+ * sqrt(ssnr k) / sqrt(pw) (sqrt(ssnr k) where pw <= 1e-12), ssnr = ref_optlp(k, iref), k the
+ * shell number */
+void orc_shellnorm_factors_mode(const orc_geom *g, const float *ref, const float *optlp, int pssnr, double *scale)
+{
     const int P = g->pftsz, Ks = g->kstop - g->kfrom + 1;
     for (int ik = 0; ik < Ks; ++ik) {
         const double pw = sqsum_kf(P, ref + 2 * ik * P) / (double)P;
         const double o = optlp ? (double)optlp[ik] : 1.0;
-        scale[ik] = pw > 1e-12 ? o / sqrt(pw) : o;
+        const double w = pssnr ? sqrt(o * (double)(g->kfrom + ik)) : o;
+        scale[ik] = pw > 1e-12 ? w / sqrt(pw) : w;
+    }
+}
+
+/* prep_matchfilt (:999-1019), the l_pssnr branch: every shell k <= kstop of the particle times
+ * sqrt(k) / sqrt(pw_ptcl) (sqrt(k) where pw_ptcl <= 1e-12) and, sample by sample,
+ * sqrt(1 + ssnr |CTF(n,k)|^2) (sqrt(1 + ssnr) without CTF), ssnr = ref_optlp(k, iref) */
+void orc_prep_matchfilt_pssnr(const orc_geom *g, const double *ctfmat, const float *optlp, float *ptcl)
+{
+    const int P = g->pftsz, Ks = g->kstop - g->kfrom + 1;
+    for (int ik = 0; ik < Ks; ++ik) {
+        const double pw = sqsum_kf(P, ptcl + 2 * ik * P) / (double)P;
+        const double ssnr = optlp ? (double)optlp[ik] : 1.0;
+        double w = sqrt((double)(g->kfrom + ik));
+        if (pw > 1e-12) w /= sqrt(pw);
+        for (int n = 0; n < P; ++n) {
+            const double c = ctfmat ? ctfmat[ik * P + n] : 1.0;
+            const double f = w * sqrt(1.0 + ssnr * c * c);
+            ptcl[2 * (ik * P + n)] = (float)(f * ptcl[2 * (ik * P + n)]);
+            ptcl[2 * (ik * P + n) + 1] = (float)(f * ptcl[2 * (ik * P + n) + 1]);
+        }
     }
 }
 

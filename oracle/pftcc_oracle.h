@@ -134,6 +134,10 @@ void orc_fproject_polar(const orc_geom *g, const float *polar, int box, const fl
  * shell k <= kstop of the raw reference by optlp(k) / sqrt(pw), pw = sum_n |ref(n,k)|^2 / P, or by
  * optlp(k) where pw <= 1e-12; scale[Ks] (optlp = ref_optlp(:, iref), 1 unless set_ref_optlp) */
 void orc_shellnorm_factors(const orc_geom *g, const float *ref, const float *optlp, double *scale);
+/* the same, pssnr = 1 for the l_pssnr branch: sqrt(ssnr k) / sqrt(pw), ssnr = optlp(k) */
+void orc_shellnorm_factors_mode(const orc_geom *g, const float *ref, const float *optlp, int pssnr, double *scale);
+/* prep_matchfilt, the l_pssnr branch (:999-1019): the particle ptcl[K][P] rescaled in place */
+void orc_prep_matchfilt_pssnr(const orc_geom *g, const double *ctfmat, const float *optlp, float *ptcl);
 /* SavitzkyGolay_filter (simple_math.f90:3511-3588): 7-point quartic smoothing (nl = nr = 3, m = 4)
  * of y[n] in place, points left of the first omitted, the last 3 points unchanged */
 void orc_savgol7(int n, double *y);

@@ -136,6 +136,7 @@ SIGNATURES = {
     "pftcc_assign_pinds": [_h, _ip],
     "pftcc_calc_roinv_corrmat": [_h, _fp],
     "pftcc_set_ref_optlp": [_h, C.c_int, _fp],
+    "pftcc_set_pssnr": [_h, C.c_int],
     "pftcc_prep_matchfilt": [_h, C.c_int, C.c_int, C.c_int],
     "pftcc_prep_matchfilt_batch": [_h, C.c_int, _ip, _ip, _ip],
     "pftcc_set_objfun": [_h, C.c_int],

@@ -1,5 +1,5 @@
-// k_matchfilt.cu -- the matched-filter mode (params_glob%l_match_filt) of
-// simple_polarft_corrcalc.f90:
+// k_matchfilt.cu -- the matched-filter mode (params_glob%l_match_filt, with its l_pssnr
+// variant) of simple_polarft_corrcalc.f90:
 //   k_shellnorm       the factors of shellnorm_and_filter_ref(_8) (:756-807): shell k <= kstop of
 //                     a raw reference scaled by ref_optlp(k, iref) / sqrt(pw), pw its mean power
 //                     sum_n |ref(n,k)|^2 / P (FP64), or by ref_optlp(k, iref) where pw <= 1e-12;
@@ -52,10 +52,12 @@ __device__ void mf_shell_power(const float2 *x, int Ks, int P, double *out)
     }
 }
 
+// pssnr (params_glob%l_pssnr, :763-770 / :789-796): sqrt(ssnr k) / sqrt(pw) in place of
+// optlp / sqrt(pw), ssnr = ref_optlp(k, iref), k the shell number
 __global__ void __launch_bounds__(MF_THREADS) k_shellnorm(Geom g, const float2 *__restrict__ refs_even,
                                                           const float2 *__restrict__ refs_odd,
                                                           const float *__restrict__ optlp, int nrefs, int r0, int n,
-                                                          float *__restrict__ snorm)
+                                                          int pssnr, float *__restrict__ snorm)
 {
     extern __shared__ double pw[];   // [Ks]
     const int set = blockIdx.x / n, r = r0 + blockIdx.x % n;
@@ -64,8 +66,43 @@ __global__ void __launch_bounds__(MF_THREADS) k_shellnorm(Geom g, const float2 *
     __syncthreads();
     for (int k = threadIdx.x; k < g.Ks; k += blockDim.x) {
         const double p = pw[k] / (double)g.P, o = (double)optlp[(size_t)r * g.Ks + k];
-        snorm[((size_t)set * nrefs + r) * g.Ks + k] = (float)(p > 1e-12 ? o / sqrt(p) : o);
+        const double w = pssnr ? sqrt(o * (double)(g.kfrom + k)) : o;
+        snorm[((size_t)set * nrefs + r) * g.Ks + k] = (float)(p > 1e-12 ? w / sqrt(p) : w);
     }
+}
+
+// prep_matchfilt's l_pssnr branch (:999-1019): shell k <= kstop of the held particle times
+// sqrt(k) / sqrt(pw) (sqrt(k) where pw <= 1e-12) and sqrt(1 + ssnr |CTF(n,k)|^2) per sample,
+// ssnr = ref_optlp(k, iref); written back with its square sum (set_ptcl_pft); one block per request
+__global__ void __launch_bounds__(MF_THREADS) k_prep_pssnr(Geom g, const int4 *__restrict__ reqs,
+                                                           const float *__restrict__ ctfmats,
+                                                           const float *__restrict__ optlp, float2 *__restrict__ ptcls,
+                                                           float *__restrict__ sqsums)
+{
+    extern __shared__ double pw[];   // [Ks]
+    __shared__ double red[MF_THREADS / 32];
+    const int4 rq = reqs[blockIdx.x];   // iref (0-based), slot, irot, pad
+    const int P = g.P, Ks = g.Ks;
+    float2 *q = ptcls + (size_t)rq.y * g.K * P;
+    const float *ctf = ctfmats ? ctfmats + (size_t)rq.y * g.K * P : nullptr;
+    const float *o = optlp + (size_t)rq.x * Ks;
+    mf_shell_power(q, Ks, P, pw);
+    __syncthreads();
+    double s = 0.0;
+    for (int e = threadIdx.x; e < Ks * P; e += blockDim.x) {
+        const int k = e / P;
+        const double p = pw[k] / (double)P;
+        double w = sqrt((double)(g.kfrom + k));
+        if (p > 1e-12) w /= sqrt(p);
+        const double c = ctf ? (double)ctf[e] : 1.0;
+        const float f = (float)(w * sqrt(1.0 + (double)o[k] * c * c));
+        float2 v = q[e];
+        v = make_float2(v.x * f, v.y * f);
+        q[e] = v;
+        s += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    s = mf_block_sum(s, red);
+    if (threadIdx.x == 0) sqsums[rq.y] = (float)s;
 }
 
 __global__ void k_shellnorm_apply(int M, int Ks, int J, int nrs, int rows_pad, int nshifts, int nrefs,
@@ -213,8 +250,8 @@ cudaError_t launch_shellnorm(pftcc_handle *h, int r0, int n)
 {
     if (n <= 0) return cudaSuccess;
     PFTCC_LAUNCH(h);
-    k_shellnorm<<<2 * n, MF_THREADS, (size_t)h->g.Ks * sizeof(double), h->stream>>>(h->g, h->refs_even, h->refs_odd, h->d_optlp, h->nrefs, r0, n,
-                                                     h->d_snorm);
+    k_shellnorm<<<2 * n, MF_THREADS, (size_t)h->g.Ks * sizeof(double), h->stream>>>(
+        h->g, h->refs_even, h->refs_odd, h->d_optlp, h->nrefs, r0, n, h->pssnr, h->d_snorm);
     return cudaGetLastError();
 }
 
@@ -234,6 +271,13 @@ cudaError_t launch_prep_matchfilt(pftcc_handle *h, const void *reqs_dev, int nre
 {
     if (nreq <= 0) return cudaSuccess;
     const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
+    static_assert(sizeof(MatchReq) == sizeof(int4), "request layout");
+    if (h->pssnr) {
+        PFTCC_LAUNCH(h);
+        k_prep_pssnr<<<nreq, MF_THREADS, (size_t)h->g.Ks * sizeof(double), h->stream>>>(
+            h->g, static_cast<const int4 *>(reqs_dev), ctf, h->d_optlp, h->ptcls, h->sqsums);
+        return cudaGetLastError();
+    }
     PFTCC_LAUNCH(h);
     k_prep_matchfilt<<<nreq, MF_THREADS, (size_t)6 * h->g.Ks * sizeof(double), h->stream>>>(h->g, static_cast<const MatchReq *>(reqs_dev), h->refs_even,
                                                          h->refs_odd, ctf, h->d_iseven, h->d_optlp, h->ptcls,

@@ -523,6 +523,17 @@ int pftcc_set_objfun(pftcc_handle *h, int objfun)
     return PFTCC_OK;
 }
 
+int pftcc_set_pssnr(pftcc_handle *h, int on)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    if (on && !h->cfg.match_filt)
+        return set_err(h, PFTCC_ERR_STATE, "set_pssnr: l_pssnr needs the matched-filter mode (cfg.match_filt)");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    h->pssnr = on ? 1 : 0;
+    h->ws.ptcl_spectra_valid = 0;
+    return PFTCC_OK;
+}
+
 int pftcc_set_ref_optlp(pftcc_handle *h, int iref, const float *optlp)
 {
     if (!h || !optlp) return set_err(h, PFTCC_ERR_ARG, "set_ref_optlp: bad arguments");

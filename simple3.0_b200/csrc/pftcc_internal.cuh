@@ -124,6 +124,7 @@ struct pftcc_handle {
     // and the shell factors of shellnorm_and_filter_ref [2 sets][nrefs][Ks]
     float *d_optlp = nullptr;
     float *d_snorm = nullptr;
+    int pssnr = 0;                       // params_glob%l_pssnr (within the matched-filter mode)
     // particle ingestion state (k_ingest.cu: cuFFT plans and scratch)
     void *ingest = nullptr;
     // the orientation derivatives of the references (fdf_project_polar), [nrefs][3][K][P]

@@ -333,6 +333,10 @@ class polarft_corrcalc:
         return out
 
     # ---- the matched-filter mode (new(..., match_filt=True)) ----------------------------------
+    def set_pssnr(self, on: bool = True):
+        """params_glob%l_pssnr within the matched-filter mode (pftcc_set_pssnr)"""
+        self._check(self._L.pftcc_set_pssnr(self._h, int(bool(on))))
+
     def set_ref_optlp(self, iref: int, optlp):
         """ref_optlp(kfrom:kstop, iref) = optlp (the reference's matched filter)"""
         a = np.ascontiguousarray(optlp, np.float32)

@@ -129,3 +129,46 @@ def test_prep_matchfilt(pkg, O):
         pc.set_ref_optlp(1, np.ones(w.kto - w.kfrom + 1, np.float32))
     assert e.value.status == pkg._lib.ERR_STATE
     pc.kill()
+
+
+def test_pssnr_mode(pkg, O):
+    """l_pssnr (pftcc_set_pssnr): the correlators use the reference scaled to power ssnr k per
+    shell (shellnorm_and_filter_ref :763-770), the m-domain search too, and prep_matchfilt
+    rescales the particle by sqrt(k / power) sqrt(1 + ssnr |CTF|^2) (:999-1019)"""
+    w = pkg.synth.config0(nrefs=3, nptcls=3)
+    pc, refs, parts, opt = build(pkg, w, "ref")
+    g = O.geom(w.nrots, w.kfrom, w.kto, w.box, kstop=w.kto - 3)
+    t = O.tables(g)
+    try:
+        pc.set_pssnr(True)
+        for i in range(3):
+            c = O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[i]), float(parts.dfy[i]),
+                                          float(parts.angast[i])))
+            pft = pc.get_ptcl_pft(i + 1)
+            for r in (1, 2, 3):
+                s = O.shellnorm_factors(g, refs[r - 1], opt.get(r), pssnr=True)
+                rs = refs[r - 1].astype(np.complex64).copy()
+                rs[:g.Ks] = (rs[:g.Ks] * s[:, None].astype(np.float32)).astype(np.complex64)
+                assert relerr(pc.gencorrs(r, i + 1, [0.4, 0.3]), O.gencorrs(g, t, rs, pft, c, [0.4, 0.3])) < 2e-5
+                want = O.gencorr_for_rot(g, t, rs, pft, 7, c, np.array([0.4, 0.3]), True)
+                assert abs(pc.gencorr_for_rot_8(r, i + 1, np.array([0.4, 0.3]), 7) - want) < 1e-6
+        # prep_matchfilt in the pssnr mode against the oracle
+        before = pc.get_ptcl_pft(2)
+        c = O.ctfmat(g, t, O.make_ctf(w.smpd, w.kv, w.cs, w.fraca, float(parts.dfx[1]), float(parts.dfy[1]),
+                                      float(parts.angast[1])))
+        pc.prep_matchfilt(2, 3, 11)
+        want = O.prep_matchfilt_pssnr(g, before, c, opt[3])
+        got = pc.get_ptcl_pft(2)
+        assert np.max(np.abs(got - want)) < 2e-6 * np.max(np.abs(want))
+        sq = np.sum(np.abs(got[:g.Ks].astype(np.complex128)) ** 2)
+        assert abs(pc.get_sqsum_ptcl(2) - sq) < 1e-5 * sq
+        pc.set_pssnr(False)
+    finally:
+        pc.kill()
+    # the mode needs the matched filter
+    plain = pkg.polarft_corrcalc()
+    plain.new(1, (1, 1), box=64, nrots=128, kfromto=(2, 20), ctf=False)
+    with pytest.raises(pkg.PftccError) as e:
+        plain.set_pssnr(True)
+    assert e.value.status == pkg._lib.ERR_STATE
+    plain.kill()

@@ -93,3 +93,29 @@ def test_prep_matchfilt_identical_pair(O):
     ref = rand_pft(np.random.default_rng(9), g.K, g.pftsz)
     got = O.prep_matchfilt(g, ref, ref, 1)
     assert np.allclose(np.mean(np.abs(got.astype(np.complex128)) ** 2, axis=1), 1.0, rtol=1e-5)
+
+
+def test_pssnr_factors_and_particle_weights(O):
+    """the l_pssnr branches (shellnorm_and_filter_ref :763-770; prep_matchfilt :999-1019): the
+    reference's shell k scaled to power ssnr k (ssnr = ref_optlp(k)); the particle's shell k to
+    power k times sqrt(1 + ssnr |CTF|^2) sample by sample"""
+    g = O.geom(128, 2, 20, 64, kstop=17)
+    t = O.tables(g)
+    rng = np.random.default_rng(3)
+    ref = rand_pft(rng, g.K, g.pftsz)
+    ssnr = rng.uniform(0.1, 3.0, g.Ks).astype(np.float32)
+    s = O.shellnorm_factors(g, ref, ssnr, pssnr=True)
+    k = np.arange(g.kfrom, g.kstop + 1)
+    pw = np.mean(np.abs(ref[:g.Ks].astype(np.complex128) * s[:, None]) ** 2, axis=1)
+    assert np.allclose(pw, ssnr.astype(np.float64) * k, rtol=1e-6)
+    z = ref.copy()
+    z[2] = 0
+    assert O.shellnorm_factors(g, z, ssnr, pssnr=True)[2] == pytest.approx(float(np.sqrt(float(ssnr[2]) * k[2])))
+    ptcl = rand_pft(rng, g.K, g.pftsz)
+    ctf = O.ctfmat(g, t, O.make_ctf(dfx=1.8, dfy=1.7, angast=10.0))
+    got = O.prep_matchfilt_pssnr(g, ptcl, ctf, ssnr)
+    q = ptcl[:g.Ks].astype(np.complex128)
+    w = np.sqrt(k) / np.sqrt(np.mean(np.abs(q) ** 2, axis=1))
+    want = q * w[:, None] * np.sqrt(1.0 + ssnr.astype(np.float64)[:, None] * ctf[:g.Ks] ** 2)
+    assert np.allclose(got[:g.Ks], want, rtol=1e-6, atol=1e-6 * np.abs(want).max())
+    assert np.array_equal(got[g.Ks:], ptcl[g.Ks:])                 # shells beyond kstop untouched
