@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--ntop", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-arms", action="store_true", help="skip the FP32 / exact / reference-frame arms")
+    ap.add_argument("--no-autotune", action="store_true", help="the automatic wave sizes, no autotuner")
+    ap.add_argument("--wisdom", default=os.path.join(ROOT, "simple3.0_b200", "wisdom.txt"),
+                    help="the autotuner's wisdom file (read, and appended when a shape is tuned)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
@@ -257,6 +260,11 @@ def run_ours(args):
         if world > 1:
             dist.all_gather_into_tensor(gathered, best)
 
+    # wave / tile sizes from the autotuner (untimed; a wisdom line for this shape skips the timing)
+    tuning = None
+    if args.precision in ("bf16x3", "fp32") and not args.no_autotune:
+        step()      # the particles' polar FTs and CTFs for the tuning searches
+        tuning = pc.autotune(shifts, args.precision, args.ntop, wisdom=args.wisdom)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
@@ -376,7 +384,8 @@ def run_ours(args):
                 "config": {"workload": w.name, "nrefs": w.nrefs, "nptcls": w.nptcls, "nshifts": ns,
                            "nrots": w.nrots, "kfromto": [w.kfrom, w.kto], "box": w.box,
                            "precision": args.precision, "ntop_rescore": args.ntop, "ctf_frame": "ptcl",
-                           "l2": "inputs larger than L2 (1.33 GB particle FTs)", "parallelism": f"dp{world}"},
+                           "l2": "inputs larger than L2 (1.33 GB particle FTs)", "parallelism": f"dp{world}",
+                           "tuning": tuning},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clocks}
         if arms is not None:
@@ -419,9 +428,13 @@ def other_arms(pkg, pc, w, shifts, parts, r_host, ctfp, cmats, best, stream, dev
 
     out = {}
     k = max(1, min(args.steps, 3))
-    # plain FP32: the m-domain contraction on the CUDA cores, FP32 end to end
+    # plain FP32: the m-domain contraction on the CUDA cores, FP32 end to end, with its own tuning
+    bf16_tuning = pc.get_tuning()
+    t32 = None if args.no_autotune else pc.autotune(shifts, "fp32", args.ntop, wisdom=args.wisdom)
     ms32 = timed(lambda: pc.search_best_dev(shifts, "fp32", args.ntop, best.data_ptr()), k, 1)
+    pc.set_tuning(bf16_tuning["w_rows"], bf16_tuning["w_cols"], bf16_tuning["s1_stages"])
     out["fp32_mdomain"] = {"value": evals_per_step(w, ns) * world / (ms32 / 1e3), "ms_per_step": ms32, "steps": k,
+                           "tuning": t32,
                            "what": "search_best PFTCC_PREC_FP32 (particle frame, the same top-8 re-score), "
                                    "inputs resident"}
     # the exact drop-in kernel (direct sums, FP32 products, FP64 accumulation) on a bounded

@@ -360,6 +360,24 @@ typedef struct { int irot, found_better, nevals, ncycles; float corr, shift[2], 
 int pftcc_shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts *opts, int n, const pftcc_shsrch_req *req,
                        pftcc_shsrch_out *out);
 
+/* wave and tile sizes of the m-domain search (no counterpart in the reference; FFTW's plans
+ * and wisdom file play this role there, simple_polarft_corrcalc.f90:391-408): w_rows x w_cols
+ * (reference x shift) rows by particle columns per stage-1 / stage-2 round (multiples of 64 and
+ * 128; the stage-1 output of a round takes (nrots/2 + 1) w_rows w_cols x 8 bytes), s1_stages the
+ * depth of the tcgen05 kernel's row-tile ring (2..4).  0 keeps the automatic choice.  The sizes
+ * change only how the work is cut, never a result. */
+typedef struct { int w_rows, w_cols, s1_stages, from_wisdom; } pftcc_tuning;
+int pftcc_set_tuning(pftcc_handle *h, const pftcc_tuning *t);
+int pftcc_get_tuning(const pftcc_handle *h, pftcc_tuning *t);
+/* the autotuner: times the search (precision, ntop, the shift list) on the handle's current
+ * references and particles over candidate wave sizes and ring depths (coordinate descent from
+ * the automatic choice, each candidate run twice and the second run timed with CUDA events) and
+ * keeps the fastest on the handle.  With wisdom (a file path, nullable) a line for this search's
+ * shape (device, nrots, shells, rows, columns, precision, frame, ntop) is read first and, when
+ * found, used without timing (out->from_wisdom = 1); otherwise the tuned line is appended. */
+int pftcc_autotune(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, const char *wisdom,
+                   pftcc_tuning *out);
+
 /* stochastic neighbourhood hill climbing over the references for every held particle
  * (strategy2D_snhc srch_snhc, simple_strategy2D_snhc.f90:33-93, with shcloc,
  * simple_rnd.f90:273-295): order is [nptcls][nrefs] (slot order; each row the particle's

@@ -65,6 +65,10 @@ class PrepOpts(C.Structure):
                 ("griddev", C.c_int)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("w_rows", C.c_int), ("w_cols", C.c_int), ("s1_stages", C.c_int), ("from_wisdom", C.c_int)]
+
+
 class ShsrchOpts(C.Structure):
     _fields_ = [("opt_angle", C.c_int), ("coarse_init", C.c_int), ("maxits", C.c_int), ("max_evals", C.c_int),
                 ("halfrot", C.c_float), ("pad", C.c_int)]
@@ -156,6 +160,9 @@ SIGNATURES = {
     "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
                            C.POINTER(RefineOut)],
     "pftcc_gencorrs_noalloc": [_h, C.c_int, _ip, _ip, _fp, _vp],
+    "pftcc_set_tuning": [_h, C.POINTER(Tuning)],
+    "pftcc_get_tuning": [_h, C.POINTER(Tuning)],
+    "pftcc_autotune": [_h, C.c_int, _fp, C.c_int, C.c_int, C.c_char_p, C.POINTER(Tuning)],
     "pftcc_shsrch_batch": [_h, C.c_int, C.POINTER(ShsrchOpts), C.c_int, C.POINTER(ShsrchReq), C.POINTER(ShsrchOut)],
     "pftcc_search_snhc": [_h, _ip, _fp, _ip, C.c_int, C.c_ulonglong, C.c_int, C.POINTER(SnhcOut)],
     "pftcc_get_nrots": [_h, _ip],

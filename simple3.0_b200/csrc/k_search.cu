@@ -1143,13 +1143,20 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     // mid-tile, so one spare tile of zero columns
     const int cols_pad = (np + COL_TILE - 1) / COL_TILE * COL_TILE + COL_TILE;
     const int rows_pad = (nrs + S1_TILE - 1) / S1_TILE * S1_TILE;
-    // wave sizes: rows x cols per stage-1/stage-2 round, X scratch ~ 3 GiB max
+    // wave sizes: rows x cols per stage-1/stage-2 round; automatic: 4096 x up to 4096 with the
+    // stage-1 output X within 8 GiB; a tuning (pftcc_set_tuning / the autotuner) may ask for other
+    // sizes, X then within 24 GiB
     int W_rows = std::min(rows_pad, 4096);
     int W_cols = std::min(cols_pad - COL_TILE, 4096);
-    while ((size_t)M * W_rows * W_cols * sizeof(float2) > (8ull << 30) && W_cols > COL_TILE) W_cols /= 2;
+    size_t x_budget = 8ull << 30;
+    if (h->tune.w_rows > 0) { W_rows = std::min(rows_pad, std::max(S1_TILE, h->tune.w_rows / S1_TILE * S1_TILE)); x_budget = 24ull << 30; }
+    if (h->tune.w_cols > 0) { W_cols = std::min(cols_pad - COL_TILE, std::max(COL_TILE, h->tune.w_cols / COL_TILE * COL_TILE)); x_budget = 24ull << 30; }
+    while ((size_t)M * W_rows * W_cols * sizeof(float2) > x_budget && W_cols > COL_TILE) W_cols /= 2;
+    W_cols = std::max(COL_TILE, W_cols / COL_TILE * COL_TILE);
     const int nr_wave_max = (W_rows + ns - 1) / ns + 2;
-    // (re)allocate the workspace when the geometry or counts change
-    const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M;
+    // (re)allocate the workspace when the geometry, the counts or the wave change
+    const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M ||
+                         ws.W_rows != W_rows || ws.W_cols != W_cols;
     if (realloc) {
         void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.Yn, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref,
                         ws.A16, ws.B16, ws.best};
@@ -1170,6 +1177,7 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
             (st = ensure_ws(h, (void **)&ws.cand_ref, (size_t)cols_pad * sizeof(int) + (size_t)P * sizeof(int), "perm")))
             return st;
         ws.nrs_pad = rows_pad; ws.np_pad = cols_pad; ws.nshifts = ns; ws.M = M; ws.nrs = nrs;
+        ws.W_rows = W_rows; ws.W_cols = W_cols;
         ws.X_elems = (size_t)M * W_rows * W_cols;
     }
     int *d_perm = ws.cand_ref;

@@ -584,7 +584,7 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     const size_t tail = 512 + STAGE_BYTES;
     if (ACC_COLS + 2 * 4 * KC > TMEM_COLS)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: particle tiles too large for tensor memory");
-    int stages = 4;
+    int stages = h->tune.s1_stages >= 2 && h->tune.s1_stages <= 4 ? h->tune.s1_stages : 4;
     while (stages > 1 && 1024 + a_bytes + stages * 2 * b_bytes + tail > 227 * 1024) --stages;
     if (1024 + a_bytes + stages * 2 * b_bytes + tail > 227 * 1024)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");

@@ -1680,6 +1680,122 @@ int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int
     return PFTCC_OK;
 }
 
+int pftcc_set_tuning(pftcc_handle *h, const pftcc_tuning *t)
+{
+    if (!h || !t) return set_err(h, PFTCC_ERR_ARG, "set_tuning: bad arguments");
+    if (t->w_rows < 0 || t->w_cols < 0 || (t->s1_stages != 0 && (t->s1_stages < 2 || t->s1_stages > 4)))
+        return set_err(h, PFTCC_ERR_ARG, "set_tuning: w_rows, w_cols >= 0 and s1_stages 0 or 2..4");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    h->tune = *t;
+    h->tune.from_wisdom = 0;
+    return PFTCC_OK;
+}
+
+int pftcc_get_tuning(const pftcc_handle *h, pftcc_tuning *t)
+{
+    if (!h || !t) return PFTCC_ERR_ARG;
+    *t = h->tune;
+    return PFTCC_OK;
+}
+
+// the wisdom line of a search shape: the device and what decides the work's cut
+static std::string wisdom_key(pftcc_handle *h, int nshifts, int precision, int ntop)
+{
+    cudaDeviceProp pr{};
+    cudaGetDeviceProperties(&pr, h->dev);
+    std::string dev = pr.name;
+    for (char &c : dev)
+        if (c == ' ') c = '_';
+    return "pftcc-wisdom-v1 " + dev + " sms=" + std::to_string(pr.multiProcessorCount) + " nrots=" +
+           std::to_string(h->g.N) + " shells=" + std::to_string(h->g.Ks) + " rows=" +
+           std::to_string((long long)h->nrefs * std::max(1, nshifts)) + " cols=" + std::to_string(h->nptcls) +
+           " prec=" + std::to_string(precision) + " frame=" + std::to_string(h->cfg.ctf_frame) + " ntop=" +
+           std::to_string(ntop) + " objfun=" + std::to_string(h->objfun);
+}
+
+int pftcc_autotune(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, const char *wisdom,
+                   pftcc_tuning *out)
+{
+    if (!h || nshifts < 0 || (nshifts > 0 && !shifts) || ntop < 0 || ntop > 8 ||
+        (precision != PFTCC_PREC_FP32 && precision != PFTCC_PREC_BF16X3))
+        return set_err(h, PFTCC_ERR_ARG, "autotune: bad arguments (FP32 or BF16X3 searches are tuned)");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    const std::string key = wisdom_key(h, nshifts, precision, ntop);
+    if (wisdom) {
+        if (FILE *f = std::fopen(wisdom, "r")) {
+            char line[1024];
+            pftcc_tuning t{};
+            bool found = false;
+            while (std::fgets(line, sizeof line, f)) {
+                std::string l(line);
+                const size_t arrow = l.find(" -> ");
+                if (arrow == std::string::npos || l.substr(0, arrow) != key) continue;
+                if (std::sscanf(l.c_str() + arrow + 4, "w_rows=%d w_cols=%d s1_stages=%d", &t.w_rows, &t.w_cols,
+                                &t.s1_stages) == 3)
+                    found = true;   // the last matching line wins
+            }
+            std::fclose(f);
+            if (found) {
+                h->tune = t;
+                h->tune.from_wisdom = 1;
+                if (out) *out = h->tune;
+                return PFTCC_OK;
+            }
+        }
+    }
+    ST(ensure(h, (void **)&h->d_best, &h->best_cap, (size_t)h->nptcls * sizeof(pftcc_best), "best"));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0), "autotune");
+    CK(cudaEventCreate(&e1), "autotune");
+    // one timed search (after an untimed one that sizes the workspace) per candidate
+    auto timed = [&](const pftcc_tuning &t, float *ms) -> int {
+        h->tune = t;
+        for (int rep = 0; rep < 2; ++rep) {
+            if (rep == 1) CK(cudaEventRecord(e0, h->stream), "autotune");
+            ST(search_mdomain(h, nshifts, shifts, precision, ntop, h->d_best, nullptr));
+            if (rep == 1) CK(cudaEventRecord(e1, h->stream), "autotune");
+        }
+        CK(cudaEventSynchronize(e1), "autotune");
+        CK(cudaEventElapsedTime(ms, e0, e1), "autotune");
+        return PFTCC_OK;
+    };
+    const int rows = (int)std::min<long long>((long long)h->nrefs * std::max(1, nshifts), 1 << 30);
+    pftcc_tuning best{0, 0, 0, 0};
+    float best_ms = 0.f;
+    int st = timed(best, &best_ms);
+    const int wr_c[] = {2048, 4096, 8192, 16384}, wc_c[] = {512, 1024, 2048, 4096, 8192}, s1_c[] = {2, 3, 4};
+    for (int dim = 0; dim < 3 && st == PFTCC_OK; ++dim) {
+        const int *vals = dim == 0 ? wc_c : dim == 1 ? wr_c : s1_c;
+        const int nv = dim == 0 ? 5 : dim == 1 ? 4 : 3;
+        for (int v = 0; v < nv && st == PFTCC_OK; ++v) {
+            pftcc_tuning t = best;
+            if (dim == 0) { if (vals[v] > h->nptcls + 127) continue; t.w_cols = vals[v]; }
+            if (dim == 1) { if (vals[v] > rows + 63) continue; t.w_rows = vals[v]; }
+            if (dim == 2) t.s1_stages = vals[v];
+            float ms = 0.f;
+            st = timed(t, &ms);
+            if (st == PFTCC_ERR_OOM) { st = PFTCC_OK; continue; }   // a wave too large for the free memory
+            if (st == PFTCC_OK && ms < best_ms) { best_ms = ms; best = t; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->tune = best;
+    h->tune.from_wisdom = 0;
+    if (st != PFTCC_OK) return st;
+    if (wisdom) {
+        if (FILE *f = std::fopen(wisdom, "a")) {
+            std::fprintf(f, "%s -> w_rows=%d w_cols=%d s1_stages=%d ms=%.3f\n", key.c_str(), best.w_rows, best.w_cols,
+                         best.s1_stages, best_ms);
+            std::fclose(f);
+        }
+    }
+    if (out) *out = h->tune;
+    return PFTCC_OK;
+}
+
 int pftcc_search_best(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out)
 {
     if (!h || !out) return set_err(h, PFTCC_ERR_ARG, "search_best: bad arguments");

@@ -68,6 +68,7 @@ struct UmmaState {
 // m-domain search workspace (sized on first use, reused across calls)
 struct SearchWS {
     int nshifts = 0, nrs = 0, nrs_pad = 0, np_pad = 0, M = 0, Mpad = 0;
+    int W_rows = 0, W_cols = 0;  // the wave the buffers were sized for
     float2 *UA = nullptr;        // [M][nrs_pad][Ks] ref-side spectra (FP32 path)
     float2 *UB = nullptr;        // [M][np_pad][Ks] particle-side spectra (FP32 path)
     double2 *RU = nullptr;       // [nrefs][J][Ks] spectra of |ref|^2, J = P/2+1
@@ -155,6 +156,7 @@ struct pftcc_handle {
     std::string last_err;
     long long launches = 0;
     long long wait_limit = 0;            // pipeline-wait polls of the tcgen05 kernels (0 = default)
+    pftcc_tuning tune{};                 // wave and tile sizes of the m-domain search (0 = automatic)
     cudaStream_t own_stream = nullptr;
     // per-kernel-class event timing
     int prof = 0;

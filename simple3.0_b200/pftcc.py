@@ -19,6 +19,7 @@ computation runs in the CUDA library; there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -688,6 +689,25 @@ class polarft_corrcalc:
 
     def synchronize(self):
         self._check(self._L.pftcc_synchronize(self._h))
+
+    def set_tuning(self, w_rows: int = 0, w_cols: int = 0, s1_stages: int = 0):
+        """wave and tile sizes of the m-domain search (0 = automatic; pftcc_set_tuning)"""
+        self._check(self._L.pftcc_set_tuning(self._h, C.byref(_lib.Tuning(int(w_rows), int(w_cols), int(s1_stages), 0))))
+
+    def get_tuning(self) -> dict:
+        t = _lib.Tuning()
+        self._check(self._L.pftcc_get_tuning(self._h, C.byref(t)))
+        return {"w_rows": t.w_rows, "w_cols": t.w_cols, "s1_stages": t.s1_stages, "from_wisdom": bool(t.from_wisdom)}
+
+    def autotune(self, shifts=None, precision="bf16x3", ntop: int = 8, wisdom: str | None = None) -> dict:
+        """the autotuner (pftcc_autotune): the fastest wave / tile sizes for this search on the held
+        data, read from or appended to the wisdom file"""
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        t = _lib.Tuning()
+        self._check(self._L.pftcc_autotune(self._h, ns, None if sh is None else _f32p(sh), _PRECS[precision],
+                                           int(ntop), None if wisdom is None else os.fsencode(wisdom), C.byref(t)))
+        return {"w_rows": t.w_rows, "w_cols": t.w_cols, "s1_stages": t.s1_stages, "from_wisdom": bool(t.from_wisdom)}
 
     def set_wait_limit(self, polls: int):
         """polls of a tensor-core pipeline wait before the call gives up with PFTCC_ERR_TIMEOUT
