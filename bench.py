@@ -644,7 +644,7 @@ def run_batching_report(args):
            "geometry_chunks": {g: sum(1 for s_ in spec if s_[0] == g) for g in "ABC"},
            "particles": sum(s_[2] for s_ in spec), "evals": evals, "data_seconds": round(t_gen, 1)}
     results = {}
-    for workers in (1, 2):
+    for workers in (1, 2, 4):
         times = []
         for _ in range(args.repeats):
             torch.cuda.synchronize()
@@ -655,7 +655,7 @@ def run_batching_report(args):
         out[f"workers_{workers}"] = {"seconds": round(t, 3), "seconds_all": [round(x, 3) for x in times],
                                      "evals_per_s": evals / t, "chunks_per_s": len(chunks) / t}
     out["identical_results"] = all(np.array_equal(a.view(np.int32).reshape(len(a), -1), c.view(np.int32).reshape(len(c), -1))
-                                   for a, c in zip(results[1], results[2]))
+                                   for w_ in (2, 4) for a, c in zip(results[1], results[w_]))
     print(json.dumps(out), flush=True)
 
 
