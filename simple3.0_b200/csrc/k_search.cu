@@ -542,13 +542,11 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 // (spectra FP64, products FP32, transform FP64); stored as the FP32 factor
 // Dinv[rl][col][rho] = 1/sqrt(D(rho) * sqsum_ptcl(col)) the correlations are scaled by.
 // Two kernels per wave:
-//   k_norm_y: Y for every (reference, particle) pair of the wave as a batched complex
-//            GEMM over the shells -- a block takes 32 references x 64 particles and 8
-//            values of j, stages the j-th |ref|^2 and CTF^2 spectra of its tile in shared
-//            memory (k-major, FP32), and each thread accumulates 2 references x 4
-//            particles with two-lane FP32 FMAs (these factors rank the search's
-//            candidates; the re-score forms its own normaliser in FP64); Y[rl][cl][j],
-//            scaled by wgt_j / P, stored FP64 for the transform;
+//   k_norm_y2: Y for every (reference, particle) pair of the wave as a batched complex
+//            product over the shells, from FP32 copies of the spectra transposed to
+//            [j][k][reference] and [j][k][particle] (k_norm_cvt), two-lane FP32 FMAs (these
+//            factors rank the search's candidates; the re-score forms its own normaliser in
+//            FP64); Y[rl][cl][j] unscaled, FP32;
 //   k_norm:  D from Y, one block per particle column, NORM_RB = 32 references at a time:
 //            lane = reference, each thread NORM_GPT residues g < P/Q, and for each g the Q
 //            rotations rho = g + q P/Q at once: with S_r = sum_{j = r mod Q} Y(j) w_P^{j g},
@@ -560,78 +558,83 @@ __global__ void __launch_bounds__(256) k_stage1_fp32(int Ks, int P, const float2
 // (l2, l2 + 1) of its pass B: Dinv[rl][col][l2 >> 1][l1][b][l2 & 1] for
 // rot = 2 (l2 + p2 l1) + b (rho = rot mod P; for odd p2 lane 1 of the last pair repeats
 // l2 = p2 - 1; 4 P1 ceil(p2 / 2) values), multiplied by dscale.
-constexpr int NORM_RB = 32;
-constexpr int NORM_GPT = 3;
-constexpr int NY_R = 32, NY_C = 64, NY_J = 8;
-
-__global__ void __launch_bounds__(256) k_norm_y(Geom g, const double2 *__restrict__ RU, const double2 *__restrict__ CV,
-                                                int r0, int nr, int c0, int ncols, double2 *__restrict__ Y)
+// FP32 copies of the normaliser's spectra, transposed so that the contraction below reads
+// them coalesced: RUf[j][k][r] = RU[r][j][k] (|ref|^2 spectra), CVf[j][k][c] = CV[c][j][k]
+// (CTF^2 spectra); the values the FP64 spectra round to, as the contraction always used
+constexpr int CVT_BLOCKS = 8 * 148;   // grid-stride copy, 8 blocks per SM of a B200
+__global__ void k_norm_cvt(int n, int J, int Ks, int n_pad, const double2 *__restrict__ src, float2 *__restrict__ dst)
 {
-    extern __shared__ float4 sy4[];
-    const int P = g.P, Ks = g.Ks, J = P / 2 + 1;
-    // the j-th spectra of the tile in FP32, laid out for the two-lane products:
-    // sr[k][r] = (u.x, u.x, u.y, u.y) of |ref|^2, sc[k][c] = (v.x, v.y, v.y, -v.x) of CTF^2, so that
-    // conj(u) v accumulates as fma2((u.x, u.x), (v.x, v.y)) + fma2((u.y, u.y), (v.y, -v.x))
-    float4 *sr = sy4;                        // [Ks][NY_R]
-    float4 *sc = sy4 + (size_t)Ks * NY_R;    // [Ks][NY_C]
-    const int cb = blockIdx.x * NY_C, rb = blockIdx.y * NY_R, j0 = blockIdx.z * NY_J;
-    const int tc = threadIdx.x & 15, tr = threadIdx.x >> 4;   // particles tc + 16 q, references tr + 16 i
-    const double invP = 1.0 / P;
-    for (int j = j0; j < min(J, j0 + NY_J); ++j) {
-        __syncthreads();
-        for (int e = threadIdx.x; e < NY_R * Ks; e += blockDim.x) {
-            const int r = e / Ks, k = e - r * Ks;
-            float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (rb + r < nr) {
-                const double2 u = __ldg(RU + ((size_t)(r0 + rb + r) * J + j) * Ks + k);
-                w = make_float4((float)u.x, (float)u.x, (float)u.y, (float)u.y);
-            }
-            sr[(size_t)k * NY_R + r] = w;
+    const long long tot = (long long)n_pad * J * Ks;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e % n_pad);
+        const long long jk = e / n_pad;   // j * Ks + k
+        float2 v = make_float2(0.f, 0.f);
+        if (r < n) {
+            const double2 u = src[(size_t)r * J * Ks + jk];
+            v = make_float2((float)u.x, (float)u.y);
         }
-        for (int e = threadIdx.x; e < NY_C * Ks; e += blockDim.x) {
-            const int c = e / Ks, k = e - c * Ks;
-            float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (cb + c < ncols) {
-                const double2 v = __ldg(CV + ((size_t)(c0 + cb + c) * J + j) * Ks + k);
-                w = make_float4((float)v.x, (float)v.y, (float)v.y, -(float)v.x);
-            }
-            sc[(size_t)k * NY_C + c] = w;
-        }
-        __syncthreads();
-        float2 acc[2][4];
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
-#pragma unroll 4
-        for (int k = 0; k < Ks; ++k) {
-            float4 u[2], v[4];
-#pragma unroll
-            for (int i = 0; i < 2; ++i) u[i] = sr[(size_t)k * NY_R + tr + 16 * i];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) v[q] = sc[(size_t)k * NY_C + tc + 16 * q];
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    acc[i][q] = __ffma2_rn(make_float2(u[i].x, u[i].y), make_float2(v[q].x, v[q].y), acc[i][q]);
-                    acc[i][q] = __ffma2_rn(make_float2(u[i].z, u[i].w), make_float2(v[q].z, v[q].w), acc[i][q]);
-                }
-        }
-        const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) * invP;
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = rb + tr + 16 * i, c = cb + tc + 16 * q;
-                if (r < nr && c < ncols)
-                    Y[((size_t)r * ncols + c) * J + j] = make_double2(wgt * acc[i][q].x, wgt * acc[i][q].y);
-            }
+        dst[e] = v;
     }
 }
 
+// Y(j) = sum_k conj(RU(j,k)) CV(j,k) for every (reference, particle) pair of a wave: FP32 products
+// accumulated in FP32 as two lane-pair fmas per complex product, (u.x, u.x)(v.x, v.y) +
+// (u.y, u.y)(v.y, -v.x), k in increasing order.  Block: one j, NY2_R = 8 references x 512
+// particles, 4 warps; every thread takes the 8 references (their spectra read at one address per
+// warp) and the particles l + 32 q (q < 4) of its warp's 128 (coalesced reads), 32 accumulators.
+// Y[(rl * ncols + cl) * J + j] unscaled (the transform applies the weights wgt_j / P).
+constexpr int NY2_R = 8, NY2_C = 512;
+__global__ void __launch_bounds__(128) k_norm_y2(int Ks, int J, const float2 *__restrict__ RUf, int nrefs_p,
+                                                 const float2 *__restrict__ CVf, int cols_pad, int r0, int nr, int c0,
+                                                 int ncols, float2 *__restrict__ Y)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rb = blockIdx.y * NY2_R, cb = blockIdx.x * NY2_C + warp * 128, j = blockIdx.z;
+    if (cb >= ncols) return;
+    int rr[NY2_R], cc[4];   // clamped reads; the stores are masked
+#pragma unroll
+    for (int i = 0; i < NY2_R; ++i) rr[i] = r0 + min(rb + i, nr - 1);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cc[q] = c0 + min(cb + lane + 32 * q, ncols - 1);
+    const float2 *ur = RUf + (size_t)j * Ks * nrefs_p;
+    const float2 *vr = CVf + (size_t)j * Ks * cols_pad;
+    float2 acc[NY2_R][4];
+#pragma unroll
+    for (int i = 0; i < NY2_R; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
+#pragma unroll 2
+    for (int k = 0; k < Ks; ++k) {
+        float2 v[4], vb[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            v[q] = __ldg(vr + (size_t)k * cols_pad + cc[q]);
+            vb[q] = make_float2(v[q].y, -v[q].x);
+        }
+#pragma unroll
+        for (int i = 0; i < NY2_R; ++i) {
+            const float2 u = __ldg(ur + (size_t)k * nrefs_p + rr[i]);
+            const float2 ux = make_float2(u.x, u.x), uy = make_float2(u.y, u.y);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc[i][q] = __ffma2_rn(ux, v[q], acc[i][q]);
+                acc[i][q] = __ffma2_rn(uy, vb[q], acc[i][q]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NY2_R; ++i)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int rl = rb + i, cl = cb + lane + 32 * q;
+            if (rl < nr && cl < ncols) Y[((size_t)rl * ncols + cl) * J + j] = acc[i][q];
+        }
+}
+
+constexpr int NORM_RB = 32;
+constexpr int NORM_GPT = 3;
 template <int Q>
-__global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict__ Yg, int nr, int c0, int ncols,
+__global__ void __launch_bounds__(256) k_norm(Geom g, const float2 *__restrict__ Yg, int nr, int c0, int ncols,
                                               int dcols, const float *__restrict__ sqp, float *__restrict__ D, int p2,
                                               double dscale)
 {
@@ -655,7 +658,9 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
         __syncthreads();
         for (int it = threadIdx.x; it < nb * J; it += blockDim.x) {
             const int rb = it / J, j = it - rb * J;
-            Y[(size_t)rb * Jp + j] = Yg[((size_t)(rb0 + rb) * ncols + cl) * J + j];
+            const float2 a = Yg[((size_t)(rb0 + rb) * ncols + cl) * J + j];
+            const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
+            Y[(size_t)rb * Jp + j] = make_double2(wgt * a.x, wgt * a.y);
         }
         __syncthreads();
         if (lane < nb) {
@@ -735,7 +740,7 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const double2 *__restrict_
 //           w_{P/2}^{-n1 k2}, into buf[reference][k2][n1];
 //   pass 2, task (reference, k2): a length-N1 DFT over n1 -> conj z(k2 + N2 k1).
 template <int N1, int N2>
-__global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg, int nr, int c0, int ncols, int dcols,
+__global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg, int nr, int c0, int ncols, int dcols,
                                                   const float *__restrict__ sqp, float *__restrict__ D, int p2,
                                                   double dscale, int eu)
 {
@@ -762,19 +767,21 @@ __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg
         __syncthreads();
         for (int t = threadIdx.x; t < nb * N1; t += blockDim.x) {
             const int kl = t / N1, n1 = t - kl * N1;
-            const double2 *y = Yg + ((size_t)(rb0 + kl) * ncols + cl) * J;
+            const float2 *y = Yg + ((size_t)(rb0 + kl) * ncols + cl) * J;
+            // Y(j) times wgt_j / P: 1 / P at j = 0 and j = P/2, 2 / P otherwise
+            const double w1 = 1.0 / P, w2 = 2.0 / P;
             double2 x[N2];
 #pragma unroll
             for (int n2 = 0; n2 < N2; ++n2) {
                 const int j = n1 + N1 * n2;
                 double2 hj, hh;
                 if (j == 0) {
-                    hj = make_double2(y[0].x, 0.0);
-                    hh = make_double2(y[H].x, 0.0);
+                    hj = make_double2(w1 * y[0].x, 0.0);
+                    hh = make_double2(w1 * y[H].x, 0.0);
                 } else {
-                    const double2 a = y[j], b = y[H - j];
-                    hj = make_double2(0.5 * a.x, 0.5 * a.y);
-                    hh = make_double2(0.5 * b.x, -0.5 * b.y);
+                    const float2 a = y[j], b = y[H - j];
+                    hj = make_double2(0.5 * (w2 * a.x), 0.5 * (w2 * a.y));
+                    hh = make_double2(0.5 * (w2 * b.x), -0.5 * (w2 * b.y));
                 }
                 const double2 ev = sfft::d_add(hj, hh), od = sfft::d_mul(sfft::d_sub(hj, hh), wp[j]);
                 x[n2] = make_double2(ev.x - od.y, -(ev.y + od.x));   // conj(ev + i od)
@@ -827,7 +834,7 @@ __global__ void __launch_bounds__(256) k_norm_fft(const double2 *__restrict__ Yg
 }
 
 template <int N1, int N2>
-static cudaError_t launch_norm_fft(pftcc_handle *h, const double2 *Y, int nr, int c0, int ncols, int dcols,
+static cudaError_t launch_norm_fft(pftcc_handle *h, const float2 *Y, int nr, int c0, int ncols, int dcols,
                                    const float *sqp, float *D, int p2, double dscale, int eu)
 {
     constexpr int H = N1 * N2, NB = 256 / (N1 > N2 ? N1 : N2);
@@ -838,19 +845,17 @@ static cudaError_t launch_norm_fft(pftcc_handle *h, const double2 *Y, int nr, in
     return cudaGetLastError();
 }
 
-static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const double2 *RU, const double2 *CV, int r0, int nr,
-                               int c0, int ncols, int dcols, const float *sqp, double2 *Y, float *D, int p2,
-                               double dscale, int eu)
+static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const float2 *RUf, int nrefs_p, const float2 *CVf,
+                               int cols_pad, int r0, int nr, int c0, int ncols, int dcols, const float *sqp, float2 *Y,
+                               float *D, int p2, double dscale, int eu)
 {
     const int J = g.P / 2 + 1;
     cudaError_t e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_NORM);
     {
-        const size_t smem = (size_t)g.Ks * (NY_R + NY_C) * sizeof(float4);
-        if ((e = smem_limit((const void *)k_norm_y, smem))) return e;
-        dim3 grid((ncols + NY_C - 1) / NY_C, (nr + NY_R - 1) / NY_R, (J + NY_J - 1) / NY_J);
-        k_norm_y<<<grid, 256, smem, h->stream>>>(g, RU, CV, r0, nr, c0, ncols, Y);
+        dim3 grid((ncols + NY2_C - 1) / NY2_C, (nr + NY2_R - 1) / NY2_R, J);
+        k_norm_y2<<<grid, 128, 0, h->stream>>>(g.Ks, J, RUf, nrefs_p, CVf, cols_pad, r0, nr, c0, ncols, Y);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     PFTCC_LAUNCH(h);
@@ -1153,13 +1158,24 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
     if (h->tune.w_cols > 0) { W_cols = std::min(cols_pad - COL_TILE, std::max(COL_TILE, h->tune.w_cols / COL_TILE * COL_TILE)); x_budget = 24ull << 30; }
     while ((size_t)M * W_rows * W_cols * sizeof(float2) > x_budget && W_cols > COL_TILE) W_cols /= 2;
     W_cols = std::max(COL_TILE, W_cols / COL_TILE * COL_TILE);
+    // compile-time transforms for the common lengths; the generic radix loop otherwise, whose
+    // shared memory holds a (cc, id) pair per wave row: its rows are capped to fit 227 KB
+    const bool fast_s2 = stage2_fast_supported(P);
+    int T = 128;
+    while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
+    auto smem_generic = [&](int rows) {
+        return 2 * (size_t)P * sizeof(float2) + (size_t)P * T * sizeof(float2) +
+               (size_t)(rows + 8) * (sizeof(float) + sizeof(int));
+    };
+    if (!fast_s2)
+        while (smem_generic(W_rows) > 227 * 1024 && W_rows > S1_TILE) W_rows = std::max(S1_TILE, W_rows / 2 / S1_TILE * S1_TILE);
     const int nr_wave_max = (W_rows + ns - 1) / ns + 2;
     // (re)allocate the workspace when the geometry, the counts or the wave change
     const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M ||
                          ws.W_rows != W_rows || ws.W_cols != W_cols;
     if (realloc) {
-        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.D, ws.Yn, ws.X, ws.cand, ws.sqp, ws.shifts, ws.cand_ref,
-                        ws.A16, ws.B16, ws.best};
+        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.RUf, ws.CVf, ws.D, ws.Yn, ws.X, ws.cand, ws.sqp, ws.shifts,
+                        ws.cand_ref, ws.A16, ws.B16, ws.best};
         for (void *b : bufs) dev_free(h, b);
         umma_free(h);
         ws = SearchWS{};
@@ -1169,7 +1185,9 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
             (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
             (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
             (st = ensure_ws(h, (void **)&ws.D, (size_t)nr_wave_max * W_cols * std::max(2 * P, stage2_fast_dlen(P)) * sizeof(float), "D")) ||
-            (st = ensure_ws(h, (void **)&ws.Yn, (size_t)nr_wave_max * W_cols * J * sizeof(double2), "Y")) ||
+            (st = ensure_ws(h, (void **)&ws.RUf, (size_t)h->nrefs * J * Ks * sizeof(float2), "RUf")) ||
+            (st = ensure_ws(h, (void **)&ws.CVf, (size_t)cols_pad * J * Ks * sizeof(float2), "CVf")) ||
+            (st = ensure_ws(h, (void **)&ws.Yn, (size_t)nr_wave_max * W_cols * J * sizeof(float2), "Y")) ||
             (st = ensure_ws(h, (void **)&ws.X, (size_t)M * W_rows * W_cols * sizeof(float2), "X")) ||
             (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||
             (st = ensure_ws(h, (void **)&ws.sqp, (size_t)cols_pad * sizeof(float), "sqp")) ||
@@ -1204,22 +1222,20 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
             CKE(cudaGetLastError(), "euclid weights");
         }
         PFTCC_LAUNCH(h);
+        k_norm_cvt<<<CVT_BLOCKS, 256, 0, h->stream>>>(np, J, Ks, cols_pad, ws.CV, ws.CVf);
+        CKE(cudaGetLastError(), "CV copy");
+        PFTCC_LAUNCH(h);
         k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
         CKE(cudaGetLastError(), "cand_init");
     }
     const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKE(smem_limit((const void *)k_stage1_fp32, smem_s1), "attr");
-    int T = 128;
-    while (T > 32 && (size_t)P * T * sizeof(float2) > 180 * 1024) T -= 32;
-    const size_t smem_s2 = 2 * (size_t)P * sizeof(float2) + (size_t)P * T * sizeof(float2) +
-                           (size_t)(W_rows + 8) * (sizeof(float) + sizeof(int));
-    CKE(smem_limit((const void *)k_stage2, smem_s2), "attr");
+    const size_t smem_s2 = smem_generic(W_rows);
+    if (!fast_s2) CKE(smem_limit((const void *)k_stage2, smem_s2), "attr");
     S2Params sp{};
     sp.N = N; sp.P = P; sp.nf = plan.nf; sp.T = T;
     for (int i = 0; i < plan.nf; ++i) sp.f[i] = plan.f[i];
     sp.nshifts = ns;
-    // compile-time transforms for the common lengths; the generic radix loop otherwise
-    const bool fast_s2 = stage2_fast_supported(P);
     // the top-ntop re-score: FP32 m-domain in the particle frame, the exact kernel in
     // the reference frame
     const bool md_rescore = ntop > 0 && fast_s2 && h->cfg.ctf_frame == PFTCC_FRAME_PTCL;
@@ -1237,7 +1253,10 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         CKE(cudaGetLastError(), "spec_r2");
         CKE(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref");
         if (h->cfg.match_filt)   // the references' shell factors (shellnorm_and_filter_ref) on their spectra
-            CKE(launch_shellnorm_apply(h, M, nrs, rows_pad, ns, grp, ws.UA, ws.RU), "shell factors"); }
+            CKE(launch_shellnorm_apply(h, M, nrs, rows_pad, ns, grp, ws.UA, ws.RU), "shell factors");
+        PFTCC_LAUNCH(h);
+        k_norm_cvt<<<CVT_BLOCKS, 256, 0, h->stream>>>(h->nrefs, J, Ks, h->nrefs, ws.RU, ws.RUf);
+        CKE(cudaGetLastError(), "RU copy"); }
         if (precision == PFTCC_PREC_BF16X3) {
             int st = umma_stage1(h, M, Ks, ws.UA, 0, nrs, rows_pad, ws.UB, gc0, gc1 - gc0, cols_pad, nullptr, 1, grp);
             if (st != PFTCC_OK) return st;
@@ -1261,7 +1280,8 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
                     CKE(cudaGetLastError(), "stage1");
                 }
                 // the split-radix stage 2 reads the factor in its visiting order, times 1/(2N)
-                CKE(launch_norm(h, g, ws.RU, ws.CV, r_lo, r_hi - r_lo + 1, c0, cols, cols_t, ws.sqp, ws.Yn, ws.D,
+                CKE(launch_norm(h, g, ws.RUf, h->nrefs, ws.CVf, cols_pad, r_lo, r_hi - r_lo + 1, c0, cols, cols_t,
+                                ws.sqp, ws.Yn, ws.D,
                                 fast_s2 ? stage2_fast_p2(P) : 0, 1.0 / (2.0 * N), eu), "norm");
                 if (fast_s2) {
                     e = launch_stage2_fast(h, P, rows, rows_t, cols_t, row0, ns, r_lo, cols_t, c0, cols, nrs, ws.X, ws.D,

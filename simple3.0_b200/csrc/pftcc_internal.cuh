@@ -73,8 +73,10 @@ struct SearchWS {
     float2 *UB = nullptr;        // [M][np_pad][Ks] particle-side spectra (FP32 path)
     double2 *RU = nullptr;       // [nrefs][J][Ks] spectra of |ref|^2, J = P/2+1
     double2 *CV = nullptr;       // [np_pad][J][Ks] spectra of CTF^2
+    float2 *RUf = nullptr;       // [J][Ks][nrefs] FP32 copy of RU for the normaliser's contraction
+    float2 *CVf = nullptr;       // [J][Ks][np_pad] FP32 copy of CV
     float *D = nullptr;          // [wave refs][np_pad][P] rotation-dependent normaliser
-    double2 *Yn = nullptr;       // [wave refs][wave cols][P/2+1] its spectra (k_norm_y)
+    float2 *Yn = nullptr;        // [wave refs][wave cols][P/2+1] its spectra (k_norm_y2)
     float2 *X = nullptr;         // [M][wave rows][wave cols] stage-1 output of one wave
     size_t X_elems = 0;
     float2 *cand = nullptr;      // [np_pad][8] packed (cc, rs*N+rot) candidates
