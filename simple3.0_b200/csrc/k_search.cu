@@ -229,19 +229,22 @@ template <int N1, int N2>
 __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref_fft(
     Geom g, int nshifts, const float2 *__restrict__ refs, const float *__restrict__ shifts,
     const double *__restrict__ argtransf, const double *__restrict__ argtransf1, int rs0, int nrs, int rows_pad,
-    float2 *__restrict__ UA)
+    float2 *__restrict__ UA, int kb_per_block)
 {
     constexpr int N = N1 * N2, P = N / 2, NPT = (P + SPEC_THREADS - 1) / SPEC_THREADS;
     extern __shared__ float4 smem4[];
     const int Ks = g.Ks, M = P + 1;
+    // this block's shells [ka, kz): blockIdx.y selects kb_per_block batches of sfft::KB
+    const int ka = blockIdx.y * kb_per_block * sfft::KB, kz = min(Ks, ka + kb_per_block * sfft::KB);
     double2 *tw = reinterpret_cast<double2 *>(smem4);                              // [N] w_N^{-e}
     double2 *buf = tw + N;                                                          // the transform buffer
     float2 *a = reinterpret_cast<float2 *>(buf + sfft::buf_elems<N1, N2>());       // [KB][P]
     const int row = blockIdx.x;
     const int rs = rs0 + row;
     if (rs >= nrs) {   // zero padding rows
-        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
-            const int m = e / Ks, k = e - m * Ks;
+        const int nk = kz - ka;
+        for (int e = threadIdx.x; e < M * nk; e += blockDim.x) {
+            const int m = e / nk, k = ka + e - m * nk;
             UA[((size_t)m * rows_pad + row) * Ks + k] = make_float2(0.f, 0.f);
         }
         return;
@@ -263,10 +266,15 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ref_fft(
         if (n < P) {
             sincos(argtransf[n] * sx + argtransf[P + n] * sy, &pi[i], &pr[i]);
             sincos(argtransf1[n] * sx + argtransf1[P + n] * sy, &qi[i], &qr[i]);
+            // the recurrence carried to the block's first shell by the same steps as below
+            for (int k = 0; k < ka; ++k) {
+                const double nr = pr[i] * qr[i] - pi[i] * qi[i], ni = pr[i] * qi[i] + pi[i] * qr[i];
+                pr[i] = nr; pi[i] = ni;
+            }
         }
     }
-    for (int k0 = 0; k0 < Ks; k0 += sfft::KB) {
-        const int nk = min(sfft::KB, Ks - k0);
+    for (int k0 = ka; k0 < kz; k0 += sfft::KB) {
+        const int nk = min(sfft::KB, kz - k0);
 #pragma unroll
         for (int i = 0; i < NPT; ++i) {
             const int n = threadIdx.x + i * SPEC_THREADS;
@@ -301,23 +309,28 @@ template <int N1, int N2>
 __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl_fft(
     Geom g, const float2 *__restrict__ ptcls, const float *__restrict__ ctfmats, const int *__restrict__ perm,
     int ncols, int cols_pad, float2 *__restrict__ UB, double2 *__restrict__ CV, float *__restrict__ sqp_out,
-    const float *__restrict__ sqsums)
+    const float *__restrict__ sqsums, int kb_per_block)
 {
     constexpr int N = N1 * N2, P = N / 2, J = P / 2 + 1;
     extern __shared__ float4 smem4[];
     const int Ks = g.Ks, M = P + 1;
+    const int ka = blockIdx.y * kb_per_block * sfft::KB, kz = min(Ks, ka + kb_per_block * sfft::KB);
     double2 *tw = reinterpret_cast<double2 *>(smem4);                              // [N]
     double2 *buf = tw + N;
     float2 *b = reinterpret_cast<float2 *>(buf + sfft::buf_elems<N1, N2>());       // [KB][P]
     float *c2 = reinterpret_cast<float *>(b + sfft::KB * P);                        // [KB][P]
     const int col = blockIdx.x;
     if (col >= ncols) {
-        for (int e = threadIdx.x; e < M * Ks; e += blockDim.x) {
-            const int m = e / Ks, k = e - m * Ks;
+        const int nk = kz - ka;
+        for (int e = threadIdx.x; e < M * nk; e += blockDim.x) {
+            const int m = e / nk, k = ka + e - m * nk;
             UB[((size_t)m * cols_pad + col) * Ks + k] = make_float2(0.f, 0.f);
         }
-        for (int e = threadIdx.x; e < J * Ks; e += blockDim.x) CV[(size_t)col * J * Ks + e] = make_double2(0.0, 0.0);
-        if (threadIdx.x == 0) sqp_out[col] = 1.f;
+        for (int e = threadIdx.x; e < J * nk; e += blockDim.x) {
+            const int j = e / nk, k = ka + e - j * nk;
+            CV[(size_t)col * J * Ks + (size_t)j * Ks + k] = make_double2(0.0, 0.0);
+        }
+        if (threadIdx.x == 0 && blockIdx.y == 0) sqp_out[col] = 1.f;
         return;
     }
     const int slot = perm[col];
@@ -328,9 +341,9 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl_fft(
     }
     const float2 *Q = ptcls + (size_t)slot * g.K * P;
     const float *C = ctfmats ? ctfmats + (size_t)slot * g.K * P : nullptr;
-    if (threadIdx.x == 0) sqp_out[col] = sqsums[slot];
-    for (int k0 = 0; k0 < Ks; k0 += sfft::KB) {
-        const int nk = min(sfft::KB, Ks - k0);
+    if (threadIdx.x == 0 && blockIdx.y == 0) sqp_out[col] = sqsums[slot];
+    for (int k0 = ka; k0 < kz; k0 += sfft::KB) {
+        const int nk = min(sfft::KB, kz - k0);
         for (int e = threadIdx.x; e < nk * P; e += blockDim.x) {   // e = kl P + n
             const float c = C ? C[(size_t)k0 * P + e] : 1.f;
             const float2 q = Q[(size_t)k0 * P + e];
@@ -357,6 +370,12 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_ptcl_fft(
     }
 }
 
+// shell batches per spectra block: all of a row's batches in one block when the rows fill the
+// GPU many times over (the transform tables are then built once per row), one batch per block
+// when they do not (a search without shifts has one row per reference)
+static int spec_batches(const Geom &g) { return (g.Ks + sfft::KB - 1) / sfft::KB; }
+static int spec_kb_per_block(const Geom &g, int rows) { return rows >= 16 * 148 ? spec_batches(g) : 1; }
+
 template <int N1, int N2> static size_t spec_ref_fft_smem(int)
 {
     return (size_t)N1 * N2 * sizeof(double2) + (size_t)sfft::buf_elems<N1, N2>() * sizeof(double2) +
@@ -376,9 +395,11 @@ static cudaError_t launch_spec_ref_fft(pftcc_handle *h, const Geom &g, int ns, c
     const size_t smem = spec_ref_fft_smem<N1, N2>(0);
     cudaError_t e = smem_limit((const void *)k_spec_ref_fft<N1, N2>, smem);
     if (e != cudaSuccess) return e;
+    const int kbpb = spec_kb_per_block(g, rows_pad);
+    const dim3 grid(rows_pad, (spec_batches(g) + kbpb - 1) / kbpb);
     PFTCC_LAUNCH(h);
-    k_spec_ref_fft<N1, N2><<<rows_pad, SPEC_THREADS, smem, h->stream>>>(g, ns, refs, shifts, h->argtransf,
-                                                                         h->argtransf1, 0, nrs, rows_pad, UA);
+    k_spec_ref_fft<N1, N2><<<grid, SPEC_THREADS, smem, h->stream>>>(g, ns, refs, shifts, h->argtransf, h->argtransf1, 0,
+                                                                    nrs, rows_pad, UA, kbpb);
     return cudaGetLastError();
 }
 
@@ -407,9 +428,11 @@ static cudaError_t launch_spec_ptcl_fft(pftcc_handle *h, const Geom &g, const fl
     const size_t smem = spec_ptcl_fft_smem<N1, N2>(0);
     cudaError_t e = smem_limit((const void *)k_spec_ptcl_fft<N1, N2>, smem);
     if (e != cudaSuccess) return e;
+    const int kbpb = spec_kb_per_block(g, cols_pad);
+    const dim3 grid(cols_pad, (spec_batches(g) + kbpb - 1) / kbpb);
     PFTCC_LAUNCH(h);
-    k_spec_ptcl_fft<N1, N2><<<cols_pad, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, perm, np, cols_pad, UB, CV,
-                                                                          sqp, h->sqsums);
+    k_spec_ptcl_fft<N1, N2><<<grid, SPEC_THREADS, smem, h->stream>>>(g, h->ptcls, ctf, perm, np, cols_pad, UB, CV, sqp,
+                                                                     h->sqsums, kbpb);
     return cudaGetLastError();
 }
 
@@ -451,6 +474,69 @@ __global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2(Geom g, const float2 *
         }
         RU[(size_t)r * J * Ks + (size_t)j * Ks + k] = make_double2(ur, ui);
     }
+}
+
+// The same |ref|^2 spectra by the FP64 transforms of length N = 2P (spec_fft.cuh): RU(j) is
+// F(2j) / 2 of the transform of |ref|^2 continued periodically over the full circle, as the
+// CTF^2 spectra of k_spec_ptcl_fft.  Block (reference, kb_per_block batches of sfft::KB shells).
+template <int N1, int N2>
+__global__ void __launch_bounds__(SPEC_THREADS) k_spec_r2_fft(Geom g, const float2 *__restrict__ refs,
+                                                              double2 *__restrict__ RU, int kb_per_block)
+{
+    constexpr int N = N1 * N2, P = N / 2, J = P / 2 + 1;
+    extern __shared__ float4 smem4[];
+    const int Ks = g.Ks;
+    const int ka = blockIdx.y * kb_per_block * sfft::KB, kz = min(Ks, ka + kb_per_block * sfft::KB);
+    double2 *tw = reinterpret_cast<double2 *>(smem4);                              // [N]
+    double2 *buf = tw + N;
+    double *u2 = reinterpret_cast<double *>(buf + sfft::buf_elems<N1, N2>());      // [KB][P]
+    const int r = blockIdx.x;
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sn, cs;
+        sincospi(-2.0 * e / N, &sn, &cs);
+        tw[e] = make_double2(cs, sn);
+    }
+    const float2 *R = refs + (size_t)r * g.K * P;
+    for (int k0 = ka; k0 < kz; k0 += sfft::KB) {
+        const int nk = min(sfft::KB, kz - k0);
+        for (int e = threadIdx.x; e < nk * P; e += blockDim.x) {   // e = kl P + n
+            const float2 x = R[(size_t)k0 * P + e];
+            u2[e] = (double)x.x * x.x + (double)x.y * x.y;
+        }
+        auto getc = [&](int kl, int n) { return make_double2(u2[kl * P + (n < P ? n : n - P)], 0.0); };
+        auto putc = [&](int kl, int m, double2 F) {
+            if (!(m & 1) && m <= P) RU[(size_t)r * J * Ks + (size_t)(m >> 1) * Ks + k0 + kl] = make_double2(0.5 * F.x, 0.5 * F.y);
+        };
+        sfft::batch_fft<N1, N2>(nk, getc, putc, buf, tw);
+    }
+}
+
+template <int N1, int N2> static cudaError_t launch_spec_r2_fft(pftcc_handle *h, const Geom &g, const float2 *refs,
+                                                                  double2 *RU)
+{
+    const size_t smem = (size_t)N1 * N2 * sizeof(double2) + (size_t)sfft::buf_elems<N1, N2>() * sizeof(double2) +
+                        (size_t)sfft::KB * (N1 * N2 / 2) * sizeof(double);
+    cudaError_t e = smem_limit((const void *)k_spec_r2_fft<N1, N2>, smem);
+    if (e != cudaSuccess) return e;
+    const int kbpb = spec_kb_per_block(g, h->nrefs);
+    const dim3 grid(h->nrefs, (spec_batches(g) + kbpb - 1) / kbpb);
+    PFTCC_LAUNCH(h);
+    k_spec_r2_fft<N1, N2><<<grid, SPEC_THREADS, smem, h->stream>>>(g, refs, RU, kbpb);
+    return cudaGetLastError();
+}
+
+// |ref|^2 spectra: the transforms for the supported lengths, the direct sums otherwise
+static cudaError_t launch_spec_r2(pftcc_handle *h, const Geom &g, const float2 *refs, double2 *RU)
+{
+    switch (g.P) {
+    case 64: return launch_spec_r2_fft<16, 8>(h, g, refs, RU);
+    case 180: return launch_spec_r2_fft<24, 15>(h, g, refs, RU);
+    case 300: return launch_spec_r2_fft<24, 25>(h, g, refs, RU);
+    default: break;
+    }
+    PFTCC_LAUNCH(h);
+    k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, RU);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -739,17 +825,21 @@ __global__ void __launch_bounds__(256) k_norm(Geom g, const float2 *__restrict__
 //   pass 1, task (reference, n1): a length-N2 DFT over n2 of conj Zh(n1 + N1 n2), times
 //           w_{P/2}^{-n1 k2}, into buf[reference][k2][n1];
 //   pass 2, task (reference, k2): a length-N1 DFT over n1 -> conj z(k2 + N2 k1).
-template <int N1, int N2>
+// P2C: the stage-2 split P = P1 x P2C the factors are laid out for (compile-time, so that the
+// layout's index arithmetic divides by a constant), or 0 for the natural layout
+template <int N1, int N2, int P2C>
 __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg, int nr, int c0, int ncols, int dcols,
-                                                  const float *__restrict__ sqp, float *__restrict__ D, int p2,
-                                                  double dscale, int eu)
+                                                  const float *__restrict__ sqp, float *__restrict__ D, double dscale,
+                                                  int eu)
 {
     constexpr int H = N1 * N2, P = 2 * H, J = H + 1;
+    constexpr int p2 = P2C;
     constexpr int NB = 256 / (N1 > N2 ? N1 : N2);
     extern __shared__ double2 sd[];
     double2 *tw = sd;                 // [H] w_{P/2}^{-e}
     double2 *wp = tw + H;             // [H] w_P^{+e}
     double2 *buf = wp + H;            // [NB][N2][N1 + 1]
+    float2 *ys = reinterpret_cast<float2 *>(buf + NB * N2 * (N1 + 1));   // [NB][J] the batch's Y rows
     const int cl = blockIdx.x;
     if (cl >= ncols) return;
     const int col = c0 + cl;
@@ -761,13 +851,18 @@ __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg,
         wp[e] = make_double2(cs, sn);
     }
     const double sq = (double)sqp[col];
-    const int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 4 * p1 * ((p2 + 1) / 2) : P;
+    constexpr int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 4 * p1 * ((p2 + 1) / 2) : P;
     for (int rb0 = 0; rb0 < nr; rb0 += NB) {
         const int nb = min(NB, nr - rb0);
         __syncthreads();
+        for (int e = threadIdx.x; e < nb * J; e += blockDim.x) {   // rows of J values, coalesced
+            const int kl = e / J, j = e - kl * J;
+            ys[e] = Yg[((size_t)(rb0 + kl) * ncols + cl) * J + j];
+        }
+        __syncthreads();
         for (int t = threadIdx.x; t < nb * N1; t += blockDim.x) {
             const int kl = t / N1, n1 = t - kl * N1;
-            const float2 *y = Yg + ((size_t)(rb0 + kl) * ncols + cl) * J;
+            const float2 *y = ys + (size_t)kl * J;
             // Y(j) times wgt_j / P: 1 / P at j = 0 and j = P/2, 2 / P otherwise
             const double w1 = 1.0 / P, w2 = 2.0 / P;
             double2 x[N2];
@@ -813,7 +908,7 @@ __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg,
                     const float a = (float)(d * sq);
                     float y = rsqrtf(a);
                     y = y * fmaf(-0.5f * a, y * y, 1.5f);
-                    if (p2 == 0) {
+                    if constexpr (p2 == 0) {
                         dst[rho] = y;
                     } else {
                         // the Euclidean objective: the additive term -(D + sum_k w_k |ptcl_k|^2) / 2,
@@ -833,16 +928,26 @@ __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg,
     }
 }
 
-template <int N1, int N2>
+template <int N1, int N2, int P2C>
+static cudaError_t launch_norm_fft_k(pftcc_handle *h, const float2 *Y, int nr, int c0, int ncols, int dcols,
+                                     const float *sqp, float *D, double dscale, int eu)
+{
+    constexpr int H = N1 * N2, NB = 256 / (N1 > N2 ? N1 : N2);
+    const size_t smem = (size_t)(2 * H + NB * N2 * (N1 + 1)) * sizeof(double2) + (size_t)NB * (H + 1) * sizeof(float2);
+    cudaError_t e = smem_limit((const void *)k_norm_fft<N1, N2, P2C>, smem);
+    if (e != cudaSuccess) return e;
+    k_norm_fft<N1, N2, P2C><<<ncols, 256, smem, h->stream>>>(Y, nr, c0, ncols, dcols, sqp, D, dscale, eu);
+    return cudaGetLastError();
+}
+
+// the natural layout (p2 == 0) or the stage-2 split of the length (the only split served)
+template <int N1, int N2, int P2F>
 static cudaError_t launch_norm_fft(pftcc_handle *h, const float2 *Y, int nr, int c0, int ncols, int dcols,
                                    const float *sqp, float *D, int p2, double dscale, int eu)
 {
-    constexpr int H = N1 * N2, NB = 256 / (N1 > N2 ? N1 : N2);
-    const size_t smem = (size_t)(2 * H + NB * N2 * (N1 + 1)) * sizeof(double2);
-    cudaError_t e = smem_limit((const void *)k_norm_fft<N1, N2>, smem);
-    if (e != cudaSuccess) return e;
-    k_norm_fft<N1, N2><<<ncols, 256, smem, h->stream>>>(Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
-    return cudaGetLastError();
+    if (p2 == 0) return launch_norm_fft_k<N1, N2, 0>(h, Y, nr, c0, ncols, dcols, sqp, D, dscale, eu);
+    if (p2 == P2F) return launch_norm_fft_k<N1, N2, P2F>(h, Y, nr, c0, ncols, dcols, sqp, D, dscale, eu);
+    return cudaErrorInvalidValue;
 }
 
 static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const float2 *RUf, int nrefs_p, const float2 *CVf,
@@ -860,9 +965,9 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const float2 *RUf
     }
     PFTCC_LAUNCH(h);
     switch (g.P) {
-    case 64: return launch_norm_fft<8, 4>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
-    case 180: return launch_norm_fft<10, 9>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
-    case 300: return launch_norm_fft<15, 10>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
+    case 64: return launch_norm_fft<8, 4, 8>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
+    case 180: return launch_norm_fft<10, 9, 15>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
+    case 300: return launch_norm_fft<15, 10, 20>(h, Y, nr, c0, ncols, dcols, sqp, D, p2, dscale, eu);
     default: break;
     }
     if (eu) return cudaErrorInvalidValue;   // the Euclidean objective needs the transform lengths above
@@ -1247,10 +1352,8 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
         const int gc0 = grp == 0 ? 0 : n_even, gc1 = grp == 0 ? n_even : np;
         if (gc1 <= gc0) continue;
         const float2 *refs = grp == 0 ? h->refs_even : h->refs_odd;
-        PFTCC_LAUNCH(h);
         { KTimer kt(h, PFTCC_K_SPEC_REF);
-        k_spec_r2<<<h->nrefs, SPEC_THREADS, 0, h->stream>>>(g, refs, ws.RU);
-        CKE(cudaGetLastError(), "spec_r2");
+        CKE(launch_spec_r2(h, g, refs, ws.RU), "spec_r2");
         CKE(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref");
         if (h->cfg.match_filt)   // the references' shell factors (shellnorm_and_filter_ref) on their spectra
             CKE(launch_shellnorm_apply(h, M, nrs, rows_pad, ns, grp, ws.UA, ws.RU), "shell factors");

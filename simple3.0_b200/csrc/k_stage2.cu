@@ -742,22 +742,33 @@ __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, 
         wp[e] = make_double2(cs, sn);
     }
     __syncthreads();
-    // A: Y
-    for (int e = t; e < nc * J; e += blockDim.x) {
+    // A: Y, eight lanes per (candidate, j) over the shells (coalesced reads), summed by shuffles;
+    // the loop runs the same trips in every warp so that the shuffles see all lanes
+    const int l8 = t & 7, grp = t >> 3;
+    constexpr int NGRP = RS_THREADS / 8;
+    for (int base = 0; base < nc * J; base += NGRP) {
+        const int e = base + grp;
         const int c = e / J, j = e - c * J;
-        const int rs = rs_s[c];
+        const int rs = e < nc * J ? rs_s[c] : -1;
         double yr = 0.0, yi = 0.0;
         if (rs >= 0) {
             const double2 *ru = RU + ((size_t)(rs / nshifts) * J + j) * Ks;
             const double2 *cv = CV + ((size_t)cl * J + j) * Ks;
-            for (int k = 0; k < Ks; ++k) {
+            for (int k = l8; k < Ks; k += 8) {
                 const double2 u = ru[k], v = cv[k];
                 yr += u.x * v.x + u.y * v.y;
                 yi += u.x * v.y - u.y * v.x;
             }
         }
-        const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
-        Ys[c * J + j] = make_double2(wgt * yr, wgt * yi);
+#pragma unroll
+        for (int o = 4; o; o >>= 1) {
+            yr += __shfl_xor_sync(0xffffffffu, yr, o);
+            yi += __shfl_xor_sync(0xffffffffu, yi, o);
+        }
+        if (e < nc * J && l8 == 0) {
+            const double wgt = ((j == 0 || 2 * j == P) ? 1.0 : 2.0) / P;
+            Ys[c * J + j] = make_double2(wgt * yr, wgt * yi);
+        }
     }
     __syncthreads();
     // B: D, pass 1 (c, n1) then pass 2 (c, k2)
@@ -807,21 +818,27 @@ __global__ void __launch_bounds__(RS_THREADS) k_rescore_md(int ncols, int ntop, 
             }
         }
     }
-    // C: X
+    // C: X, eight lanes per (candidate, m) over the shells as in A
     const size_t pa = (size_t)rows_pad * Ks, pb = (size_t)cols_pad * Ks;
-    for (int e = t; e < nc * M; e += blockDim.x) {
+    for (int base = 0; base < nc * M; base += NGRP) {
+        const int e = base + grp;
         const int c = e / M, m = e - c * M;
-        const int rs = rs_s[c];
+        const int rs = e < nc * M ? rs_s[c] : -1;
         float xr = 0.f, xi = 0.f;
         if (rs >= 0) {
             const float2 *a = UA + (size_t)rs * Ks + (size_t)m * pa, *b = UB + (size_t)cl * Ks + (size_t)m * pb;
-            for (int k = 0; k < Ks; ++k) {
+            for (int k = l8; k < Ks; k += 8) {
                 const float2 av = a[k], bv = b[k];
                 xr = fmaf(av.x, bv.x, fmaf(av.y, bv.y, xr));
                 xi = fmaf(av.y, bv.x, fmaf(-av.x, bv.y, xi));
             }
         }
-        Xs[c * M + m] = make_float2(4.f * xr, 4.f * xi);
+#pragma unroll
+        for (int o = 4; o; o >>= 1) {
+            xr += __shfl_xor_sync(0xffffffffu, xr, o);
+            xi += __shfl_xor_sync(0xffffffffu, xi, o);
+        }
+        if (e < nc * M && l8 == 0) Xs[c * M + m] = make_float2(4.f * xr, 4.f * xi);
     }
     __syncthreads();
     // D: transform and argmax per candidate, two lanes of warp 0 per candidate (lanes 2c, 2c + 1):

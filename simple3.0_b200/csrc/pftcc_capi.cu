@@ -270,7 +270,7 @@ static void free_all(pftcc_handle *h)
     void *ptrs[] = {h->refs_even, h->refs_odd, h->ptcls, h->sqsums, h->ctfmats, h->d_iseven, h->d_ctfp, h->polar,
                     h->argtransf, h->argtransf1, h->pol_off, h->pol_w, h->pol_stage, h->d_work, h->d_groups,
                     h->d_out, h->d_shifts, h->d_dout, h->d_best, h->ws.UA, h->ws.UB, h->ws.RU, h->ws.CV,
-                    h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
+                    h->ws.RUf, h->ws.CVf, h->ws.D, h->ws.Yn, h->ws.X, h->ws.cand, h->ws.sqp, h->ws.A16, h->ws.B16, h->ws.shifts, h->ws.best,
                     h->ws.cand_ref, h->vol_cube, h->d_sig2, h->d_pxls, h->drefs_even, h->drefs_odd, h->d_optlp,
                     h->d_snorm};
     for (void *p : ptrs) dev_free(h, p);
@@ -374,8 +374,9 @@ int pftcc_new(const pftcc_config *cfg, const int *ptcl_mask, const int *eoarr, p
         return fail(PFTCC_ERR_NODEV, "no CUDA device visible");
     }
     if (c.device < 0 || c.device >= ndev) return fail(PFTCC_ERR_NODEV, "device ordinal out of range");
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, c.device) != cudaSuccess || prop.major != 10)
+    // one attribute, not the whole property record (which takes milliseconds to gather)
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, c.device) != cudaSuccess || major != 10)
         return fail(PFTCC_ERR_NODEV, "device is not sm_100 (B200)");
     h->dev = c.device;
     if (cudaSetDevice(h->dev) != cudaSuccess) return fail(PFTCC_ERR_NODEV, "cudaSetDevice failed");
