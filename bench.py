@@ -57,13 +57,14 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--chunks", type=int, default=64, help="chunks of the batching report")
     ap.add_argument("--repeats", type=int, default=3, help="timed runs per worker count in the batching report")
-    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project", "euclid", "ingest"],
+    ap.add_argument("--report", default="", choices=["", "precision", "refine", "batching", "project", "euclid", "ingest", "hbm"],
                     help="precision: error of the FP32 and BF16-split paths against the FP64-accumulated direct "
                          "kernel over a particle sample; refine: the continuous shift/defocus refinement of every "
                          "particle at +-5 rotations around its pose against the exhaustive GPU shift grid (each "
                          "prints a report line instead of the bench line); batching: a queue of chunks of the "
                          "three batching geometries, U[50,300] references x U[500,5000] particles each; project: "
-                         "the polar projector on the config-1 geometry")
+                         "the polar projector on the config-1 geometry; hbm: write-only, read-only and copy "
+                         "rates of this GPU's memory (the denominators of the stage-1 / stage-2 fractions)")
     ap.add_argument("--grid-ptcls", type=int, default=200, help="particles whose problems also run the exhaustive grid")
     ap.add_argument("--report-ptcls", type=int, default=256, help="particles in the precision sample")
     return ap.parse_args()
@@ -361,6 +362,7 @@ def run_ours(args):
         arms = other_arms(pkg, pc, w, shifts, parts, r_host, ctfp, cmats, best, stream, dev, args, world)
     if arms is not None:
         arms["bf16x3_over_fp32"] = value / arms["fp32_mdomain"]["value"]
+    if args.precision == "bf16x3":
         # the contraction's tensor work (3 issued BF16 products per complex MAC) over the whole step
         fl3, _ = algorithmic_costs(w, ns, "stage1")
         st1 = prof.get("stage1", (0.0, 0))
@@ -853,8 +855,45 @@ def run_ingest_report(args):
           flush=True)
 
 
+def run_hbm_report(args):
+    """DRAM rates of this GPU on 8 GiB buffers (far above L2), CUDA events, best of 10 after 3
+    warm-ups: write-only (a memset), read-only (a max-reduction over FP32, whose output is one
+    value) and copy (read + write bytes).  Stage 1 of the search writes its spectra and reads
+    little, stage 2 reads them and writes little, so these are the rates their fractions use."""
+    import torch
+    dev = torch.device("cuda", 0)
+    n = (8 << 30) // 4
+    a = torch.ones(n, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        best = float("inf")
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        return best
+
+    nb = n * 4
+    t_w = timed(lambda: b.zero_())
+    t_r = timed(lambda: torch.amax(a))
+    t_c = timed(lambda: b.copy_(a))
+    print(json.dumps({"report": "hbm", "bytes": nb, "write_only_gbs": nb / t_w / 1e9, "read_only_gbs": nb / t_r / 1e9,
+                      "copy_gbs": 2 * nb / t_c / 1e9, "how": "8 GiB FP32: zero_ (write), amax (read), copy_ "
+                      "(read + write bytes); best of 10 after 3 warm-ups, CUDA events"}), flush=True)
+
+
 def main():
     args = parse()
+    if args.report == "hbm":
+        run_hbm_report(args)
+        return
     if args.report == "ingest":
         run_ingest_report(args)
         return
