@@ -674,22 +674,26 @@ __global__ void __launch_bounds__(128) k_norm_y2(int Ks, int J, const float2 *__
                                                  const float2 *__restrict__ CVf, int cols_pad, int r0, int nr, int c0,
                                                  int ncols, float2 *__restrict__ Y)
 {
+    __shared__ float2 us[64][NY2_R];     // the block's references' spectra at this j, [k][reference]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rb = blockIdx.y * NY2_R, cb = blockIdx.x * NY2_C + warp * 128, j = blockIdx.z;
-    if (cb >= ncols) return;
-    int rr[NY2_R], cc[4];   // clamped reads; the stores are masked
-#pragma unroll
-    for (int i = 0; i < NY2_R; ++i) rr[i] = r0 + min(rb + i, nr - 1);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) cc[q] = c0 + min(cb + lane + 32 * q, ncols - 1);
     const float2 *ur = RUf + (size_t)j * Ks * nrefs_p;
     const float2 *vr = CVf + (size_t)j * Ks * cols_pad;
+    for (int e = threadIdx.x; e < NY2_R * Ks; e += blockDim.x) {   // clamped reads (the stores are masked)
+        const int k = e / NY2_R, i = e - k * NY2_R;
+        us[k][i] = __ldg(ur + (size_t)k * nrefs_p + r0 + min(rb + i, nr - 1));
+    }
+    __syncthreads();
+    if (cb >= ncols) return;
+    int cc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cc[q] = c0 + min(cb + lane + 32 * q, ncols - 1);
     float2 acc[NY2_R][4];
 #pragma unroll
     for (int i = 0; i < NY2_R; ++i)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
-#pragma unroll 2
+#pragma unroll 4
     for (int k = 0; k < Ks; ++k) {
         float2 v[4], vb[4];
 #pragma unroll
@@ -699,7 +703,7 @@ __global__ void __launch_bounds__(128) k_norm_y2(int Ks, int J, const float2 *__
         }
 #pragma unroll
         for (int i = 0; i < NY2_R; ++i) {
-            const float2 u = __ldg(ur + (size_t)k * nrefs_p + rr[i]);
+            const float2 u = us[k][i];
             const float2 ux = make_float2(u.x, u.x), uy = make_float2(u.y, u.y);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -852,13 +856,23 @@ __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg,
     }
     const double sq = (double)sqp[col];
     constexpr int p1 = p2 > 0 ? P / p2 : 0, dlen = p2 > 0 ? 4 * p1 * ((p2 + 1) / 2) : P;
+    // a batch's Y rows (J values each, coalesced) by asynchronous 8-byte copies: the first batch's
+    // before the loop, every later batch's while the previous batch's pass 2 runs (pass 1 has
+    // consumed ys by then)
+    auto fetch = [&](int b0) {
+        const int n = min(NB, nr - b0);
+        for (int e = threadIdx.x; e < n * J; e += blockDim.x) {
+            const int kl = e / J, j = e - kl * J;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(ys + e)),
+                         "l"(Yg + ((size_t)(b0 + kl) * ncols + cl) * J + j)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    fetch(0);
     for (int rb0 = 0; rb0 < nr; rb0 += NB) {
         const int nb = min(NB, nr - rb0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < nb * J; e += blockDim.x) {   // rows of J values, coalesced
-            const int kl = e / J, j = e - kl * J;
-            ys[e] = Yg[((size_t)(rb0 + kl) * ncols + cl) * J + j];
-        }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         __syncthreads();
         for (int t = threadIdx.x; t < nb * N1; t += blockDim.x) {
             const int kl = t / N1, n1 = t - kl * N1;
@@ -888,6 +902,7 @@ __global__ void __launch_bounds__(256) k_norm_fft(const float2 *__restrict__ Yg,
                 row[k2 * (N1 + 1)] = (k2 == 0 || n1 == 0) ? x[k2] : sfft::d_mul(x[k2], tw[n1 * k2]);
         }
         __syncthreads();
+        if (rb0 + NB < nr) fetch(rb0 + NB);
         for (int t = threadIdx.x; t < nb * N2; t += blockDim.x) {
             const int kl = t / N2, k2 = t - kl * N2;
             const double2 *row = buf + ((size_t)kl * N2 + k2) * (N1 + 1);
