@@ -669,49 +669,72 @@ __global__ void k_norm_cvt(int n, int J, int Ks, int n_pad, const double2 *__res
 // particles, 4 warps; every thread takes the 8 references (their spectra read at one address per
 // warp) and the particles l + 32 q (q < 4) of its warp's 128 (coalesced reads), 32 accumulators.
 // Y[(rl * ncols + cl) * J + j] unscaled (the transform applies the weights wgt_j / P).
-constexpr int NY2_R = 8, NY2_C = 512;
+constexpr int NY2_R = 8, NY2_C = 512, NY2_KC = 8;   // references, particles and shells per chunk of a block
+constexpr size_t NY2_SMEM = 2 * (size_t)NY2_KC * NY2_C * sizeof(float2);
 __global__ void __launch_bounds__(128) k_norm_y2(int Ks, int J, const float2 *__restrict__ RUf, int nrefs_p,
                                                  const float2 *__restrict__ CVf, int cols_pad, int r0, int nr, int c0,
                                                  int ncols, float2 *__restrict__ Y)
 {
     __shared__ float2 us[64][NY2_R];     // the block's references' spectra at this j, [k][reference]
+    extern __shared__ float2 cvs[];      // [2][NY2_KC][NY2_C] its particles' spectra, NY2_KC shells per chunk
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rb = blockIdx.y * NY2_R, cb = blockIdx.x * NY2_C + warp * 128, j = blockIdx.z;
+    const int rb = blockIdx.y * NY2_R, cb0 = blockIdx.x * NY2_C, cb = cb0 + warp * 128, j = blockIdx.z;
     const float2 *ur = RUf + (size_t)j * Ks * nrefs_p;
     const float2 *vr = CVf + (size_t)j * Ks * cols_pad;
     for (int e = threadIdx.x; e < NY2_R * Ks; e += blockDim.x) {   // clamped reads (the stores are masked)
         const int k = e / NY2_R, i = e - k * NY2_R;
         us[k][i] = __ldg(ur + (size_t)k * nrefs_p + r0 + min(rb + i, nr - 1));
     }
-    __syncthreads();
-    if (cb >= ncols) return;
-    int cc[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) cc[q] = c0 + min(cb + lane + 32 * q, ncols - 1);
+    // the particles' spectra in chunks of NY2_KC shells by asynchronous 8-byte copies, the next chunk
+    // in flight while this one is used (clamped columns; the stores are masked)
+    const int nch = (Ks + NY2_KC - 1) / NY2_KC;
+    auto fetch = [&](int ch) {
+        float2 *dst = cvs + (size_t)(ch & 1) * NY2_KC * NY2_C;
+        const int k0 = ch * NY2_KC, nk = min(NY2_KC, Ks - k0);
+        for (int e = threadIdx.x; e < nk * NY2_C; e += blockDim.x) {
+            const int kk = e / NY2_C, c = e - kk * NY2_C;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst + e)),
+                         "l"(vr + (size_t)(k0 + kk) * cols_pad + c0 + min(cb0 + c, ncols - 1))
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    fetch(0);
+    const bool active = cb < ncols;
     float2 acc[NY2_R][4];
 #pragma unroll
     for (int i = 0; i < NY2_R; ++i)
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[i][q] = make_float2(0.f, 0.f);
+    for (int ch = 0; ch < nch; ++ch) {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();    // chunk ch landed for everyone; chunk ch - 1's buffer is free
+        if (ch + 1 < nch) fetch(ch + 1);
+        const float2 *cv = cvs + (size_t)(ch & 1) * NY2_KC * NY2_C + warp * 128 + lane;
+        const int k0 = ch * NY2_KC, nk = min(NY2_KC, Ks - k0);
+        if (active) {
 #pragma unroll 4
-    for (int k = 0; k < Ks; ++k) {
-        float2 v[4], vb[4];
+            for (int kk = 0; kk < nk; ++kk) {
+                float2 v[4], vb[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            v[q] = __ldg(vr + (size_t)k * cols_pad + cc[q]);
-            vb[q] = make_float2(v[q].y, -v[q].x);
-        }
+                for (int q = 0; q < 4; ++q) {
+                    v[q] = cv[kk * NY2_C + 32 * q];
+                    vb[q] = make_float2(v[q].y, -v[q].x);
+                }
 #pragma unroll
-        for (int i = 0; i < NY2_R; ++i) {
-            const float2 u = us[k][i];
-            const float2 ux = make_float2(u.x, u.x), uy = make_float2(u.y, u.y);
+                for (int i = 0; i < NY2_R; ++i) {
+                    const float2 u = us[k0 + kk][i];
+                    const float2 ux = make_float2(u.x, u.x), uy = make_float2(u.y, u.y);
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                acc[i][q] = __ffma2_rn(ux, v[q], acc[i][q]);
-                acc[i][q] = __ffma2_rn(uy, vb[q], acc[i][q]);
+                    for (int q = 0; q < 4; ++q) {
+                        acc[i][q] = __ffma2_rn(ux, v[q], acc[i][q]);
+                        acc[i][q] = __ffma2_rn(uy, vb[q], acc[i][q]);
+                    }
+                }
             }
         }
     }
+    if (!active) return;
 #pragma unroll
     for (int i = 0; i < NY2_R; ++i)
 #pragma unroll
@@ -975,7 +998,9 @@ static cudaError_t launch_norm(pftcc_handle *h, const Geom &g, const float2 *RUf
     KTimer kt(h, PFTCC_K_NORM);
     {
         dim3 grid((ncols + NY2_C - 1) / NY2_C, (nr + NY2_R - 1) / NY2_R, J);
-        k_norm_y2<<<grid, 128, 0, h->stream>>>(g.Ks, J, RUf, nrefs_p, CVf, cols_pad, r0, nr, c0, ncols, Y);
+        e = smem_limit((const void *)k_norm_y2, NY2_SMEM);
+        if (e != cudaSuccess) return e;
+        k_norm_y2<<<grid, 128, NY2_SMEM, h->stream>>>(g.Ks, J, RUf, nrefs_p, CVf, cols_pad, r0, nr, c0, ncols, Y);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     PFTCC_LAUNCH(h);
