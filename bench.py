@@ -658,6 +658,21 @@ def run_batching_report(args):
                                      "evals_per_s": evals / t, "chunks_per_s": len(chunks) / t}
     out["identical_results"] = all(np.array_equal(a.view(np.int32).reshape(len(a), -1), c.view(np.int32).reshape(len(c), -1))
                                    for w_ in (2, 4) for a, c in zip(results[1], results[w_]))
+    # the grouped search: one handle and one pftcc_search_groups call per geometry (one persistent
+    # stage-1 launch and one stage-2 launch over all its chunks), after an untimed pass
+    b.search_grouped(chunks)
+    times = []
+    for _ in range(args.repeats):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        grouped = b.search_grouped(chunks)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    out["grouped"] = {"seconds": round(t, 3), "seconds_all": [round(x, 3) for x in times], "evals_per_s": evals / t,
+                      "chunks_per_s": len(chunks) / t,
+                      "identical_to_queue": all(np.array_equal(a.view(np.int32).reshape(len(a), -1),
+                                                               c.view(np.int32).reshape(len(c), -1))
+                                                for a, c in zip(results[1], grouped))}
     print(json.dumps(out), flush=True)
 
 

@@ -310,6 +310,18 @@ int pftcc_search_best(pftcc_handle *h, int nshifts, const float *shifts, int pre
                       pftcc_best *out);
 int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop,
                           void *out_dev);
+/* The search of a queue of independent chunks held in one handle: group q searches the particle
+ * slots slot_first[q]..slot_first[q]+nslot[q]-1 (1-based, disjoint between groups) against the
+ * references ref_first[q]..ref_first[q]+nref[q]-1 (1-based) over the shift list, as
+ * pftcc_search_best would for that chunk alone (the strategies' matcher loop over its particle
+ * batches, simple_strategy2D_matcher.f90:220-297, each batch against its own references); iref
+ * in out is the handle's reference index.  m-domain precisions only (PFTCC_PREC_FP32 or
+ * PFTCC_PREC_BF16X3), the correlation objective.  Every chunk's (references x shifts) x particles
+ * block is a wave; the waves share one persistent tcgen05 stage-1 launch over all their work items
+ * (a device-resident wave table) and one stage-2 launch over all their particles.  Slots outside
+ * every group return iref = 0, ishift = -1, corr = -inf. */
+int pftcc_search_groups(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
+                        const int *nslot, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out);
 /* adjoint: f and grad3 = d f / d(shift_x, shift_y, defocus[micron]) per request, with
  * the particle's CTF evaluated at defocus + ddf; the shift part is
  * gencorr_grad_for_rot_8 (:1863-1925) in the branch cfg.match_filt selects */

@@ -11,12 +11,14 @@ release the interpreter lock while they run).
 """
 from __future__ import annotations
 
+import ctypes as C
 import dataclasses
 import threading
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
+from . import _lib
 from .pftcc import ctfparams_array, polarft_corrcalc
 
 
@@ -104,6 +106,98 @@ class SearchQueue:
         torch.cuda.synchronize(self.device)      # chunk inputs made on other streams are complete
         with ThreadPoolExecutor(max_workers=self.workers) as ex:
             return list(ex.map(self._one, chunks))
+
+
+def _ctf_records(chunks) -> object:
+    """the chunks' per-particle CTF parameters, concatenated, as the C ABI's record array"""
+    n = sum(ch.nptcls for ch in chunks)
+    dt = np.dtype([("smpd", np.float32), ("kv", np.float32), ("cs", np.float32), ("fraca", np.float32),
+                   ("dfx", np.float32), ("dfy", np.float32), ("angast", np.float32), ("phshift", np.float32),
+                   ("l_phaseplate", np.int32)])
+    assert dt.itemsize == C.sizeof(_lib.CtfParams)
+    rec = np.zeros(n, dt)
+    o = 0
+    for ch in chunks:
+        s = slice(o, o + ch.nptcls)
+        rec["smpd"][s], rec["kv"][s], rec["cs"][s], rec["fraca"][s] = ch.smpd, ch.kv, ch.cs, ch.fraca
+        rec["dfx"][s] = ch.dfx
+        rec["dfy"][s] = ch.dfx if ch.dfy is None else ch.dfy
+        rec["angast"][s] = 0.0 if ch.angast is None else ch.angast
+        o += ch.nptcls
+    arr = (_lib.CtfParams * n)()
+    C.memmove(arr, rec.ctypes.data, rec.nbytes)
+    return arr
+
+
+def _search_geometry(cs, precision, ntop, device, stream):
+    """one geometry's chunks in one handle, searched by one pftcc_search_groups call"""
+    import torch
+    nrefs = sum(ch.nrefs for ch in cs)
+    nptcls = sum(ch.nptcls for ch in cs)
+    pc = polarft_corrcalc()
+    try:
+        c0 = cs[0]
+        pc.new(nrefs, (1, nptcls), box=c0.box, nrots=c0.nrots, kfromto=(c0.kfrom, c0.kto), ctf=True,
+               ctf_frame="ptcl", device=device)
+        if stream is not None:
+            pc.set_stream(stream)
+        # the references through pinned host memory (one upload per reference set)
+        refs = torch.empty((nrefs,) + tuple(np.asarray(c0.refs).shape[1:]), dtype=torch.complex64, pin_memory=True)
+        r = 0
+        for ch in cs:
+            refs[r:r + ch.nrefs] = torch.from_numpy(np.asarray(ch.refs, np.complex64))
+            r += ch.nrefs
+        pc.set_refs(1, refs.numpy(), True)
+        pc.set_refs(1, refs.numpy(), False)
+        groups, r, s = [], 1, 1
+        for ch in cs:
+            if hasattr(ch.cmats, "data_ptr"):
+                pc.polarize_ptcls_dev(s - 1, ch.nptcls, ch.cmats.contiguous().data_ptr())
+            else:
+                pc.polarize_ptcls(s - 1, np.asarray(ch.cmats))
+            groups.append((r, ch.nrefs, s, ch.nptcls))
+            r += ch.nrefs
+            s += ch.nptcls
+        pc.create_polar_absctfmats(_ctf_records(cs))
+        out = pc.search_groups(groups, c0.shifts, precision, ntop)
+        res = []
+        for (r0, _, s0, n) in groups:
+            x = out[s0 - 1:s0 - 1 + n].copy()
+            x["iref"] -= (r0 - 1) * (x["iref"] > 0)
+            res.append(x)
+        return res
+    finally:
+        pc.kill()
+
+
+def search_grouped(chunks, precision: str = "bf16x3", ntop: int = 8, device: int = 0, streams: int = 3) -> list:
+    """The queue as grouped searches: the chunks of each geometry (box, nrots, shells, shift list)
+    go into one handle -- their references and particles concatenated -- and one
+    pftcc_search_groups call searches every chunk's particles against its own references (one
+    persistent tensor-core launch over all the chunks' work items per batch of waves, one
+    transform launch over all their particles).  The geometries run on up to `streams` host
+    threads with their own CUDA streams.  Returns each chunk's result as search_chunk does, in
+    submission order."""
+    import torch
+    by_geom = {}
+    for i, ch in enumerate(chunks):
+        sh = None if ch.shifts is None else np.ascontiguousarray(ch.shifts, np.float32).reshape(-1, 2)
+        key = (ch.box, ch.nrots, ch.kfrom, ch.kto, None if sh is None else sh.tobytes())
+        by_geom.setdefault(key, []).append(i)
+    keys = list(by_geom)
+    torch.cuda.synchronize(device)      # chunk inputs made on other streams are complete
+    strs = [torch.cuda.Stream(device=device) for _ in range(max(1, min(streams, len(keys))))]
+
+    def one(k):
+        st = strs[keys.index(k) % len(strs)]
+        return _search_geometry([chunks[i] for i in by_geom[k]], precision, ntop, device, st.cuda_stream)
+
+    results = [None] * len(chunks)
+    with ThreadPoolExecutor(max_workers=len(strs)) as ex:
+        for k, res in zip(keys, ex.map(one, keys)):
+            for i, x in zip(by_geom[k], res):
+                results[i] = x
+    return results
 
 
 GEOMETRIES = {"A": "config0", "B": "config1", "C": "geometry_c"}   # box 64 / 128 / 200

@@ -1478,3 +1478,281 @@ int search_mdomain(pftcc_handle *h, int nshifts_in, const float *shifts_host, in
 }
 
 }  // namespace pftcc
+
+namespace pftcc {
+
+cudaError_t launch_stage2_waves(pftcc_handle *h, int P, std::vector<S2Wave> &waves, int nshifts, int nrs_total,
+                                float2 *cand, float *ccall, const int *perm, int eu);
+
+// every held particle's best out of a searched group starts as "not searched" (reference 0)
+__global__ void k_best_clear(pftcc_best *out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = pftcc_best{0, 0, -1, -INFINITY};
+}
+
+// The grouped search: group q searches the particle slots [slot0[q], slot0[q] + nslot[q]) against
+// the references [ref0[q], ref0[q] + nref[q]) (0-based), as search_mdomain searches all of them
+// against all references.  The columns are ordered by parity, then group; consecutive groups of a
+// parity form column batches of at most GB_COLS particles (a larger group is a batch of its own),
+// whose spectra, packed operands and candidates are formed per batch, so that the workspace scales
+// with the batch and not with the queue.  Each (parity, group) block of columns against its group's
+// (reference, shift) rows is one wave, cut into several where its packed spectrum would pass the
+// per-wave budget; the waves of a batch run as ONE persistent tcgen05 stage-1 launch over all their
+// work items (the device wave table, umma_stage1_waves), the normaliser per wave, and ONE stage-2
+// launch over all their columns (launch_stage2_waves).  A wave's stage-1 tiles are aligned (64
+// rows, 128 columns) and may take in a neighbouring group's rows or particles, which its stage 2
+// then leaves out.
+constexpr int GB_COLS = 8192;
+
+int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const int *nref, const int *slot0,
+                          const int *nslot, int nshifts_in, const float *shifts_host, int precision, int ntop,
+                          pftcc_best *out_dev)
+{
+    const Geom &g = h->g;
+    const int N = g.P * 2, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
+    if (h->objfun == PFTCC_OBJFUN_EUCLID)
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "search_groups: the correlation objective only");
+    if (!stage2_fast_supported(P))
+        return set_err(h, PFTCC_ERR_UNSUPPORTED, "search_groups: nrots/2 in {64, 180, 300}");
+    if (Ks > 64) return set_err(h, PFTCC_ERR_UNSUPPORTED, "m-domain search supports at most 64 shells");
+    if (precision != PFTCC_PREC_BF16X3 && precision != PFTCC_PREC_FP32)
+        return set_err(h, PFTCC_ERR_ARG, "search_groups: precision FP32 or BF16X3");
+    const int ns = std::max(1, nshifts_in);
+    const long long nrs_ll = (long long)h->nrefs * ns;
+    if (nrs_ll * N >= (1LL << 31)) return set_err(h, PFTCC_ERR_ARG, "nrefs * nshifts * nrots too large for candidate ids");
+    const int nrs = (int)nrs_ll;
+    // the groups: particle ranges disjoint and within the held slots, reference ranges within nrefs
+    std::vector<int> owner(h->nptcls, -1);
+    for (int q = 0; q < ngroups; ++q) {
+        if (nref[q] < 1 || ref0[q] < 0 || ref0[q] + nref[q] > h->nrefs || nslot[q] < 0 || slot0[q] < 0 ||
+            slot0[q] + nslot[q] > h->nptcls)
+            return set_err(h, PFTCC_ERR_INDEX, "search_groups: group " + std::to_string(q) + " outside the references or slots");
+        for (int i = slot0[q]; i < slot0[q] + nslot[q]; ++i) {
+            if (owner[i] >= 0) return set_err(h, PFTCC_ERR_ARG, "search_groups: groups share particle slot " + std::to_string(i + 1));
+            owner[i] = q;
+        }
+    }
+    // columns: even slots first, then odd, each parity in group order
+    std::vector<int> perm;
+    std::vector<int> cb(2 * ngroups), ce(2 * ngroups);
+    for (int par = 0; par < 2; ++par)
+        for (int q = 0; q < ngroups; ++q) {
+            cb[2 * q + par] = (int)perm.size();
+            for (int i = slot0[q]; i < slot0[q] + nslot[q]; ++i)
+                if ((h->iseven[i] != 0) == (par == 0)) perm.push_back(i);
+            ce[2 * q + par] = (int)perm.size();
+        }
+    const int np = (int)perm.size();
+    // column batches: (parity, first group, end group, first column, columns)
+    struct Batch { int par, q0, q1, c0, n; };
+    std::vector<Batch> batches;
+    int widest = 0;
+    for (int par = 0; par < 2; ++par)
+        for (int q = 0; q < ngroups;) {
+            int q1 = q, n = 0;
+            while (q1 < ngroups) {
+                const int w = ce[2 * q1 + par] - cb[2 * q1 + par];
+                if (q1 > q && n + w > GB_COLS) break;
+                n += w;
+                ++q1;
+            }
+            if (n > 0) {
+                batches.push_back(Batch{par, q, q1, cb[2 * q + par], n});
+                widest = std::max(widest, n);
+            }
+            q = q1;
+        }
+    cudaError_t e;
+#define CKG(x, w) do { e = (x); if (e != cudaSuccess) return cuda_err(h, e, w); } while (0)
+    PFTCC_LAUNCH(h);
+    k_best_clear<<<(h->nptcls + 255) / 256, 256, 0, h->stream>>>(out_dev, h->nptcls);
+    CKG(cudaGetLastError(), "clear");
+    if (np == 0) return PFTCC_OK;
+    const int cols_pad = (widest + COL_TILE - 1) / COL_TILE * COL_TILE + COL_TILE;   // one batch's columns
+    const int rows_pad = (nrs + S1_TILE - 1) / S1_TILE * S1_TILE;
+    SearchWS &ws = h->ws;
+    // the spectra and candidate buffers of one batch (marked as a grouped layout by W_rows = W_cols
+    // = 0); the column order, the waves' packed spectra, normalising factors and Y grow as needed
+    const bool realloc = ws.nrs_pad != rows_pad || ws.np_pad != cols_pad || ws.nshifts != ns || ws.M != M ||
+                         ws.W_rows != 0 || ws.W_cols != 0;
+    if (realloc) {
+        void *bufs[] = {ws.UA, ws.UB, ws.RU, ws.CV, ws.RUf, ws.CVf, ws.D, ws.Yn, ws.X, ws.cand, ws.sqp, ws.shifts,
+                        ws.cand_ref, ws.A16, ws.B16, ws.best};
+        for (void *b : bufs) dev_free(h, b);
+        umma_free(h);
+        ws = SearchWS{};
+        int st;
+        if ((st = ensure_ws(h, (void **)&ws.UA, (size_t)M * rows_pad * Ks * sizeof(float2), "UA")) ||
+            (st = ensure_ws(h, (void **)&ws.UB, (size_t)M * cols_pad * Ks * sizeof(float2), "UB")) ||
+            (st = ensure_ws(h, (void **)&ws.RU, (size_t)h->nrefs * J * Ks * sizeof(double2), "RU")) ||
+            (st = ensure_ws(h, (void **)&ws.CV, (size_t)cols_pad * J * Ks * sizeof(double2), "CV")) ||
+            (st = ensure_ws(h, (void **)&ws.RUf, (size_t)h->nrefs * J * Ks * sizeof(float2), "RUf")) ||
+            (st = ensure_ws(h, (void **)&ws.CVf, (size_t)cols_pad * J * Ks * sizeof(float2), "CVf")) ||
+            (st = ensure_ws(h, (void **)&ws.cand, (size_t)cols_pad * 8 * sizeof(float2), "cand")) ||
+            (st = ensure_ws(h, (void **)&ws.sqp, (size_t)cols_pad * sizeof(float), "sqp")) ||
+            (st = ensure_ws(h, (void **)&ws.shifts, (size_t)ns * 2 * sizeof(float) + 64, "shifts")))
+            return st;
+        ws.nrs_pad = rows_pad; ws.np_pad = cols_pad; ws.nshifts = ns; ws.M = M; ws.nrs = nrs;
+        ws.W_rows = 0; ws.W_cols = 0;
+        ws.X_elems = 0;
+    }
+    {
+        int st = ensure(h, (void **)&ws.cand_ref, &ws.perm_bytes, (size_t)np * sizeof(int), "column order");
+        if (st) return st;
+    }
+    int *d_perm = ws.cand_ref;
+    CKG(cudaMemcpyAsync(d_perm, perm.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->stream), "perm");
+    std::vector<float> sh(2 * ns, 0.f);
+    if (nshifts_in > 0) std::copy(shifts_host, shifts_host + 2 * ns, sh.begin());
+    CKG(cudaMemcpyAsync(ws.shifts, sh.data(), sh.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream), "shifts");
+    const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
+    const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
+    CKG(smem_limit((const void *)k_stage1_fp32, smem_s1), "attr");
+    const int p2 = stage2_fast_p2(P), dlen = stage2_fast_dlen(P);
+    const bool md_rescore = ntop > 0 && h->cfg.ctf_frame == PFTCC_FRAME_PTCL;
+    {
+        const int st = umma_reset(h);    // the device error word of the bounded waits
+        if (st != PFTCC_OK) return st;
+    }
+    // a wave's packed spectrum within 1 GiB; a batch's waves within 2 GiB of Z and 1 GiB of factors
+    // at a time
+    const size_t z_wave_max = 1ull << 30, z_batch_max = 2ull << 30, d_batch_max = 1ull << 30;
+    struct WavePlan { int r_lo, r_hi, a_lo, a_hi, c_lo, c_hi, t_lo, t_hi; };
+    int cur_par = -1;
+    for (const Batch &bt : batches) {
+        const int par = bt.par;
+        if (par != cur_par) {   // the reference side of this parity (all references)
+            cur_par = par;
+            const float2 *refs = par == 0 ? h->refs_even : h->refs_odd;
+            KTimer kt(h, PFTCC_K_SPEC_REF);
+            CKG(launch_spec_r2(h, g, refs, ws.RU), "spec_r2");
+            CKG(launch_spec_ref(h, g, ns, refs, ws.shifts, nrs, rows_pad, ws.UA), "spec_ref");
+            if (h->cfg.match_filt)
+                CKG(launch_shellnorm_apply(h, M, nrs, rows_pad, ns, par, ws.UA, ws.RU), "shell factors");
+            PFTCC_LAUNCH(h);
+            k_norm_cvt<<<CVT_BLOCKS, 256, 0, h->stream>>>(h->nrefs, J, Ks, h->nrefs, ws.RU, ws.RUf);
+            CKG(cudaGetLastError(), "RU copy");
+        }
+        // this batch's particles: columns bt.c0 .. bt.c0 + bt.n - 1 of the order, batch-local 0 .. n - 1
+        const int *bperm = d_perm + bt.c0;
+        {
+            KTimer kt(h, PFTCC_K_SPEC_PTCL);
+            CKG(launch_spec_ptcl(h, g, ctf, bperm, bt.n, cols_pad, ws.UB, ws.CV, ws.sqp), "spec_ptcl");
+            PFTCC_LAUNCH(h);
+            k_norm_cvt<<<CVT_BLOCKS, 256, 0, h->stream>>>(bt.n, J, Ks, cols_pad, ws.CV, ws.CVf);
+            CKG(cudaGetLastError(), "CV copy");
+            PFTCC_LAUNCH(h);
+            k_cand_init<<<(cols_pad * 8 + 255) / 256, 256, 0, h->stream>>>(ws.cand, cols_pad);
+            CKG(cudaGetLastError(), "cand_init");
+        }
+        if (precision == PFTCC_PREC_BF16X3) {
+            int st = umma_stage1(h, M, Ks, ws.UA, 0, nrs, rows_pad, ws.UB, 0, bt.n, cols_pad, nullptr, 1, par);
+            if (st != PFTCC_OK) return st;
+        }
+        // the batch's waves: per group, rows cut to keep a wave's Z within its budget
+        std::vector<WavePlan> plan;
+        for (int q = bt.q0; q < bt.q1; ++q) {
+            const int c_lo = cb[2 * q + par] - bt.c0, c_hi = ce[2 * q + par] - bt.c0;
+            if (c_hi <= c_lo) continue;
+            const int t_lo = c_lo / COL_TILE, t_hi = (c_hi + COL_TILE - 1) / COL_TILE;
+            const size_t zcol = (size_t)(t_hi - t_lo) * COL_TILE * P * sizeof(float2);   // Z bytes per row
+            int rows_max = (int)std::max<size_t>(S1_TILE, z_wave_max / zcol / S1_TILE * S1_TILE);
+            for (int r_lo = ref0[q] * ns, r_end = (ref0[q] + nref[q]) * ns; r_lo < r_end;) {
+                const int a_lo = r_lo / S1_TILE * S1_TILE;
+                const int r_hi = std::min(r_end, a_lo + rows_max);
+                const int a_hi = (r_hi + S1_TILE - 1) / S1_TILE * S1_TILE;
+                plan.push_back(WavePlan{r_lo, r_hi, a_lo, a_hi, c_lo, c_hi, t_lo, t_hi});
+                r_lo = r_hi;
+            }
+        }
+        // sets of waves: one stage-1 launch, the normalisers, one stage-2 launch each
+        for (size_t w0 = 0; w0 < plan.size();) {
+            size_t zb = 0, db = 0, yb = 0, w1 = w0;
+            while (w1 < plan.size()) {
+                const WavePlan &p = plan[w1];
+                const size_t z = (size_t)P * (p.a_hi - p.a_lo) * (p.t_hi - p.t_lo) * COL_TILE * sizeof(float2);
+                const int nrw = (p.r_hi - 1) / ns - p.r_lo / ns + 1;
+                const size_t d = (size_t)nrw * (p.c_hi - p.c_lo) * std::max(2 * P, dlen) * sizeof(float);
+                const size_t y = (size_t)nrw * (p.c_hi - p.c_lo) * J * sizeof(float2);
+                if (w1 > w0 && (zb + z > z_batch_max || db + d > d_batch_max)) break;
+                zb += z; db += d; yb = std::max(yb, y); ++w1;
+            }
+            int st = ensure(h, (void **)&ws.X, &ws.X_elems, zb, "grouped Z");
+            if (st) return st;
+            st = ensure(h, (void **)&ws.D, &ws.D_bytes, db, "grouped factors");
+            if (st) return st;
+            st = ensure(h, (void **)&ws.Yn, &ws.Y_bytes, yb, "grouped Y");
+            if (st) return st;
+            std::vector<S1Wave> s1;
+            std::vector<S2Wave> s2;
+            size_t zo = 0, dof = 0;
+            for (size_t i = w0; i < w1; ++i) {
+                const WavePlan &p = plan[i];
+                const int xrows = p.a_hi - p.a_lo, xcols = (p.t_hi - p.t_lo) * COL_TILE;
+                float2 *Xw = reinterpret_cast<float2 *>(reinterpret_cast<char *>(ws.X) + zo);
+                float *Dw = reinterpret_cast<float *>(reinterpret_cast<char *>(ws.D) + dof);
+                const int r_lo_ref = p.r_lo / ns, nrw = (p.r_hi - 1) / ns - r_lo_ref + 1;
+                const int cols = p.c_hi - p.c_lo;
+                if (precision == PFTCC_PREC_BF16X3) {
+                    s1.push_back(S1Wave{Xw, p.a_lo / 32, xrows / 32, p.t_lo, p.t_hi - p.t_lo, 0, 0, 0, 0});
+                } else {
+                    dim3 grid(xrows / S1_TILE, xcols / S1_TILE, P / 2 + 1);
+                    PFTCC_LAUNCH(h);
+                    KTimer kt(h, PFTCC_K_STAGE1);
+                    k_stage1_fp32<<<grid, 256, smem_s1, h->stream>>>(Ks, P, ws.UA, rows_pad, p.a_lo, ws.UB, cols_pad,
+                                                                    p.t_lo * COL_TILE, Xw, xrows, xcols);
+                    CKG(cudaGetLastError(), "stage1");
+                }
+                CKG(launch_norm(h, g, ws.RUf, h->nrefs, ws.CVf, cols_pad, r_lo_ref, nrw, p.c_lo, cols, cols, ws.sqp,
+                                ws.Yn, Dw, p2, 1.0 / (2.0 * N), 0), "norm");
+                s2.push_back(S2Wave{Xw, Dw, p.r_lo, p.r_hi - p.r_lo, p.r_lo - p.a_lo, xrows, xcols, p.c_lo, cols,
+                                    p.c_lo - p.t_lo * COL_TILE, r_lo_ref, cols, 0, 0});
+                zo += (size_t)P * xrows * xcols * sizeof(float2);
+                dof += (size_t)nrw * cols * std::max(2 * P, dlen) * sizeof(float);
+            }
+            if (precision == PFTCC_PREC_BF16X3) {
+                st = umma_stage1_waves(h, M, s1);
+                if (st != PFTCC_OK) return st;
+            }
+            e = launch_stage2_waves(h, P, s2, ns, nrs, ws.cand, nullptr, bperm, 0);
+            if (e != cudaSuccess)
+                return set_err(h, e == cudaErrorMemoryAllocation ? PFTCC_ERR_OOM : PFTCC_ERR_CUDA,
+                               std::string("grouped stage 2: ") + cudaGetErrorString(e));
+            w0 = w1;
+        }
+        // the batch's best: the FP32 m-domain re-score (particle frame), or the exact re-score of the
+        // top ntop in the reference frame, or the top 1
+        if (md_rescore) {
+            CKG(launch_rescore_md(h, P, bt.n, ntop, Ks, ns, nshifts_in > 0, ws.UA, rows_pad, ws.UB, cols_pad, ws.RU,
+                                  ws.CV, ws.sqp, ws.cand, bperm, 0, out_dev, 0), "rescore");
+        } else if (ntop == 0) {
+            PFTCC_LAUNCH(h);
+            k_finish<<<(bt.n + 127) / 128, 128, 0, h->stream>>>(ws.cand, bperm, bt.n, N, ns, nshifts_in > 0, 0, out_dev,
+                                                                nullptr, nullptr);
+            CKG(cudaGetLastError(), "finish");
+        } else {
+            int st = ensure(h, (void **)&h->d_work, &h->work_cap,
+                            std::max<size_t>((size_t)bt.n * ntop * sizeof(Work), 4096), "work");
+            if (st) return st;
+            st = ensure(h, (void **)&h->d_groups, &h->group_cap, std::max<size_t>((size_t)bt.n * sizeof(Group), 256),
+                        "groups");
+            if (st) return st;
+            PFTCC_LAUNCH(h);
+            k_finish<<<(bt.n + 127) / 128, 128, 0, h->stream>>>(ws.cand, bperm, bt.n, N, ns, nshifts_in > 0, ntop,
+                                                                out_dev, h->d_work, h->d_groups);
+            CKG(cudaGetLastError(), "finish");
+            CKG(launch_exact(h, h->d_groups, bt.n, h->d_work, ws.shifts, MODE_BEST, exact_frame(h), 1, nullptr,
+                             out_dev),
+                "rescore");
+        }
+    }
+    {
+        int st = umma_check(h);
+        if (st != PFTCC_OK) return st;
+    }
+#undef CKG
+    return PFTCC_OK;
+}
+
+}  // namespace pftcc

@@ -523,7 +523,7 @@ __device__ __forceinline__ void triple_corr(const GetX &getx, const Dinv &dinv, 
 
 // ---------------------------------------------------------------------------------------
 struct S2Fast {
-    int rows, xrows, xcols, row0, nshifts, r0, dcols, col0, N, nrs_total;
+    int nshifts, N, nrs_total, nwaves;
     float escale;   // the Euclidean objective: the transform's scale 1/(2N) (the factors are additive)
 };
 
@@ -544,11 +544,24 @@ __device__ __forceinline__ bool ranks_above(float c, int id, float c2, int id2) 
 // the end the block merges those lists with the particle's running top-8.
 // X here is the packed spectrum Z, P planes of [col][row].
 template <int P1, int P2, int ROWS, int NT, bool WRITE, bool EU>
-__global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const float2 *__restrict__ X,
-                                                            const float *__restrict__ Dinv, float2 *__restrict__ cand,
-                                                            float *__restrict__ ccall, const int *__restrict__ perm)
+__global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const TwTables tw, const S2Wave *__restrict__ waves,
+                                                            float2 *__restrict__ cand, float *__restrict__ ccall,
+                                                            const int *__restrict__ perm)
 {
     constexpr int Q2 = (P2 + 1) / 2, DLEN = s2_dlen<P1, P2>(), NPA = (P1 + 1) / 2;
+    // this block's wave (the last one starting at or before it) and column within it
+    int lo = 0, hi = sp.nwaves - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&waves[mid].blk0) <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    const S2Wave *W = waves + lo;
+    const int cl = (int)blockIdx.x - __ldg(&W->blk0);
+    const float2 *X = reinterpret_cast<const float2 *>(__ldg(reinterpret_cast<const unsigned long long *>(&W->X)));
+    const float *Dinv = reinterpret_cast<const float *>(__ldg(reinterpret_cast<const unsigned long long *>(&W->D)));
+    const int w_rows = __ldg(&W->rows), w_row0 = __ldg(&W->row0), w_rofs = __ldg(&W->rofs);
+    const int w_xrows = __ldg(&W->xrows), w_xcols = __ldg(&W->xcols), w_col0 = __ldg(&W->col0);
+    const int w_zc0 = __ldg(&W->zc0), w_r0 = __ldg(&W->r0), w_dcols = __ldg(&W->dcols);
     extern __shared__ float4 smem4[];
     const int t = threadIdx.x;
     const int role = t / ROWS, lr = t - role * ROWS;
@@ -568,10 +581,10 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
         twb[e] = make_float2(-wa.y, -wb.y);
     }
     __syncthreads();
-    const int cl = blockIdx.x;
-    // Z offsets in float2 units fit 32 bits (the launcher checks P xcols xrows < 2^32)
-    const uint32_t plane = (uint32_t)sp.xcols * (uint32_t)sp.xrows;
-    const float2 *Xc = X + (size_t)cl * sp.xrows;
+    // Z offsets in float2 units fit 32 bits (the launcher checks P xcols xrows < 2^32); the wave's
+    // rows start at Z row w_rofs
+    const uint32_t plane = (uint32_t)w_xcols * (uint32_t)w_xrows;
+    const float2 *Xc = X + (size_t)(w_zc0 + cl) * w_xrows + w_rofs;
     float kc[8];
     int ki[8];
 #pragma unroll
@@ -590,22 +603,22 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
         };
     };
     float2 na[P2], nb[P2];   // the first class pair of this thread's next row
-    if (lr < sp.rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(lr), na, nb);
-    for (int base = 0; base < sp.rows; base += ROWS) {
+    if (lr < w_rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(lr), na, nb);
+    for (int base = 0; base < w_rows; base += ROWS) {
         const int row = base + lr;
-        const bool active = row < sp.rows;
-        const int grow = sp.row0 + row;
+        const bool active = row < w_rows;
+        const int grow = w_row0 + row;
         // this row's reference: its factors in pass-B order
         const float4 *Dr = reinterpret_cast<const float4 *>(
-            Dinv + ((size_t)(grow / sp.nshifts - sp.r0) * sp.dcols + cl) * DLEN);
+            Dinv + ((size_t)(grow / sp.nshifts - w_r0) * w_dcols + cl) * DLEN);
         if (active) passA_pk<P1, P2>(ca, ce, zload(row), slab, ROWS, twa, twb, tw, na, nb);
         asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(32 * NT) : "memory");
-        if (row + ROWS < sp.rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(row + ROWS), na, nb);
+        if (row + ROWS < w_rows && ca < ce) load_pair<P1, P2>(ca, min(ca + 1, ce - 1), zload(row + ROWS), na, nb);
         float best = -INFINITY;
         int brot = 0;
         if (active) {
             if constexpr (WRITE) {
-                float *cc_out = ccall + ((size_t)perm[sp.col0 + cl] * sp.nrs_total + grow) * sp.N;
+                float *cc_out = ccall + ((size_t)perm[w_col0 + cl] * sp.nrs_total + grow) * sp.N;
                 passB_all<P1, P2, EU>(lb0, lb1, slab, ROWS, tw, Dr, sp.escale, cc_out, best, brot);
             } else {
                 passB_search<P1, P2, EU>(lb0, lb1, slab, ROWS, tw, Dr, sp.escale, best, brot);
@@ -644,7 +657,7 @@ __global__ void __launch_bounds__(NT * ROWS, 1) k_stage2_fast(S2Fast sp, const T
 #pragma unroll
         for (int k = 0; k < 8; ++k) { ccs[8 * lr + k] = kc[k]; ids[8 * lr + k] = ki[k]; }
     }
-    float2 *cp = cand + (size_t)(sp.col0 + cl) * 8;
+    float2 *cp = cand + (size_t)(w_col0 + cl) * 8;
     if (t < 8) {
         const float2 c = cp[t];
         ccs[8 * ROWS + t] = c.x;
@@ -928,10 +941,9 @@ int stage2_fast_dlen(int P)
 }
 
 template <int P1, int P2>
-static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const float2 *X, const float *Dinv,
-                             float2 *cand, float *ccall, const int *perm, bool eu)
+static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int blocks, const S2Wave *waves_dev, float2 *cand,
+                             float *ccall, const int *perm, bool eu)
 {
-    if ((unsigned long long)P1 * P2 * sp.xcols * sp.xrows >= (1ull << 32)) return cudaErrorInvalidValue;
     TwTables tw;
     fill_tw(tw, P1 * P2);
     // row slabs of P complex (the two-lane layout): 128 rows in flight up to P = 200, 64
@@ -947,21 +959,54 @@ static cudaError_t launch_s2(pftcc_handle *h, const S2Fast &sp, int cols, const 
     if (e != cudaSuccess) return e;
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE2);
-    kern<<<cols, NT * ROWS, smem, h->stream>>>(sp, tw, X, Dinv, cand, ccall, perm);
+    kern<<<blocks, NT * ROWS, smem, h->stream>>>(sp, tw, waves_dev, cand, ccall, perm);
     return cudaGetLastError();
+}
+
+// every wave of the list in one launch, one block per column (blk0 filled in)
+cudaError_t launch_stage2_waves(pftcc_handle *h, int P, std::vector<S2Wave> &waves, int nshifts, int nrs_total,
+                                float2 *cand, float *ccall, const int *perm, int eu)
+{
+    UmmaState &us = h->ws.umma;
+    const int nw = (int)waves.size();
+    if (nw == 0) return cudaSuccess;
+    long long blocks = 0;
+    for (S2Wave &w : waves) {
+        if ((unsigned long long)P * w.xcols * w.xrows >= (1ull << 32) || w.cols <= 0 || w.rows <= 0 ||
+            w.zc0 + w.cols > w.xcols || w.rofs + w.rows > w.xrows)
+            return cudaErrorInvalidValue;
+        w.blk0 = (int)blocks;
+        blocks += w.cols;
+    }
+    if (blocks >= (1LL << 31)) return cudaErrorInvalidValue;
+    if (us.s2waves_cap < nw) {
+        dev_free(h, us.d_s2waves);
+        us.d_s2waves = nullptr;
+        us.s2waves_cap = 0;
+        const int cap = std::max(nw, 16);
+        if (dev_alloc(h, (void **)&us.d_s2waves, (size_t)cap * sizeof(S2Wave), "stage-2 waves") != PFTCC_OK)
+            return cudaErrorMemoryAllocation;
+        us.s2waves_cap = cap;
+    }
+    cudaError_t e = cudaMemcpyAsync(us.d_s2waves, waves.data(), (size_t)nw * sizeof(S2Wave), cudaMemcpyHostToDevice,
+                                    h->stream);
+    if (e != cudaSuccess) return e;
+    S2Fast sp{nshifts, 2 * P, nrs_total, nw, 1.0f / (2.0f * (float)(2 * P))};
+    switch (P) {
+    case 64: return launch_s2<8, 8>(h, sp, (int)blocks, us.d_s2waves, cand, ccall, perm, eu != 0);
+    case 180: return launch_s2<12, 15>(h, sp, (int)blocks, us.d_s2waves, cand, ccall, perm, eu != 0);
+    case 300: return launch_s2<15, 20>(h, sp, (int)blocks, us.d_s2waves, cand, ccall, perm, eu != 0);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launch_stage2_fast(pftcc_handle *h, int P, int rows, int xrows, int xcols, int row0, int nshifts, int r0,
                                int dcols, int col0, int cols, int nrs_total, const float2 *X, const float *Dinv,
                                float2 *cand, float *ccall, const int *perm, int eu)
 {
-    S2Fast sp{rows, xrows, xcols, row0, nshifts, r0, dcols, col0, 2 * P, nrs_total, 1.0f / (2.0f * (float)(2 * P))};
-    switch (P) {
-    case 64: return launch_s2<8, 8>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
-    case 180: return launch_s2<12, 15>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
-    case 300: return launch_s2<15, 20>(h, sp, cols, X, Dinv, cand, ccall, perm, eu != 0);
-    default: return cudaErrorInvalidValue;
-    }
+    std::vector<S2Wave> w(1);
+    w[0] = S2Wave{X, Dinv, row0, rows, 0, xrows, xcols, col0, cols, 0, r0, dcols, 0, 0};
+    return launch_stage2_waves(h, P, w, nshifts, nrs_total, cand, ccall, perm, eu);
 }
 
 template <int P1, int P2, bool EU>

@@ -58,17 +58,14 @@ struct UmmaParams {
     int M;              // m planes of the packed operands (P + 1)
     int Kp;             // padded real K per operand part (multiple of 16)
     int KC;             // 8-element chunks per operand row: 2*Kp/8 (hi then lo)
-    int n_ptiles;       // particle tiles in the wave
-    int ptile0;         // first particle tile of the wave (group relative)
     int ptiles_m;       // particle tiles per m plane in the packed particle operand
-    int n_rtiles;       // rs tiles in the wave
-    int rtile0;         // first rs tile of the wave
     int rtiles_m;       // rs tiles per m plane in the packed row operand
     int stages;         // N-tile ring depth (each stage holds the row tiles of both planes)
     const __nv_bfloat16 *P16;   // packed particle operand, one contiguous tile per (m, particle tile)
     const __nv_bfloat16 *R16;   // packed row operand, one contiguous tile per (m, rs tile)
-    float2 *X;          // output Z: [P][xcols][xrows]
-    int xrows, xcols;
+    const S1Wave *waves;        // the launch's waves (device), items of wave w from waves[w].item0
+    const CUtensorMap *maps;    // each wave's Z as a tensor map (device, 64-byte aligned)
+    int nwaves, nitems;
     int *err;           // device error word (0 = ok)
     long long wait_limit;   // polls of a pipeline wait before the kernel gives up (the drains of
                             // copies and MMAs already issued always use WAIT_LIMIT)
@@ -203,7 +200,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---- the GEMM ------------------------------------------------------------------------
-__global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ CUtensorMap tmX, UmmaParams up)
+// the wave of work item w: the cursor `wv` only moves forward, as every role walks its items in
+// increasing order
+__device__ __forceinline__ void wave_of(const UmmaParams &up, int w, int &wv)
+{
+    while (wv + 1 < up.nwaves && w >= __ldg(&up.waves[wv + 1].item0)) ++wv;
+}
+
+__global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_constant__ UmmaParams up)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -246,8 +250,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
     const uint32_t tmem_base = *tmem_slot;
     // work item = (plane pair mp, particle tile): planes mA = mp and mB = P - mp (mp = 0
     // pairs plane 0 with plane P, mp = P/2 of an even P pairs the plane with itself)
-    const int P = up.M - 1, npairs = P / 2 + 1;
-    const int nitems = npairs * up.n_ptiles;
+    const int P = up.M - 1;
+    const int nitems = up.nitems;
     auto fail = [&](int code) {
         if (!*abort_flag) atomicCAS(up.err, 0, code);
         *abort_flag = 1;
@@ -257,17 +261,22 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
         // ------------------------------------------------------------ TMA producer
         long long itb = 0, na = 0;     // row-tile stages and particle tiles loaded
         bool ok = true;
+        int wv = 0;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
-            const int mp = w / up.n_ptiles, pt = w - mp * up.n_ptiles;
+            wave_of(up, w, wv);
+            const S1Wave *W = up.waves + wv;
+            const int n_pt = __ldg(&W->n_ptiles), wi = w - __ldg(&W->item0);
+            const int mp = wi / n_pt, pt = wi - mp * n_pt;
+            const int pt0 = __ldg(&W->ptile0), rt0 = __ldg(&W->rtile0), n_rt = __ldg(&W->n_rtiles);
             const int pm[2] = {mp, mp == 0 ? P : P - mp};
             // both planes' particle tiles, one at a time through sA (the MMA issuer copies each to TMEM)
             for (int h = 0; h < 2; ++h, ++na) {
                 if (na > 0 && !mbar_wait(a_empty, (uint32_t)((na - 1) & 1), abort_flag, up.wait_limit)) { fail(1); ok = false; break; }
                 mbar_expect_tx(a_full, a_bytes);
-                bulk_load(sA, up.P16 + (size_t)(pm[h] * up.ptiles_m + up.ptile0 + pt) * (a_bytes / 2), a_bytes, a_full);
+                bulk_load(sA, up.P16 + (size_t)(pm[h] * up.ptiles_m + pt0 + pt) * (a_bytes / 2), a_bytes, a_full);
             }
             if (!ok) break;
-            for (int j = 0; j < up.n_rtiles; ++j, ++itb) {
+            for (int j = 0; j < n_rt; ++j, ++itb) {
                 const int s = (int)(itb % up.stages);
                 if (itb >= up.stages && !mbar_wait(empty + s, (uint32_t)((itb / up.stages - 1) & 1), abort_flag, up.wait_limit)) {
                     fail(2); ok = false; break;
@@ -275,7 +284,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                 mbar_expect_tx(full + s, 2 * b_bytes);
                 for (int h = 0; h < 2; ++h)
                     bulk_load(sB + ((size_t)s * 2 + h) * b_bytes,
-                              up.R16 + (size_t)(pm[h] * up.rtiles_m + up.rtile0 + j) * (b_bytes / 2), b_bytes, full + s);
+                              up.R16 + (size_t)(pm[h] * up.rtiles_m + rt0 + j) * (b_bytes / 2), b_bytes, full + s);
             }
         }
         // drain: every issued copy must land before the CTA exits
@@ -295,9 +304,11 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
         const int ksteps = up.Kp / 16, lo_off = up.Kp / 8;
         const int acol = up.KC * 4;              // TMEM columns of one plane's particle tile (8 per 16-wide K step)
         long long itb = 0, tacc = 0, na = 0;
-        int ii = 0;
+        int ii = 0, wv = 0;
         bool ok = true;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x, ++ii) {
+            wave_of(up, w, wv);
+            const int n_rt = __ldg(&up.waves[wv].n_rtiles);
             if (ii > 0) {
                 // the previous item's MMAs read the TMEM particle tiles: let them finish first
                 umma_commit(item_done);
@@ -312,7 +323,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                 umma_commit(a_empty);            // sA reusable once the copies have read it
             }
             if (!ok) break;
-            for (int j = 0; j < up.n_rtiles; ++j, ++itb, ++tacc) {
+            for (int j = 0; j < n_rt; ++j, ++itb, ++tacc) {
                 const int s = (int)(itb % up.stages);
                 if (!mbar_wait(full + s, (uint32_t)((itb / up.stages) & 1), abort_flag, up.wait_limit)) { fail(4); ok = false; break; }
                 const int acc = (int)(tacc & 1);
@@ -349,14 +360,20 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
         long long tacc = 0;
         bool ok = true;
         const int N = 2 * P;
+        int wv = 0;
         for (int w = blockIdx.x; w < nitems && ok; w += gridDim.x) {
-            const int mp = w / up.n_ptiles, pt = w - mp * up.n_ptiles;
+            wave_of(up, w, wv);
+            const S1Wave *W = up.waves + wv;
+            const CUtensorMap *tmX = up.maps + wv;
+            const int n_pt = __ldg(&W->n_ptiles), wi = w - __ldg(&W->item0);
+            const int mp = wi / n_pt, pt = wi - mp * n_pt;
+            const int n_rt = __ldg(&W->n_rtiles), xcols = __ldg(&W->xcols);
             const int mA = mp, mB = mp == 0 ? P : P - mp;
             const bool two = mp != 0 && mB != mA;      // a second output plane
             const float2 wA = wn_of(mA, N), wB = wn_of(mB, N);
             // rows of this warp: particles 32q .. 32q+31 of the tile = box rows of Z's tensor map
-            const int yA = mA * up.xcols + pt * U_BM + 32 * q, yB = (two ? mB : 0) * up.xcols + pt * U_BM + 32 * q;
-            for (int j = 0; j < up.n_rtiles; ++j, ++tacc) {
+            const int yA = mA * xcols + pt * U_BM + 32 * q, yB = (two ? mB : 0) * xcols + pt * U_BM + 32 * q;
+            for (int j = 0; j < n_rt; ++j, ++tacc) {
                 const int acc = (int)(tacc & 1);
                 // warp-uniform outcome: the .sync.aligned TMEM loads below must run on all 32 lanes
                 const bool got = __all_sync(0xffffffffu, mbar_wait(t_full + acc, (uint32_t)((tacc / 2) & 1), abort_flag, up.wait_limit));
@@ -398,8 +415,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) k_umma_stage1(const __grid_const
                     if (lane == 0) {
                         // x in floats: complex rs = j * U_RS + 16 c, two floats each (a multiple of 32)
                         const int x = 2 * (j * U_RS + 16 * c);
-                        tma_store_2d(&tmX, stg_w, x, yA);
-                        if (two) tma_store_2d(&tmX, stg_w + STAGE_TILE, x, yB);
+                        tma_store_2d(tmX, stg_w, x, yA);
+                        if (two) tma_store_2d(tmX, stg_w + STAGE_TILE, x, yB);
                         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                     }
                 }
@@ -564,19 +581,60 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
     }
     if (rs0 % U_RS || nrs_w % U_RS || (c0 - us.group_c0) % U_BM || ncols_w % U_BM)
         return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave not tile aligned");
-    const int rtile0 = rs0 / U_RS, n_rtiles = nrs_w / U_RS;
-    const int ptile0 = (c0 - us.group_c0) / U_BM, n_ptiles = ncols_w / U_BM;
-    if (rtile0 + n_rtiles > us.rtiles || ptile0 + n_ptiles > us.ptiles)
-        return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave outside the packed operands");
+    std::vector<S1Wave> w(1);
+    w[0] = S1Wave{X, rs0 / U_RS, nrs_w / U_RS, (c0 - us.group_c0) / U_BM, ncols_w / U_BM, 0, 0, 0, 0};
+    return umma_stage1_waves(h, M, w);
+}
+
+int umma_stage1_waves(pftcc_handle *h, int M, std::vector<S1Wave> &waves)
+{
+    SearchWS &ws = h->ws;
+    UmmaState &us = ustate(h);
+    const int Kp = us.Kp, KC = us.KC;
+    cudaError_t e;
+    const int nw = (int)waves.size();
+    if (nw == 0) return PFTCC_OK;
+    const int npairs = (M - 1) / 2 + 1;        // plane pairs (m, P - m)
+    long long nitems = 0;
+    for (S1Wave &w : waves) {
+        if (w.n_rtiles <= 0 || w.n_ptiles <= 0 || w.rtile0 < 0 || w.ptile0 < 0 || w.rtile0 + w.n_rtiles > us.rtiles ||
+            w.ptile0 + w.n_ptiles > us.ptiles)
+            return set_err(h, PFTCC_ERR_ARG, "umma stage 1: wave outside the packed operands");
+        w.item0 = (int)nitems;
+        w.xrows = w.n_rtiles * U_RS;
+        w.xcols = w.n_ptiles * U_BM;
+        nitems += (long long)npairs * w.n_ptiles;
+    }
+    if (nitems >= (1LL << 31)) return set_err(h, PFTCC_ERR_ARG, "umma stage 1: too many work items");
     if (((uintptr_t)ws.A16 & 15) != 0 || ((uintptr_t)ws.B16 & 15) != 0)
         return set_err(h, PFTCC_ERR_ARG, "umma stage 1: packed operands not 16-byte aligned");
-    CUtensorMap tmX;
-    int st = make_xmap(h, &tmX, X, nrs_w, ncols_w, M - 1);   // Z has P = M - 1 planes
-    if (st) return st;
+    // the waves' Z tensor maps, and both tables on the device (stream-ordered after any launch that
+    // still reads the previous contents)
+    std::vector<CUtensorMap> maps(nw);
+    for (int i = 0; i < nw; ++i) {
+        int st = make_xmap(h, &maps[i], waves[i].X, waves[i].xrows, waves[i].xcols, M - 1);   // Z has P = M - 1 planes
+        if (st) return st;
+    }
+    if (us.waves_cap < nw) {
+        dev_free(h, us.d_waves);
+        dev_free(h, us.d_maps);
+        us.d_waves = nullptr;
+        us.d_maps = nullptr;
+        us.waves_cap = 0;
+        const int cap = std::max(nw, 16);
+        int st = dev_alloc(h, (void **)&us.d_waves, (size_t)cap * sizeof(S1Wave), "stage-1 waves");
+        if (st) return st;
+        st = dev_alloc(h, &us.d_maps, (size_t)cap * sizeof(CUtensorMap), "stage-1 tensor maps");
+        if (st) return st;
+        if (((uintptr_t)us.d_maps & 63) != 0) return set_err(h, PFTCC_ERR_CUDA, "stage-1 tensor maps not 64-byte aligned");
+        us.waves_cap = cap;
+    }
+    if ((e = cudaMemcpyAsync(us.d_waves, waves.data(), (size_t)nw * sizeof(S1Wave), cudaMemcpyHostToDevice, h->stream)) ||
+        (e = cudaMemcpyAsync(us.d_maps, maps.data(), (size_t)nw * sizeof(CUtensorMap), cudaMemcpyHostToDevice, h->stream)))
+        return cuda_err(h, e, "stage-1 wave tables");
     UmmaParams up{};
     up.M = M; up.Kp = Kp; up.KC = KC;
-    up.n_ptiles = n_ptiles; up.ptile0 = ptile0; up.ptiles_m = us.ptiles;
-    up.n_rtiles = n_rtiles; up.rtile0 = rtile0; up.rtiles_m = us.rtiles;
+    up.ptiles_m = us.ptiles; up.rtiles_m = us.rtiles;
     const size_t a_bytes = (size_t)U_BM * KC * 16, b_bytes = (size_t)U_BN * KC * 16;
     // 1 KiB alignment slack, one particle tile on its way to TMEM, the N ring (per stage both
     // planes' row tiles), 512 B of barriers and the epilogue's staging tiles; both planes'
@@ -590,17 +648,19 @@ int umma_stage1(pftcc_handle *h, int M, int Ks, const float2 *UA, int rs0, int n
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "umma stage 1: operands too large for shared memory");
     up.stages = stages;
     up.P16 = ws.B16; up.R16 = ws.A16;
-    up.X = X; up.xrows = nrs_w; up.xcols = ncols_w;
+    up.waves = us.d_waves;
+    up.maps = reinterpret_cast<const CUtensorMap *>(us.d_maps);
+    up.nwaves = nw;
+    up.nitems = (int)nitems;
     up.err = us.err;
     up.wait_limit = h->wait_limit > 0 ? h->wait_limit : WAIT_LIMIT;
     const size_t smem = 1024 + a_bytes + stages * 2 * b_bytes + tail;
     if ((e = smem_limit((const void *)k_umma_stage1, smem)) != cudaSuccess)
         return cuda_err(h, e, "umma attr");
-    const int nitems = ((M - 1) / 2 + 1) * n_ptiles;   // plane pairs x particle tiles
-    const int grid = std::min(nitems, us.sms);
+    const int grid = (int)std::min<long long>(nitems, us.sms);
     PFTCC_LAUNCH(h);
     KTimer kt(h, PFTCC_K_STAGE1);
-    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(tmX, up);
+    k_umma_stage1<<<grid, U_THREADS, smem, h->stream>>>(up);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_err(h, e, "umma stage 1 launch");
     return PFTCC_OK;
 }
@@ -632,7 +692,12 @@ void umma_free(pftcc_handle *h)
 {
     UmmaState &us = ustate(h);
     dev_free(h, us.err);
+    dev_free(h, us.d_waves);
+    dev_free(h, us.d_maps);
     us.err = nullptr;
+    us.d_waves = nullptr;
+    us.d_maps = nullptr;
+    us.waves_cap = 0;
 }
 
 }  // namespace pftcc

@@ -1797,6 +1797,25 @@ int pftcc_autotune(pftcc_handle *h, int nshifts, const float *shifts, int precis
     return PFTCC_OK;
 }
 
+int pftcc_search_groups(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
+                        const int *nslot, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out)
+{
+    if (!h || !out || ngroups < 0 || (ngroups > 0 && (!ref_first || !nref || !slot_first || !nslot)) || nshifts < 0 ||
+        (nshifts > 0 && !shifts) || ntop < 0 || ntop > 8)
+        return set_err(h, PFTCC_ERR_ARG, "search_groups: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    ST(ensure(h, (void **)&h->d_best, &h->best_cap, (size_t)h->nptcls * sizeof(pftcc_best), "best"));
+    std::vector<int> r0(ngroups), s0(ngroups);
+    for (int q = 0; q < ngroups; ++q) { r0[q] = ref_first[q] - 1; s0[q] = slot_first[q] - 1; }
+    ST(search_mdomain_groups(h, ngroups, r0.data(), nref, s0.data(), nslot, nshifts, shifts, precision, ntop, h->d_best));
+    CK(cudaMemcpyAsync(out, h->d_best, (size_t)h->nptcls * sizeof(pftcc_best), cudaMemcpyDeviceToHost, h->stream),
+       "search download");
+    CK(cudaStreamSynchronize(h->stream), "search_groups");
+    return PFTCC_OK;
+}
+
 int pftcc_search_best(pftcc_handle *h, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out)
 {
     if (!h || !out) return set_err(h, PFTCC_ERR_ARG, "search_best: bad arguments");

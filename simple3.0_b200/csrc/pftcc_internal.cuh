@@ -59,10 +59,40 @@ struct Group {          // all work items of one particle slot
 
 enum { MODE_FULL = 0, MODE_BEST = 1, MODE_ITEMMAX = 2 };   // ITEMMAX: out[w.out] = max over rotations
 
-// state of the tcgen05 stage 1 (packed operand geometry, device error word)
+// One wave of a tcgen05 stage-1 launch: the (reference, shift) row tiles [rtile0, rtile0 + n_rtiles)
+// of the packed row operand against the particle tiles [ptile0, ptile0 + n_ptiles) of the packed
+// particle operand (tiles counted from the parity group's first column), into the packed spectrum
+// X = Z [P][xcols][xrows] with xrows = 32 n_rtiles, xcols = 128 n_ptiles.  item0: the wave's first
+// work item (plane pair, particle tile) in the launch, the prefix over the waves before it.
+struct S1Wave {
+    float2 *X;
+    int rtile0, n_rtiles, ptile0, n_ptiles;
+    int item0, xrows, xcols, pad;
+};
+
+// One wave of a stage-2 launch: the particle columns [col0, col0 + cols) (absolute column order)
+// against the (reference, shift) rows [row0, row0 + rows) of Z = X [P][xcols][xrows]; row row0 + i
+// sits at Z row rofs + i, column col0 + c at Z column zc0 + c; the normalising factors D
+// [reference - r0][dcols][dlen] hold column col0 + c at c.  blk0: the wave's first block in the
+// launch (one block per column).
+struct S2Wave {
+    const float2 *X;
+    const float *D;
+    int row0, rows, rofs, xrows, xcols;
+    int col0, cols, zc0, r0, dcols;
+    int blk0, pad;
+};
+
+// state of the tcgen05 stage 1 (packed operand geometry, the device tables of a launch's waves and
+// their tensor maps, device error word)
 struct UmmaState {
     int Kp = 0, KC = 0, rtiles = 0, ptiles = 0, group_c0 = 0, sms = 0;
     int *err = nullptr;
+    S1Wave *d_waves = nullptr;
+    void *d_maps = nullptr;     // CUtensorMap[waves_cap], 64-byte aligned
+    int waves_cap = 0;
+    S2Wave *d_s2waves = nullptr;   // the stage-2 launch's waves
+    int s2waves_cap = 0;
 };
 
 // m-domain search workspace (sized on first use, reused across calls)
@@ -79,6 +109,8 @@ struct SearchWS {
     float2 *Yn = nullptr;        // [wave refs][wave cols][P/2+1] its spectra (k_norm_y2)
     float2 *X = nullptr;         // [M][wave rows][wave cols] stage-1 output of one wave
     size_t X_elems = 0;
+    size_t D_bytes = 0, Y_bytes = 0;   // D and Y capacities of the grouped search (0 otherwise)
+    size_t perm_bytes = 0;             // capacity of the grouped search's column order (cand_ref)
     float2 *cand = nullptr;      // [np_pad][8] packed (cc, rs*N+rot) candidates
     float *sqp = nullptr;        // [np_pad]
     __nv_bfloat16 *A16 = nullptr;  // tcgen05 operands, see k_umma.cu
@@ -284,7 +316,10 @@ int refine_batch(pftcc_handle *h, int n, const pftcc_refine_req *req, const doub
 int shsrch_batch(pftcc_handle *h, int mode, const pftcc_shsrch_opts &o, int n, const pftcc_shsrch_req *req,
                  const int *slots, pftcc_shsrch_out *out);
 
-// tcgen05 stage 1 (k_umma.cu)
+// tcgen05 stage 1 (k_umma.cu): every wave of the list in one persistent launch (the waves' X,
+// rtile0, n_rtiles, ptile0, n_ptiles given; item0, xrows and xcols filled in), after the operands
+// were packed by umma_stage1(..., prepare = 1, ...)
+int umma_stage1_waves(pftcc_handle *h, int M, std::vector<S1Wave> &waves);
 // the device error word cleared once per search (every stage-1 launch of the search may set it)
 int umma_reset(pftcc_handle *h);
 int umma_check(pftcc_handle *h);
@@ -293,6 +328,11 @@ void umma_free(pftcc_handle *h);
 // m-domain search (k_search.cu)
 int search_mdomain(pftcc_handle *h, int nshifts, const float *shifts_host, int precision, int ntop,
                    pftcc_best *out_dev, float *ccall_dev);
+// the grouped search: group q's particle slots [slot0[q], +nslot[q]) against its references
+// [ref0[q], +nref[q]) (0-based), every group's waves in shared launches
+int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const int *nref, const int *slot0,
+                          const int *nslot, int nshifts_in, const float *shifts_host, int precision, int ntop,
+                          pftcc_best *out_dev);
 
 }  // namespace pftcc
 

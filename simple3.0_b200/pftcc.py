@@ -488,6 +488,22 @@ class polarft_corrcalc:
         dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("ishift", np.int32), ("corr", np.float32)])
         return np.frombuffer(out, dtype=dt).copy()
 
+    def search_groups(self, groups, shifts=None, precision="bf16x3", ntop: int = 8) -> np.ndarray:
+        """pftcc_search_groups: groups is a sequence of (ref_first, nref, slot_first, nslot), 1-based;
+        each group's particle slots are searched against its references only.  Structured array
+        (iref, irot, ishift, corr) per held particle slot (iref 0 outside every group)."""
+        n = self.get_nptcls()
+        g = np.ascontiguousarray(np.asarray(groups, np.int32).reshape(-1, 4))
+        cols = [np.ascontiguousarray(g[:, i]) for i in range(4)]
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        out = (_lib.Best * n)()
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self._L.pftcc_search_groups(self._h, g.shape[0], ip(cols[0]), ip(cols[1]), ip(cols[2]), ip(cols[3]),
+                                                ns, None if sh is None else _f32p(sh), _PRECS[precision], int(ntop), out))
+        dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("ishift", np.int32), ("corr", np.float32)])
+        return np.frombuffer(out, dtype=dt).copy()
+
     def search_snhc(self, order, prev_corr, nrefs_bound: int, seed: int, cls_pops=None, precision="exact"):
         """stochastic neighbourhood hill climbing (srch_snhc + shcloc) for every held particle:
         order (nptcls, nrefs) 1-based visiting orders, prev_corr (nptcls,); returns a structured
