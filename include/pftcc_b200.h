@@ -322,6 +322,18 @@ int pftcc_search_best_dev(pftcc_handle *h, int nshifts, const float *shifts, int
  * every group return iref = 0, ishift = -1, corr = -inf. */
 int pftcc_search_groups(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
                         const int *nslot, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out);
+/* The same into device memory (out_dev: nptcls pftcc_best records), enqueued on the handle's stream
+ * with no host synchronisation and no read-back of the bounded waits' error word (check it with
+ * pftcc_search_check once the stream has run).  After one call outside stream capture with the
+ * same arguments (which sizes the workspace and the staging of its tables), the call may be
+ * captured into a CUDA graph on the handle's stream (pftcc_set_stream); the graph replays the
+ * groups and shifts given at capture, and a later capture of a call on the same handle replaces
+ * them.  Inside a capture a call that would allocate returns PFTCC_ERR_STATE. */
+int pftcc_search_groups_dev(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
+                            const int *nslot, int nshifts, const float *shifts, int precision, int ntop, void *out_dev);
+/* the bounded waits' error word of the searches since the last check: PFTCC_ERR_TIMEOUT when a
+ * wait gave up (synchronises the handle's stream) */
+int pftcc_search_check(pftcc_handle *h);
 /* adjoint: f and grad3 = d f / d(shift_x, shift_y, defocus[micron]) per request, with
  * the particle's CTF evaluated at defocus + ddf; the shift part is
  * gencorr_grad_for_rot_8 (:1863-1925) in the branch cfg.match_filt selects */

@@ -157,6 +157,8 @@ SIGNATURES = {
     "pftcc_search_best": [_h, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],
     "pftcc_search_best_dev": [_h, C.c_int, _fp, C.c_int, C.c_int, _vp],
     "pftcc_search_groups": [_h, C.c_int, _ip, _ip, _ip, _ip, C.c_int, _fp, C.c_int, C.c_int, C.POINTER(Best)],
+    "pftcc_search_groups_dev": [_h, C.c_int, _ip, _ip, _ip, _ip, C.c_int, _fp, C.c_int, C.c_int, _vp],
+    "pftcc_search_check": [_h],
     "pftcc_grad_batch": [_h, C.c_int, C.POINTER(GradReq), _dp, _dp],
     "pftcc_refine_batch": [_h, C.c_int, C.POINTER(RefineReq), _dp, _dp, C.c_int, C.c_double, C.c_double,
                            C.POINTER(RefineOut)],

@@ -129,8 +129,10 @@ def _ctf_records(chunks) -> object:
     return arr
 
 
-def _search_geometry(cs, precision, ntop, device, stream):
-    """one geometry's chunks in one handle, searched by one pftcc_search_groups call"""
+def grouped_handle(cs, device: int = 0, stream=None):
+    """One handle holding the chunks cs (of one geometry): references concatenated, particles in
+    consecutive slots, their CTFs; returns (handle, groups) with groups as pftcc_search_groups
+    takes them, (first reference, references, first slot, particles) per chunk, 1-based."""
     import torch
     nrefs = sum(ch.nrefs for ch in cs)
     nptcls = sum(ch.nptcls for ch in cs)
@@ -159,7 +161,17 @@ def _search_geometry(cs, precision, ntop, device, stream):
             r += ch.nrefs
             s += ch.nptcls
         pc.create_polar_absctfmats(_ctf_records(cs))
-        out = pc.search_groups(groups, c0.shifts, precision, ntop)
+    except BaseException:
+        pc.kill()
+        raise
+    return pc, groups
+
+
+def _search_geometry(cs, precision, ntop, device, stream):
+    """one geometry's chunks in one handle, searched by one pftcc_search_groups call"""
+    pc, groups = grouped_handle(cs, device, stream)
+    try:
+        out = pc.search_groups(groups, cs[0].shifts, precision, ntop)
         res = []
         for (r0, _, s0, n) in groups:
             x = out[s0 - 1:s0 - 1 + n].copy()

@@ -1507,9 +1507,23 @@ constexpr int GB_COLS = 8192;
 
 int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const int *nref, const int *slot0,
                           const int *nslot, int nshifts_in, const float *shifts_host, int precision, int ntop,
-                          pftcc_best *out_dev)
+                          pftcc_best *out_dev, int check)
 {
     const Geom &g = h->g;
+    // the tables of this call go through the staging arena of its kind: outside capture the stream
+    // drains first (the arena's earlier contents have landed) and the call's staging bytes are
+    // recorded, so that the capture arena can be sized for a later capture of the same call
+    const bool cap = capturing(h);
+    if (cap) {
+        h->pin_off[1] = 0;
+        if (h->pin_cap[1] < h->pin_need || !h->pin[1])
+            return set_err(h, PFTCC_ERR_STATE, "search_groups during graph capture: run the same call once outside capture first");
+    } else {
+        const cudaError_t e0 = cudaStreamSynchronize(h->stream);
+        if (e0 != cudaSuccess) return cuda_err(h, e0, "search_groups");
+        h->pin_off[0] = 0;
+        h->pin_total = 0;
+    }
     const int N = g.P * 2, P = g.P, Ks = g.Ks, M = P + 1, J = P / 2 + 1;
     if (h->objfun == PFTCC_OBJFUN_EUCLID)
         return set_err(h, PFTCC_ERR_UNSUPPORTED, "search_groups: the correlation objective only");
@@ -1602,10 +1616,14 @@ int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const i
         if (st) return st;
     }
     int *d_perm = ws.cand_ref;
-    CKG(cudaMemcpyAsync(d_perm, perm.data(), np * sizeof(int), cudaMemcpyHostToDevice, h->stream), "perm");
     std::vector<float> sh(2 * ns, 0.f);
     if (nshifts_in > 0) std::copy(shifts_host, shifts_host + 2 * ns, sh.begin());
-    CKG(cudaMemcpyAsync(ws.shifts, sh.data(), sh.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream), "shifts");
+    {
+        int st = stage_upload(h, d_perm, perm.data(), np * sizeof(int), "column order");
+        if (st) return st;
+        st = stage_upload(h, ws.shifts, sh.data(), sh.size() * sizeof(float), "shifts");
+        if (st) return st;
+    }
     const float *ctf = (h->cfg.with_ctf && h->ctf_ready) ? h->ctfmats : nullptr;
     const size_t smem_s1 = 4 * (size_t)Ks * S1_TILE * sizeof(float2);
     CKG(smem_limit((const void *)k_stage1_fp32, smem_s1), "attr");
@@ -1747,7 +1765,18 @@ int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const i
                 "rescore");
         }
     }
-    {
+    if (!cap) {
+        // the capture arena holds a later capture of this call's tables
+        h->pin_need = h->pin_total;
+        if (h->pin_cap[1] < h->pin_need) {
+            if (h->pin[1]) cudaFreeHost(h->pin[1]);
+            h->pin[1] = nullptr;
+            h->pin_cap[1] = 0;
+            CKG(cudaMallocHost(&h->pin[1], h->pin_need), "pinned capture staging");
+            h->pin_cap[1] = h->pin_need;
+        }
+    }
+    if (check && !cap) {
         int st = umma_check(h);
         if (st != PFTCC_OK) return st;
     }

@@ -988,9 +988,8 @@ cudaError_t launch_stage2_waves(pftcc_handle *h, int P, std::vector<S2Wave> &wav
             return cudaErrorMemoryAllocation;
         us.s2waves_cap = cap;
     }
-    cudaError_t e = cudaMemcpyAsync(us.d_s2waves, waves.data(), (size_t)nw * sizeof(S2Wave), cudaMemcpyHostToDevice,
-                                    h->stream);
-    if (e != cudaSuccess) return e;
+    if (stage_upload(h, us.d_s2waves, waves.data(), (size_t)nw * sizeof(S2Wave), "stage-2 waves") != PFTCC_OK)
+        return cudaErrorInvalidValue;
     S2Fast sp{nshifts, 2 * P, nrs_total, nw, 1.0f / (2.0f * (float)(2 * P))};
     switch (P) {
     case 64: return launch_s2<8, 8>(h, sp, (int)blocks, us.d_s2waves, cand, ccall, perm, eu != 0);

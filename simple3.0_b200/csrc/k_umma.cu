@@ -629,9 +629,12 @@ int umma_stage1_waves(pftcc_handle *h, int M, std::vector<S1Wave> &waves)
         if (((uintptr_t)us.d_maps & 63) != 0) return set_err(h, PFTCC_ERR_CUDA, "stage-1 tensor maps not 64-byte aligned");
         us.waves_cap = cap;
     }
-    if ((e = cudaMemcpyAsync(us.d_waves, waves.data(), (size_t)nw * sizeof(S1Wave), cudaMemcpyHostToDevice, h->stream)) ||
-        (e = cudaMemcpyAsync(us.d_maps, maps.data(), (size_t)nw * sizeof(CUtensorMap), cudaMemcpyHostToDevice, h->stream)))
-        return cuda_err(h, e, "stage-1 wave tables");
+    {
+        int st = stage_upload(h, us.d_waves, waves.data(), (size_t)nw * sizeof(S1Wave), "stage-1 waves");
+        if (st) return st;
+        st = stage_upload(h, us.d_maps, maps.data(), (size_t)nw * sizeof(CUtensorMap), "stage-1 tensor maps");
+        if (st) return st;
+    }
     UmmaParams up{};
     up.M = M; up.Kp = Kp; up.KC = KC;
     up.ptiles_m = us.ptiles; up.rtiles_m = us.rtiles;

@@ -66,10 +66,48 @@ static cudaError_t pool_ready(int dev)
     return cudaSuccess;
 }
 
+bool capturing(const pftcc_handle *h)
+{
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(h->stream, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone;
+}
+
+int stage_upload(pftcc_handle *h, void *dst_dev, const void *src, size_t bytes, const char *what)
+{
+    if (bytes == 0) return PFTCC_OK;
+    const int a = capturing(h) ? 1 : 0;
+    const size_t need = (bytes + 63) / 64 * 64;
+    if (h->pin_off[a] + need > h->pin_cap[a]) {
+        if (a) return set_err(h, PFTCC_ERR_STATE, std::string("staging of ") + what +
+                                                      " during graph capture: run the same call once outside capture first");
+        // the arena's earlier contents may still be on their way: drain the stream, then reuse or grow
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return cuda_err(h, e, "staging");
+        h->pin_off[0] = 0;
+        if (need > h->pin_cap[0]) {
+            if (h->pin[0]) cudaFreeHost(h->pin[0]);
+            h->pin[0] = nullptr;
+            h->pin_cap[0] = 0;
+            const size_t cap = std::max<size_t>(need, 1 << 20);
+            if ((e = cudaMallocHost(&h->pin[0], cap)) != cudaSuccess) return cuda_err(h, e, "pinned staging");
+            h->pin_cap[0] = cap;
+        }
+    }
+    char *stg = static_cast<char *>(h->pin[a]) + h->pin_off[a];
+    std::memcpy(stg, src, bytes);
+    h->pin_off[a] += need;
+    if (!a) h->pin_total += need;
+    const cudaError_t e = cudaMemcpyAsync(dst_dev, stg, bytes, cudaMemcpyHostToDevice, h->stream);
+    return e == cudaSuccess ? PFTCC_OK : cuda_err(h, e, what);
+}
+
 int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what)
 {
     *p = nullptr;
     if (bytes == 0) return PFTCC_OK;
+    if (capturing(h))
+        return set_err(h, PFTCC_ERR_STATE, std::string("device allocation of ") + what +
+                                               " during graph capture: run the same call once outside capture first");
     cudaError_t e = pool_ready(h->dev);
     if (e == cudaSuccess) e = cudaMallocAsync(p, bytes, h->stream);
     // the buffer may next be used on another stream (pftcc_set_stream): complete the allocation
@@ -280,6 +318,7 @@ static void free_all(pftcc_handle *h)
     for (cudaEvent_t e : h->prof_pool) cudaEventDestroy(e);
     cudaStream_t own = h->own_stream ? h->own_stream : h->stream;
     if (own) cudaStreamDestroy(own);
+    for (void *&p : h->pin) { if (p) cudaFreeHost(p); p = nullptr; }
 }
 
 static int alloc_ptcl_arrays(pftcc_handle *h)
@@ -1797,19 +1836,51 @@ int pftcc_autotune(pftcc_handle *h, int nshifts, const float *shifts, int precis
     return PFTCC_OK;
 }
 
+static int search_groups_args(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref,
+                              const int *slot_first, const int *nslot, int nshifts, const float *shifts, int ntop)
+{
+    if (!h || ngroups < 0 || (ngroups > 0 && (!ref_first || !nref || !slot_first || !nslot)) || nshifts < 0 ||
+        (nshifts > 0 && !shifts) || ntop < 0 || ntop > 8)
+        return set_err(h, PFTCC_ERR_ARG, "search_groups: bad arguments");
+    return PFTCC_OK;
+}
+
+int pftcc_search_groups_dev(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
+                            const int *nslot, int nshifts, const float *shifts, int precision, int ntop, void *out_dev)
+{
+    ST(search_groups_args(h, ngroups, ref_first, nref, slot_first, nslot, nshifts, shifts, ntop));
+    if (!out_dev) return set_err(h, PFTCC_ERR_ARG, "search_groups_dev: bad arguments");
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    ST(check_ctf_state(h));
+    std::vector<int> r0(ngroups), s0(ngroups);
+    for (int q = 0; q < ngroups; ++q) { r0[q] = ref_first[q] - 1; s0[q] = slot_first[q] - 1; }
+    ST(search_mdomain_groups(h, ngroups, r0.data(), nref, s0.data(), nslot, nshifts, shifts, precision, ntop,
+                             (pftcc_best *)out_dev, 0));
+    return PFTCC_OK;
+}
+
+int pftcc_search_check(pftcc_handle *h)
+{
+    if (!h) return PFTCC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(h->mtx);
+    cudaSetDevice(h->dev);
+    return umma_check(h);
+}
+
 int pftcc_search_groups(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
                         const int *nslot, int nshifts, const float *shifts, int precision, int ntop, pftcc_best *out)
 {
-    if (!h || !out || ngroups < 0 || (ngroups > 0 && (!ref_first || !nref || !slot_first || !nslot)) || nshifts < 0 ||
-        (nshifts > 0 && !shifts) || ntop < 0 || ntop > 8)
-        return set_err(h, PFTCC_ERR_ARG, "search_groups: bad arguments");
+    ST(search_groups_args(h, ngroups, ref_first, nref, slot_first, nslot, nshifts, shifts, ntop));
+    if (!out) return set_err(h, PFTCC_ERR_ARG, "search_groups: bad arguments");
     std::lock_guard<std::mutex> lk(h->mtx);
     cudaSetDevice(h->dev);
     ST(check_ctf_state(h));
     ST(ensure(h, (void **)&h->d_best, &h->best_cap, (size_t)h->nptcls * sizeof(pftcc_best), "best"));
     std::vector<int> r0(ngroups), s0(ngroups);
     for (int q = 0; q < ngroups; ++q) { r0[q] = ref_first[q] - 1; s0[q] = slot_first[q] - 1; }
-    ST(search_mdomain_groups(h, ngroups, r0.data(), nref, s0.data(), nslot, nshifts, shifts, precision, ntop, h->d_best));
+    ST(search_mdomain_groups(h, ngroups, r0.data(), nref, s0.data(), nslot, nshifts, shifts, precision, ntop, h->d_best,
+                             1));
     CK(cudaMemcpyAsync(out, h->d_best, (size_t)h->nptcls * sizeof(pftcc_best), cudaMemcpyDeviceToHost, h->stream),
        "search download");
     CK(cudaStreamSynchronize(h->stream), "search_groups");

@@ -192,6 +192,13 @@ struct pftcc_handle {
     long long wait_limit = 0;            // pipeline-wait polls of the tcgen05 kernels (0 = default)
     pftcc_tuning tune{};                 // wave and tile sizes of the m-domain search (0 = automatic)
     cudaStream_t own_stream = nullptr;
+    // pinned host staging of the small per-call tables (column order, shifts, wave tables): one
+    // arena for calls made outside stream capture, one for a captured call, whose memcpy nodes
+    // read it at every replay
+    void *pin[2] = {nullptr, nullptr};
+    size_t pin_cap[2] = {0, 0}, pin_off[2] = {0, 0};
+    size_t pin_total = 0;    // staging bytes since the last uncaptured grouped search began
+    size_t pin_need = 0;     // staging bytes of the last uncaptured grouped search
     // per-kernel-class event timing
     int prof = 0;
     struct ProfEv { int cls; cudaEvent_t a, b; };
@@ -226,6 +233,11 @@ int cuda_err(pftcc_handle *h, cudaError_t e, const char *what);
 int dev_alloc(pftcc_handle *h, void **p, size_t bytes, const char *what);
 void dev_free(pftcc_handle *h, void *p);
 int ensure(pftcc_handle *h, void **p, size_t *cap, size_t bytes, const char *what);
+// whether the handle's stream is capturing a CUDA graph
+bool capturing(const pftcc_handle *h);
+// a host table to the device through the pinned staging arena of the call's kind (see the
+// handle's pin fields); outside capture the arena wraps (after the stream drains) and grows
+int stage_upload(pftcc_handle *h, void *dst_dev, const void *src, size_t bytes, const char *what);
 
 // ---- kernels (launch wrappers return cudaError_t of the launch) ---------------------
 cudaError_t launch_polarize(pftcc_handle *h, const float2 *cmats, int n, int first_slot);
@@ -332,7 +344,7 @@ int search_mdomain(pftcc_handle *h, int nshifts, const float *shifts_host, int p
 // [ref0[q], +nref[q]) (0-based), every group's waves in shared launches
 int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const int *nref, const int *slot0,
                           const int *nslot, int nshifts_in, const float *shifts_host, int precision, int ntop,
-                          pftcc_best *out_dev);
+                          pftcc_best *out_dev, int check);
 
 }  // namespace pftcc
 

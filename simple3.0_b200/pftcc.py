@@ -504,6 +504,24 @@ class polarft_corrcalc:
         dt = np.dtype([("iref", np.int32), ("irot", np.int32), ("ishift", np.int32), ("corr", np.float32)])
         return np.frombuffer(out, dtype=dt).copy()
 
+    def search_groups_dev(self, groups, shifts, precision, ntop: int, out_dev_ptr: int):
+        """pftcc_search_groups_dev: the grouped search into device memory (nptcls 16-byte records at
+        out_dev_ptr), enqueued on the handle's stream without synchronising; capturable in a CUDA
+        graph after one uncaptured call with the same arguments"""
+        g = np.ascontiguousarray(np.asarray(groups, np.int32).reshape(-1, 4))
+        self._keep = [np.ascontiguousarray(g[:, i]) for i in range(4)]
+        sh = None if shifts is None else np.ascontiguousarray(shifts, np.float32).reshape(-1, 2)
+        ns = 0 if sh is None else sh.shape[0]
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        k = self._keep
+        self._check(self._L.pftcc_search_groups_dev(self._h, g.shape[0], ip(k[0]), ip(k[1]), ip(k[2]), ip(k[3]), ns,
+                                                    None if sh is None else _f32p(sh), _PRECS[precision], int(ntop),
+                                                    C.c_void_p(out_dev_ptr)))
+
+    def search_check(self):
+        """raise if a bounded wait of the searches since the last check gave up"""
+        self._check(self._L.pftcc_search_check(self._h))
+
     def search_snhc(self, order, prev_corr, nrefs_bound: int, seed: int, cls_pops=None, precision="exact"):
         """stochastic neighbourhood hill climbing (srch_snhc + shcloc) for every held particle:
         order (nptcls, nrefs) 1-based visiting orders, prev_corr (nptcls,); returns a structured

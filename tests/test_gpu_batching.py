@@ -86,3 +86,52 @@ def test_grouped_search_with_shifts_and_unsearched_slots(pkg):
     with pytest.raises(pkg.PftccError):
         pc.search_groups([g0, (1, 2, 3, 5)], sh, "bf16x3", 8)     # groups sharing particle slots
     pc.kill()
+
+
+def test_grouped_search_captured_in_a_graph(pkg):
+    """pftcc_search_groups_dev: after one call outside capture, the same call captured into a CUDA
+    graph on the handle's stream replays to the uncaptured call's result, bit for bit, every time
+    (the outputs cleared in between); the bounded waits report no error; a first call inside a
+    capture (nothing sized yet) is refused with PFTCC_ERR_STATE"""
+    import torch
+    b = pkg.batching
+    chunks = [b.synthetic_chunk("B", nr, npt, seed=70 + i) for i, (nr, npt) in enumerate([(9, 150), (12, 70), (5, 200)])]
+    side = torch.cuda.Stream()
+    pc, groups = b.grouped_handle(chunks, stream=side.cuda_stream)
+    try:
+        n = sum(ch.nptcls for ch in chunks)
+        out = torch.zeros((n, 4), dtype=torch.int32, device="cuda")
+        with torch.cuda.stream(side):
+            pc.search_groups_dev(groups, None, "bf16x3", 8, out.data_ptr())
+        torch.cuda.synchronize()
+        pc.search_check()
+        want = out.clone()
+        host = pc.search_groups(groups, None, "bf16x3", 8)
+        assert np.array_equal(want.cpu().numpy().view(np.int32).reshape(-1), host.view(np.int32).reshape(-1))
+        g = torch.cuda.CUDAGraph()
+        out.zero_()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=side):
+            pc.search_groups_dev(groups, None, "bf16x3", 8, out.data_ptr())
+        for _ in range(2):
+            out.zero_()
+            torch.cuda.synchronize()
+            g.replay()
+            torch.cuda.synchronize()
+            assert torch.equal(out, want)
+        pc.search_check()
+        del g
+    finally:
+        pc.kill()
+    # nothing sized: refused inside the capture, with the capture then abandoned by the caller
+    pc2, groups2 = b.grouped_handle(chunks[:1], stream=side.cuda_stream)
+    try:
+        out2 = torch.zeros((chunks[0].nptcls, 4), dtype=torch.int32, device="cuda")
+        g2 = torch.cuda.CUDAGraph()
+        with pytest.raises(pkg.PftccError) as e:
+            with torch.cuda.graph(g2, stream=side):
+                pc2.search_groups_dev(groups2, None, "bf16x3", 8, out2.data_ptr())
+        assert e.value.status == 3      # PFTCC_ERR_STATE
+    finally:
+        torch.cuda.synchronize()
+        pc2.kill()
