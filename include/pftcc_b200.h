@@ -331,8 +331,9 @@ int pftcc_search_groups(pftcc_handle *h, int ngroups, const int *ref_first, cons
  * them.  Inside a capture a call that would allocate returns PFTCC_ERR_STATE. */
 int pftcc_search_groups_dev(pftcc_handle *h, int ngroups, const int *ref_first, const int *nref, const int *slot_first,
                             const int *nslot, int nshifts, const float *shifts, int precision, int ntop, void *out_dev);
-/* the bounded waits' error word of the searches since the last check: PFTCC_ERR_TIMEOUT when a
- * wait gave up (synchronises the handle's stream) */
+/* the bounded waits' error word of every search since the last check (graph replays included):
+ * PFTCC_ERR_TIMEOUT when a wait gave up, and the word is cleared; synchronises the handle's
+ * stream, so it is called outside stream capture */
 int pftcc_search_check(pftcc_handle *h);
 /* adjoint: f and grad3 = d f / d(shift_x, shift_y, defocus[micron]) per request, with
  * the particle's CTF evaluated at defocus + ddf; the shift part is

@@ -1630,7 +1630,7 @@ int search_mdomain_groups(pftcc_handle *h, int ngroups, const int *ref0, const i
     const int p2 = stage2_fast_p2(P), dlen = stage2_fast_dlen(P);
     const bool md_rescore = ntop > 0 && h->cfg.ctf_frame == PFTCC_FRAME_PTCL;
     {
-        const int st = umma_reset(h);    // the device error word of the bounded waits
+        const int st = umma_reset(h);    // the device error word of the bounded waits (allocated once)
         if (st != PFTCC_OK) return st;
     }
     // a wave's packed spectrum within 1 GiB; a batch's waves within 2 GiB of Z and 1 GiB of factors

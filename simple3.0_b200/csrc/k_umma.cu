@@ -668,17 +668,19 @@ int umma_stage1_waves(pftcc_handle *h, int M, std::vector<S1Wave> &waves)
     return PFTCC_OK;
 }
 
+// the device error word of the bounded waits, zeroed once when it is allocated: it then holds the
+// first expiry of any search since the last umma_check, graph replays included
 int umma_reset(pftcc_handle *h)
 {
     UmmaState &us = ustate(h);
-    if (!us.err) {
-        const int st = dev_alloc(h, (void **)&us.err, sizeof(int), "umma error word");
-        if (st) return st;
-    }
+    if (us.err) return PFTCC_OK;
+    const int st = dev_alloc(h, (void **)&us.err, sizeof(int), "umma error word");
+    if (st) return st;
     const cudaError_t e = cudaMemsetAsync(us.err, 0, sizeof(int), h->stream);
     return e == cudaSuccess ? PFTCC_OK : cuda_err(h, e, "umma error word reset");
 }
 
+// reads the error word after the stream has drained and clears it when a wait had expired
 int umma_check(pftcc_handle *h)
 {
     UmmaState &us = ustate(h);
@@ -686,6 +688,7 @@ int umma_check(pftcc_handle *h)
     int v = 0;
     cudaError_t e = cudaMemcpyAsync(&v, us.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && v != 0) e = cudaMemsetAsync(us.err, 0, sizeof(int), h->stream);
     if (e != cudaSuccess) return cuda_err(h, e, "umma error word");
     if (v != 0) return set_err(h, PFTCC_ERR_TIMEOUT, "tcgen05 stage 1: bounded wait expired (code " + std::to_string(v) + ")");
     return PFTCC_OK;
