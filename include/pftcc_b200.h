@@ -56,7 +56,9 @@ typedef struct pftcc_handle pftcc_handle;
  * (boxmatch :235, ring2 -> nrots :251-252, kfromto/kstop :256-258, ctf :355-356,
  * l_match_filt :254; l_pssnr through pftcc_set_pssnr).  Not served: clsfrcs = 'yes'
  * (l_clsfrcs :415, which filters with the column ref_optlp(:, iptcl) of the particle's global
- * index, :976-980); the matched filter is always ref_optlp(:, iref). */
+ * index, :976-980): ref_optlp is allocated with nrefs columns (:255), so that mode reads past the
+ * array for every iptcl > nrefs and has no defined result to reproduce; the matched filter is
+ * always ref_optlp(:, iref). */
 typedef struct {
     int nrefs;            /* new(nrefs, ...)                                    */
     int pfromto[2];       /* new(..., pfromto, ...), global particle index range */
